@@ -1,0 +1,122 @@
+/*
+ * pamo_b200 -- C ABI of the B200 (sm_100a) PaMO mesh-optimization hot path.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (PAMO_OK on success) except
+ *     pamo_simplify, whose signature mirrors the reference's void C ABI.
+ *   - Pointers named d_* are device pointers on the context's device; h_* are
+ *     host pointers.  Buffers are owned by the caller unless stated otherwise.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Calls return after the stream work they enqueue has completed unless
+ *     stated otherwise.
+ *   - A context holds the device state one simplification carries between
+ *     rounds (the reference's CUSimp_Free object).  It is not thread safe: use
+ *     one context per host thread.
+ *   - Failures never fall back to another implementation: a missing device or
+ *     a CUDA error is reported as PAMO_ERR_NO_DEVICE / PAMO_ERR_DEVICE.
+ */
+#ifndef PAMO_B200_H
+#define PAMO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PAMO_OK 0
+#define PAMO_ERR_INVALID_ARG 1
+#define PAMO_ERR_OOM 2
+#define PAMO_ERR_BUDGET_EXCEEDED 3
+#define PAMO_ERR_DEVICE 4
+#define PAMO_ERR_NO_DEVICE 5
+#define PAMO_ERR_CAPACITY 6
+
+typedef struct pamo_ctx pamo_ctx;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int pamo_version(void);
+
+/* Human-readable name of a status code (static storage). */
+const char *pamo_status_string(int status);
+
+/* Creates a context bound to CUDA device `device`. */
+int pamo_ctx_create(int device, pamo_ctx **out);
+
+/* Releases the context and all device memory it owns. */
+int pamo_ctx_destroy(pamo_ctx *ctx);
+
+/*
+ * One stage-2 collapse round.  Replaces CUDSP_Free.forward
+ * (simp_cuda/src/pybind.cpp:52-103, which calls CUSimp_Free::forward,
+ * simp_cuda/src/cusimp_free.cu:891-1048).
+ *
+ *   d_points [n_pts*3] f32, d_tris [n_tris*3] i32: the round's input mesh.
+ *   d_verts_undo [n_verts_undo] i32: the undo list the previous round returned.
+ *   scale, threshold, is_stuck, init: as in the reference (init applies the
+ *     reference's round-0 face permutation).
+ *   Outputs (caller-allocated): d_out_points [n_pts*3], d_out_tris [n_tris*3],
+ *     d_out_occ [n_pts], d_out_map [n_pts]; *n_out_undo receives the length of
+ *     the round's undo list, which pamo_free_copy_undo copies out.
+ *
+ * The adjacency order inside each vertex's face list is ascending face index
+ * (the reference fills it in atomicAdd order), which makes every output
+ * deterministic.
+ */
+int pamo_free_forward(pamo_ctx *ctx, const float *d_points, const int *d_tris, const int *d_verts_undo,
+                      int n_verts_undo, int n_pts, int n_tris, float scale, float threshold, int is_stuck, int init,
+                      void *stream, float *d_out_points, int *d_out_tris, int *d_out_occ, int *d_out_map,
+                      int *n_out_undo);
+
+/* Copies the first n entries of the last round's undo list to d_out. */
+int pamo_free_copy_undo(pamo_ctx *ctx, int *d_out, int n, void *stream);
+
+/*
+ * The whole stage-2 loop of PaMO.run (simp_cuda/pamo/__init__.py:122-189,
+ * stage 1 off): centring by the mean face centroid (numpy float32 order),
+ * scale = max bbox extent, the init permutation, collapse rounds with the
+ * reference's stuck / tolerance / target logic, and compaction between rounds,
+ * all resident on the device.
+ *   target_faces = max(int(ratio * n_tris), min_verts) as PaMO.run computes it.
+ * On success *out_n_pts / *out_n_tris hold the result size and *out_rounds the
+ * number of rounds; fetch the mesh with pamo_stage2_fetch.
+ */
+int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
+                    long long target_faces, int tolerance, float threshold, int iters, void *stream, int *out_n_pts,
+                    int *out_n_tris, int *out_rounds);
+
+/*
+ * Copies the result of the last pamo_stage2_run: vertices with the centring
+ * offset added back (float32, as PaMO.run's "verts + tris_mean"), and faces.
+ * `to_host` != 0 means out_points/out_tris are host pointers.
+ */
+int pamo_stage2_fetch(pamo_ctx *ctx, float *out_points, int *out_tris, int to_host, void *stream);
+
+/* Centring offset (tris_mean) of the last pamo_stage2_run, host float[3]. */
+int pamo_stage2_offset(pamo_ctx *ctx, float *h_out3);
+
+/*
+ * Per-round statistics of the last pamo_stage2_run / pamo_free_forward:
+ * h_out[0..7] = {n_edges, n_collapsed, n_collapsed_with_coincident,
+ *               n_undo_passes, n_undo_vertices, candidate_pairs_pass0,
+ *               faces_in, faces_out}
+ */
+int pamo_stage2_last_round_stats(pamo_ctx *ctx, long long *h_out8);
+
+/*
+ * Host-pointer simplifier.  Same signature and meaning as the reference's
+ * Blender C ABI pamo_simplify (pamo_blender/cusimpinterface.cu:57): rounds until
+ * four rounds without progress, output written to caller buffers sized like the
+ * input, in_out_nv_ni = {n_verts, n_tris} in and out.  Uses an internal context
+ * on device 0 (like the reference's static simplifier it is not re-entrant).
+ */
+void pamo_simplify(float *in_verts, int *in_tris, float *out_verts, int *out_tris, int *in_out_nv_ni,
+                   float threshold);
+
+/* pamo_simplify with an explicit context and a status code. */
+int pamo_simplify_ctx(pamo_ctx *ctx, const float *h_in_verts, const int *h_in_tris, float *h_out_verts,
+                      int *h_out_tris, int *in_out_nv_ni, float threshold);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PAMO_B200_H */

@@ -1,0 +1,174 @@
+"""pamo_b200: the PaMO mesh-optimization hot path on NVIDIA B200 (sm_100a).
+
+Drop-in surface (simp_cuda/pamo/__init__.py):
+
+    PaMO(input_mesh, use_stage1=True, use_stage3=True).run(
+        points, triangles, ratio, tolerance=4, threshold=1e-3, iter=1000000,
+        min_verts=10000000000) -> (verts: np.ndarray [n,3], faces: np.ndarray [m,3])
+
+and the per-round extension class ``CUDSP_Free`` (simp_cuda/src/pybind.cpp).
+All compute runs in libpamo_b200.so (hand-written CUDA for sm_100a) through its
+C ABI; torch only provides device memory and the current stream.
+"""
+from __future__ import annotations
+
+import copy
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import Context, PamoError, check
+
+__all__ = ["PaMO", "CUDSP_Free", "Context", "PamoError", "stage2_run"]
+__version__ = "0.1.0"
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _stream_ptr(device):
+    torch = _torch()
+    return ctypes_void(torch.cuda.current_stream(device).cuda_stream)
+
+
+def ctypes_void(x):
+    import ctypes
+
+    return ctypes.c_void_p(int(x) if x else 0)
+
+
+def _mesh_arrays(mesh):
+    """(V float64 [n,3], F int64 [m,3]) from a trimesh-like object or a (V, F) pair."""
+    if isinstance(mesh, (tuple, list)) and len(mesh) == 2:
+        V, F = mesh
+    else:
+        V, F = mesh.vertices, mesh.faces
+    return np.asarray(V, dtype=np.float64), np.asarray(F, dtype=np.int64)
+
+
+class CUDSP_Free:
+    """One stage-2 simplifier; mirrors the reference's pybind class
+    (simp_cuda/src/pybind.cpp:16-103): ``forward`` runs one collapse round and
+    returns cloned ``(verts[n,3] f32, tris[m,3] i32, verts_occ[n,1] i32,
+    verts_map[n,1] i32, verts_undo[k] i32)`` CUDA tensors."""
+
+    def __init__(self, device: int = 0):
+        self.ctx = Context(device)
+
+    def forward(self, points, triangles, verts_undo, n_verts_undo, scale, threshold, is_stuck, init):
+        torch = _torch()
+        for name, t in (("points", points), ("triangles", triangles), ("verts_undo", verts_undo)):
+            if not t.is_cuda:
+                raise AssertionError(f"{name} must be a CUDA tensor")
+            if not t.is_contiguous():
+                raise AssertionError(f"{name} must be contiguous")
+        if points.dtype != torch.float32:
+            raise RuntimeError("points type must match the pamo class")
+        if triangles.dtype != torch.int32:
+            raise RuntimeError("triangles type must match the pamo class")
+        n, m = int(points.shape[0]), int(triangles.shape[0])
+        dev = points.device
+        ov = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        ot = torch.empty((m, 3), dtype=torch.int32, device=dev)
+        oo = torch.empty((n, 1), dtype=torch.int32, device=dev)
+        om = torch.empty((n, 1), dtype=torch.int32, device=dev)
+        import ctypes
+
+        nu = ctypes.c_int(0)
+        stream = _stream_ptr(dev)
+        check("pamo_free_forward", _lib.lib().pamo_free_forward(
+            self.ctx.handle, points.data_ptr(), triangles.data_ptr(),
+            verts_undo.data_ptr() if int(n_verts_undo) > 0 else None, int(n_verts_undo), n, m, float(scale),
+            float(threshold), int(bool(is_stuck)), int(bool(init)), stream, ov.data_ptr(), ot.data_ptr(),
+            oo.data_ptr(), om.data_ptr(), ctypes.byref(nu)))
+        undo = torch.empty((nu.value,), dtype=torch.int32, device=dev)
+        check("pamo_free_copy_undo", _lib.lib().pamo_free_copy_undo(
+            self.ctx.handle, undo.data_ptr() if nu.value else None, nu.value, stream))
+        return ov, ot, oo, om, undo
+
+
+def stage2_run(ctx: Context, points, triangles, target_faces: int, tolerance=4, threshold=1e-3, iters=1000000):
+    """Device-resident stage-2 loop of PaMO.run.  Returns (verts, faces) CUDA
+    tensors (verts already shifted back by the centring offset) and the number of
+    rounds."""
+    import ctypes
+
+    torch = _torch()
+    points = points.contiguous()
+    triangles = triangles.contiguous()
+    dev = points.device
+    stream = _stream_ptr(dev)
+    on, om, rounds = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    check("pamo_stage2_run", _lib.lib().pamo_stage2_run(
+        ctx.handle, points.data_ptr(), triangles.data_ptr(), int(points.shape[0]), int(triangles.shape[0]),
+        int(min(int(target_faces), 2**62)), int(tolerance), float(threshold), int(min(iters, 2**31 - 1)), stream,
+        ctypes.byref(on), ctypes.byref(om), ctypes.byref(rounds)))
+    v = torch.empty((on.value, 3), dtype=torch.float32, device=dev)
+    f = torch.empty((om.value, 3), dtype=torch.int32, device=dev)
+    check("pamo_stage2_fetch", _lib.lib().pamo_stage2_fetch(ctx.handle, v.data_ptr(), f.data_ptr(), 0, stream))
+    return v, f, rounds.value
+
+
+class PaMO:
+    """Drop-in for the reference's ``PaMO`` (simp_cuda/pamo/__init__.py:18-205).
+
+    ``input_mesh`` is any object with ``vertices``/``faces`` (e.g. a trimesh) or a
+    ``(V, F)`` pair; it is kept as the ground truth for stage 3.
+    """
+
+    def __init__(self, input_mesh, use_stage1=True, use_stage3=True, device: int = 0, verbose: bool = True):
+        self.use_stage1 = use_stage1
+        self.use_stage3 = use_stage3
+        self.verbose = verbose
+        if verbose:
+            print("Stage1 : ", self.use_stage1)
+            print("Stage3 : ", self.use_stage3)
+        V, F = _mesh_arrays(input_mesh)
+        self.bbox = np.stack([V.min(0), V.max(0)]) if len(V) else np.zeros((2, 3))
+        self.gt_mesh = (copy.deepcopy(V), copy.deepcopy(F))
+        self.ctx = Context(device)
+        self.device = device
+        self.target_faces = None
+        self.last_rounds = 0
+        self.timings = {}
+        if use_stage1:
+            from . import remesh  # noqa: F401  (raises if stage 1 is unavailable)
+        if use_stage3:
+            from .safe_project import Stage3Config, Stage3System
+
+            self.config = Stage3Config()
+            self.system = Stage3System(self.config, device=device)
+
+    def run(self, points, triangles, ratio, tolerance=4, threshold=1e-3, iter=1000000, min_verts=10000000000):
+        torch = _torch()
+        self.target_faces = max(int(ratio * len(triangles)), min_verts)
+        if self.verbose:
+            print("Target faces : {}".format(self.target_faces))
+        if self.use_stage1:
+            from .remesh import remesh_tensors
+
+            t0 = time.time()
+            points, triangles = remesh_tensors(points, triangles, self.target_faces)
+            self.timings["stage1"] = time.time() - t0
+            if self.verbose:
+                print(f"Time for Remeshing: {self.timings['stage1']} sec")
+        t0 = time.time()
+        v, f, rounds = stage2_run(self.ctx, points, triangles, self.target_faces, tolerance, threshold, iter)
+        self.last_rounds = rounds
+        verts = v.cpu().numpy()
+        faces = f.cpu().numpy()
+        self.timings["stage2"] = time.time() - t0
+        if self.verbose:
+            print(f"Time for Simplification: {self.timings['stage2']} sec")
+        if self.use_stage3:
+            from .safe_project import process
+
+            t0 = time.time()
+            verts, faces = process(self.gt_mesh[0], self.gt_mesh[1], verts, faces, 5, system=self.system,
+                                   config=self.config)
+            self.timings["stage3"] = time.time() - t0
+        return verts, faces

@@ -1,0 +1,26 @@
+// Round-0 face permutation.  The reference shuffles the faces with
+// thrust::shuffle and a default-constructed thrust::default_random_engine
+// (simp_cuda/src/cusimp_free.cu:937-941); every later decision (edge order, key
+// tie-breaks, adjacency order) depends on it, so the same open-source CCCL
+// routine is called here on the context's stream.
+#include <thrust/execution_policy.h>
+#include <thrust/random.h>
+#include <thrust/shuffle.h>
+
+#include "stage2.cuh"
+
+namespace pamo {
+
+int stage2_shuffle_faces(int4 *tris, int m, cudaStream_t s)
+{
+    if (m <= 1) return PAMO_OK;
+    try {
+        thrust::default_random_engine rng;
+        thrust::shuffle(thrust::cuda::par.on(s), tris, tris + m, rng);
+    } catch (...) {
+        return PAMO_ERR_DEVICE;
+    }
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+}  // namespace pamo

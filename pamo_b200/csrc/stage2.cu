@@ -1,0 +1,929 @@
+// Stage-2 collapse round on the device (sm_100a).
+//
+// One round follows the reference's CUSimp_Free::forward
+// (simp_cuda/src/cusimp_free.cu:891-1048) decision for decision, with a B200
+// layout and fewer passes:
+//   face pass A   plane of every face (fp32, reference order), vertex degrees,
+//                 per-face descending-edge counts                 [:276-289,306-317,337-348]
+//   2 scans       vertex->face CSR offsets, edge offsets
+//   face pass B   CSR fill + edge emission                          [:291-304,319-335]
+//   vertex pass   canonical (ascending face) order of each CSR segment, then the
+//                 quadric sum in that order                          [:350-366]
+//   edge pass     cost (link condition, edge lengths, flip and skinny terms,
+//                 quadric at the midpoint, u32 quantisation) fused with the
+//                 64-bit key min over each endpoint                  [:382-610]
+//   edge pass     independent-set test + collapse + skinny rollback  [:639-774]
+//   scan/scatter  collapsed list in edge order
+//   face pass     degenerate faces removed                           [:218-232]
+//   edge pass     coincident-endpoint collapses                      [:234-274]
+//   LBVH          build over the round's faces, refit, query of the faces touched
+//                 by collapses, pair tests                           [bvh/self_intersect.cuh]
+//   undo passes   candidates, restore, re-check (<= 5)               [:776-878,1015-1040]
+//   scan          pts_map = exclusive scan of occupancy              [:1042-1045]
+// The key independent set uses a per-vertex minimum: an edge wins iff its key is
+// the minimum over every face touching either endpoint (the reference's per-face
+// minimum), which equals: key == vmin[u] == vmin[v] and no vertex of those faces
+// has a smaller vmin.
+#include <cstdio>
+#include <cstring>
+
+#include "scan.cuh"
+#include "stage2.cuh"
+#include "tritri.cuh"
+
+namespace pamo {
+
+#define S2_TRY_EARLY(expr)                                \
+    do {                                                  \
+        cudaError_t _e = (expr);                          \
+        if (_e != cudaSuccess) return map_cuda_error(_e); \
+    } while (0)
+
+namespace {
+
+constexpr float kCostRange = 10.0f;
+
+__device__ __forceinline__ uint32_t quantise_cost(float c)
+{
+    // the reference converts with a saturating float->u32 conversion
+    return (uint32_t)(tclamp(c, 0.0f, kCostRange) / kCostRange * 4294967296.0f);
+}
+
+__global__ void k_round_init(const float4 *__restrict__ opts, const int4 *__restrict__ otris, float4 *pts,
+                             int4 *tris, int *occ, int *deg, int *cursor, unsigned long long *vmin, int n, int m)
+{
+    long long N = (long long)(n + 1 > m ? n + 1 : m);
+    PAMO_GRID_STRIDE(i, N)
+    {
+        if (i < n) {
+            pts[i] = opts[i];
+            occ[i] = 1;
+            deg[i] = 0;
+            cursor[i] = 0;
+            vmin[i] = ~0ull;
+        } else if (i == n) {
+            occ[n] = 0;
+            deg[n] = 0;
+        }
+        if (i < m) tris[i] = otris[i];
+    }
+}
+
+__global__ void k_face_a(const float4 *__restrict__ pts, const int4 *__restrict__ tris, int m, int *deg,
+                         int *ecount, float4 *plane)
+{
+    PAMO_GRID_STRIDE(f, m)
+    {
+        int4 t = tris[f];
+        if (face_dead(t)) {
+            ecount[f] = 0;
+            continue;
+        }
+        atomicAdd(&deg[t.x], 1);
+        atomicAdd(&deg[t.y], 1);
+        atomicAdd(&deg[t.z], 1);
+        ecount[f] = (t.x > t.y) + (t.y > t.z) + (t.z > t.x);
+        V3 v0 = v3(pts[t.x]), v1 = v3(pts[t.y]), v2 = v3(pts[t.z]);
+        V3 nrm = vcross(vsub(v1, v0), vsub(v2, v0));
+        nrm = vdivs(nrm, vnorm(nrm));
+        float d = -vdot(nrm, v0);
+        plane[f] = make_float4(nrm.x, nrm.y, nrm.z, d);
+    }
+}
+
+__global__ void k_face_b(const int4 *__restrict__ tris, int m, const int *__restrict__ first_near, int *cursor,
+                         int *near_tris, const int *__restrict__ first_edge, int2 *edges)
+{
+    PAMO_GRID_STRIDE(f, m)
+    {
+        int4 t = tris[f];
+        if (face_dead(t)) continue;
+        near_tris[first_near[t.x] + atomicAdd(&cursor[t.x], 1)] = (int)f;
+        near_tris[first_near[t.y] + atomicAdd(&cursor[t.y], 1)] = (int)f;
+        near_tris[first_near[t.z] + atomicAdd(&cursor[t.z], 1)] = (int)f;
+        int e = first_edge[f];
+        if (t.x > t.y) edges[e++] = make_int2(t.y, t.x);
+        if (t.y > t.z) edges[e++] = make_int2(t.z, t.y);
+        if (t.z > t.x) edges[e++] = make_int2(t.x, t.z);
+    }
+}
+
+// Canonical segment order, then the quadric sum p p^T in that order.
+__global__ void k_vertex_quadric(const int *__restrict__ first_near, int *near_tris,
+                                 const float4 *__restrict__ plane, float4 *quad, int n)
+{
+    PAMO_GRID_STRIDE(v, n)
+    {
+        int a = first_near[v], b = first_near[v + 1];
+        for (int i = a + 1; i < b; ++i) {
+            int x = near_tris[i], j = i - 1;
+            while (j >= a && near_tris[j] > x) {
+                near_tris[j + 1] = near_tris[j];
+                --j;
+            }
+            near_tris[j + 1] = x;
+        }
+        float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f, q6 = 0.f, q7 = 0.f, q8 = 0.f, q9 = 0.f;
+        for (int s = a; s < b; ++s) {
+            float4 p = plane[near_tris[s]];
+            q0 += p.x * p.x; q1 += p.x * p.y; q2 += p.x * p.z; q3 += p.x * p.w;
+            q4 += p.y * p.y; q5 += p.y * p.z; q6 += p.y * p.w;
+            q7 += p.z * p.z; q8 += p.z * p.w; q9 += p.w * p.w;
+        }
+        quad[3 * v + 0] = make_float4(q0, q1, q2, q3);
+        quad[3 * v + 1] = make_float4(q4, q5, q6, q7);
+        quad[3 * v + 2] = make_float4(q8, q9, 0.f, 0.f);
+    }
+}
+
+__device__ __forceinline__ int next_after(int4 t, int v)
+{
+    if (t.x == v) return t.y;
+    if (t.y == v) return t.z;
+    if (t.z == v) return t.x;
+    return -2;
+}
+
+__device__ __forceinline__ float skinny_term(V3 n0, V3 n1, V3 n2)
+{
+    // edge_length / triangle_area (cusimp_free.cu:368-380) and the penalty with
+    // the reference's precedence: only the first square divides (:533,573)
+    float l01 = vnorm(vsub(n0, n1));
+    float l12 = vnorm(vsub(n1, n2));
+    float l20 = vnorm(vsub(n2, n0));
+    float s = (l01 + l12 + l20) / 2.0f;
+    float area = sqrtf(s * (s - l01) * (s - l12) * (s - l20));
+    const float c4s3 = 4.0f * sqrtf(3.0f);
+    float e = c4s3 * area / (l01 * l01) + (l12 * l12) + (l20 * l20) + 0.0000001f;
+    return 1.0f - tclamp(e, 0.0f, 1.0f);
+}
+
+struct CostArgs {
+    const int2 *edges;
+    const int *n_edges;
+    const float4 *pts;
+    const int4 *tris;
+    const int *first_near;
+    const int *near_tris;
+    const float4 *quad;
+    const uint8_t *invalid;
+    uint32_t *edge_cost;
+    unsigned long long *vmin;
+    float tres, edge_s;
+    int is_stuck;
+};
+
+// Returns true when the reference writes a new cost for the edge.
+__device__ bool edge_cost_value(const CostArgs &A, int u, int v, uint32_t &out)
+{
+    if (A.invalid[u] && A.invalid[v]) {
+        out = 0xFFFFFFFFu;
+        return true;
+    }
+    if (A.is_stuck) return false;
+    const int ua = A.first_near[u], ub = A.first_near[u + 1];
+    const int va = A.first_near[v], vb = A.first_near[v + 1];
+    int dup = 0;
+    for (int a = ua; a < ub; ++a) {
+        int iu = next_after(A.tris[A.near_tris[a]], u);
+        for (int b = va; b < vb; ++b) {
+            int iv = next_after(A.tris[A.near_tris[b]], v);
+            if (iu == iv) dup++;
+            if (dup > 2) {
+                out = 0xFFFFFFFFu;
+                return true;
+            }
+        }
+    }
+    if (dup != 2) return false;
+
+    float elen = 0.0f;
+    int nedge = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        int lo = pass ? va : ua, hi = pass ? vb : ub;
+        for (int a = lo; a < hi; ++a) {
+            int4 t = A.tris[A.near_tris[a]];
+            if (t.x > t.y) { elen += vnorm(vsub(v3(A.pts[t.x]), v3(A.pts[t.y]))); nedge++; }
+            if (t.y > t.z) { elen += vnorm(vsub(v3(A.pts[t.y]), v3(A.pts[t.z]))); nedge++; }
+            if (t.z > t.x) { elen += vnorm(vsub(v3(A.pts[t.z]), v3(A.pts[t.x]))); nedge++; }
+        }
+    }
+    V3 v0 = v3(A.pts[u]), v1 = v3(A.pts[v]);
+    elen = elen / (float)nedge / A.edge_s * A.tres;
+    elen = elen + vnorm(vsub(v0, v1)) / A.edge_s * A.tres;
+    V3 mid = vmid(v0, v1);
+
+    float Qa = 0.0f;
+    int ntri = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        int w = pass ? v : u, other = pass ? u : v;
+        int lo = pass ? va : ua, hi = pass ? vb : ub;
+        for (int a = lo; a < hi; ++a) {
+            int4 t = A.tris[A.near_tris[a]];
+            if (face_has(t, other)) continue;
+            V3 o0 = v3(A.pts[t.x]), o1 = v3(A.pts[t.y]), o2 = v3(A.pts[t.z]);
+            V3 n0 = t.x == w ? mid : o0;
+            V3 n1 = t.y == w ? mid : o1;
+            V3 n2 = t.z == w ? mid : o2;
+            V3 on = vcross(vsub(o1, o0), vsub(o2, o0));
+            on = vdivs(on, vnorm(on));
+            V3 nn = vcross(vsub(n1, n0), vsub(n2, n0));
+            nn = vdivs(nn, vnorm(nn));
+            if (vdot(on, nn) < 0) {
+                out = 0xFFFFFFFFu;
+                return true;
+            }
+            Qa += skinny_term(n0, n1, n2);
+            ntri++;
+        }
+    }
+    Qa = 5.0f * Qa;
+    float4 a0 = A.quad[3 * u], a1 = A.quad[3 * u + 1], a2 = A.quad[3 * u + 2];
+    float4 b0 = A.quad[3 * v], b1 = A.quad[3 * v + 1], b2 = A.quad[3 * v + 2];
+    float m00 = a0.x + b0.x, m01 = a0.y + b0.y, m02 = a0.z + b0.z, m03 = a0.w + b0.w;
+    float m11 = a1.x + b1.x, m12 = a1.y + b1.y, m13 = a1.z + b1.z, m22 = a1.w + b1.w;
+    float m23 = a2.x + b2.x, m33 = a2.y + b2.y;
+    float x = mid.x, y = mid.y, z = mid.z, w = 1.0f;
+    float r0 = m00 * x + m01 * y + m02 * z + m03 * w;
+    float r1 = m01 * x + m11 * y + m12 * z + m13 * w;
+    float r2 = m02 * x + m12 * y + m22 * z + m23 * w;
+    float r3 = m03 * x + m13 * y + m23 * z + m33 * w;
+    float qe = r0 * x + r1 * y + r2 * z + r3 * w;
+    float cost = qe / (A.edge_s * A.edge_s);
+    out = quantise_cost(cost + elen + Qa / (float)ntri * A.tres);
+    return true;
+}
+
+__global__ void __launch_bounds__(kThreads) k_edge_cost(CostArgs A)
+{
+    const int E = *A.n_edges;
+    PAMO_GRID_STRIDE(e, E)
+    {
+        int2 ed = A.edges[e];
+        uint32_t c;
+        if (edge_cost_value(A, ed.x, ed.y, c)) A.edge_cost[e] = c;
+        else c = A.edge_cost[e];  // the reference keeps the previous round's value
+        unsigned long long key = ((unsigned long long)c << 32) | (unsigned)e;
+        atomicMin(&A.vmin[ed.x], key);
+        atomicMin(&A.vmin[ed.y], key);
+    }
+}
+
+__device__ __forceinline__ bool is_skinny(V3 p, V3 q, V3 r)
+{
+    V3 pq = vsub(q, p), pr = vsub(r, p), qr = vsub(r, q);
+    float lpq = sqrtf(vdot(pq, pq)), lpr = sqrtf(vdot(pr, pr)), lqr = sqrtf(vdot(qr, qr));
+    float ml = fmaxf(lpq, fmaxf(lpr, lqr));
+    V3 c = vcross(pq, pr);
+    float thr = (float)(1e-6 * (double)ml * (double)ml);
+    float area = 0.5f * sqrtf(c.x * c.x + c.y * c.y + c.z * c.z);
+    return area < thr;
+}
+
+struct CollapseArgs {
+    const int2 *edges;
+    const int *n_edges;
+    const uint32_t *edge_cost;
+    const unsigned long long *vmin;
+    const int *first_near;
+    const int *near_tris;
+    const float4 *opts;
+    const int4 *otris;
+    float4 *pts;
+    int4 *tris;
+    int *occ;
+    int *eflag;
+    uint32_t collapse_t;
+};
+
+__device__ __forceinline__ bool faces_min_ok(const CollapseArgs &A, int lo, int hi, unsigned long long key)
+{
+    for (int a = lo; a < hi; ++a) {
+        int4 t = A.otris[A.near_tris[a]];  // round input: never written during this pass
+        if (A.vmin[t.x] < key || A.vmin[t.y] < key || A.vmin[t.z] < key) return false;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
+{
+    const int E = *A.n_edges;
+    PAMO_GRID_STRIDE(e, E)
+    {
+        int win = 0;
+        uint32_t c = A.edge_cost[e];
+        if (c <= A.collapse_t) {
+            int2 ed = A.edges[e];
+            const int u = ed.x, v = ed.y;
+            unsigned long long key = ((unsigned long long)c << 32) | (unsigned)e;
+            const int ua = A.first_near[u], ub = A.first_near[u + 1];
+            const int va = A.first_near[v], vb = A.first_near[v + 1];
+            if (A.vmin[u] == key && A.vmin[v] == key && faces_min_ok(A, ua, ub, key) && faces_min_ok(A, va, vb, key)) {
+                win = 1;
+                V3 p0 = v3(A.opts[u]), p1 = v3(A.opts[v]);
+                V3 mid = vmid(p0, p1);
+                A.pts[u] = make_float4(mid.x, mid.y, mid.z, 0.f);
+                A.pts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+                A.occ[v] = 0;
+                for (int a = ua; a < ub; ++a) {
+                    int f = A.near_tris[a];
+                    int4 t = A.tris[f];
+                    if (face_has(t, v)) A.tris[f] = make_int4(-1, -1, -1, 0);
+                }
+                for (int a = va; a < vb; ++a) {
+                    int f = A.near_tris[a];
+                    int4 t = A.tris[f];
+                    if (face_has(t, u)) t = make_int4(-1, -1, -1, 0);
+                    else if (t.x == v) t.x = u;
+                    else if (t.y == v) t.y = u;
+                    else if (t.z == v) t.z = u;
+                    A.tris[f] = t;
+                }
+                bool sk = false;
+                for (int pass = 0; pass < 2 && !sk; ++pass) {
+                    int lo = pass ? va : ua, hi = pass ? vb : ub;
+                    for (int a = lo; a < hi; ++a) {
+                        int4 t = A.tris[A.near_tris[a]];
+                        if (t.x == -1) continue;
+                        if (is_skinny(v3(A.pts[t.x]), v3(A.pts[t.y]), v3(A.pts[t.z]))) {
+                            sk = true;
+                            break;
+                        }
+                    }
+                }
+                if (sk) {  // roll back; the edge stays in the collapsed list
+                    A.occ[v] = 1;
+                    A.pts[u] = A.opts[u];
+                    A.pts[v] = A.opts[v];
+                    for (int a = ua; a < ub; ++a) A.tris[A.near_tris[a]] = A.otris[A.near_tris[a]];
+                    for (int a = va; a < vb; ++a) A.tris[A.near_tris[a]] = A.otris[A.near_tris[a]];
+                }
+            }
+        }
+        A.eflag[e] = win;
+    }
+}
+
+// list[pos[i]] = i for flagged i (pos = exclusive scan of the flags)
+__global__ void k_scatter_flagged(const int *__restrict__ flags, const int *__restrict__ pos, const int *d_n,
+                                  int *list, int list_offset)
+{
+    const int N = *d_n;
+    PAMO_GRID_STRIDE(i, N)
+    {
+        if (flags[i]) list[list_offset + pos[i]] = (int)i;
+    }
+}
+
+__global__ void k_remove_invalid_faces(int4 *tris, int m)
+{
+    PAMO_GRID_STRIDE(f, m)
+    {
+        int4 t = tris[f];
+        if (face_dead(t)) continue;
+        if (t.x == t.y || t.y == t.z || t.z == t.x) tris[f] = make_int4(-1, -1, -1, 0);
+    }
+}
+
+__global__ void k_line_flags(const int2 *edges, const int *n_edges, const float4 *pts, int *eflag, int *count)
+{
+    const int E = *n_edges;
+    int local = 0;
+    PAMO_GRID_STRIDE(e, E)
+    {
+        int2 ed = edges[e];
+        float4 p = pts[ed.x], q = pts[ed.y];
+        int f = (p.x == q.x && p.y == q.y && p.z == q.z);
+        eflag[e] = f;
+        local += f;
+    }
+    if (local) atomicAdd(count, local);
+}
+
+// Coincident-endpoint collapses: positions were read (k_line_flags) before any
+// write; the writes are applied here in edge order by one thread.  Runs only
+// when at least one edge was flagged (rare: needs exactly equal coordinates).
+__global__ void k_line_apply(const int2 *edges, const int *n_edges, const int *eflag, const int *first_near,
+                             const int *near_tris, float4 *pts, int4 *tris, int *occ, int *collapsed,
+                             RoundCounters *cnt)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int E = *n_edges;
+    int nm = cnt->n_main, k = 0;
+    if (cnt->n_line > 0) {
+        for (int e = 0; e < E; ++e) {
+            if (!eflag[e]) continue;
+            int u = edges[e].x, v = edges[e].y;
+            collapsed[nm + k++] = e;
+            pts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+            occ[v] = 0;
+            for (int a = first_near[u]; a < first_near[u + 1]; ++a) {
+                int f = near_tris[a];
+                if (face_has(tris[f], v)) tris[f] = make_int4(-1, -1, -1, 0);
+            }
+            for (int a = first_near[v]; a < first_near[v + 1]; ++a) {
+                int f = near_tris[a];
+                int4 t = tris[f];
+                if (face_has(t, u)) t = make_int4(-1, -1, -1, 0);
+                else if (t.x == v) t.x = u;
+                else if (t.y == v) t.y = u;
+                else if (t.z == v) t.z = u;
+                tris[f] = t;
+            }
+        }
+    }
+    cnt->n_line = k;
+    cnt->n_total = nm + k;
+    int window = ((nm + 511) / 512) * 512;  // grid of the reference's undo-candidate launch
+    cnt->n_considered = cnt->n_total < window ? cnt->n_total : window;
+}
+
+__global__ void k_mark_active(const int *collapsed, const RoundCounters *cnt, const int2 *edges,
+                              const int *first_near, const int *near_tris, uint8_t *active)
+{
+    const int N = cnt->n_considered;
+    PAMO_GRID_STRIDE(p, N)
+    {
+        int2 ed = edges[collapsed[p]];
+        for (int a = first_near[ed.x]; a < first_near[ed.x + 1]; ++a) active[near_tris[a]] = 1;
+        for (int a = first_near[ed.y]; a < first_near[ed.y + 1]; ++a) active[near_tris[a]] = 1;
+    }
+}
+
+constexpr int kStack = 96;
+
+__device__ __forceinline__ bool box_overlap(float4 alo, float4 ahi, float3 qlo, float3 qhi)
+{
+    return !(ahi.x < qlo.x || qhi.x < alo.x || ahi.y < qlo.y || qhi.y < alo.y || ahi.z < qlo.z || qhi.z < alo.z);
+}
+
+__device__ __forceinline__ int shared_indices(int4 a, int4 b)
+{
+    return (a.x == b.x) + (a.x == b.y) + (a.x == b.z) + (a.y == b.x) + (a.y == b.y) + (a.y == b.z) +
+           (a.z == b.x) + (a.z == b.y) + (a.z == b.z);
+}
+
+// For each active live face, enumerate overlapping leaves and append candidate
+// pairs.  A pair of two active faces is emitted once (by the lower index);
+// pairs sharing two or more vertex indices are never reported by the reference
+// and are dropped here.
+__global__ void __launch_bounds__(kThreads) k_query(const BvhNode *__restrict__ nodes, const int *__restrict__ vals,
+                                                    const int *scene, const float4 *__restrict__ pts,
+                                                    const int4 *__restrict__ tris, const uint8_t *__restrict__ active,
+                                                    int m, uint2 *pairs, long long cap_pairs, RoundCounters *cnt)
+{
+    const int L = scene[7];
+    int stack[kStack];
+    PAMO_GRID_STRIDE(ff, m)
+    {
+        const int f = (int)ff;
+        if (!active[f] || L < 2) continue;
+        int4 t = tris[f];
+        if (t.x == -1) continue;
+        float4 a = pts[t.x], b = pts[t.y], c = pts[t.z];
+        float3 qlo = make_float3(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)));
+        float3 qhi = make_float3(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)));
+        int sp = 0;
+        stack[sp++] = 0;
+        // a tree visits each of its L-1 inner nodes at most once per query; the
+        // bound only guards against a corrupted hierarchy
+        int budget = 2 * L + 16;
+        while (sp > 0) {
+            if (--budget < 0) {
+                atomicAdd(&cnt->stack_overflow, 1);
+                break;
+            }
+            const BvhNode nd = nodes[stack[--sp]];
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                float4 lo = side ? nd.rlo : nd.llo;
+                float4 hi = side ? nd.rhi : nd.lhi;
+                if (!box_overlap(lo, hi, qlo, qhi)) continue;
+                int child = __float_as_int(lo.w);
+                if (child < 0) {
+                    int g = vals[~child];
+                    if (g == f) continue;
+                    if (active[g] && g < f) continue;
+                    int4 tg = tris[g];
+                    if (shared_indices(t, tg) >= 2) continue;
+                    int pos = atomicAdd(&cnt->n_pairs, 1);
+                    if (pos < cap_pairs) pairs[pos] = make_uint2((unsigned)f, (unsigned)g);
+                    else atomicAdd(&cnt->pair_overflow, 1);
+                } else if (sp < kStack) {
+                    stack[sp++] = child;
+                } else {
+                    atomicAdd(&cnt->stack_overflow, 1);
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void load_face(const float4 *pts, int4 t, float out[3][3], int idx[3])
+{
+    idx[0] = t.x; idx[1] = t.y; idx[2] = t.z;
+    float4 p[3] = {pts[t.x], pts[t.y], pts[t.z]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        out[a][0] = p[a].x; out[a][1] = p[a].y; out[a][2] = p[a].z;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_pairs(const uint2 *pairs, const RoundCounters *cnt,
+                                                    long long cap_pairs, const float4 *__restrict__ pts,
+                                                    const int4 *__restrict__ tris, uint8_t *isect, float eps)
+{
+    long long N = cnt->n_pairs < cap_pairs ? cnt->n_pairs : cap_pairs;
+    PAMO_GRID_STRIDE(k, N)
+    {
+        uint2 pr = pairs[k];
+        float A[3][3], B[3][3];
+        int ia[3], ib[3];
+        load_face(pts, tris[pr.x], A, ia);
+        load_face(pts, tris[pr.y], B, ib);
+        if (pair_flag_directed(A, ia, B, ib, eps) || pair_flag_directed(B, ib, A, ia, eps)) {
+            isect[pr.x] = 1;
+            isect[pr.y] = 1;
+        }
+    }
+}
+
+__global__ void k_undo_flags(const int *collapsed, const RoundCounters *cnt, const int2 *edges,
+                             const int *first_near, const int *near_tris, const uint8_t *isect, int *uflag)
+{
+    const int N = cnt->n_considered;
+    PAMO_GRID_STRIDE(p, N)
+    {
+        int2 ed = edges[collapsed[p]];
+        int hit = 0;
+        for (int a = first_near[ed.x]; a < first_near[ed.x + 1] && !hit; ++a) hit = isect[near_tris[a]];
+        for (int a = first_near[ed.y]; a < first_near[ed.y + 1] && !hit; ++a) hit = isect[near_tris[a]];
+        uflag[p] = hit;
+    }
+}
+
+__global__ void k_undo_scatter(const int *uflag, const int *upos, const RoundCounters *cnt, const int *collapsed,
+                               const int2 *edges, int *undo_edges, int *tmp_undo)
+{
+    const int N = cnt->n_considered;
+    PAMO_GRID_STRIDE(p, N)
+    {
+        if (!uflag[p]) continue;
+        int k = upos[p];
+        int e = collapsed[p];
+        int2 ed = edges[e];
+        undo_edges[k] = e;
+        tmp_undo[2 * k] = ed.x;
+        tmp_undo[2 * k + 1] = ed.y;
+    }
+}
+
+__global__ void k_undo_apply(const int *undo_edges, const RoundCounters *cnt, const int2 *edges,
+                             const int *first_near, const int *near_tris, const float4 *opts, const int4 *otris,
+                             float4 *pts, int4 *tris, int *occ)
+{
+    const int N = cnt->n_undo;
+    PAMO_GRID_STRIDE(k, N)
+    {
+        int2 ed = edges[undo_edges[k]];
+        int u = ed.x, v = ed.y;
+        occ[v] = 1;
+        pts[u] = opts[u];
+        pts[v] = opts[v];
+        for (int a = first_near[u]; a < first_near[u + 1]; ++a) tris[near_tris[a]] = otris[near_tris[a]];
+        for (int a = first_near[v]; a < first_near[v + 1]; ++a) tris[near_tris[a]] = otris[near_tris[a]];
+    }
+}
+
+// undo_list[first + i] = pts_map[tmp_undo[i]]: the map in pts_map at this point is
+// the previous round's (cusimp_free.cu:869-878 runs before :1042-1045).
+__global__ void k_rearrange(const int *tmp_undo, const int *pts_map, int *undo_list, int first, int count)
+{
+    PAMO_GRID_STRIDE(i, count) undo_list[first + i] = pts_map[tmp_undo[i]];
+}
+
+__global__ void k_mark_invalid(const int *undo_in, int n, uint8_t *table)
+{
+    PAMO_GRID_STRIDE(i, n) table[undo_in[i]] = 1;
+}
+
+__global__ void k_face_live_flags(const int4 *tris, int m, int *fflag)
+{
+    PAMO_GRID_STRIDE(f, m) fflag[f] = tris[f].x >= 0;
+}
+
+__global__ void k_compact(const float4 *pts, const int *occ, const int *pts_map, int n, const int4 *tris,
+                          const int *fflag, const int *fpos, int m, float4 *opts, int4 *otris, RoundCounters *cnt)
+{
+    long long N = n > m ? n : m;
+    PAMO_GRID_STRIDE(i, N)
+    {
+        if (i < n && occ[i]) opts[pts_map[i]] = pts[i];
+        if (i < m && fflag[i]) {
+            int4 t = tris[i];
+            otris[fpos[i]] = make_int4(pts_map[t.x], pts_map[t.y], pts_map[t.z], 0);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt->n_pts_next = pts_map[n];
+        cnt->n_tris_next = fpos[m - 1 >= 0 ? m - 1 : 0] + (m > 0 ? fflag[m - 1] : 0);
+    }
+}
+
+__global__ void k_validate_faces(const int *tris, int m, int n, int *bad)
+{
+    int local = 0;
+    PAMO_GRID_STRIDE(f, m)
+    {
+        int a = tris[3 * f], b = tris[3 * f + 1], c = tris[3 * f + 2];
+        bool dead = a == -1 && b == -1 && c == -1;
+        bool ok = a >= 0 && a < n && b >= 0 && b < n && c >= 0 && c < n;
+        local += !(dead || ok);
+    }
+    if (local) atomicAdd(bad, local);
+}
+
+__global__ void k_validate_range(const int *v, int count, int hi, int *bad)
+{
+    int local = 0;
+    PAMO_GRID_STRIDE(i, count) local += (v[i] < 0 || v[i] > hi);
+    if (local) atomicAdd(bad, local);
+}
+
+}  // namespace
+
+int Stage2::validate(const int *d_tris, int n, int m, const int *d_undo, int n_undo, int undo_hi, cudaStream_t s)
+{
+    int *bad = dev_misc + 32;
+    S2_TRY_EARLY(cudaMemsetAsync(bad, 0, 4, s));
+    if (m > 0) k_validate_faces<<<grid_for(m), kThreads, 0, s>>>(d_tris, m, n, bad);
+    if (n_undo > 0) k_validate_range<<<grid_for(n_undo), kThreads, 0, s>>>(d_undo, n_undo, undo_hi, bad);
+    S2_TRY_EARLY(cudaMemcpyAsync(hcnt, bad, 4, cudaMemcpyDeviceToHost, s));
+    S2_TRY_EARLY(cudaStreamSynchronize(s));
+    return hcnt->n_main == 0 ? PAMO_OK : PAMO_ERR_INVALID_ARG;
+}
+
+// ---------------------------------------------------------------------------
+// buffers
+
+void Stage2::release()
+{
+    void *p[] = {edge_cost, pts_map, undo_list, tmp_undo, invalid_table, opts, pts, otris, tris, occ,
+                 first_near, cursor, near_tris, first_edge, edges, plane, quad, vmin, eflag, collapsed,
+                 active, isect, uflag, undo_edges, fflag, pairs, scan_scratch, dev_misc, dcnt};
+    for (void *q : p)
+        if (q) cudaFree(q);
+    if (hcnt) cudaFreeHost(hcnt);
+    if (h_scalars) cudaFreeHost(h_scalars);
+    edge_cost = nullptr; pts_map = nullptr; undo_list = nullptr; tmp_undo = nullptr; invalid_table = nullptr;
+    opts = pts = nullptr; otris = tris = nullptr; occ = nullptr;
+    first_near = cursor = near_tris = first_edge = nullptr; edges = nullptr; plane = quad = nullptr;
+    vmin = nullptr; eflag = collapsed = nullptr; active = isect = nullptr; uflag = undo_edges = fflag = nullptr;
+    pairs = nullptr; scan_scratch = nullptr; dev_misc = nullptr; dcnt = nullptr; hcnt = nullptr; h_scalars = nullptr;
+    bvh.release();
+    cap_pts = cap_tris = cap_edges = cap_undo = cap_pairs = 0;
+}
+
+int Stage2::ensure(long long n, long long m)
+{
+    if (n <= cap_pts && m <= cap_tris && dcnt) return PAMO_OK;
+    long long cp = n > cap_pts ? n : cap_pts;
+    long long ct = m > cap_tris ? m : cap_tris;
+    release();
+    cp = cp > 4 ? cp : 4;
+    ct = ct > 4 ? ct : 4;
+    long long ce = 3 * ct;
+    long long cu = 16 * (cp + 1) + 6 * ct + 16;
+    long long big = (cp + 1 > ce + 1 ? cp + 1 : ce + 1);
+    big = big > ct + 1 ? big : ct + 1;
+    scan_scratch_len = scan_scratch_ints(big);
+#define ALLOC(ptr, bytes)                                             \
+    do {                                                              \
+        if (cudaMalloc((void **)&ptr, (size_t)(bytes)) != cudaSuccess) { \
+            release();                                                \
+            return PAMO_ERR_OOM;                                      \
+        }                                                             \
+    } while (0)
+    ALLOC(edge_cost, (ce + 1) * 4);
+    ALLOC(pts_map, (cp + 1) * 4);
+    ALLOC(undo_list, cu * 4);
+    ALLOC(tmp_undo, cu * 4);
+    ALLOC(invalid_table, cp + 1);
+    ALLOC(opts, (cp + 1) * 16);
+    ALLOC(pts, (cp + 1) * 16);
+    ALLOC(otris, (ct + 1) * 16);
+    ALLOC(tris, (ct + 1) * 16);
+    ALLOC(occ, (cp + 1) * 4);
+    ALLOC(first_near, (cp + 1) * 4);
+    ALLOC(cursor, (cp + 1) * 4);
+    ALLOC(near_tris, 3 * (ct + 1) * 4);
+    ALLOC(first_edge, (ct + 1) * 4);
+    ALLOC(edges, (ce + 1) * 8);
+    ALLOC(plane, (ct + 1) * 16);
+    ALLOC(quad, 3 * (cp + 1) * 16);
+    ALLOC(vmin, (cp + 1) * 8);
+    ALLOC(eflag, (ce + 1) * 4);
+    ALLOC(collapsed, (ce + 1) * 4);
+    ALLOC(active, ct + 1);
+    ALLOC(isect, ct + 1);
+    ALLOC(uflag, (ce + 1) * 4);
+    ALLOC(undo_edges, (ce + 1) * 4);
+    ALLOC(fflag, (ct + 1) * 4);
+    ALLOC(scan_scratch, scan_scratch_len * 4);
+    ALLOC(dev_misc, 256);
+    ALLOC(dcnt, sizeof(RoundCounters));
+#undef ALLOC
+    if (cudaMallocHost((void **)&hcnt, sizeof(RoundCounters)) != cudaSuccess) {
+        release();
+        return PAMO_ERR_OOM;
+    }
+    if (cudaMallocHost((void **)&h_scalars, 64) != cudaSuccess) {
+        release();
+        return PAMO_ERR_OOM;
+    }
+    // state the reference reads stale starts at zero
+    cudaMemset(edge_cost, 0, (ce + 1) * 4);
+    cudaMemset(pts_map, 0, (cp + 1) * 4);
+    cudaMemset(undo_list, 0, cu * 4);
+    cudaMemset(tmp_undo, 0, cu * 4);
+    cudaMemset(invalid_table, 0, cp + 1);
+    cap_pts = cp;
+    cap_tris = ct;
+    cap_edges = ce;
+    cap_undo = cu;
+    if (bvh.ensure(ct) != cudaSuccess) {
+        release();
+        return PAMO_ERR_OOM;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return PAMO_ERR_DEVICE;
+    return ensure_pairs(16 * ct);
+}
+
+int Stage2::ensure_pairs(long long n)
+{
+    if (n <= cap_pairs && pairs) return PAMO_OK;
+    if (pairs) cudaFree(pairs);
+    pairs = nullptr;
+    cap_pairs = 0;
+    if (cudaMalloc((void **)&pairs, (size_t)n * sizeof(uint2)) != cudaSuccess) return PAMO_ERR_OOM;
+    cap_pairs = n;
+    return PAMO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// one round
+
+#define S2_TRY(expr)                                  \
+    do {                                              \
+        cudaError_t _e = (expr);                      \
+        if (_e != cudaSuccess) return map_cuda_error(_e); \
+    } while (0)
+
+static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s)
+{
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(S.isect, 0, (size_t)m, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(&S.dcnt->n_pairs, 0, 2 * sizeof(int), s)) != cudaSuccess) return e;  // n_pairs, overflow
+    if ((e = lbvh_refit(S.bvh, S.pts, S.tris, m, s)) != cudaSuccess) return e;
+    k_query<<<grid_for(m), kThreads, 0, s>>>(S.bvh.nodes, S.bvh.vals, S.bvh.scene, S.pts, S.tris, S.active, m,
+                                             S.pairs, S.cap_pairs, S.dcnt);
+    k_pairs<<<grid_for(S.cap_pairs), kThreads, 0, s>>>(S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris, S.isect, 1e-3f);
+    return cudaGetLastError();
+}
+
+static cudaError_t undo_check(Stage2 &S, cudaStream_t s)
+{
+    const long long NC = S.cap_edges;
+    k_undo_flags<<<grid_for(NC), kThreads, 0, s>>>(S.collapsed, S.dcnt, S.edges, S.first_near, S.near_tris, S.isect,
+                                                   S.uflag);
+    // positions of the flagged entries (in collapsed-list order)
+    cudaError_t e = exclusive_scan(S.uflag, S.eflag, NC, &S.dcnt->n_considered, S.scan_scratch, &S.dcnt->n_undo, s);
+    if (e != cudaSuccess) return e;
+    k_undo_scatter<<<grid_for(NC), kThreads, 0, s>>>(S.uflag, S.eflag, S.dcnt, S.collapsed, S.edges, S.undo_edges,
+                                                     S.tmp_undo);
+    return cudaGetLastError();
+}
+
+int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, const int *d_undo_in, int n_undo_in,
+                  int *n_undo_out, cudaStream_t s)
+{
+    int nvu = 0, first = 0;
+    S2_TRY(cudaMemsetAsync(dcnt, 0, sizeof(RoundCounters), s));
+    if (is_stuck) {
+        if (n_undo_in > 0) {
+            S2_TRY(cudaMemcpyAsync(tmp_undo, d_undo_in, (size_t)n_undo_in * 4, cudaMemcpyDeviceToDevice, s));
+            k_rearrange<<<grid_for(n_undo_in), kThreads, 0, s>>>(tmp_undo, pts_map, undo_list, 0, n_undo_in);
+        }
+        nvu += n_undo_in;
+        first += n_undo_in;
+    } else if (n_undo_in != 0) {
+        S2_TRY(cudaMemsetAsync(invalid_table, 0, (size_t)cap_pts + 1, s));
+    }
+    if (n_undo_in > 0) k_mark_invalid<<<grid_for(n_undo_in), kThreads, 0, s>>>(d_undo_in, n_undo_in, invalid_table);
+
+    const float tres = threshold, edge_s = scale;
+    // host-side conversion as in the reference (cusimp_free.cu:923): the
+    // template clamp, then float -> u32 keeping the low 32 bits when out of range
+    float ct = (0.0f > threshold) ? 0.0f : threshold;
+    ct = (ct < kCostRange) ? ct : kCostRange;
+    const uint32_t collapse_t = (uint32_t)(unsigned long long)(ct / kCostRange * 4294967296.0f);
+
+    k_round_init<<<grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s>>>(opts, otris, pts, tris, occ, first_near,
+                                                                       cursor, vmin, n, m);
+    k_face_a<<<grid_for(m), kThreads, 0, s>>>(pts, tris, m, first_near, first_edge, plane);
+    if (m > 0) S2_TRY(cudaMemsetAsync(first_edge + m, 0, 4, s));
+    S2_TRY(exclusive_scan(first_near, first_near, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
+    S2_TRY(exclusive_scan(first_edge, first_edge, (long long)m + 1, nullptr, scan_scratch, &dcnt->n_edges, s));
+    const int *d_n_edges = &dcnt->n_edges;
+    k_face_b<<<grid_for(m), kThreads, 0, s>>>(tris, m, first_near, cursor, near_tris, first_edge, edges);
+    k_vertex_quadric<<<grid_for(n), kThreads, 0, s>>>(first_near, near_tris, plane, quad, n);
+    // the hierarchy only depends on the round input: build it now
+    S2_TRY(lbvh_build(bvh, pts, tris, m, s));
+
+    const long long EMAX = 3LL * m;
+    CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, quad, invalid_table, edge_cost, vmin,
+                tres, edge_s, is_stuck ? 1 : 0};
+    k_edge_cost<<<grid_for(EMAX), kThreads, 0, s>>>(ca);
+    CollapseArgs cl{edges, d_n_edges, edge_cost, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
+                    collapse_t};
+    k_collapse<<<grid_for(EMAX), kThreads, 0, s>>>(cl);
+    S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
+    k_scatter_flagged<<<grid_for(EMAX), kThreads, 0, s>>>(eflag, uflag, d_n_edges, collapsed, 0);
+    k_remove_invalid_faces<<<grid_for(m), kThreads, 0, s>>>(tris, m);
+    k_line_flags<<<grid_for(EMAX), kThreads, 0, s>>>(edges, d_n_edges, pts, eflag, &dcnt->n_line);
+    k_line_apply<<<1, 32, 0, s>>>(edges, d_n_edges, eflag, first_near, near_tris, pts, tris, occ, collapsed, dcnt);
+
+    S2_TRY(cudaMemsetAsync(active, 0, (size_t)m, s));
+    k_mark_active<<<grid_for(EMAX), kThreads, 0, s>>>(collapsed, dcnt, edges, first_near, near_tris, active);
+    S2_TRY(isect_pass(*this, m, s));
+    S2_TRY(undo_check(*this, s));
+    S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+    S2_TRY(cudaStreamSynchronize(s));
+    if (hcnt->pair_overflow > 0) {
+        // candidate buffer too small: grow and redo the pass
+        long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
+        int rc = ensure_pairs(need);
+        if (rc) return rc;
+        S2_TRY(isect_pass(*this, m, s));
+        S2_TRY(undo_check(*this, s));
+        S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+        S2_TRY(cudaStreamSynchronize(s));
+        if (hcnt->pair_overflow > 0) return PAMO_ERR_CAPACITY;
+    }
+    if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
+    last_stats[0] = hcnt->n_edges;
+    last_stats[1] = hcnt->n_main;
+    last_stats[2] = hcnt->n_total;
+    last_stats[5] = hcnt->n_pairs;
+    last_stats[6] = m;
+    int cnt_undo = hcnt->n_undo;
+    nvu += 2 * cnt_undo;
+    if (nvu > cap_undo) return PAMO_ERR_CAPACITY;
+    int it = 0;
+    while (cnt_undo != 0) {
+        it++;
+        k_undo_apply<<<grid_for(cnt_undo), kThreads, 0, s>>>(undo_edges, dcnt, edges, first_near, near_tris, opts,
+                                                              otris, pts, tris, occ);
+        if (nvu - first > 0)
+            k_rearrange<<<grid_for(nvu - first), kThreads, 0, s>>>(tmp_undo, pts_map, undo_list, first, nvu - first);
+        first += 2 * cnt_undo;
+        S2_TRY(isect_pass(*this, m, s));
+        S2_TRY(undo_check(*this, s));
+        S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+        S2_TRY(cudaStreamSynchronize(s));
+        if (hcnt->pair_overflow > 0) {
+            long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
+            int rc = ensure_pairs(need);
+            if (rc) return rc;
+            S2_TRY(isect_pass(*this, m, s));
+            S2_TRY(undo_check(*this, s));
+            S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+            S2_TRY(cudaStreamSynchronize(s));
+            if (hcnt->pair_overflow > 0) return PAMO_ERR_CAPACITY;
+        }
+        if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
+        cnt_undo = hcnt->n_undo;
+        nvu += 2 * cnt_undo;
+        if (nvu > cap_undo) return PAMO_ERR_CAPACITY;
+        if (it == 5) break;
+    }
+    last_stats[3] = it;
+    last_stats[4] = nvu;
+    // pts_map = exclusive scan of occ[0..n]
+    S2_TRY(exclusive_scan(occ, pts_map, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
+    *n_undo_out = nvu;
+    return PAMO_OK;
+}
+
+int Stage2::compact(int n, int m, cudaStream_t s)
+{
+    k_face_live_flags<<<grid_for(m), kThreads, 0, s>>>(tris, m, fflag);
+    S2_TRY(exclusive_scan(fflag, uflag, m, nullptr, scan_scratch, nullptr, s));
+    k_compact<<<grid_for(n > m ? n : m), kThreads, 0, s>>>(pts, occ, pts_map, n, tris, fflag, uflag, m, opts, otris,
+                                                           dcnt);
+    S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+    S2_TRY(cudaStreamSynchronize(s));
+    return PAMO_OK;
+}
+
+}  // namespace pamo

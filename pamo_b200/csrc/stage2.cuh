@@ -1,0 +1,87 @@
+// Stage-2 simplification state and round driver (host side).
+#pragma once
+
+#include "common.cuh"
+#include "lbvh.cuh"
+
+namespace pamo {
+
+// Device counters of one round (one struct, copied to the host in one go).
+struct RoundCounters {
+    int n_main;          // collapsed edges chosen by the independent set
+    int n_line;          // coincident-endpoint edges collapsed afterwards
+    int n_total;         // n_main + n_line
+    int n_considered;    // collapsed-list prefix the undo check looks at
+    int n_undo;          // undo edges found by the last check
+    int n_pairs;         // candidate pairs found by the last query
+    int pair_overflow;   // pairs dropped for lack of buffer space
+    int stack_overflow;  // traversals that ran out of stack
+    int n_pts_next;      // compaction result
+    int n_tris_next;
+    int n_edges;
+    int pad[5];
+};
+
+struct Stage2 {
+    int device = 0;
+    long long cap_pts = 0, cap_tris = 0, cap_edges = 0, cap_undo = 0, cap_pairs = 0;
+
+    // persistent between rounds (the reference reads these stale)
+    uint32_t *edge_cost = nullptr;
+    int *pts_map = nullptr;
+    int *undo_list = nullptr;
+    int *tmp_undo = nullptr;
+    uint8_t *invalid_table = nullptr;
+
+    // round input ("original" snapshot) and working copies
+    float4 *opts = nullptr, *pts = nullptr;
+    int4 *otris = nullptr, *tris = nullptr;
+    int *occ = nullptr;
+    int *first_near = nullptr, *cursor = nullptr, *near_tris = nullptr;
+    int *first_edge = nullptr;
+    int2 *edges = nullptr;
+    float4 *plane = nullptr;
+    float4 *quad = nullptr;  // 3 float4 per vertex (10 used)
+    unsigned long long *vmin = nullptr;
+    int *eflag = nullptr;
+    int *collapsed = nullptr;
+    uint8_t *active = nullptr;
+    uint8_t *isect = nullptr;
+    int *uflag = nullptr;
+    int *undo_edges = nullptr;
+    int *fflag = nullptr;  // face compaction flags
+    uint2 *pairs = nullptr;
+    int *scan_scratch = nullptr;
+    long long scan_scratch_len = 0;
+    int *dev_misc = nullptr;  // scalars: [0] tris_mean-bits etc.
+    RoundCounters *dcnt = nullptr;
+    RoundCounters *hcnt = nullptr;  // pinned
+    float *h_scalars = nullptr;     // pinned: [0..2] offset, [3] scale
+    Lbvh bvh;
+
+    // input staging for the per-round ABI ([n,3] layouts)
+    // results of the device loop
+    int res_n_pts = 0, res_n_tris = 0, res_rounds = 0;
+    float offset[3] = {0, 0, 0};
+    long long last_stats[8] = {0};
+
+    int ensure(long long n_pts, long long n_tris);
+    // Rejects faces whose indices are outside [0, n) (other than removed faces
+    // -1,-1,-1) and undo entries outside [0, undo_hi]; nothing else runs on bad input.
+    int validate(const int *d_tris_aos3, int n, int m, const int *d_undo, int n_undo, int undo_hi, cudaStream_t s);
+    int ensure_pairs(long long n);
+    void release();
+
+    // One round on opts/otris (already holding the input; init shuffle applied
+    // by the caller).  d_undo_in: device list of n_undo_in entries.
+    int round(int n, int m, float scale, float threshold, bool is_stuck, const int *d_undo_in, int n_undo_in,
+              int *n_undo_out, cudaStream_t s);
+
+    // compaction of the round's output into opts/otris for the next round;
+    // returns new sizes through hcnt (after a sync).
+    int compact(int n, int m, cudaStream_t s);
+};
+
+int stage2_shuffle_faces(int4 *tris, int m, cudaStream_t s);  // reference init permutation
+
+}  // namespace pamo
