@@ -50,29 +50,42 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled through NVML during the timed region
+    (in-process, every 100 ms)."""
+
+    REASONS = {  # nvmlClocksEventReason bits
+        "sw_power_cap": 0x4,
+        "hw_slowdown": 0x8,
+        "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40,
+        "hw_power_brake_slowdown": 0x80,
+    }
 
     def __init__(self, index=0):
         self.index = index
         self.samples = []
         self._stop = threading.Event()
         self._t = None
+        self.error = None
 
     def start(self):
         def run():
-            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap")
-            while not self._stop.is_set():
-                try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.samples.append([x.strip() for x in out.split(",")])
-                except Exception:
-                    pass
-                self._stop.wait(0.2)
+            try:
+                import pynvml as N
+
+                N.nvmlInit()
+                h = N.nvmlDeviceGetHandleByIndex(self.index)
+                mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+                while not self._stop.is_set():
+                    sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                    try:
+                        rs = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    except Exception:
+                        rs = N.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                    self.samples.append((sm, mx, rs))
+                    self._stop.wait(0.1)
+            except Exception as e:  # no NVML: report that instead of clocks
+                self.error = repr(e)
 
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
@@ -81,11 +94,11 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and "Active" in s[3 + k]})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "error": self.error}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({k for s in self.samples for k, bit in self.REASONS.items() if s[2] & bit})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(s[1] for s in self.samples)),
                 "reasons": reasons, "samples": len(self.samples)}
 
 
@@ -163,6 +176,29 @@ def _sample_fraction(args, sample_rounds):
     return float(sum(sizes[:sample_rounds])) / tot if tot else None
 
 
+def roofline_edge_cost(phases, round_faces, peaks):
+    """HBM roofline of the edge-cost kernel (one launch per round).
+
+    Algorithmic bytes per round with F faces (closed mesh: E = 1.5 F edges,
+    V = 0.5 F vertices), each array read or written once: edges 8 B/edge,
+    cost write 4 B/edge, CSR offsets 4 B/vertex, CSR entries 12 B/face, faces
+    (int4) 16 B/face, points (float4) 16 B/vertex, quadrics 48 B/vertex,
+    invalid flags 1 B/vertex, per-vertex key minimum read+write 16 B/vertex:
+    12 E + 85 V + 28 F = 88.5 B/face."""
+    ph = phases.get("edge_cost")
+    if not ph or not ph["ms"] or not round_faces:
+        return None
+    total_bytes = sum(88.5 * f for f in round_faces)
+    t = ph["ms"] / 1e3
+    achieved = total_bytes / t / 1e9
+    peak = peaks.get("hbm_gbs") or 6650.0
+    return {"bound": "hbm", "kernel": "k_edge_cost", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "launches": ph["calls"],
+            "avg_launch_ms": ph["ms"] / max(ph["calls"], 1),
+            "bytes_per_launch_avg": total_bytes / max(ph["calls"], 1),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs") else "fallback"}
+
+
 def product_arm(args):
     import torch
 
@@ -232,6 +268,18 @@ def product_arm(args):
         torch.cuda.synchronize()
         lat.append(time.perf_counter() - t0)
     clocks = clk.stop()
+    # one more run with per-phase CUDA events (outside the timed region)
+    L.pamo_profile_enable(ctx.handle, 1)
+    run_resident()
+    torch.cuda.synchronize()
+    ph_ms = (ctypes.c_double * 16)()
+    ph_calls = (ctypes.c_longlong * 16)()
+    nph = L.pamo_profile_read(ctx.handle, ph_ms, ph_calls, 16)
+    L.pamo_profile_enable(ctx.handle, 0)
+    phases = {_lib.PHASES[i]: {"ms": ph_ms[i], "calls": ph_calls[i]} for i in range(min(nph, len(_lib.PHASES)))}
+    sizes = (ctypes.c_int * 4096)()
+    nr = L.pamo_stage2_round_sizes(ctx.handle, sizes, 4096)
+    round_faces = [sizes[i] for i in range(min(nr, 4096))]
     ms_max = dev_ms
     e2e_ms = float(np.mean(lat)) * 1e3
     if ws > 1:
@@ -257,7 +305,9 @@ def product_arm(args):
             "e2e": {"value": e2e, "unit": "Mfaces/s", "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
                     "d2h_bytes_per_step": int(d2h)},
             "clocks": clocks,
-            "peaks_used": {"hbm_gbs": peaks.get("hbm_gbs")},
+            "phases_ms": {k: round(v["ms"], 3) for k, v in phases.items()},
+            "roofline": roofline_edge_cost(phases, round_faces, peaks),
+            "round_faces": round_faces if args.dump_rounds else None,
         }
         print(json.dumps(line))
     if ws > 1:
@@ -274,6 +324,7 @@ def main():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2"])
     ap.add_argument("--sample-rounds", type=int, default=3)
+    ap.add_argument("--dump-rounds", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

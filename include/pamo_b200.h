@@ -102,6 +102,34 @@ int pamo_stage2_offset(pamo_ctx *ctx, float *h_out3);
 int pamo_stage2_last_round_stats(pamo_ctx *ctx, long long *h_out8);
 
 /*
+ * Whole-mesh self-intersection check with the reference's pair predicate
+ * (replaces selfx::self_intersect, simp_cuda/src/bvh/self_intersect.cuh:151-392,
+ * as a standalone check): d_out_flags[f] = 1 for every face of an intersecting
+ * pair.  Unlike the reference the pair list has no capacity cap.  Faces
+ * (-1,-1,-1) are ignored.  *out_n_pairs (optional) receives the number of
+ * candidate pairs tested.
+ */
+int pamo_self_intersect(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
+                        unsigned char *d_out_flags, long long *out_n_pairs, void *stream);
+
+/*
+ * Device timing of the stage-2 phases (no reference counterpart; diagnostics).
+ * pamo_profile_enable(ctx, 1) resets and starts accumulating CUDA-event times
+ * per phase; pamo_profile_read copies up to `cap` phase totals (ms) and call
+ * counts and returns the number of phases.  Phase order: setup, lbvh build,
+ * edge cost, collapse, cleanup, refit, query, pair tests, undo, compaction.
+ */
+int pamo_profile_enable(pamo_ctx *ctx, int enable);
+int pamo_profile_read(pamo_ctx *ctx, double *h_ms, long long *h_calls, int cap);
+
+/*
+ * Faces entering each round of the last pamo_stage2_run (no reference
+ * counterpart; PaMO.run prints nothing of the kind).  Writes up to `cap` entries
+ * and returns the number of rounds (negative status on bad arguments).
+ */
+int pamo_stage2_round_sizes(pamo_ctx *ctx, int *h_out, int cap);
+
+/*
  * Host-pointer simplifier.  Same signature and meaning as the reference's
  * Blender C ABI pamo_simplify (pamo_blender/cusimpinterface.cu:57): rounds until
  * four rounds without progress, output written to caller buffers sized like the

@@ -39,6 +39,8 @@ def lib():
         for name in ("s2o_undo_list", "s2o_edges", "s2o_collapsed", "s2o_first_near", "s2o_near"):
             getattr(L, name).restype = ctypes.POINTER(ctypes.c_int)
             getattr(L, name).argtypes = [ctypes.c_void_p]
+        L.s2o_isect0.restype = ctypes.POINTER(ctypes.c_uint8)
+        L.s2o_isect0.argtypes = [ctypes.c_void_p]
         L.s2o_edge_cost.restype = ctypes.POINTER(ctypes.c_uint32)
         L.s2o_edge_cost.argtypes = [ctypes.c_void_p]
         L.s2o_Q.restype = ctypes.POINTER(ctypes.c_float)
@@ -128,6 +130,10 @@ class Stage2Oracle:
         s = self.stats()
         n = s["n_total"]
         return np.ctypeslib.as_array(lib().s2o_collapsed(self._c), shape=(max(n, 1),))[:n].copy()
+
+    def isect0(self, n_tris):
+        """Per-face flags of the last round's first self-intersection pass."""
+        return np.ctypeslib.as_array(lib().s2o_isect0(self._c), shape=(max(n_tris, 1),))[:n_tris].copy()
 
     def quadrics(self, n_pts):
         return np.ctypeslib.as_array(lib().s2o_Q(self._c), shape=(n_pts * 10,)).reshape(n_pts, 10).copy()

@@ -82,16 +82,20 @@ static inline float tri_area(v3 p0, v3 p1, v3 p2)
 
 /* The skinny penalty term of compute_edge_cost_kernel (cusimp_free.cu:533,573),
  * with the reference's operator precedence: only the first square divides.
- * The device evaluates pow(float,2) in single precision; it equals the single
- * rounding of l*l, which is what is computed here. */
+ * Built with nvcc and libstdc++, pow(float, 2) there is std::pow's promoting
+ * overload, so the squares are doubles and everything after the fp32 numerator
+ * 4*sqrt(3)*area is evaluated in double, then rounded once by float(...).  The
+ * square of a float is exact in double. */
 static inline float skinny_term(v3 n0, v3 n1, v3 n2)
 {
     float l01 = vnorm(vsub(n0, n1));
     float l12 = vnorm(vsub(n1, n2));
     float l20 = vnorm(vsub(n2, n0));
     const float c4s3 = 4.0f * sqrtf(3.0f);
-    float e = c4s3 * tri_area(n0, n1, n2) / (l01 * l01) + (l12 * l12) + (l20 * l20) + 0.0000001f;
-    return 1.0f - fclamp_t(e, 0.0f, 1.0f);
+    float num = c4s3 * tri_area(n0, n1, n2);
+    double e = (double)num / ((double)l01 * (double)l01) + (double)l12 * (double)l12 + (double)l20 * (double)l20 +
+               (double)0.0000001f;
+    return 1.0f - fclamp_t((float)e, 0.0f, 1.0f);
 }
 
 /* is_skinny_triangle, cusimp_free.cu:617-637 */
@@ -299,6 +303,7 @@ typedef struct {
     uint64_t *tri_min;
     int *collapsed;
     unsigned char *isect;
+    unsigned char *isect0; /* flags of the round's first intersection pass */
     int *undo_edges;
     unsigned char *line_flag;
     /* round stats */
@@ -335,11 +340,12 @@ static int ctx_alloc(s2o_ctx *c, int cap_pts, int cap_tris)
     c->tri_min = zalloc(T * 8);
     c->collapsed = zalloc(E * 4);
     c->isect = zalloc(T);
+    c->isect0 = zalloc(T);
     c->undo_edges = zalloc(E * 4);
     c->line_flag = zalloc(E);
     return c->edge_cost && c->pts_map && c->undo_list && c->tmp_undo && c->invalid_table && c->pts &&
                    c->opts && c->tris && c->otris && c->occ && c->first_near && c->near && c->first_edge &&
-                   c->edges && c->Q && c->tri_min && c->collapsed && c->isect && c->undo_edges && c->line_flag
+                   c->edges && c->Q && c->tri_min && c->collapsed && c->isect && c->isect0 && c->undo_edges && c->line_flag
                ? S2O_OK
                : S2O_ERR_OOM;
 }
@@ -755,6 +761,7 @@ int s2o_forward(s2o_ctx *c, const float *pts, const int *tris, const int *undo_i
     memset(c->n_cand_pairs, 0, sizeof(c->n_cand_pairs));
     memset(c->undo_counts, 0, sizeof(c->undo_counts));
     c->n_cand_pairs[0] = self_intersect(c, eps);
+    memcpy(c->isect0, c->isect, (size_t)n_tris);
     int cnt = undo_candidates(c);
     c->undo_counts[0] = cnt;
     nvu += 2 * cnt;
@@ -793,6 +800,7 @@ int s2o_forward(s2o_ctx *c, const float *pts, const int *tris, const int *undo_i
 }
 
 const int *s2o_undo_list(const s2o_ctx *c) { return c->undo_list; }
+const unsigned char *s2o_isect0(const s2o_ctx *c) { return c->isect0; }
 int s2o_n_edges(const s2o_ctx *c) { return c->n_edges; }
 const int *s2o_edges(const s2o_ctx *c) { return c->edges; }
 const uint32_t *s2o_edge_cost(const s2o_ctx *c) { return c->edge_cost; }

@@ -20,7 +20,7 @@ import numpy as np
 from . import _lib
 from ._lib import Context, PamoError, check
 
-__all__ = ["PaMO", "CUDSP_Free", "Context", "PamoError", "stage2_run"]
+__all__ = ["PaMO", "CUDSP_Free", "Context", "PamoError", "stage2_run", "self_intersect"]
 __version__ = "0.1.0"
 
 
@@ -111,6 +111,22 @@ def stage2_run(ctx: Context, points, triangles, target_faces: int, tolerance=4, 
     f = torch.empty((om.value, 3), dtype=torch.int32, device=dev)
     check("pamo_stage2_fetch", _lib.lib().pamo_stage2_fetch(ctx.handle, v.data_ptr(), f.data_ptr(), 0, stream))
     return v, f, rounds.value
+
+
+def self_intersect(ctx: Context, points, triangles):
+    """Per-face flags (uint8 CUDA tensor) of the faces in intersecting pairs, with
+    the reference's pair predicate; also returns the number of candidate pairs."""
+    import ctypes
+
+    torch = _torch()
+    points = points.contiguous()
+    triangles = triangles.contiguous()
+    out = torch.zeros(int(triangles.shape[0]), dtype=torch.uint8, device=points.device)
+    npairs = ctypes.c_longlong(0)
+    check("pamo_self_intersect", _lib.lib().pamo_self_intersect(
+        ctx.handle, points.data_ptr(), triangles.data_ptr(), int(points.shape[0]), int(triangles.shape[0]),
+        out.data_ptr(), ctypes.byref(npairs), _stream_ptr(points.device)))
+    return out, npairs.value
 
 
 class PaMO:

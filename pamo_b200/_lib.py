@@ -36,6 +36,10 @@ SIGNATURES = {
     "pamo_stage2_fetch": (_i, [_vp, _vp, _vp, _i, _vp]),
     "pamo_stage2_offset": (_i, [_vp, _vp]),
     "pamo_stage2_last_round_stats": (_i, [_vp, _vp]),
+    "pamo_self_intersect": (_i, [_vp, _vp, _vp, _i, _i, _vp, ctypes.POINTER(_ll), _vp]),
+    "pamo_profile_enable": (_i, [_vp, _i]),
+    "pamo_profile_read": (_i, [_vp, _vp, _vp, _i]),
+    "pamo_stage2_round_sizes": (_i, [_vp, _vp, _i]),
     "pamo_simplify": (None, [_vp, _vp, _vp, _vp, _vp, _f]),
     "pamo_simplify_ctx": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f]),
 }
@@ -67,6 +71,10 @@ def lib():
 def check(fn: str, code: int):
     if code != PAMO_OK:
         raise PamoError(fn, code)
+
+
+PHASES = ["setup", "lbvh_build", "edge_cost", "collapse", "cleanup", "refit", "query", "pair_tests", "undo",
+          "compact"]
 
 
 class Context:

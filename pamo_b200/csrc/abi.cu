@@ -311,8 +311,10 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
 
     int n = n_pts, m = n_tris, count = 0, rounds = 0, n_undo = 0;
     bool stuck = false;
+    S.round_faces.clear();
     for (int it = 0; it < iters; ++it) {
         int prev = m;
+        S.round_faces.push_back(m);
         int nvu = 0;
         RET_IF(S.round(n, m, scale, threshold, stuck, n_undo ? ctx->undo_prev : nullptr, n_undo, &nvu, s));
         rounds++;
@@ -375,6 +377,51 @@ int pamo_stage2_last_round_stats(pamo_ctx *ctx, long long *h_out8)
     if (!ctx || !h_out8) return PAMO_ERR_INVALID_ARG;
     for (int k = 0; k < 8; ++k) h_out8[k] = ctx->s2.last_stats[k];
     return PAMO_OK;
+}
+
+int pamo_self_intersect(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
+                        unsigned char *d_out_flags, long long *out_n_pairs, void *stream)
+{
+    if (!ctx || n_pts <= 0 || n_tris < 0 || !d_points || (n_tris && (!d_tris || !d_out_flags))) return PAMO_ERR_INVALID_ARG;
+    RET_IF(set_device(ctx));
+    cudaStream_t s = (cudaStream_t)stream;
+    Stage2 &S = ctx->s2;
+    RET_IF(S.ensure(n_pts, n_tris));
+    RET_IF(S.validate(d_tris, n_pts, n_tris, nullptr, 0, 0, s));
+    k_aos3_to_f4<<<grid_for(n_pts), kThreads, 0, s>>>(d_points, S.opts, n_pts);
+    k_aos3_to_i4<<<grid_for(n_tris), kThreads, 0, s>>>(d_tris, S.otris, n_tris);
+    RET_IF(S.self_intersect_all(n_pts, n_tris, s));
+    if (n_tris) CU_RET(cudaMemcpyAsync(d_out_flags, S.isect, (size_t)n_tris, cudaMemcpyDeviceToDevice, s));
+    CU_RET(cudaStreamSynchronize(s));
+    if (out_n_pairs) *out_n_pairs = S.hcnt->n_pairs;
+    return PAMO_OK;
+}
+
+int pamo_profile_enable(pamo_ctx *ctx, int enable)
+{
+    if (!ctx) return PAMO_ERR_INVALID_ARG;
+    ctx->s2.prof.on = enable != 0;
+    ctx->s2.prof.reset();
+    return PAMO_OK;
+}
+
+int pamo_profile_read(pamo_ctx *ctx, double *h_ms, long long *h_calls, int cap)
+{
+    if (!ctx || cap < 0) return PAMO_ERR_INVALID_ARG;
+    int n = cap < PH_COUNT ? cap : PH_COUNT;
+    for (int i = 0; i < n; ++i) {
+        if (h_ms) h_ms[i] = ctx->s2.prof.ms[i];
+        if (h_calls) h_calls[i] = ctx->s2.prof.calls[i];
+    }
+    return PH_COUNT;
+}
+
+int pamo_stage2_round_sizes(pamo_ctx *ctx, int *h_out, int cap)
+{
+    if (!ctx || cap < 0 || (cap && !h_out)) return -PAMO_ERR_INVALID_ARG;
+    int n = (int)ctx->s2.round_faces.size();
+    for (int i = 0; i < n && i < cap; ++i) h_out[i] = ctx->s2.round_faces[i];
+    return n;
 }
 
 int pamo_simplify_ctx(pamo_ctx *ctx, const float *h_in_verts, const int *h_in_tris, float *h_out_verts,

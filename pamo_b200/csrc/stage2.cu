@@ -153,9 +153,13 @@ __device__ __forceinline__ float skinny_term(V3 n0, V3 n1, V3 n2)
     float l20 = vnorm(vsub(n2, n0));
     float s = (l01 + l12 + l20) / 2.0f;
     float area = sqrtf(s * (s - l01) * (s - l12) * (s - l20));
+    // pow(float, 2) in the reference resolves to std::pow's promoting overload:
+    // the squares and the sum after the fp32 numerator are doubles, rounded once
     const float c4s3 = 4.0f * sqrtf(3.0f);
-    float e = c4s3 * area / (l01 * l01) + (l12 * l12) + (l20 * l20) + 0.0000001f;
-    return 1.0f - tclamp(e, 0.0f, 1.0f);
+    float num = c4s3 * area;
+    double e = (double)num / pow((double)l01, 2.0) + pow((double)l12, 2.0) + pow((double)l20, 2.0) +
+               (double)0.0000001f;
+    return 1.0f - tclamp((float)e, 0.0f, 1.0f);
 }
 
 struct CostArgs {
@@ -652,6 +656,61 @@ __global__ void k_validate_range(const int *v, int count, int hi, int *bad)
 
 }  // namespace
 
+void Profiler::begin(int phase, cudaStream_t s)
+{
+    if (!on) return;
+    if (open_phase >= 0) end(s);
+    if (used + 2 > kPool || n_marks >= kPool / 2) return;  // pool full: drop (collect() frees it)
+    for (int k = 0; k < 2; ++k)
+        if (!ev[used + k]) cudaEventCreate(&ev[used + k]);
+    cudaEventRecord(ev[used], s);
+    marks[n_marks][0] = phase;
+    marks[n_marks][1] = used;
+    open_phase = phase;
+    used += 2;
+}
+
+void Profiler::end(cudaStream_t s)
+{
+    if (!on || open_phase < 0) return;
+    cudaEventRecord(ev[marks[n_marks][1] + 1], s);
+    n_marks++;
+    open_phase = -1;
+}
+
+void Profiler::collect()
+{
+    if (!on) return;
+    for (int i = 0; i < n_marks; ++i) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, ev[marks[i][1]], ev[marks[i][1] + 1]) == cudaSuccess) {
+            ms[marks[i][0]] += t;
+            calls[marks[i][0]]++;
+        }
+    }
+    n_marks = 0;
+    used = 0;
+}
+
+void Profiler::reset()
+{
+    for (int i = 0; i < PH_COUNT; ++i) {
+        ms[i] = 0;
+        calls[i] = 0;
+    }
+    n_marks = used = 0;
+    open_phase = -1;
+}
+
+void Profiler::release()
+{
+    for (int i = 0; i < kPool; ++i)
+        if (ev[i]) {
+            cudaEventDestroy(ev[i]);
+            ev[i] = nullptr;
+        }
+}
+
 int Stage2::validate(const int *d_tris, int n, int m, const int *d_undo, int n_undo, int undo_hi, cudaStream_t s)
 {
     int *bad = dev_misc + 32;
@@ -675,6 +734,7 @@ void Stage2::release()
         if (q) cudaFree(q);
     if (hcnt) cudaFreeHost(hcnt);
     if (h_scalars) cudaFreeHost(h_scalars);
+    prof.release();
     edge_cost = nullptr; pts_map = nullptr; undo_list = nullptr; tmp_undo = nullptr; invalid_table = nullptr;
     opts = pts = nullptr; otris = tris = nullptr; occ = nullptr;
     first_near = cursor = near_tris = first_edge = nullptr; edges = nullptr; plane = quad = nullptr;
@@ -784,15 +844,20 @@ static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s)
     cudaError_t e;
     if ((e = cudaMemsetAsync(S.isect, 0, (size_t)m, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&S.dcnt->n_pairs, 0, 2 * sizeof(int), s)) != cudaSuccess) return e;  // n_pairs, overflow
+    S.prof.begin(PH_REFIT, s);
     if ((e = lbvh_refit(S.bvh, S.pts, S.tris, m, s)) != cudaSuccess) return e;
+    S.prof.begin(PH_QUERY, s);
     k_query<<<grid_for(m), kThreads, 0, s>>>(S.bvh.nodes, S.bvh.vals, S.bvh.scene, S.pts, S.tris, S.active, m,
                                              S.pairs, S.cap_pairs, S.dcnt);
+    S.prof.begin(PH_PAIRS, s);
     k_pairs<<<grid_for(S.cap_pairs), kThreads, 0, s>>>(S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris, S.isect, 1e-3f);
+    S.prof.end(s);
     return cudaGetLastError();
 }
 
 static cudaError_t undo_check(Stage2 &S, cudaStream_t s)
 {
+    S.prof.begin(PH_UNDO, s);
     const long long NC = S.cap_edges;
     k_undo_flags<<<grid_for(NC), kThreads, 0, s>>>(S.collapsed, S.dcnt, S.edges, S.first_near, S.near_tris, S.isect,
                                                    S.uflag);
@@ -801,6 +866,7 @@ static cudaError_t undo_check(Stage2 &S, cudaStream_t s)
     if (e != cudaSuccess) return e;
     k_undo_scatter<<<grid_for(NC), kThreads, 0, s>>>(S.uflag, S.eflag, S.dcnt, S.collapsed, S.edges, S.undo_edges,
                                                      S.tmp_undo);
+    S.prof.end(s);
     return cudaGetLastError();
 }
 
@@ -828,6 +894,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     ct = (ct < kCostRange) ? ct : kCostRange;
     const uint32_t collapse_t = (uint32_t)(unsigned long long)(ct / kCostRange * 4294967296.0f);
 
+    prof.begin(PH_SETUP, s);
     k_round_init<<<grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s>>>(opts, otris, pts, tris, occ, first_near,
                                                                        cursor, vmin, n, m);
     k_face_a<<<grid_for(m), kThreads, 0, s>>>(pts, tris, m, first_near, first_edge, plane);
@@ -838,17 +905,21 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     k_face_b<<<grid_for(m), kThreads, 0, s>>>(tris, m, first_near, cursor, near_tris, first_edge, edges);
     k_vertex_quadric<<<grid_for(n), kThreads, 0, s>>>(first_near, near_tris, plane, quad, n);
     // the hierarchy only depends on the round input: build it now
+    prof.begin(PH_LBVH_BUILD, s);
     S2_TRY(lbvh_build(bvh, pts, tris, m, s));
 
     const long long EMAX = 3LL * m;
+    prof.begin(PH_EDGE_COST, s);
     CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, quad, invalid_table, edge_cost, vmin,
                 tres, edge_s, is_stuck ? 1 : 0};
     k_edge_cost<<<grid_for(EMAX), kThreads, 0, s>>>(ca);
     CollapseArgs cl{edges, d_n_edges, edge_cost, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
                     collapse_t};
+    prof.begin(PH_COLLAPSE, s);
     k_collapse<<<grid_for(EMAX), kThreads, 0, s>>>(cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
     k_scatter_flagged<<<grid_for(EMAX), kThreads, 0, s>>>(eflag, uflag, d_n_edges, collapsed, 0);
+    prof.begin(PH_CLEANUP, s);
     k_remove_invalid_faces<<<grid_for(m), kThreads, 0, s>>>(tris, m);
     k_line_flags<<<grid_for(EMAX), kThreads, 0, s>>>(edges, d_n_edges, pts, eflag, &dcnt->n_line);
     k_line_apply<<<1, 32, 0, s>>>(edges, d_n_edges, eflag, first_near, near_tris, pts, tris, occ, collapsed, dcnt);
@@ -859,6 +930,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     S2_TRY(undo_check(*this, s));
     S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
     S2_TRY(cudaStreamSynchronize(s));
+    prof.collect();
     if (hcnt->pair_overflow > 0) {
         // candidate buffer too small: grow and redo the pass
         long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
@@ -882,6 +954,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     int it = 0;
     while (cnt_undo != 0) {
         it++;
+        prof.begin(PH_UNDO, s);
         k_undo_apply<<<grid_for(cnt_undo), kThreads, 0, s>>>(undo_edges, dcnt, edges, first_near, near_tris, opts,
                                                               otris, pts, tris, occ);
         if (nvu - first > 0)
@@ -891,6 +964,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
         S2_TRY(undo_check(*this, s));
         S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
         S2_TRY(cudaStreamSynchronize(s));
+        prof.collect();
         if (hcnt->pair_overflow > 0) {
             long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
             int rc = ensure_pairs(need);
@@ -910,19 +984,48 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     last_stats[3] = it;
     last_stats[4] = nvu;
     // pts_map = exclusive scan of occ[0..n]
+    prof.begin(PH_COMPACT, s);
     S2_TRY(exclusive_scan(occ, pts_map, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
+    prof.end(s);
     *n_undo_out = nvu;
+    return PAMO_OK;
+}
+
+int Stage2::self_intersect_all(int n, int m, cudaStream_t s)
+{
+    // faces of opts/otris; every live face queries the hierarchy
+    k_round_init<<<grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s>>>(opts, otris, pts, tris, occ, first_near,
+                                                                       cursor, vmin, n, m);
+    S2_TRY(cudaMemsetAsync(dcnt, 0, sizeof(RoundCounters), s));
+    S2_TRY(cudaMemsetAsync(active, 1, (size_t)m, s));
+    S2_TRY(lbvh_build(bvh, pts, tris, m, s));
+    S2_TRY(isect_pass(*this, m, s));
+    S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+    S2_TRY(cudaStreamSynchronize(s));
+    if (hcnt->pair_overflow > 0) {
+        long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
+        int rc = ensure_pairs(need);
+        if (rc) return rc;
+        S2_TRY(isect_pass(*this, m, s));
+        S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+        S2_TRY(cudaStreamSynchronize(s));
+        if (hcnt->pair_overflow > 0) return PAMO_ERR_CAPACITY;
+    }
+    if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
     return PAMO_OK;
 }
 
 int Stage2::compact(int n, int m, cudaStream_t s)
 {
+    prof.begin(PH_COMPACT, s);
     k_face_live_flags<<<grid_for(m), kThreads, 0, s>>>(tris, m, fflag);
     S2_TRY(exclusive_scan(fflag, uflag, m, nullptr, scan_scratch, nullptr, s));
     k_compact<<<grid_for(n > m ? n : m), kThreads, 0, s>>>(pts, occ, pts_map, n, tris, fflag, uflag, m, opts, otris,
                                                            dcnt);
+    prof.end(s);
     S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
     S2_TRY(cudaStreamSynchronize(s));
+    prof.collect();
     return PAMO_OK;
 }
 

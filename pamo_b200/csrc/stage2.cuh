@@ -1,6 +1,8 @@
 // Stage-2 simplification state and round driver (host side).
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 #include "lbvh.cuh"
 
@@ -22,8 +24,44 @@ struct RoundCounters {
     int pad[5];
 };
 
+// Optional per-phase device timing (CUDA events on the round's stream, read at
+// the round's synchronisation points).
+enum Phase {
+    PH_SETUP = 0,   // round init, face pass A, CSR/edge scans, face pass B, quadrics
+    PH_LBVH_BUILD,  // Morton codes, radix sort, hierarchy
+    PH_EDGE_COST,   // k_edge_cost
+    PH_COLLAPSE,    // k_collapse + collapsed-list compaction
+    PH_CLEANUP,     // degenerate faces, coincident-endpoint collapses
+    PH_REFIT,       // leaf boxes + bottom-up refit
+    PH_QUERY,       // hierarchy traversal -> candidate pairs
+    PH_PAIRS,       // triangle-pair tests
+    PH_UNDO,        // undo candidates, restore, list rearrangement
+    PH_COMPACT,     // pts_map scan + compaction for the next round
+    PH_COUNT
+};
+
+struct Profiler {
+    bool on = false;
+    double ms[PH_COUNT] = {0};
+    long long calls[PH_COUNT] = {0};
+    static constexpr int kPool = 256;
+    cudaEvent_t ev[kPool] = {};
+    int used = 0;
+    int marks[kPool / 2][2] = {};  // (phase, first event index)
+    int n_marks = 0;
+    int open_phase = -1;
+
+    void begin(int phase, cudaStream_t s);
+    void end(cudaStream_t s);
+    void collect();  // after the stream was synchronised
+    void reset();
+    void release();
+};
+
 struct Stage2 {
     int device = 0;
+    Profiler prof;
+    std::vector<int> round_faces;  // faces entering each round of the last loop
     long long cap_pts = 0, cap_tris = 0, cap_edges = 0, cap_undo = 0, cap_pairs = 0;
 
     // persistent between rounds (the reference reads these stale)
@@ -76,6 +114,10 @@ struct Stage2 {
     // by the caller).  d_undo_in: device list of n_undo_in entries.
     int round(int n, int m, float scale, float threshold, bool is_stuck, const int *d_undo_in, int n_undo_in,
               int *n_undo_out, cudaStream_t s);
+
+    // Whole-mesh self-intersection of opts/otris: isect[f] = 1 for every face of
+    // a pair the reference's selfx::self_intersect reports (all pairs, no cap).
+    int self_intersect_all(int n, int m, cudaStream_t s);
 
     // compaction of the round's output into opts/otris for the next round;
     // returns new sizes through hcnt (after a sync).

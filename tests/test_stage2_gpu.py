@@ -191,3 +191,33 @@ def test_pamo_simplify_c_abi(torch_cuda):
     assert (n, m) == (len(ov), len(of))
     assert np.array_equal(bits(outv[:n]), bits(ov))
     assert np.array_equal(outf[:m], of)
+
+
+def test_self_intersect_matches_reference_fixtures(torch_cuda):
+    """LBVH + pair test on whole meshes against the reference's own
+    selfx::self_intersect flags (tests/golden/isect.npz)."""
+    import os
+
+    import pamo_b200
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "isect.npz"))
+    ctx = pamo_b200.Context(0)
+    for name in ("two_spheres", "crumpled", "folded_grids", "soup"):
+        V, F, want = g[f"{name}_V"], g[f"{name}_F"], g[f"{name}_flags"]
+        got, npairs = pamo_b200.self_intersect(ctx, torch_cuda.from_numpy(V).cuda(), torch_cuda.from_numpy(F).cuda())
+        got = got.cpu().numpy()
+        assert npairs > 0
+        if name == "soup":  # beyond the reference's pair capacity: a superset of its flags
+            assert np.all(got[want == 1] == 1) and got.sum() > want.sum()
+        else:
+            assert np.array_equal(got, want), name
+
+
+def test_self_intersect_clean_meshes_report_nothing(torch_cuda):
+    import pamo_b200
+    from pamo_b200 import meshgen as mg
+
+    ctx = pamo_b200.Context(0)
+    for V, F in (mg.displaced_icosphere(5, 0), mg.noisy_torus(128, 128, 1), mg.thin_shell_pair(20000, 2e-3, 1)):
+        got, _ = pamo_b200.self_intersect(ctx, torch_cuda.from_numpy(V).cuda(), torch_cuda.from_numpy(F).cuda())
+        assert int(got.sum()) == 0
