@@ -249,6 +249,10 @@ def product_arm(args):
         dist.barrier()
     clk = ClockSampler(local)
     clk.start()
+    for _ in range(100):  # NVML initialisation stalls the device briefly: let it finish first
+        if clk.samples or clk.error:
+            break
+        time.sleep(0.05)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()

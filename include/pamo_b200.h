@@ -130,6 +130,59 @@ int pamo_profile_read(pamo_ctx *ctx, double *h_ms, long long *h_calls, int cap);
 int pamo_stage2_round_sizes(pamo_ctx *ctx, int *h_out, int cap);
 
 /*
+ * Stage-3 safe projection settings; field for field the defaults of the
+ * reference's Stage3Config (simp_cuda/safe_project/src/pamo_safe_project/
+ * config.py:6-73) that the default energy set uses.  pamo_s3_default_config
+ * fills them.
+ */
+typedef struct pamo_s3_config {
+    int n_newton_iters;      /* 10 */
+    int n_cg_iters;          /* 40 */
+    int n_line_search_iters; /* 10 */
+    int ccd_max_iters;       /* 100 */
+    int spd_max_iters;       /* 3 */
+    float d_hat;             /* 1e-3 */
+    float coll_stiffness;    /* 1e2 */
+    float contact_detection_radius; /* 1e-2 */
+    float ee_classify_thres; /* 1e-3 */
+    float ccd_slackness;     /* 0.7 */
+    float ccd_thickness;     /* 1e-6 */
+    float elas_young_modulus;  /* 1e-1 */
+    float elas_poisson_ratio;  /* 0.0 */
+    float hinge_stiffness;     /* 1e-2 */
+    float mesh2gt_dist_stiffness; /* 1e3 */
+    long long max_blocks;      /* 2^25: contact blocks before the radius is halved */
+} pamo_s3_config;
+
+void pamo_s3_default_config(pamo_s3_config *cfg);
+
+/*
+ * Stage-3 safe projection of a simplified mesh towards its ground truth.
+ * Replaces Stage3System.register_mesh + n_steps x Stage3System.step
+ * (simp_cuda/safe_project/src/pamo_safe_project/system.py:167-272,411-470) as
+ * pamo_safe_project.process calls them (processing.py:62-99), after the
+ * caller's normalisation.  All arrays are device arrays in the normalised frame:
+ *   d_gt_v [n_gt_v*3] f32, d_gt_f [n_gt_f*3] i32  ground truth
+ *   d_v [n_v*3] f32, d_f [n_f*3] i32              mesh to project
+ *   d_e [n_e*2] i32                               its unique edges
+ *   d_h [n_h*4] i32                               its hinges (x0 | x1 x2 edge | x3)
+ *   d_vor [n_v] f32                               Voronoi vertex areas
+ * do_nothing != 0 skips the steps (the reference's small-angle guard).
+ * The projected vertices are written to d_out_v [n_v*3].
+ */
+int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int n_gt_v, int n_gt_f,
+                      const float *d_v, const int *d_f, int n_v, int n_f, const int *d_e, int n_e, const int *d_h,
+                      int n_h, const float *d_vor, int n_steps, int do_nothing, const pamo_s3_config *cfg,
+                      void *stream, float *d_out_v);
+
+/*
+ * Diagnostics of the last pamo_safe_project call (no reference counterpart):
+ * h_out[0] total energy at the end, [1] contact blocks of the last detection,
+ * [2] Newton iterations run.
+ */
+int pamo_safe_project_stats(pamo_ctx *ctx, double *h_out3);
+
+/*
  * Host-pointer simplifier.  Same signature and meaning as the reference's
  * Blender C ABI pamo_simplify (pamo_blender/cusimpinterface.cu:57): rounds until
  * four rounds without progress, output written to caller buffers sized like the

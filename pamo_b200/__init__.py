@@ -181,10 +181,13 @@ class PaMO:
         if self.verbose:
             print(f"Time for Simplification: {self.timings['stage2']} sec")
         if self.use_stage3:
-            from .safe_project import process
+            from .safe_project import merge_vertices, process
 
             t0 = time.time()
-            verts, faces = process(self.gt_mesh[0], self.gt_mesh[1], verts, faces, 5, system=self.system,
+            # the reference wraps the stage-2 result in trimesh.Trimesh(process=True),
+            # which merges coincident vertices (pamo/__init__.py:193-203)
+            v2, f2 = merge_vertices(verts.astype(np.float64), faces)
+            verts, faces = process(self.gt_mesh[0], self.gt_mesh[1], v2, f2, 5, system=self.system,
                                    config=self.config)
             self.timings["stage3"] = time.time() - t0
         return verts, faces

@@ -40,6 +40,10 @@ SIGNATURES = {
     "pamo_profile_enable": (_i, [_vp, _i]),
     "pamo_profile_read": (_i, [_vp, _vp, _vp, _i]),
     "pamo_stage2_round_sizes": (_i, [_vp, _vp, _i]),
+    "pamo_s3_default_config": (None, [_vp]),
+    "pamo_safe_project": (_i, [_vp, _vp, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _i, _vp, _i, _vp, _i, _i, _vp, _vp,
+                               _vp]),
+    "pamo_safe_project_stats": (_i, [_vp, _vp]),
     "pamo_simplify": (None, [_vp, _vp, _vp, _vp, _vp, _f]),
     "pamo_simplify_ctx": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f]),
 }

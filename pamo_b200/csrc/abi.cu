@@ -7,10 +7,18 @@
 
 #include "scan.cuh"
 #include "stage2.cuh"
+#include "stage3.cuh"
+
+namespace pamo {
+int s3_validate(const int *a, long long count, int hi, int *d_bad, int *h_bad, cudaStream_t st);
+int s3_fetch(const float4 *q, float *out, int n, cudaStream_t st);
+}  // namespace pamo
 
 struct pamo_ctx {
     int device = 0;
     pamo::Stage2 s2;
+    pamo::s3::Stage3 s3;
+    double s3_stats[3] = {0, 0, 0};
     int *undo_prev = nullptr;  // copy of the previous round's undo list (PaMO.run passes a clone)
     long long undo_prev_cap = 0;
     float *stage = nullptr;  // [n*3] staging for host transfers
@@ -74,21 +82,59 @@ __global__ void k_face_means(const float *pts, const int *tris, int m, float *mx
 
 // numpy's .mean(axis=0) of a C-contiguous (F,3) float32 array adds the rows one
 // after another into a float32 accumulator (no pairwise split on this axis), then
-// divides by F.  That chain is inherently sequential: one thread per coordinate.
-__global__ void k_sequential_mean(const float *mx, const float *my, const float *mz, int m, float *out)
+// divides by F.  That chain is inherently sequential.  One block: warps 1..31
+// stream the next chunk into shared memory while thread 0 runs the three
+// coordinate chains (interleaved, so the FADD latency is the bound) on the
+// current chunk.
+constexpr int kMeanChunk = 4096;
+
+__global__ void __launch_bounds__(1024) k_sequential_mean(const float *mx, const float *my, const float *mz, int m,
+                                                          float *out)
 {
-    int c = threadIdx.x;
-    if (c >= 3 || m <= 0) return;
-    const float *src = c == 0 ? mx : (c == 1 ? my : mz);
-    float s = src[0];
-    int f = 1;
-    for (; f + 8 <= m; f += 8) {
-        float v0 = src[f], v1 = src[f + 1], v2 = src[f + 2], v3 = src[f + 3];
-        float v4 = src[f + 4], v5 = src[f + 5], v6 = src[f + 6], v7 = src[f + 7];
-        s += v0; s += v1; s += v2; s += v3; s += v4; s += v5; s += v6; s += v7;
+    extern __shared__ float sm[];  // 2 buffers x 3 coordinates x kMeanChunk
+    if (m <= 0) return;
+    const int n_chunks = (m + kMeanChunk - 1) / kMeanChunk;
+    auto load = [&](int c, int buf) {
+        float *dst = sm + buf * 3 * kMeanChunk;
+        int base = c * kMeanChunk;
+        int cnt = min(kMeanChunk, m - base);
+        for (int i = threadIdx.x - 32; i < cnt; i += blockDim.x - 32) {
+            dst[i] = mx[base + i];
+            dst[kMeanChunk + i] = my[base + i];
+            dst[2 * kMeanChunk + i] = mz[base + i];
+        }
+    };
+    if (threadIdx.x >= 32) load(0, 0);
+    __syncthreads();
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    for (int c = 0; c < n_chunks; ++c) {
+        const int buf = c & 1;
+        if (threadIdx.x >= 32) {
+            if (c + 1 < n_chunks) load(c + 1, buf ^ 1);
+        } else if (threadIdx.x == 0) {
+            const float *b = sm + buf * 3 * kMeanChunk;
+            int cnt = min(kMeanChunk, m - c * kMeanChunk);
+            int i = 0;
+            if (c == 0) {  // the accumulator starts from the first row
+                sx = b[0];
+                sy = b[kMeanChunk];
+                sz = b[2 * kMeanChunk];
+                i = 1;
+            }
+#pragma unroll 8
+            for (; i < cnt; ++i) {
+                sx += b[i];
+                sy += b[kMeanChunk + i];
+                sz += b[2 * kMeanChunk + i];
+            }
+        }
+        __syncthreads();
     }
-    for (; f < m; ++f) s += src[f];
-    out[c] = s / (float)m;
+    if (threadIdx.x == 0) {
+        out[0] = sx / (float)m;
+        out[1] = sy / (float)m;
+        out[2] = sz / (float)m;
+    }
 }
 
 __global__ void k_centre(const float *pts, int n, const float *mean, float4 *out, int *bounds)
@@ -228,6 +274,7 @@ int pamo_ctx_destroy(pamo_ctx *ctx)
     if (set_device(ctx) == PAMO_OK) {
         cudaDeviceSynchronize();
         ctx->s2.release();
+        ctx->s3.release();
         if (ctx->undo_prev) cudaFree(ctx->undo_prev);
         if (ctx->stage) cudaFree(ctx->stage);
         if (ctx->istage) cudaFree(ctx->istage);
@@ -294,7 +341,11 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
     float *bounds_f = reinterpret_cast<float *>(S.dev_misc + 16);
     k_face_means<<<grid_for(n_tris), kThreads, 0, s>>>(d_points, d_tris, n_tris, mxyz, mxyz + n_tris,
                                                        mxyz + 2LL * n_tris);
-    k_sequential_mean<<<1, 32, 0, s>>>(mxyz, mxyz + n_tris, mxyz + 2LL * n_tris, n_tris, mean_dev);
+    {
+        const int smem = 2 * 3 * kMeanChunk * (int)sizeof(float);
+        CU_RET(cudaFuncSetAttribute(k_sequential_mean, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_sequential_mean<<<1, 1024, smem, s>>>(mxyz, mxyz + n_tris, mxyz + 2LL * n_tris, n_tris, mean_dev);
+    }
     k_bounds_init<<<1, 32, 0, s>>>(bounds);
     k_centre<<<grid_for(n_pts), kThreads, 0, s>>>(d_points, n_pts, mean_dev, S.opts, bounds);
     k_bounds_to_float<<<1, 32, 0, s>>>(bounds, bounds_f);
@@ -422,6 +473,74 @@ int pamo_stage2_round_sizes(pamo_ctx *ctx, int *h_out, int cap)
     int n = (int)ctx->s2.round_faces.size();
     for (int i = 0; i < n && i < cap; ++i) h_out[i] = ctx->s2.round_faces[i];
     return n;
+}
+
+void pamo_s3_default_config(pamo_s3_config *c)
+{
+    if (!c) return;
+    c->n_newton_iters = 10;
+    c->n_cg_iters = 40;
+    c->n_line_search_iters = 10;
+    c->ccd_max_iters = 100;
+    c->spd_max_iters = 3;
+    c->d_hat = 1e-3f;
+    c->coll_stiffness = 1e2f;
+    c->contact_detection_radius = 1e-2f;
+    c->ee_classify_thres = 1e-3f;
+    c->ccd_slackness = 0.7f;
+    c->ccd_thickness = 1e-6f;
+    c->elas_young_modulus = 1e-1f;
+    c->elas_poisson_ratio = 0.0f;
+    c->hinge_stiffness = 1e-2f;
+    c->mesh2gt_dist_stiffness = 1e3f;
+    c->max_blocks = 1LL << 25;
+}
+
+int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int n_gt_v, int n_gt_f,
+                      const float *d_v, const int *d_f, int n_v, int n_f, const int *d_e, int n_e, const int *d_h,
+                      int n_h, const float *d_vor, int n_steps, int do_nothing, const pamo_s3_config *cfg,
+                      void *stream, float *d_out_v)
+{
+    if (!ctx || n_gt_v <= 0 || n_gt_f <= 0 || n_v <= 0 || n_f <= 0 || n_e < 0 || n_h < 0 || n_steps < 0 || !d_gt_v ||
+        !d_gt_f || !d_v || !d_f || (n_e && !d_e) || (n_h && !d_h) || !d_vor || !d_out_v)
+        return PAMO_ERR_INVALID_ARG;
+    RET_IF(set_device(ctx));
+    cudaStream_t s = (cudaStream_t)stream;
+    pamo::s3::Stage3 &S = ctx->s3;
+    if (cfg) S.cfg = *cfg;
+    else pamo_s3_default_config(&S.cfg);
+    if (S.cfg.n_newton_iters < 0 || S.cfg.n_cg_iters < 0 || S.cfg.n_line_search_iters < 0 || S.cfg.ccd_max_iters < 0 ||
+        S.cfg.spd_max_iters < 0 || !(S.cfg.d_hat > 0.f) || S.cfg.max_blocks <= 0)
+        return PAMO_ERR_INVALID_ARG;
+    RET_IF(S.ensure(n_v, n_f, n_e, n_h, n_gt_v, n_gt_f));
+    int *bad = S.iscal + 8;
+    RET_IF(s3_validate(d_f, 3LL * n_f, n_v, bad, S.h_iscal, s));
+    RET_IF(s3_validate(d_e, 2LL * n_e, n_v, bad, S.h_iscal, s));
+    RET_IF(s3_validate(d_h, 4LL * n_h, n_v, bad, S.h_iscal, s));
+    RET_IF(s3_validate(d_gt_f, 3LL * n_gt_f, n_gt_v, bad, S.h_iscal, s));
+    S.do_nothing = do_nothing != 0;
+    RET_IF(S.register_mesh(d_gt_v, d_gt_f, n_gt_v, n_gt_f, d_v, d_f, n_v, n_f, d_e, n_e, d_h, n_h, d_vor, s));
+    int newton = 0;
+    for (int k = 0; k < n_steps; ++k) {
+        RET_IF(S.step(s));
+        if (!S.do_nothing) newton += S.cfg.n_newton_iters;
+    }
+    RET_IF(s3_fetch(S.q, d_out_v, n_v, s));
+    double e = 0;
+    RET_IF(S.energy_now(&e, s));
+    CU_RET(cudaMemcpyAsync(S.h_iscal, S.iscal, 4, cudaMemcpyDeviceToHost, s));
+    CU_RET(cudaStreamSynchronize(s));
+    ctx->s3_stats[0] = e;
+    ctx->s3_stats[1] = S.h_iscal[0];
+    ctx->s3_stats[2] = newton;
+    return PAMO_OK;
+}
+
+int pamo_safe_project_stats(pamo_ctx *ctx, double *h_out3)
+{
+    if (!ctx || !h_out3) return PAMO_ERR_INVALID_ARG;
+    for (int k = 0; k < 3; ++k) h_out3[k] = ctx->s3_stats[k];
+    return PAMO_OK;
 }
 
 int pamo_simplify_ctx(pamo_ctx *ctx, const float *h_in_verts, const int *h_in_tris, float *h_out_verts,

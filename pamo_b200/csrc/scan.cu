@@ -69,12 +69,44 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_down(const int *in, int *
     }
 }
 
+// Small inputs: one block, 16 consecutive items per thread.
+constexpr int kSingleThreads = 1024;
+constexpr int kSingleItems = 16;
+
+__global__ void __launch_bounds__(kSingleThreads) k_scan_single(const int *in, int *out, long long n_max,
+                                                                const int *d_n, int *d_total)
+{
+    const long long n = d_n ? (long long)*d_n : n_max;
+    const long long base = (long long)threadIdx.x * kSingleItems;
+    int v[kSingleItems];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kSingleItems; ++k) {
+        long long i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        sum += v[k];
+    }
+    int tot;
+    int ex = block_excl_scan<kSingleThreads>(sum, tot);
+#pragma unroll
+    for (int k = 0; k < kSingleItems; ++k) {
+        long long i = base + k;
+        if (i < n) out[i] = ex;
+        ex += v[k];
+    }
+    if (threadIdx.x == 0 && d_total) *d_total = tot;
+}
+
 cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *d_n, int *scratch, int *d_total,
                            cudaStream_t s)
 {
     if (n_max <= 0) {
         if (d_total) return cudaMemsetAsync(d_total, 0, sizeof(int), s);
         return cudaSuccess;
+    }
+    if (n_max <= (long long)kSingleThreads * kSingleItems) {
+        k_scan_single<<<1, kSingleThreads, 0, s>>>(in, out, n_max, d_n, d_total);
+        return cudaGetLastError();
     }
     long long tiles = (n_max + kScanTile - 1) / kScanTile;
     k_scan_reduce<<<(unsigned)tiles, kScanThreads, 0, s>>>(in, n_max, d_n, scratch);

@@ -24,6 +24,7 @@
 // the minimum over every face touching either endpoint (the reference's per-face
 // minimum), which equals: key == vmin[u] == vmin[v] and no vertex of those faces
 // has a smaller vmin.
+#include <cooperative_groups.h>
 #include <cstdio>
 #include <cstring>
 
@@ -38,6 +39,8 @@ namespace pamo {
         cudaError_t _e = (expr);                          \
         if (_e != cudaSuccess) return map_cuda_error(_e); \
     } while (0)
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -70,7 +73,7 @@ __global__ void k_round_init(const float4 *__restrict__ opts, const int4 *__rest
 }
 
 __global__ void k_face_a(const float4 *__restrict__ pts, const int4 *__restrict__ tris, int m, int *deg,
-                         int *ecount, float4 *plane)
+                         int *ecount, float4 *plane, float4 *elen)
 {
     PAMO_GRID_STRIDE(f, m)
     {
@@ -88,6 +91,9 @@ __global__ void k_face_a(const float4 *__restrict__ pts, const int4 *__restrict_
         nrm = vdivs(nrm, vnorm(nrm));
         float d = -vdot(nrm, v0);
         plane[f] = make_float4(nrm.x, nrm.y, nrm.z, d);
+        // the three edge lengths in cyclic order, as the cost kernel sums them
+        // (cusimp_free.cu:448-485): |P[i]-P[j]|, |P[j]-P[k]|, |P[k]-P[i]|
+        elen[f] = make_float4(vnorm(vsub(v0, v1)), vnorm(vsub(v1, v2)), vnorm(vsub(v2, v0)), 0.f);
     }
 }
 
@@ -109,8 +115,11 @@ __global__ void k_face_b(const int4 *__restrict__ tris, int m, const int *__rest
 }
 
 // Canonical segment order, then the quadric sum p p^T in that order.
+__device__ __forceinline__ int next_after(int4 t, int v);
+
 __global__ void k_vertex_quadric(const int *__restrict__ first_near, int *near_tris,
-                                 const float4 *__restrict__ plane, float4 *quad, int n)
+                                 const float4 *__restrict__ plane, const int4 *__restrict__ tris, float4 *quad,
+                                 int *nxt, int n)
 {
     PAMO_GRID_STRIDE(v, n)
     {
@@ -125,7 +134,9 @@ __global__ void k_vertex_quadric(const int *__restrict__ first_near, int *near_t
         }
         float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f, q6 = 0.f, q7 = 0.f, q8 = 0.f, q9 = 0.f;
         for (int s = a; s < b; ++s) {
-            float4 p = plane[near_tris[s]];
+            const int f = near_tris[s];
+            nxt[s] = next_after(tris[f], (int)v);  // vertex after v in face f (i->j->k->i)
+            float4 p = plane[f];
             q0 += p.x * p.x; q1 += p.x * p.y; q2 += p.x * p.z; q3 += p.x * p.w;
             q4 += p.y * p.y; q5 += p.y * p.z; q6 += p.y * p.w;
             q7 += p.z * p.z; q8 += p.z * p.w; q9 += p.w * p.w;
@@ -169,6 +180,9 @@ struct CostArgs {
     const int4 *tris;
     const int *first_near;
     const int *near_tris;
+    const int *nxt;
+    const float4 *plane;
+    const float4 *elen;
     const float4 *quad;
     const uint8_t *invalid;
     uint32_t *edge_cost;
@@ -189,9 +203,9 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, uint32_t &out)
     const int va = A.first_near[v], vb = A.first_near[v + 1];
     int dup = 0;
     for (int a = ua; a < ub; ++a) {
-        int iu = next_after(A.tris[A.near_tris[a]], u);
+        int iu = A.nxt[a];
         for (int b = va; b < vb; ++b) {
-            int iv = next_after(A.tris[A.near_tris[b]], v);
+            int iv = A.nxt[b];
             if (iu == iv) dup++;
             if (dup > 2) {
                 out = 0xFFFFFFFFu;
@@ -206,10 +220,12 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, uint32_t &out)
     for (int pass = 0; pass < 2; ++pass) {
         int lo = pass ? va : ua, hi = pass ? vb : ub;
         for (int a = lo; a < hi; ++a) {
-            int4 t = A.tris[A.near_tris[a]];
-            if (t.x > t.y) { elen += vnorm(vsub(v3(A.pts[t.x]), v3(A.pts[t.y]))); nedge++; }
-            if (t.y > t.z) { elen += vnorm(vsub(v3(A.pts[t.y]), v3(A.pts[t.z]))); nedge++; }
-            if (t.z > t.x) { elen += vnorm(vsub(v3(A.pts[t.z]), v3(A.pts[t.x]))); nedge++; }
+            const int f = A.near_tris[a];
+            int4 t = A.tris[f];
+            float4 l = A.elen[f];
+            if (t.x > t.y) { elen += l.x; nedge++; }
+            if (t.y > t.z) { elen += l.y; nedge++; }
+            if (t.z > t.x) { elen += l.z; nedge++; }
         }
     }
     V3 v0 = v3(A.pts[u]), v1 = v3(A.pts[v]);
@@ -223,14 +239,15 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, uint32_t &out)
         int w = pass ? v : u, other = pass ? u : v;
         int lo = pass ? va : ua, hi = pass ? vb : ub;
         for (int a = lo; a < hi; ++a) {
-            int4 t = A.tris[A.near_tris[a]];
+            const int f = A.near_tris[a];
+            int4 t = A.tris[f];
             if (face_has(t, other)) continue;
             V3 o0 = v3(A.pts[t.x]), o1 = v3(A.pts[t.y]), o2 = v3(A.pts[t.z]);
             V3 n0 = t.x == w ? mid : o0;
             V3 n1 = t.y == w ? mid : o1;
             V3 n2 = t.z == w ? mid : o2;
-            V3 on = vcross(vsub(o1, o0), vsub(o2, o0));
-            on = vdivs(on, vnorm(on));
+            // the unchanged face's unit normal is the face plane's (same expression)
+            V3 on = v3(A.plane[f]);
             V3 nn = vcross(vsub(n1, n0), vsub(n2, n0));
             nn = vdivs(nn, vnorm(nn));
             if (vdot(on, nn) < 0) {
@@ -258,18 +275,25 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, uint32_t &out)
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads) k_edge_cost(CostArgs A)
+// Threads walk the faces in the hierarchy's leaf (Morton) order and handle each
+// face's edges, so neighbouring lanes gather neighbouring vertices; the results
+// are indexed by edge, so the order of work does not change them.
+__global__ void __launch_bounds__(kThreads) k_edge_cost(CostArgs A, const int *order, const int *scene,
+                                                        const int *first_edge)
 {
-    const int E = *A.n_edges;
-    PAMO_GRID_STRIDE(e, E)
+    const int L = scene[7];
+    PAMO_GRID_STRIDE(pp, L)
     {
-        int2 ed = A.edges[e];
-        uint32_t c;
-        if (edge_cost_value(A, ed.x, ed.y, c)) A.edge_cost[e] = c;
-        else c = A.edge_cost[e];  // the reference keeps the previous round's value
-        unsigned long long key = ((unsigned long long)c << 32) | (unsigned)e;
-        atomicMin(&A.vmin[ed.x], key);
-        atomicMin(&A.vmin[ed.y], key);
+        const int f = order[pp];
+        for (int e = first_edge[f]; e < first_edge[f + 1]; ++e) {
+            int2 ed = A.edges[e];
+            uint32_t c;
+            if (edge_cost_value(A, ed.x, ed.y, c)) A.edge_cost[e] = c;
+            else c = A.edge_cost[e];  // the reference keeps the previous round's value
+            unsigned long long key = ((unsigned long long)c << 32) | (unsigned)e;
+            atomicMin(&A.vmin[ed.x], key);
+            atomicMin(&A.vmin[ed.y], key);
+        }
     }
 }
 
@@ -309,11 +333,14 @@ __device__ __forceinline__ bool faces_min_ok(const CollapseArgs &A, int lo, int 
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
+__global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A, const int *order, const int *scene,
+                                                       const int *first_edge)
 {
-    const int E = *A.n_edges;
-    PAMO_GRID_STRIDE(e, E)
+    const int L = scene[7];
+    PAMO_GRID_STRIDE(pp, L)
     {
+      const int f = order[pp];
+      for (int e = first_edge[f]; e < first_edge[f + 1]; ++e) {
         int win = 0;
         uint32_t c = A.edge_cost[e];
         if (c <= A.collapse_t) {
@@ -365,6 +392,7 @@ __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
             }
         }
         A.eflag[e] = win;
+      }
     }
 }
 
@@ -478,9 +506,10 @@ __global__ void __launch_bounds__(kThreads) k_query(const BvhNode *__restrict__ 
 {
     const int L = scene[7];
     int stack[kStack];
-    PAMO_GRID_STRIDE(ff, m)
+    // queries in leaf (Morton) order: neighbouring lanes walk neighbouring paths
+    PAMO_GRID_STRIDE(pp, L)
     {
-        const int f = (int)ff;
+        const int f = vals[pp];
         if (!active[f] || L < 2) continue;
         int4 t = tris[f];
         if (t.x == -1) continue;
@@ -510,7 +539,11 @@ __global__ void __launch_bounds__(kThreads) k_query(const BvhNode *__restrict__ 
                     if (active[g] && g < f) continue;
                     int4 tg = tris[g];
                     if (shared_indices(t, tg) >= 2) continue;
-                    int pos = atomicAdd(&cnt->n_pairs, 1);
+                    // one atomic per group of lanes appending together
+                    cg::coalesced_group grp = cg::coalesced_threads();
+                    int base = 0;
+                    if (grp.thread_rank() == 0) base = atomicAdd(&cnt->n_pairs, (int)grp.size());
+                    int pos = grp.shfl(base, 0) + (int)grp.thread_rank();
                     if (pos < cap_pairs) pairs[pos] = make_uint2((unsigned)f, (unsigned)g);
                     else atomicAdd(&cnt->pair_overflow, 1);
                 } else if (sp < kStack) {
@@ -728,7 +761,7 @@ int Stage2::validate(const int *d_tris, int n, int m, const int *d_undo, int n_u
 void Stage2::release()
 {
     void *p[] = {edge_cost, pts_map, undo_list, tmp_undo, invalid_table, opts, pts, otris, tris, occ,
-                 first_near, cursor, near_tris, first_edge, edges, plane, quad, vmin, eflag, collapsed,
+                 first_near, cursor, near_tris, first_edge, edges, plane, elen4, nxt, quad, vmin, eflag, collapsed,
                  active, isect, uflag, undo_edges, fflag, pairs, scan_scratch, dev_misc, dcnt};
     for (void *q : p)
         if (q) cudaFree(q);
@@ -737,7 +770,8 @@ void Stage2::release()
     prof.release();
     edge_cost = nullptr; pts_map = nullptr; undo_list = nullptr; tmp_undo = nullptr; invalid_table = nullptr;
     opts = pts = nullptr; otris = tris = nullptr; occ = nullptr;
-    first_near = cursor = near_tris = first_edge = nullptr; edges = nullptr; plane = quad = nullptr;
+    first_near = cursor = near_tris = first_edge = nullptr; edges = nullptr; plane = quad = elen4 = nullptr;
+    nxt = nullptr;
     vmin = nullptr; eflag = collapsed = nullptr; active = isect = nullptr; uflag = undo_edges = fflag = nullptr;
     pairs = nullptr; scan_scratch = nullptr; dev_misc = nullptr; dcnt = nullptr; hcnt = nullptr; h_scalars = nullptr;
     bvh.release();
@@ -780,6 +814,8 @@ int Stage2::ensure(long long n, long long m)
     ALLOC(first_edge, (ct + 1) * 4);
     ALLOC(edges, (ce + 1) * 8);
     ALLOC(plane, (ct + 1) * 16);
+    ALLOC(elen4, (ct + 1) * 16);
+    ALLOC(nxt, 3 * (ct + 1) * 4);
     ALLOC(quad, 3 * (cp + 1) * 16);
     ALLOC(vmin, (cp + 1) * 8);
     ALLOC(eflag, (ce + 1) * 4);
@@ -897,26 +933,26 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     prof.begin(PH_SETUP, s);
     k_round_init<<<grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s>>>(opts, otris, pts, tris, occ, first_near,
                                                                        cursor, vmin, n, m);
-    k_face_a<<<grid_for(m), kThreads, 0, s>>>(pts, tris, m, first_near, first_edge, plane);
+    k_face_a<<<grid_for(m), kThreads, 0, s>>>(pts, tris, m, first_near, first_edge, plane, elen4);
     if (m > 0) S2_TRY(cudaMemsetAsync(first_edge + m, 0, 4, s));
     S2_TRY(exclusive_scan(first_near, first_near, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
     S2_TRY(exclusive_scan(first_edge, first_edge, (long long)m + 1, nullptr, scan_scratch, &dcnt->n_edges, s));
     const int *d_n_edges = &dcnt->n_edges;
     k_face_b<<<grid_for(m), kThreads, 0, s>>>(tris, m, first_near, cursor, near_tris, first_edge, edges);
-    k_vertex_quadric<<<grid_for(n), kThreads, 0, s>>>(first_near, near_tris, plane, quad, n);
+    k_vertex_quadric<<<grid_for(n), kThreads, 0, s>>>(first_near, near_tris, plane, tris, quad, nxt, n);
     // the hierarchy only depends on the round input: build it now
     prof.begin(PH_LBVH_BUILD, s);
     S2_TRY(lbvh_build(bvh, pts, tris, m, s));
 
     const long long EMAX = 3LL * m;
     prof.begin(PH_EDGE_COST, s);
-    CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, quad, invalid_table, edge_cost, vmin,
-                tres, edge_s, is_stuck ? 1 : 0};
-    k_edge_cost<<<grid_for(EMAX), kThreads, 0, s>>>(ca);
+    CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, nxt, plane, elen4, quad, invalid_table,
+                edge_cost, vmin, tres, edge_s, is_stuck ? 1 : 0};
+    k_edge_cost<<<grid_for(m), kThreads, 0, s>>>(ca, bvh.vals, bvh.scene, first_edge);
     CollapseArgs cl{edges, d_n_edges, edge_cost, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
                     collapse_t};
     prof.begin(PH_COLLAPSE, s);
-    k_collapse<<<grid_for(EMAX), kThreads, 0, s>>>(cl);
+    k_collapse<<<grid_for(m), kThreads, 0, s>>>(cl, bvh.vals, bvh.scene, first_edge);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
     k_scatter_flagged<<<grid_for(EMAX), kThreads, 0, s>>>(eflag, uflag, d_n_edges, collapsed, 0);
     prof.begin(PH_CLEANUP, s);

@@ -79,7 +79,9 @@ struct Stage2 {
     int *first_edge = nullptr;
     int2 *edges = nullptr;
     float4 *plane = nullptr;
-    float4 *quad = nullptr;  // 3 float4 per vertex (10 used)
+    float4 *elen4 = nullptr;  // per face: lengths of edges (i,j), (j,k), (k,i)
+    int *nxt = nullptr;       // per CSR slot: the vertex after the slot's vertex in the face
+    float4 *quad = nullptr;   // 3 float4 per vertex (10 used)
     unsigned long long *vmin = nullptr;
     int *eflag = nullptr;
     int *collapsed = nullptr;

@@ -1,0 +1,1174 @@
+// Stage-3 safe projection kernels and driver (see stage3.cuh).
+//
+// Energy terms (default configuration of the reference, config.py:27-38):
+//   GT attraction   0.5 * w_i * k * |x_i - t_i|^2, t_i = closest GT point
+//                   (distance_energy.py:6-46, geometry_kernels.py:82-94)
+//   membrane        StVK in each triangle's 2-D frame, mu = E/2(1+nu), lambda
+//                   (elastic_energy.py:8-220; its Hessian product holds the frame
+//                   fixed, as the reference's does)
+//   bending         0.5 * k * (theta - theta0)^2 * l0 per interior edge
+//                   (hinge_energy.py:5-274); Hessian blocks of Tamstorf &
+//                   Grinspun (2013), SPD-projected
+//   contact         kappa * b(d), b(d) = -(d - dh)^2 ln(d / dh) for d < dh
+//                   (collision_energy.py:8-99,192-254,379-411), Gauss-Newton
+//                   Hessian kappa b''(d) grad(d) grad(d)^T
+#include <cooperative_groups.h>
+#include <cstdio>
+#include <cstring>
+
+#include "distance.cuh"
+#include "scan.cuh"
+#include "stage3.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace pamo {
+namespace s3 {
+
+namespace {
+
+constexpr int kRedBlocks = 296;  // fixed grid for deterministic reductions (2 x 148 SMs)
+constexpr int kStack = 96;
+
+enum { D_ENERGY = 0, D_ENERGY_PREV, D_ZR, D_ZR_LAST, D_VAV };
+enum { I_NB = 0, I_OVERFLOW, I_STACK };
+
+__device__ __forceinline__ F3 ld(const float4 *a, int i) { return f3(a[i]); }
+__device__ __forceinline__ void st(float4 *a, int i, F3 v) { a[i] = make_float4(v.x, v.y, v.z, 0.f); }
+__device__ __forceinline__ void atomic_add3(float4 *a, int i, F3 v)
+{
+    atomicAdd(&a[i].x, v.x);
+    atomicAdd(&a[i].y, v.y);
+    atomicAdd(&a[i].z, v.z);
+}
+
+// ---------------------------------------------------------------- barrier (FP64)
+__device__ __forceinline__ double barrier(double d, double dh) { return -(d - dh) * (d - dh) * log(d / dh); }
+__device__ __forceinline__ double barrier_d1(double d, double dh)
+{
+    double t = d - dh;
+    return -2.0 * t * log(d / dh) - t * t / d;
+}
+__device__ __forceinline__ double barrier_d2(double d, double dh)
+{
+    return -2.0 * log(d / dh) - 2.0 * (d - dh) / d - 1.0 + (dh * dh) / (d * d);
+}
+
+// --------------------------------------------------------------- reductions
+template <int BLOCK>
+__device__ __forceinline__ double block_sum(double v)
+{
+    __shared__ double ws[BLOCK / 32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) ws[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (wid == 0) {
+        r = lane < BLOCK / 32 ? ws[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    __syncthreads();
+    return r;
+}
+
+// sums partials[0..n) in a fixed order into dst (one warp)
+__global__ void k_finish_sum(const double *partials, int n, double *dst)
+{
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n; i += 32) v += partials[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) *dst = v;
+}
+
+// ------------------------------------------------------------ preprocessing
+__global__ void k_aos_to_f4(const float *in, float4 *a, float4 *b, int n)
+{
+    PAMO_GRID_STRIDE(i, n)
+    {
+        float4 v = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.f);
+        a[i] = v;
+        if (b) b[i] = v;
+    }
+}
+
+__global__ void k_aos_to_i4(const int *in, int4 *out, int n, int stride, int dup_last)
+{
+    PAMO_GRID_STRIDE(i, n)
+    {
+        if (stride == 3) out[i] = make_int4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0);
+        else if (stride == 2) out[i] = make_int4(in[2 * i], in[2 * i + 1], dup_last ? in[2 * i + 1] : 0, 0);
+        else out[i] = make_int4(in[4 * i], in[4 * i + 1], in[4 * i + 2], in[4 * i + 3]);
+    }
+}
+
+__device__ __forceinline__ void frame(F3 x01, F3 x02, F3 &b1, F3 &b2)
+{
+    b1 = normalized(x01);
+    b2 = x02 - dot(x02, b1) * b1;
+    b2 = normalized(b2);
+}
+
+__global__ void k_elastic_pre(const float4 *x, const int4 *tris, int nt, float *area, float4 *inv_dm)
+{
+    PAMO_GRID_STRIDE(t, nt)
+    {
+        int4 f = tris[t];
+        F3 x0 = ld(x, f.x), x1 = ld(x, f.y), x2 = ld(x, f.z);
+        F3 x01 = x1 - x0, x02 = x2 - x0;
+        area[t] = 0.5f * len(cross(x01, x02));
+        F3 b1, b2;
+        frame(x01, x02, b1, b2);
+        float a = dot(b1, x01), b = dot(b1, x02), c = dot(b2, x01), d = dot(b2, x02);
+        float det = a * d - b * c;
+        inv_dm[t] = make_float4(d / det, -b / det, -c / det, a / det);
+    }
+}
+
+__device__ __forceinline__ float hinge_theta(F3 x0, F3 x1, F3 x2, F3 x3)
+{
+    F3 e12 = normalized(x2 - x1);
+    F3 n1 = normalized(cross(e12, x0 - x1));
+    F3 n2 = normalized(cross(x3 - x1, e12));
+    return atan2f(dot(cross(n1, n2), e12), dot(n1, n2));
+}
+
+__global__ void k_hinge_pre(const float4 *x, const int4 *h, int nh, float *rest_angle, float *rest_elen)
+{
+    PAMO_GRID_STRIDE(k, nh)
+    {
+        int4 i = h[k];
+        F3 x0 = ld(x, i.x), x1 = ld(x, i.y), x2 = ld(x, i.z), x3 = ld(x, i.w);
+        rest_angle[k] = hinge_theta(x0, x1, x2, x3);
+        rest_elen[k] = len(x1 - x2);
+    }
+}
+
+// ------------------------------------------------- closest point on the GT mesh
+__device__ F3 closest_on_triangle(F3 p, F3 a, F3 b, F3 c)
+{
+    // Ericson, Real-Time Collision Detection, section 5.1.5
+    F3 ab = b - a, ac = c - a, ap = p - a;
+    float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.f && d2 <= 0.f) return a;
+    F3 bp = p - b;
+    float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.f && d4 <= d3) return b;
+    float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) return a + (d1 / (d1 - d3)) * ab;
+    F3 cp = p - c;
+    float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.f && d5 <= d6) return c;
+    float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) return a + (d2 / (d2 - d6)) * ac;
+    float va = d3 * d6 - d5 * d4;
+    if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) return b + ((d4 - d3) / ((d4 - d3) + (d5 - d6))) * (c - b);
+    float den = 1.f / (va + vb + vc);
+    return a + (vb * den) * ab + (vc * den) * ac;
+}
+
+__device__ __forceinline__ float box_dist2(float4 lo, float4 hi, F3 p)
+{
+    float dx = fmaxf(fmaxf(lo.x - p.x, 0.f), p.x - hi.x);
+    float dy = fmaxf(fmaxf(lo.y - p.y, 0.f), p.y - hi.y);
+    float dz = fmaxf(fmaxf(lo.z - p.z, 0.f), p.z - hi.z);
+    return dx * dx + dy * dy + dz * dz;
+}
+
+__global__ void __launch_bounds__(kThreads) k_closest(const float4 *q, int np, const BvhNode *nodes, const int *vals,
+                                                      const int *scene, const float4 *gpts, const int4 *gtris,
+                                                      float4 *target, int *iscal)
+{
+    const int L = scene[7];
+    int stack[kStack];
+    PAMO_GRID_STRIDE(i, np)
+    {
+        F3 p = ld(q, (int)i);
+        float best = 1e18f;  // max_dist 1e9, squared
+        F3 bestp = mk(1e9f, 1e9f, 1e9f);
+        if (L == 1) {
+            int4 t = gtris[vals[0]];
+            bestp = closest_on_triangle(p, ld(gpts, t.x), ld(gpts, t.y), ld(gpts, t.z));
+        } else if (L > 1) {
+            int sp = 0;
+            stack[sp++] = 0;
+            int budget = 4 * L + 64;
+            while (sp > 0) {
+                if (--budget < 0) {
+                    atomicAdd(&iscal[I_STACK], 1);
+                    break;
+                }
+                const BvhNode nd = nodes[stack[--sp]];
+                float dl = box_dist2(nd.llo, nd.lhi, p), dr = box_dist2(nd.rlo, nd.rhi, p);
+                int cl = __float_as_int(nd.llo.w), cr = __float_as_int(nd.rlo.w);
+                // visit the nearer child first: push it last
+                int first = dl <= dr ? 0 : 1;
+                for (int k = 0; k < 2; ++k) {
+                    int side = k == 0 ? 1 - first : first;
+                    float dd = side ? dr : dl;
+                    int child = side ? cr : cl;
+                    if (dd >= best) continue;
+                    if (child < 0) {
+                        int4 t = gtris[vals[~child]];
+                        F3 c = closest_on_triangle(p, ld(gpts, t.x), ld(gpts, t.y), ld(gpts, t.z));
+                        float d2 = dot(c - p, c - p);
+                        if (d2 < best) {
+                            best = d2;
+                            bestp = c;
+                        }
+                    } else if (sp < kStack) {
+                        stack[sp++] = child;
+                    } else {
+                        atomicAdd(&iscal[I_STACK], 1);
+                    }
+                }
+            }
+        }
+        st(target, (int)i, bestp);
+    }
+}
+
+// ------------------------------------------------------------ contact detection
+__device__ __forceinline__ bool overlap(float4 lo, float4 hi, F3 qlo, F3 qhi)
+{
+    return !(hi.x < qlo.x || qhi.x < lo.x || hi.y < qlo.y || qhi.y < lo.y || hi.z < qlo.z || qhi.z < lo.z);
+}
+
+__device__ __forceinline__ void append_block(int4 idx, int kind, int *iscal, long long cap, int4 *bidx, int *bkind)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(&iscal[I_NB], (int)g.size());
+    int pos = g.shfl(base, 0) + (int)g.thread_rank();
+    if (pos < cap) {
+        bidx[pos] = idx;
+        bkind[pos] = kind;
+    }
+}
+
+// point-triangle candidates (contact_detection.py:120-164)
+__global__ void __launch_bounds__(kThreads) k_detect_pt(const float4 *q, int np, const int4 *tris, const BvhNode *nodes,
+                                                        const int *vals, const int *scene, float thr, int *iscal,
+                                                        long long cap, int4 *bidx, int *bkind)
+{
+    const int L = scene[7];
+    int stack[kStack];
+    PAMO_GRID_STRIDE(ii, np)
+    {
+        const int i = (int)ii;
+        F3 x0 = ld(q, i);
+        F3 qlo = mk(x0.x - thr, x0.y - thr, x0.z - thr), qhi = mk(x0.x + thr, x0.y + thr, x0.z + thr);
+        int sp = 0;
+        int leaf_only = L == 1 ? 1 : 0;
+        if (L > 1) stack[sp++] = 0;
+        int budget = 2 * L + 16;
+        while (sp > 0 || leaf_only) {
+            int cand[2] = {-1, -1};
+            if (leaf_only) {
+                cand[0] = vals[0];
+                leaf_only = 0;
+            } else {
+                if (--budget < 0) {
+                    atomicAdd(&iscal[I_STACK], 1);
+                    break;
+                }
+                const BvhNode nd = nodes[stack[--sp]];
+                for (int side = 0; side < 2; ++side) {
+                    float4 lo = side ? nd.rlo : nd.llo, hi = side ? nd.rhi : nd.lhi;
+                    if (!overlap(lo, hi, qlo, qhi)) continue;
+                    int child = __float_as_int(lo.w);
+                    if (child < 0) cand[side] = vals[~child];
+                    else if (sp < kStack) stack[sp++] = child;
+                    else atomicAdd(&iscal[I_STACK], 1);
+                }
+            }
+            for (int k = 0; k < 2; ++k) {
+                int f = cand[k];
+                if (f < 0) continue;
+                int4 t = tris[f];
+                if (t.x == i || t.y == i || t.z == i) continue;
+                F3 x[4] = {x0, ld(q, t.x), ld(q, t.y), ld(q, t.z)};
+                int ty = pt_classify(x[0], x[1], x[2], x[3]);
+                float d = classified_distance(KIND_PT, ty, x);
+                if (d <= thr) append_block(make_int4(i, t.x, t.y, t.z), KIND_PT, iscal, cap, bidx, bkind);
+            }
+        }
+    }
+}
+
+// edge-edge candidates (contact_detection.py:168-216)
+__global__ void __launch_bounds__(kThreads) k_detect_ee(const float4 *q, int ne, const int4 *edges4,
+                                                        const BvhNode *nodes, const int *vals, const int *scene,
+                                                        float thr, float ee_thres, int *iscal, long long cap,
+                                                        int4 *bidx, int *bkind)
+{
+    const int L = scene[7];
+    int stack[kStack];
+    PAMO_GRID_STRIDE(ee, ne)
+    {
+        const int e0 = (int)ee;
+        int4 a = edges4[e0];
+        F3 x0 = ld(q, a.x), x1 = ld(q, a.y);
+        F3 qlo = mk(fminf(x0.x, x1.x) - thr, fminf(x0.y, x1.y) - thr, fminf(x0.z, x1.z) - thr);
+        F3 qhi = mk(fmaxf(x0.x, x1.x) + thr, fmaxf(x0.y, x1.y) + thr, fmaxf(x0.z, x1.z) + thr);
+        if (L < 2) continue;
+        int sp = 0;
+        stack[sp++] = 0;
+        int budget = 2 * L + 16;
+        while (sp > 0) {
+            if (--budget < 0) {
+                atomicAdd(&iscal[I_STACK], 1);
+                break;
+            }
+            const BvhNode nd = nodes[stack[--sp]];
+            for (int side = 0; side < 2; ++side) {
+                float4 lo = side ? nd.rlo : nd.llo, hi = side ? nd.rhi : nd.lhi;
+                if (!overlap(lo, hi, qlo, qhi)) continue;
+                int child = __float_as_int(lo.w);
+                if (child >= 0) {
+                    if (sp < kStack) stack[sp++] = child;
+                    else atomicAdd(&iscal[I_STACK], 1);
+                    continue;
+                }
+                int e1 = vals[~child];
+                if (e1 <= e0) continue;
+                int4 b = edges4[e1];
+                if (a.x == b.x || a.x == b.y || a.y == b.x || a.y == b.y) continue;
+                F3 x[4] = {x0, x1, ld(q, b.x), ld(q, b.y)};
+                int ty = ee_classify(x[0], x[1], x[2], x[3], ee_thres);
+                float d = classified_distance(KIND_EE, ty, x);
+                if (d <= thr) append_block(make_int4(a.x, a.y, b.x, b.y), KIND_EE, iscal, cap, bidx, bkind);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------- energy
+struct EArgs {
+    const float4 *q, *target;
+    const float *wk;
+    int np, nt, nh;
+    const int4 *tris;
+    const float *area;
+    const float4 *inv_dm;
+    float mu, la;
+    const int4 *hinges;
+    const float *rest_angle, *rest_elen;
+    float hinge_k;
+    const int4 *bidx;
+    const int *bkind;
+    int *bsub;
+    float *bd;
+    const int *iscal;
+    long long cap_b;
+    float d_hat, kappa, ee_thres;
+    double *partials;
+};
+
+__device__ __forceinline__ void elastic_F(const float4 *q, int4 f, float4 im, F3 &b1, F3 &b2, float F[4])
+{
+    F3 x0 = ld(q, f.x), x1 = ld(q, f.y), x2 = ld(q, f.z);
+    F3 x01 = x1 - x0, x02 = x2 - x0;
+    frame(x01, x02, b1, b2);
+    float d00 = dot(b1, x01), d01 = dot(b1, x02), d10 = dot(b2, x01), d11 = dot(b2, x02);
+    F[0] = d00 * im.x + d01 * im.z;
+    F[1] = d00 * im.y + d01 * im.w;
+    F[2] = d10 * im.x + d11 * im.z;
+    F[3] = d10 * im.y + d11 * im.w;
+}
+
+__global__ void __launch_bounds__(kThreads) k_energy(EArgs A)
+{
+    const long long nb = min((long long)A.iscal[I_NB], A.cap_b);
+    const long long total = (long long)A.np + A.nt + A.nh + nb;
+    double acc = 0.0;
+    PAMO_GRID_STRIDE(k, total)
+    {
+        if (k < A.np) {
+            F3 d = ld(A.q, (int)k) - ld(A.target, (int)k);
+            acc += (double)(0.5f * dot(d, d) * A.wk[k]);
+        } else if (k < (long long)A.np + A.nt) {
+            int t = (int)(k - A.np);
+            F3 b1, b2;
+            float F[4];
+            elastic_F(A.q, A.tris[t], A.inv_dm[t], b1, b2, F);
+            // E = 0.5 (F^T F - I)
+            float e00 = 0.5f * (F[0] * F[0] + F[2] * F[2] - 1.f);
+            float e01 = 0.5f * (F[0] * F[1] + F[2] * F[3]);
+            float e11 = 0.5f * (F[1] * F[1] + F[3] * F[3] - 1.f);
+            float tr = e00 + e11;
+            float ee = e00 * e00 + 2.f * e01 * e01 + e11 * e11;
+            acc += (double)(A.area[t] * (A.mu * ee + 0.5f * A.la * tr * tr));
+        } else if (k < (long long)A.np + A.nt + A.nh) {
+            int h = (int)(k - A.np - A.nt);
+            int4 i = A.hinges[h];
+            float th = hinge_theta(ld(A.q, i.x), ld(A.q, i.y), ld(A.q, i.z), ld(A.q, i.w));
+            float dt = th - A.rest_angle[h];
+            acc += (double)(0.5f * A.hinge_k * dt * dt * A.rest_elen[h]);
+        } else {
+            int b = (int)(k - A.np - A.nt - A.nh);
+            int4 i = A.bidx[b];
+            int kind = A.bkind[b];
+            F3 x[4] = {ld(A.q, i.x), ld(A.q, i.y), ld(A.q, i.z), ld(A.q, i.w)};
+            int ty = classify(kind, x, A.ee_thres);
+            float d = classified_distance(kind, ty, x);
+            A.bsub[b] = ty;
+            A.bd[b] = d;
+            if (d < A.d_hat) acc += barrier((double)d, (double)A.d_hat) * (double)A.kappa;
+        }
+    }
+    double r = block_sum<kThreads>(acc);
+    if (threadIdx.x == 0) A.partials[blockIdx.x] = r;
+}
+
+// --------------------------------------------------------------------- diff
+// vertex part: grad = -(x - t) w, diag = w (writes, before the atomics)
+__global__ void k_diff_vertex(const float4 *q, const float4 *target, const float *wk, int np, float4 *grad,
+                              float4 *diag)
+{
+    PAMO_GRID_STRIDE(i, np)
+    {
+        float w = wk[i];
+        F3 g = ld(q, (int)i) - ld(target, (int)i);
+        st(grad, (int)i, (-w) * g);
+        diag[i] = make_float4(w, w, w, 0.f);
+    }
+}
+
+__device__ __forceinline__ void mat3_zero(float *m)
+{
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m[k] = 0.f;
+}
+
+// Hinge gradient and Hessian blocks (Tamstorf & Grinspun 2013, in the form of
+// hinge_energy.py:91-254): writes the 16 row-major 3x3 blocks into B.
+__device__ void hinge_blocks(F3 x0, F3 x1, F3 x2, F3 x3, float rest_angle, float rest_elen, float k, F3 g[4],
+                             float B[16][9], float &dE)
+{
+    F3 e0 = x2 - x1, e1 = x0 - x2, e2 = x0 - x1, e1_ = x3 - x2, e2_ = x3 - x1;
+    float l0 = len(e0), l1 = len(e1), l2 = len(e2), l1_ = len(e1_), l2_ = len(e2_);
+    F3 u0 = normalized(e0), u1 = normalized(e1), u2 = normalized(e2), u1_ = normalized(e1_), u2_ = normalized(e2_);
+    float ca1 = dot(u2, u0), ca2 = -dot(u1, u0), ca1_ = dot(u2_, u0), ca2_ = -dot(u1_, u0);
+    float h0 = len(cross(e1, e2)) / l0, h1 = len(cross(e0, e2)) / l1, h2 = len(cross(e0, e1)) / l2;
+    float h0_ = len(cross(e1_, e2_)) / l0, h1_ = len(cross(e0, e2_)) / l1_, h2_ = len(cross(e0, e1_)) / l2_;
+    F3 n = normalized(cross(e0, e2)), n_ = normalized(cross(e2_, e0));
+    float th = atan2f(dot(cross(n, n_), e0) / l0, dot(n, n_));
+    dE = k * (th - rest_angle) * rest_elen;
+    float d2E = k * rest_elen;
+    g[0] = (-1.f / h0) * n;
+    g[3] = (-1.f / h0_) * n_;
+    g[1] = (ca2 / h1) * n + (ca2_ / h1_) * n_;
+    g[2] = (ca1 / h2) * n + (ca1_ / h2_) * n_;
+    F3 m0 = normalized(cross(e0, n)), m1 = normalized(cross(e1, n)), m2 = normalized(cross(n, e2));
+    F3 m0_ = normalized(cross(n_, e0)), m1_ = normalized(cross(n_, e1_)), m2_ = normalized(cross(e2_, n_));
+    auto outer = [](F3 a, F3 b, float *o) {
+        o[0] = a.x * b.x; o[1] = a.x * b.y; o[2] = a.x * b.z;
+        o[3] = a.y * b.x; o[4] = a.y * b.y; o[5] = a.y * b.z;
+        o[6] = a.z * b.x; o[7] = a.z * b.y; o[8] = a.z * b.z;
+    };
+    // M = n m^T; P_xy = c * M^T / (h h); Q = M / (h h); N0 = M0 / l0^2
+    float M0[9], M1[9], M2[9], M0_[9], M1_[9], M2_[9];
+    outer(n, m0, M0); outer(n, m1, M1); outer(n, m2, M2);
+    outer(n_, m0_, M0_); outer(n_, m1_, M1_); outer(n_, m2_, M2_);
+    const float il0 = 1.f / (l0 * l0);
+    float G[9];
+    auto T = [](const float *a, int r, int c) { return a[c * 3 + r]; };  // transpose access
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            const int rc = r * 3 + c;
+            // block (0,0): -sym(Q0) dE
+            float q0 = M0[rc] / (h0 * h0), q0t = T(M0, r, c) / (h0 * h0);
+            float q0_ = M0_[rc] / (h0_ * h0_), q0_t = T(M0_, r, c) / (h0_ * h0_);
+            B[0][rc] = -(q0 + q0t) * dE;
+            B[15][rc] = -(q0_ + q0_t) * dE;
+            // block (1,1): (sym(P11) - N0 + sym(P11_) - N0_) dE
+            float p11 = ca1 * T(M1, r, c) / (h1 * h1), p11t = ca1 * M1[rc] / (h1 * h1);
+            float p11_ = ca1_ * T(M1_, r, c) / (h1_ * h1_), p11_t = ca1_ * M1_[rc] / (h1_ * h1_);
+            B[5][rc] = (p11 + p11t - M0[rc] * il0 + p11_ + p11_t - M0_[rc] * il0) * dE;
+            // block (2,2): (sym(P22) - N0 + sym(P22_) - N0_) dE
+            float p22 = ca2 * T(M2, r, c) / (h2 * h2), p22t = ca2 * M2[rc] / (h2 * h2);
+            float p22_ = ca2_ * T(M2_, r, c) / (h2_ * h2_), p22_t = ca2_ * M2_[rc] / (h2_ * h2_);
+            B[10][rc] = (p22 + p22t - M0[rc] * il0 + p22_ + p22_t - M0_[rc] * il0) * dE;
+            // block (1,0): (P10 - Q1) dE ; (2,0): (P20 - Q2) dE
+            B[4][rc] = (ca1 * T(M0, r, c) / (h1 * h0) - M1[rc] / (h0 * h1)) * dE;
+            B[8][rc] = (ca2 * T(M0, r, c) / (h2 * h0) - M2[rc] / (h0 * h2)) * dE;
+            // block (1,3): (P10_ - Q1_) dE ; (2,3): (P20_ - Q2_) dE
+            B[7][rc] = (ca1_ * T(M0_, r, c) / (h1_ * h0_) - M1_[rc] / (h0_ * h1_)) * dE;
+            B[11][rc] = (ca2_ * T(M0_, r, c) / (h2_ * h0_) - M2_[rc] / (h0_ * h2_)) * dE;
+            // block (1,2): (P12 + P21^T + N0 + P12_ + P21_^T + N0_) dE
+            float p12 = ca1 * T(M2, r, c) / (h1 * h2);
+            float p21t = ca2 * M1[rc] / (h2 * h1);
+            float p12_ = ca1_ * T(M2_, r, c) / (h1_ * h2_);
+            float p21_t = ca2_ * M1_[rc] / (h2_ * h1_);
+            B[6][rc] = (p12 + p21t + M0[rc] * il0 + p12_ + p21_t + M0_[rc] * il0) * dE;
+            B[3][rc] = 0.f;
+        }
+    // + d2E * outer(g_i, g_j) on the blocks above, block (0,3) is pure outer
+    const int pairs[10][2] = {{0, 0}, {3, 3}, {1, 1}, {2, 2}, {1, 0}, {2, 0}, {1, 3}, {2, 3}, {1, 2}, {0, 3}};
+    for (int k2 = 0; k2 < 10; ++k2) {
+        int i = pairs[k2][0], j = pairs[k2][1];
+        outer(g[i], g[j], G);
+        for (int e = 0; e < 9; ++e) B[i * 4 + j][e] += d2E * G[e];
+    }
+    // mirrored blocks
+    const int mir[6][2] = {{0, 1}, {0, 2}, {3, 1}, {3, 2}, {2, 1}, {3, 0}};
+    for (int k2 = 0; k2 < 6; ++k2) {
+        int i = mir[k2][0], j = mir[k2][1];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) B[i * 4 + j][r * 3 + c] = B[j * 4 + i][c * 3 + r];
+    }
+}
+
+// Eigenvalue clamp of the symmetric part of the 9x9 matrix of hinge vertices 0-2
+// (cyclic Jacobi, `sweeps` sweeps), then vertex 3's rows and columns from
+// translation invariance.
+__device__ void spd_project(float B[16][9], int sweeps)
+{
+    float A[9][9], V[9][9];
+    for (int bi = 0; bi < 3; ++bi)
+        for (int bj = 0; bj < 3; ++bj)
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) A[bi * 3 + r][bj * 3 + c] = B[bi * 4 + bj][r * 3 + c];
+    for (int i = 0; i < 9; ++i)
+        for (int j = i + 1; j < 9; ++j) {
+            float s = 0.5f * (A[i][j] + A[j][i]);
+            A[i][j] = A[j][i] = s;
+        }
+    for (int i = 0; i < 9; ++i)
+        for (int j = 0; j < 9; ++j) V[i][j] = i == j ? 1.f : 0.f;
+    for (int sw = 0; sw < sweeps; ++sw)
+        for (int p = 0; p < 8; ++p)
+            for (int qq = p + 1; qq < 9; ++qq) {
+                float apq = A[p][qq];
+                if (!(fabsf(apq) > 1e-30f)) continue;
+                float theta = (A[qq][qq] - A[p][p]) / (2.f * apq);
+                float sg = theta >= 0.f ? 1.f : -1.f;
+                float t = sg / (fabsf(theta) + sqrtf(theta * theta + 1.f));
+                float c = 1.f / sqrtf(t * t + 1.f), s = t * c;
+                for (int k = 0; k < 9; ++k) {  // A <- A J
+                    float akp = A[k][p], akq = A[k][qq];
+                    A[k][p] = c * akp - s * akq;
+                    A[k][qq] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 9; ++k) {  // A <- J^T A
+                    float apk = A[p][k], aqk = A[qq][k];
+                    A[p][k] = c * apk - s * aqk;
+                    A[qq][k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 9; ++k) {  // V <- V J
+                    float vkp = V[k][p], vkq = V[k][qq];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][qq] = s * vkp + c * vkq;
+                }
+            }
+    float lam[9];
+    for (int i = 0; i < 9; ++i) lam[i] = fmaxf(A[i][i], 0.f);
+    for (int i = 0; i < 9; ++i)
+        for (int j = 0; j < 9; ++j) {
+            float s = 0.f;
+            for (int k = 0; k < 9; ++k) s += V[i][k] * lam[k] * V[j][k];
+            B[(i / 3) * 4 + (j / 3)][(i % 3) * 3 + (j % 3)] = s;
+        }
+    for (int j = 0; j < 3; ++j)
+        for (int e = 0; e < 9; ++e) B[12 + j][e] = -(B[0 + j][e] + B[4 + j][e] + B[8 + j][e]);
+    for (int j = 0; j < 3; ++j)
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) B[j * 4 + 3][r * 3 + c] = B[12 + j][c * 3 + r];
+    for (int e = 0; e < 9; ++e) B[15][e] = -(B[3][e] + B[7][e] + B[11][e]);
+}
+
+struct DArgs {
+    const float4 *q;
+    int nt, nh;
+    const int4 *tris;
+    const float *area;
+    const float4 *inv_dm;
+    float mu, la;
+    const int4 *hinges;
+    const float *rest_angle, *rest_elen;
+    float hinge_k;
+    int spd_iters;
+    float *hblk;
+    const int4 *bidx;
+    const int *bkind, *bsub;
+    const float *bd;
+    float4 *bg;
+    float *bb2;
+    const int *iscal;
+    long long cap_b;
+    float d_hat, kappa;
+    float4 *grad, *diag;
+};
+
+__global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
+{
+    const long long nb = min((long long)A.iscal[I_NB], A.cap_b);
+    const long long total = (long long)A.nt + A.nh + nb;
+    PAMO_GRID_STRIDE(k, total)
+    {
+        if (k < A.nt) {
+            int t = (int)k;
+            int4 f = A.tris[t];
+            F3 b1, b2;
+            float F[4];
+            float4 im = A.inv_dm[t];
+            elastic_F(A.q, f, im, b1, b2, F);
+            float e00 = 0.5f * (F[0] * F[0] + F[2] * F[2] - 1.f);
+            float e01 = 0.5f * (F[0] * F[1] + F[2] * F[3]);
+            float e11 = 0.5f * (F[1] * F[1] + F[3] * F[3] - 1.f);
+            float tr = e00 + e11;
+            // S = 2 mu E + la tr(E) I ; P = F S ; H = -W P inv_dm^T
+            float s00 = 2.f * A.mu * e00 + A.la * tr, s01 = 2.f * A.mu * e01, s11 = 2.f * A.mu * e11 + A.la * tr;
+            float P00 = F[0] * s00 + F[1] * s01, P01 = F[0] * s01 + F[1] * s11;
+            float P10 = F[2] * s00 + F[3] * s01, P11 = F[2] * s01 + F[3] * s11;
+            float W = -A.area[t];
+            float H00 = W * (P00 * im.x + P01 * im.y), H01 = W * (P00 * im.z + P01 * im.w);
+            float H10 = W * (P10 * im.x + P11 * im.y), H11 = W * (P10 * im.z + P11 * im.w);
+            F3 f1 = H00 * b1 + H10 * b2, f2 = H01 * b1 + H11 * b2;
+            F3 f0 = mk(-f1.x - f2.x, -f1.y - f2.y, -f1.z - f2.z);
+            atomic_add3(A.grad, f.x, f0);
+            atomic_add3(A.grad, f.y, f1);
+            atomic_add3(A.grad, f.z, f2);
+        } else if (k < (long long)A.nt + A.nh) {
+            int h = (int)(k - A.nt);
+            int4 i = A.hinges[h];
+            int idx[4] = {i.x, i.y, i.z, i.w};
+            F3 g[4];
+            float B[16][9];
+            float dE;
+            hinge_blocks(ld(A.q, i.x), ld(A.q, i.y), ld(A.q, i.z), ld(A.q, i.w), A.rest_angle[h], A.rest_elen[h],
+                         A.hinge_k, g, B, dE);
+            for (int a = 0; a < 4; ++a) {
+                atomic_add3(A.grad, idx[a], (-dE) * g[a]);
+                // diagonal of the unprojected block, as the reference adds it before projecting
+                atomic_add3(A.diag, idx[a], mk(B[a * 5][0], B[a * 5][4], B[a * 5][8]));
+            }
+            spd_project(B, A.spd_iters);
+            float *dst = A.hblk + (size_t)h * 144;
+            for (int b = 0; b < 16; ++b)
+                for (int e = 0; e < 9; ++e) dst[b * 9 + e] = B[b][e];
+        } else {
+            int b = (int)(k - A.nt - A.nh);
+            float d = A.bd[b];
+            if (!(d < A.d_hat)) {
+                A.bb2[b] = 0.f;
+                continue;
+            }
+            int4 i = A.bidx[b];
+            int idx[4] = {i.x, i.y, i.z, i.w};
+            F3 x[4] = {ld(A.q, i.x), ld(A.q, i.y), ld(A.q, i.z), ld(A.q, i.w)};
+            F3 g[4];
+            distance_grad(A.bkind[b], A.bsub[b], x, g);
+            double b1 = barrier_d1((double)d, (double)A.d_hat) * (double)A.kappa;
+            double b2 = barrier_d2((double)d, (double)A.d_hat) * (double)A.kappa;
+            float b1f = (float)b1, b2f = (float)b2;
+            for (int a = 0; a < 4; ++a) {
+                A.bg[4 * (size_t)b + a] = make_float4(g[a].x, g[a].y, g[a].z, 0.f);
+                atomic_add3(A.grad, idx[a], (-b1f) * g[a]);
+                atomic_add3(A.diag, idx[a], mk(b2f * g[a].x * g[a].x, b2f * g[a].y * g[a].y, b2f * g[a].z * g[a].z));
+            }
+            A.bb2[b] = b2f;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- hess * dx
+struct HArgs {
+    const float4 *q;
+    const float *wk;
+    int np, nt, nh;
+    const int4 *tris;
+    const float *area;
+    const float4 *inv_dm;
+    float mu, la;
+    const int4 *hinges;
+    const float *hblk;
+    const int4 *bidx;
+    const float4 *bg;
+    const float *bb2;
+    const int *iscal;
+    long long cap_b;
+    const float4 *dx;
+    float4 *out;
+};
+
+__global__ void k_hess_vertex(const float *wk, int np, const float4 *dx, float4 *out)
+{
+    PAMO_GRID_STRIDE(i, np) st(out, (int)i, wk[i] * ld(dx, (int)i));
+}
+
+__global__ void __launch_bounds__(kThreads) k_hess_elements(HArgs A)
+{
+    const long long nb = min((long long)A.iscal[I_NB], A.cap_b);
+    const long long total = (long long)A.nt + A.nh + nb;
+    PAMO_GRID_STRIDE(k, total)
+    {
+        if (k < A.nt) {
+            int t = (int)k;
+            int4 f = A.tris[t];
+            F3 b1, b2;
+            float F[4];
+            float4 im = A.inv_dm[t];
+            elastic_F(A.q, f, im, b1, b2, F);
+            F3 dx01 = ld(A.dx, f.y) - ld(A.dx, f.x), dx02 = ld(A.dx, f.z) - ld(A.dx, f.x);
+            float s00 = dot(b1, dx01), s01 = dot(b1, dx02), s10 = dot(b2, dx01), s11 = dot(b2, dx02);
+            float dF[4] = {s00 * im.x + s01 * im.z, s00 * im.y + s01 * im.w, s10 * im.x + s11 * im.z,
+                           s10 * im.y + s11 * im.w};
+            float e00 = 0.5f * (F[0] * F[0] + F[2] * F[2] - 1.f);
+            float e01 = 0.5f * (F[0] * F[1] + F[2] * F[3]);
+            float e11 = 0.5f * (F[1] * F[1] + F[3] * F[3] - 1.f);
+            float tr = e00 + e11;
+            // dE = 0.5 (dF^T F + F^T dF)
+            float de00 = dF[0] * F[0] + dF[2] * F[2];
+            float de01 = 0.5f * (dF[0] * F[1] + dF[2] * F[3] + F[0] * dF[1] + F[2] * dF[3]);
+            float de11 = dF[1] * F[1] + dF[3] * F[3];
+            float trd = de00 + de11;
+            float S00 = 2.f * A.mu * e00 + A.la * tr, S01 = 2.f * A.mu * e01, S11 = 2.f * A.mu * e11 + A.la * tr;
+            float T00 = 2.f * A.mu * de00 + A.la * trd, T01 = 2.f * A.mu * de01, T11 = 2.f * A.mu * de11 + A.la * trd;
+            float dP00 = dF[0] * S00 + dF[1] * S01 + F[0] * T00 + F[1] * T01;
+            float dP01 = dF[0] * S01 + dF[1] * S11 + F[0] * T01 + F[1] * T11;
+            float dP10 = dF[2] * S00 + dF[3] * S01 + F[2] * T00 + F[3] * T01;
+            float dP11 = dF[2] * S01 + dF[3] * S11 + F[2] * T01 + F[3] * T11;
+            float W = A.area[t];
+            float H00 = W * (dP00 * im.x + dP01 * im.y), H01 = W * (dP00 * im.z + dP01 * im.w);
+            float H10 = W * (dP10 * im.x + dP11 * im.y), H11 = W * (dP10 * im.z + dP11 * im.w);
+            F3 f1 = H00 * b1 + H10 * b2, f2 = H01 * b1 + H11 * b2;
+            F3 f0 = mk(-f1.x - f2.x, -f1.y - f2.y, -f1.z - f2.z);
+            atomic_add3(A.out, f.x, f0);
+            atomic_add3(A.out, f.y, f1);
+            atomic_add3(A.out, f.z, f2);
+        } else if (k < (long long)A.nt + A.nh) {
+            int h = (int)(k - A.nt);
+            int4 i = A.hinges[h];
+            int idx[4] = {i.x, i.y, i.z, i.w};
+            F3 d[4] = {ld(A.dx, i.x), ld(A.dx, i.y), ld(A.dx, i.z), ld(A.dx, i.w)};
+            const float *B = A.hblk + (size_t)h * 144;
+            for (int a = 0; a < 4; ++a) {
+                F3 s = mk(0.f, 0.f, 0.f);
+                for (int b = 0; b < 4; ++b) {
+                    const float *m = B + (a * 4 + b) * 9;
+                    s = s + mk(m[0] * d[b].x + m[1] * d[b].y + m[2] * d[b].z, m[3] * d[b].x + m[4] * d[b].y + m[5] * d[b].z,
+                               m[6] * d[b].x + m[7] * d[b].y + m[8] * d[b].z);
+                }
+                atomic_add3(A.out, idx[a], s);
+            }
+        } else {
+            int b = (int)(k - A.nt - A.nh);
+            float c = A.bb2[b];
+            if (c == 0.f) continue;
+            int4 i = A.bidx[b];
+            int idx[4] = {i.x, i.y, i.z, i.w};
+            F3 g[4];
+            float s = 0.f;
+            for (int a = 0; a < 4; ++a) {
+                g[a] = f3(A.bg[4 * (size_t)b + a]);
+                s += dot(g[a], ld(A.dx, idx[a]));
+            }
+            for (int a = 0; a < 4; ++a) atomic_add3(A.out, idx[a], (c * s) * g[a]);
+        }
+    }
+}
+
+// -------------------------------------------------------------------- CG
+__global__ void __launch_bounds__(kThreads) k_cg_init(const float4 *grad, const float4 *diag, int np, float4 *p,
+                                                      float4 *r, float4 *z, float4 *v, double *partials)
+{
+    double acc = 0.0;
+    PAMO_GRID_STRIDE(i, np)
+    {
+        F3 g = ld(grad, (int)i), d = ld(diag, (int)i);
+        F3 zz = mk(g.x / (d.x + 1e-6f), g.y / (d.y + 1e-6f), g.z / (d.z + 1e-6f));
+        p[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        st(r, (int)i, g);
+        st(z, (int)i, zz);
+        st(v, (int)i, zz);
+        acc += (double)dot(zz, g);
+    }
+    double s = block_sum<kThreads>(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(kThreads) k_dot(const float4 *a, const float4 *b, int np, double *partials)
+{
+    double acc = 0.0;
+    PAMO_GRID_STRIDE(i, np) acc += (double)dot(ld(a, (int)i), ld(b, (int)i));
+    double s = block_sum<kThreads>(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void k_shift_zr(double *dscal) { dscal[D_ZR_LAST] = dscal[D_ZR]; }
+
+// p += alpha v, r -= alpha Av (if v^T A v > 1e-16); z = r / diag; partial z.r
+__global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const float4 *Av, const float4 *diag,
+                                                        const double *dscal, int np, float4 *p, float4 *r, float4 *z,
+                                                        double *partials)
+{
+    const double vav = dscal[D_VAV];
+    const bool upd = vav > 1e-16;
+    const float alpha = upd ? (float)(dscal[D_ZR_LAST] / vav) : 0.f;
+    double acc = 0.0;
+    PAMO_GRID_STRIDE(i, np)
+    {
+        F3 rr = ld(r, (int)i);
+        if (upd) {
+            st(p, (int)i, ld(p, (int)i) + alpha * ld(v, (int)i));
+            rr = rr - alpha * ld(Av, (int)i);
+            st(r, (int)i, rr);
+        }
+        F3 d = ld(diag, (int)i);
+        F3 zz = mk(rr.x / d.x, rr.y / d.y, rr.z / d.z);
+        st(z, (int)i, zz);
+        acc += (double)dot(zz, rr);
+    }
+    double s = block_sum<kThreads>(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void k_cg_v(const float4 *z, const double *dscal, int np, float4 *v)
+{
+    const float beta = (float)(dscal[D_ZR] / dscal[D_ZR_LAST]);
+    PAMO_GRID_STRIDE(i, np) st(v, (int)i, ld(z, (int)i) + beta * ld(v, (int)i));
+}
+
+// ---------------------------------------------------------- clamp, CCD, line search
+__global__ void k_clamp(float4 *p, const float4 *q_prev, const float4 *q_det, int np, float radius)
+{
+    PAMO_GRID_STRIDE(i, np)
+    {
+        F3 pi = ld(p, (int)i), qn = ld(q_prev, (int)i), qd = ld(q_det, (int)i);
+        F3 dq = qn + pi - qd;
+        float l = len(dq);
+        if (l > radius) st(p, (int)i, radius * ((1.f / l) * dq) + qd - qn);
+    }
+}
+
+// Additive CCD (Li et al. 2021) per block, in FP64 (ccd_kernels.py:8-110).
+__global__ void __launch_bounds__(128) k_accd(const float4 *q, const float4 *pv, const int4 *bidx, const int *bkind,
+                                              const int *iscal, long long cap_b, float slack, float thick, int max_iters,
+                                              float ee_thres, float *ccd_step)
+{
+    const long long nb = min((long long)iscal[I_NB], cap_b);
+    PAMO_GRID_STRIDE(b, nb)
+    {
+        int4 i = bidx[b];
+        int kind = bkind[b];
+        int idx[4] = {i.x, i.y, i.z, i.w};
+        D3 x[4], v[4];
+        for (int a = 0; a < 4; ++a) {
+            x[a] = d3(q[idx[a]]);
+            v[a] = d3(pv[idx[a]]);
+        }
+        D3 avg = 0.25 * (v[0] + v[1] + v[2] + v[3]);
+        for (int a = 0; a < 4; ++a) v[a] = v[a] - avg;
+        double lv;
+        if (kind == KIND_PT) lv = len(v[0]) + fmax(len(v[1]), fmax(len(v[2]), len(v[3])));
+        else lv = fmax(len(v[0]), len(v[1])) + fmax(len(v[2]), len(v[3]));
+        if (lv < 1e-12) continue;
+        const double th = thick;
+        int ty = classify(kind, x, (double)ee_thres);
+        double d = classified_distance(kind, ty, x);
+        double dmt = fmax((d * d - th * th) / (sqrt(d * d) + th), 0.0);
+        const double gap = (1.0 - slack) * dmt;
+        double t = 0.0, tl = slack * dmt / lv;
+        for (int it = 0;; ++it) {
+            for (int a = 0; a < 4; ++a) x[a] = x[a] + tl * v[a];
+            ty = classify(kind, x, (double)ee_thres);
+            d = classified_distance(kind, ty, x);
+            dmt = fmax((d * d - th * th) / (sqrt(d * d) + th), 0.0);
+            if ((it > 0 && dmt <= gap) || it >= max_iters) {
+                float tf = (float)t;  // non-negative: integer order equals float order
+                atomicMin(reinterpret_cast<int *>(ccd_step), __float_as_int(tf));
+                break;
+            }
+            t = t + tl;
+            if (t > 1.0) break;
+            tl = 0.8 * dmt / lv;
+        }
+    }
+}
+
+__global__ void k_line_search(const float4 *q_prev, const float4 *p, const float *ccd_step, int n_halves,
+                              const double *dscal, int np, float4 *q)
+{
+    if (n_halves > 0 && dscal[D_ENERGY] < dscal[D_ENERGY_PREV]) return;
+    const float a = ccd_step[0] * ldexpf(1.f, -n_halves);
+    PAMO_GRID_STRIDE(i, np) st(q, (int)i, ld(q_prev, (int)i) + a * ld(p, (int)i));
+}
+
+__global__ void k_copy_energy_prev(double *dscal) { dscal[D_ENERGY_PREV] = dscal[D_ENERGY]; }
+
+__global__ void k_set_float(float *f, float v) { *f = v; }
+
+__global__ void k_scale(float *a, int n, float s)
+{
+    PAMO_GRID_STRIDE(i, n) a[i] *= s;
+}
+
+__global__ void k_validate_idx(const int *a, long long count, int hi, int *bad)
+{
+    int local = 0;
+    PAMO_GRID_STRIDE(i, count) local += (a[i] < 0 || a[i] >= hi);
+    if (local) atomicAdd(bad, local);
+}
+
+__global__ void k_f4_to_aos(const float4 *in, float *out, int n)
+{
+    PAMO_GRID_STRIDE(i, n)
+    {
+        float4 v = in[i];
+        out[3 * i] = v.x;
+        out[3 * i + 1] = v.y;
+        out[3 * i + 2] = v.z;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+#define S3_TRY(expr)                                      \
+    do {                                                  \
+        cudaError_t _e = (expr);                          \
+        if (_e != cudaSuccess) return map_cuda_error(_e); \
+    } while (0)
+
+void Stage3::release()
+{
+    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, Av, wk, tris, area, inv_dm, edges4, hinges,
+                    rest_angle, rest_elen, hblk, bidx, bkind, bsub, bd, bb2, bg, gt_pts, gt_tris, dscal, fscal, iscal,
+                    partials};
+    for (void *x : ptrs)
+        if (x) cudaFree(x);
+    if (h_iscal) cudaFreeHost(h_iscal);
+    if (h_dscal) cudaFreeHost(h_dscal);
+    q = q_prev = q_det = p = grad = diag = target = r = z = v = Av = nullptr;
+    wk = nullptr; tris = nullptr; area = nullptr; inv_dm = nullptr; edges4 = nullptr; hinges = nullptr;
+    rest_angle = rest_elen = hblk = nullptr; bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr;
+    bg = nullptr; gt_pts = nullptr; gt_tris = nullptr; dscal = nullptr; fscal = nullptr; iscal = nullptr;
+    partials = nullptr; h_iscal = nullptr; h_dscal = nullptr;
+    tri_bvh.release();
+    edge_bvh.release();
+    gt_bvh.release();
+    cap_p = cap_t = cap_e = cap_h = cap_b = cap_gp = cap_gt = 0;
+}
+
+int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, long long ngp_, long long ngt_)
+{
+    if (np_ <= cap_p && nt_ <= cap_t && ne_ <= cap_e && nh_ <= cap_h && ngp_ <= cap_gp && ngt_ <= cap_gt && dscal)
+        return PAMO_OK;
+    long long cp = np_ > cap_p ? np_ : cap_p, ct = nt_ > cap_t ? nt_ : cap_t;
+    long long ce = ne_ > cap_e ? ne_ : cap_e, ch = nh_ > cap_h ? nh_ : cap_h;
+    long long cgp = ngp_ > cap_gp ? ngp_ : cap_gp, cgt = ngt_ > cap_gt ? ngt_ : cap_gt;
+    long long cb = cap_b;
+    release();
+    cp += 1; ct += 1; ce += 1; ch += 1; cgp += 1; cgt += 1;
+#define A3(ptr, bytes)                                                   \
+    do {                                                                 \
+        if (cudaMalloc((void **)&ptr, (size_t)(bytes)) != cudaSuccess) { \
+            release();                                                   \
+            return PAMO_ERR_OOM;                                         \
+        }                                                                \
+    } while (0)
+    A3(q, cp * 16); A3(q_prev, cp * 16); A3(q_det, cp * 16); A3(p, cp * 16); A3(grad, cp * 16);
+    A3(diag, cp * 16); A3(target, cp * 16); A3(r, cp * 16); A3(z, cp * 16); A3(v, cp * 16); A3(Av, cp * 16);
+    A3(wk, cp * 4);
+    A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16);
+    A3(edges4, ce * 16);
+    A3(hinges, ch * 16); A3(rest_angle, ch * 4); A3(rest_elen, ch * 4); A3(hblk, ch * 144 * 4);
+    A3(gt_pts, cgp * 16); A3(gt_tris, cgt * 16);
+    A3(dscal, 64); A3(fscal, 64); A3(iscal, 64);
+    A3(partials, kRedBlocks * 8);
+#undef A3
+    if (cudaMallocHost((void **)&h_iscal, 64) != cudaSuccess || cudaMallocHost((void **)&h_dscal, 64) != cudaSuccess) {
+        release();
+        return PAMO_ERR_OOM;
+    }
+    cap_p = cp; cap_t = ct; cap_e = ce; cap_h = ch; cap_gp = cgp; cap_gt = cgt;
+    if (tri_bvh.ensure(ct) != cudaSuccess || edge_bvh.ensure(ce) != cudaSuccess || gt_bvh.ensure(cgt) != cudaSuccess) {
+        release();
+        return PAMO_ERR_OOM;
+    }
+    return ensure_blocks(cb > 0 ? cb : 8 * cp + 1024);
+}
+
+int Stage3::ensure_blocks(long long nb)
+{
+    if (nb <= cap_b && bidx) return PAMO_OK;
+    void *ptrs[] = {bidx, bkind, bsub, bd, bb2, bg};
+    for (void *x : ptrs)
+        if (x) cudaFree(x);
+    bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr; bg = nullptr;
+    cap_b = 0;
+    if (cudaMalloc((void **)&bidx, nb * 16) != cudaSuccess || cudaMalloc((void **)&bkind, nb * 4) != cudaSuccess ||
+        cudaMalloc((void **)&bsub, nb * 4) != cudaSuccess || cudaMalloc((void **)&bd, nb * 4) != cudaSuccess ||
+        cudaMalloc((void **)&bb2, nb * 4) != cudaSuccess || cudaMalloc((void **)&bg, nb * 64) != cudaSuccess)
+        return PAMO_ERR_OOM;
+    cap_b = nb;
+    return PAMO_OK;
+}
+
+int Stage3::register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, int n_gt_f, const float *d_v,
+                          const int *d_f, int n_v, int n_f, const int *d_e, int n_e, const int *d_h, int n_h,
+                          const float *d_vor, cudaStream_t s)
+{
+    int rc = ensure(n_v, n_f, n_e, n_h, n_gt_v, n_gt_f);
+    if (rc) return rc;
+    np = n_v; nt = n_f; ne = n_e; nh = n_h; ngp = n_gt_v; ngt = n_gt_f;
+    radius = cfg.contact_detection_radius;
+    k_aos_to_f4<<<grid_for(np), kThreads, 0, s>>>(d_v, q, q_prev, np);
+    k_aos_to_i4<<<grid_for(nt), kThreads, 0, s>>>(d_f, tris, nt, 3, 0);
+    k_aos_to_i4<<<grid_for(ne), kThreads, 0, s>>>(d_e, edges4, ne, 2, 1);
+    k_aos_to_i4<<<grid_for(nh), kThreads, 0, s>>>(d_h, hinges, nh, 4, 0);
+    k_aos_to_f4<<<grid_for(ngp), kThreads, 0, s>>>(d_gt_v, gt_pts, nullptr, ngp);
+    k_aos_to_i4<<<grid_for(ngt), kThreads, 0, s>>>(d_gt_f, gt_tris, ngt, 3, 0);
+    // Voronoi areas x GT-distance stiffness
+    S3_TRY(cudaMemcpyAsync(wk, d_vor, (size_t)np * 4, cudaMemcpyDeviceToDevice, s));
+    k_scale<<<grid_for(np), kThreads, 0, s>>>(wk, np, cfg.mesh2gt_dist_stiffness);
+    k_elastic_pre<<<grid_for(nt), kThreads, 0, s>>>(q, tris, nt, area, inv_dm);
+    k_hinge_pre<<<grid_for(nh), kThreads, 0, s>>>(q, hinges, nh, rest_angle, rest_elen);
+    S3_TRY(lbvh_build(gt_bvh, gt_pts, gt_tris, ngt, s));
+    S3_TRY(lbvh_refit(gt_bvh, gt_pts, gt_tris, ngt, s));
+    S3_TRY(lbvh_build(tri_bvh, q, tris, nt, s));
+    S3_TRY(lbvh_build(edge_bvh, q, edges4, ne, s));
+    S3_TRY(cudaMemsetAsync(iscal, 0, 64, s));
+    S3_TRY(cudaMemsetAsync(dscal, 0, 64, s));
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+int Stage3::detect(cudaStream_t s)
+{
+    // refit the hierarchies built at registration (system.py:121-152)
+    S3_TRY(lbvh_refit(tri_bvh, q, tris, nt, s));
+    S3_TRY(lbvh_refit(edge_bvh, q, edges4, ne, s));
+    for (int attempt = 0; attempt < 64; ++attempt) {
+        const float thr = 2.f * radius + cfg.d_hat;
+        S3_TRY(cudaMemsetAsync(iscal, 0, 3 * sizeof(int), s));
+        k_detect_pt<<<grid_for(np), kThreads, 0, s>>>(q, np, tris, tri_bvh.nodes, tri_bvh.vals, tri_bvh.scene, thr,
+                                                      iscal, cap_b, bidx, bkind);
+        k_detect_ee<<<grid_for(ne), kThreads, 0, s>>>(q, ne, edges4, edge_bvh.nodes, edge_bvh.vals, edge_bvh.scene, thr,
+                                                      cfg.ee_classify_thres, iscal, cap_b, bidx, bkind);
+        S3_TRY(cudaMemcpyAsync(h_iscal, iscal, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        S3_TRY(cudaStreamSynchronize(s));
+        if (h_iscal[I_STACK] > 0) return PAMO_ERR_CAPACITY;
+        long long n = h_iscal[I_NB];
+        if (n > cfg.max_blocks) {  // the reference halves the radius and retries (energy.py:940-948)
+            radius *= 0.5f;
+            continue;
+        }
+        if (n > cap_b) {
+            int rc = ensure_blocks(n + n / 4 + 1024);
+            if (rc) return rc;
+            continue;
+        }
+        return PAMO_OK;
+    }
+    return PAMO_ERR_CAPACITY;
+}
+
+static int energy_pass(Stage3 &S, cudaStream_t s)
+{
+    EArgs e{S.q, S.target, S.wk, S.np, S.nt, S.nh, S.tris, S.area, S.inv_dm,
+            S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
+            S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
+                ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
+            S.hinges, S.rest_angle, S.rest_elen, S.cfg.hinge_stiffness, S.bidx, S.bkind, S.bsub, S.bd, S.iscal, S.cap_b,
+            S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials};
+    k_energy<<<kRedBlocks, kThreads, 0, s>>>(e);
+    k_finish_sum<<<1, 32, 0, s>>>(S.partials, kRedBlocks, S.dscal + D_ENERGY);
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+static int hess_dx(Stage3 &S, const float4 *dx, float4 *out, cudaStream_t s)
+{
+    k_hess_vertex<<<grid_for(S.np), kThreads, 0, s>>>(S.wk, S.np, dx, out);
+    HArgs h{S.q, S.wk, S.np, S.nt, S.nh, S.tris, S.area, S.inv_dm,
+            S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
+            S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
+                ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
+            S.hinges, S.hblk, S.bidx, S.bg, S.bb2, S.iscal, S.cap_b, dx, out};
+    k_hess_elements<<<grid_for((long long)S.nt + S.nh + S.cap_b), kThreads, 0, s>>>(h);
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+int Stage3::newton(cudaStream_t s)
+{
+    S3_TRY(cudaMemcpyAsync(q_prev, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
+    int rc = detect(s);
+    if (rc) return rc;
+    S3_TRY(cudaMemcpyAsync(q_det, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
+    if ((rc = energy_pass(*this, s))) return rc;
+    // gradient (coefficient -1) and diagonal
+    k_diff_vertex<<<grid_for(np), kThreads, 0, s>>>(q, target, wk, np, grad, diag);
+    DArgs d{q, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
+            cfg.elas_young_modulus * cfg.elas_poisson_ratio /
+                ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
+            hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, hblk, bidx, bkind, bsub, bd, bg, bb2,
+            iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag};
+    k_diff_elements<<<grid_for((long long)nt + nh + cap_b, 128), 128, 0, s>>>(d);
+    // Jacobi-preconditioned CG (cg_solver.py:96-158)
+    k_cg_init<<<kRedBlocks, kThreads, 0, s>>>(grad, diag, np, p, r, z, v, partials);
+    k_finish_sum<<<1, 32, 0, s>>>(partials, kRedBlocks, dscal + D_ZR);
+    for (int it = 0; it < cfg.n_cg_iters; ++it) {
+        if ((rc = hess_dx(*this, v, Av, s))) return rc;
+        k_dot<<<kRedBlocks, kThreads, 0, s>>>(v, Av, np, partials);
+        k_finish_sum<<<1, 32, 0, s>>>(partials, kRedBlocks, dscal + D_VAV);
+        k_shift_zr<<<1, 1, 0, s>>>(dscal);
+        k_cg_update<<<kRedBlocks, kThreads, 0, s>>>(v, Av, diag, dscal, np, p, r, z, partials);
+        k_finish_sum<<<1, 32, 0, s>>>(partials, kRedBlocks, dscal + D_ZR);
+        k_cg_v<<<grid_for(np), kThreads, 0, s>>>(z, dscal, np, v);
+    }
+    k_clamp<<<grid_for(np), kThreads, 0, s>>>(p, q_prev, q_det, np, cfg.contact_detection_radius);
+    k_set_float<<<1, 1, 0, s>>>(fscal, 1.0f);
+    k_accd<<<grid_for(cap_b, 128), 128, 0, s>>>(q, p, bidx, bkind, iscal, cap_b, cfg.ccd_slackness, cfg.ccd_thickness,
+                                                cfg.ccd_max_iters, cfg.ee_classify_thres, fscal);
+    // line search (system.py:393-409)
+    k_copy_energy_prev<<<1, 1, 0, s>>>(dscal);
+    for (int nh_ = 0; nh_ < cfg.n_line_search_iters; ++nh_) {
+        k_line_search<<<grid_for(np), kThreads, 0, s>>>(q_prev, p, fscal, nh_, dscal, np, q);
+        if ((rc = energy_pass(*this, s))) return rc;
+    }
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+int Stage3::step(cudaStream_t s)
+{
+    if (do_nothing) return PAMO_OK;
+    S3_TRY(cudaMemsetAsync(iscal + I_STACK, 0, 4, s));
+    k_closest<<<grid_for(np), kThreads, 0, s>>>(q, np, gt_bvh.nodes, gt_bvh.vals, gt_bvh.scene, gt_pts, gt_tris, target,
+                                                iscal);
+    for (int it = 0; it < cfg.n_newton_iters; ++it) {
+        int rc = newton(s);
+        if (rc) return rc;
+    }
+    return PAMO_OK;
+}
+
+int Stage3::energy_now(double *out, cudaStream_t s)
+{
+    int rc = energy_pass(*this, s);
+    if (rc) return rc;
+    S3_TRY(cudaMemcpyAsync(h_dscal, dscal, 8, cudaMemcpyDeviceToHost, s));
+    S3_TRY(cudaStreamSynchronize(s));
+    *out = h_dscal[0];
+    return PAMO_OK;
+}
+
+}  // namespace s3
+
+int s3_validate(const int *a, long long count, int hi, int *d_bad, int *h_bad, cudaStream_t st)
+{
+    if (count <= 0) return PAMO_OK;
+    if (cudaMemsetAsync(d_bad, 0, 4, st) != cudaSuccess) return PAMO_ERR_DEVICE;
+    s3::k_validate_idx<<<grid_for(count), kThreads, 0, st>>>(a, count, hi, d_bad);
+    if (cudaMemcpyAsync(h_bad, d_bad, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PAMO_ERR_DEVICE;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return PAMO_ERR_DEVICE;
+    return *h_bad == 0 ? PAMO_OK : PAMO_ERR_INVALID_ARG;
+}
+
+int s3_fetch(const float4 *q, float *out, int n, cudaStream_t st)
+{
+    s3::k_f4_to_aos<<<grid_for(n), kThreads, 0, st>>>(q, out, n);
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+}  // namespace pamo

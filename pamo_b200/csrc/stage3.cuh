@@ -1,0 +1,71 @@
+// Stage-3 safe projection on the device (sm_100a): barrier-energy Newton
+// iterations with a matrix-free Jacobi-PCG, contact detection on LBVHs, additive
+// CCD and a halving line search (simp_cuda/safe_project/src/pamo_safe_project:
+// system.py:411-470, cg_solver.py:46-158, energy.py, kernels/*).
+//
+// Precision: positions, distances, gradients and the CG vectors are FP32; the
+// barrier value and its derivatives for d < d_hat, the CCD step search, the
+// energy sums and the CG dot products are FP64.
+#pragma once
+
+#include "../../include/pamo_b200.h"
+#include "common.cuh"
+#include "lbvh.cuh"
+
+namespace pamo {
+namespace s3 {
+
+struct Stage3 {
+    int device = 0;
+    pamo_s3_config cfg{};
+    long long cap_p = 0, cap_t = 0, cap_e = 0, cap_h = 0, cap_b = 0, cap_gp = 0, cap_gt = 0;
+    int np = 0, nt = 0, ne = 0, nh = 0, ngp = 0, ngt = 0;
+    float radius = 0.f;
+    bool do_nothing = false;
+
+    // per vertex (xyz in float4, w unused)
+    float4 *q = nullptr, *q_prev = nullptr, *q_det = nullptr, *p = nullptr, *grad = nullptr, *diag = nullptr;
+    float4 *target = nullptr, *r = nullptr, *z = nullptr, *v = nullptr, *Av = nullptr;
+    float *wk = nullptr;  // Voronoi area x GT-distance stiffness
+    // per triangle / edge / hinge
+    int4 *tris = nullptr;
+    float *area = nullptr;
+    float4 *inv_dm = nullptr;  // 2x2 row-major
+    int4 *edges4 = nullptr;    // (a, b, b, 0): a segment as a degenerate triangle for the LBVH
+    int4 *hinges = nullptr;
+    float *rest_angle = nullptr, *rest_elen = nullptr;
+    float *hblk = nullptr;  // 16 3x3 blocks per hinge (SPD-projected)
+    // contact blocks
+    int4 *bidx = nullptr;
+    int *bkind = nullptr, *bsub = nullptr;
+    float *bd = nullptr, *bb2 = nullptr;
+    float4 *bg = nullptr;  // 4 gradient vectors per block
+    // hierarchies
+    Lbvh tri_bvh, edge_bvh, gt_bvh;
+    float4 *gt_pts = nullptr;
+    int4 *gt_tris = nullptr;
+    // scalars and reduction partials
+    double *dscal = nullptr;  // [0] energy [1] energy_prev [2] zr [3] zr_last [4] vAv
+    float *fscal = nullptr;   // [0] ccd step
+    int *iscal = nullptr;     // [0] block count [1] overflow [2] stack overflow
+    double *partials = nullptr;
+    int *h_iscal = nullptr;   // pinned
+    double *h_dscal = nullptr;
+
+    int ensure(long long np_, long long nt_, long long ne_, long long nh_, long long ngp_, long long ngt_);
+    int ensure_blocks(long long nb);
+    void release();
+
+    // Inputs are device arrays in the normalised frame.
+    int register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, int n_gt_f, const float *d_v,
+                      const int *d_f, int n_v, int n_f, const int *d_e, int n_e, const int *d_h, int n_h,
+                      const float *d_vor, cudaStream_t s);
+    int step(cudaStream_t s);
+    int newton(cudaStream_t s);
+    int detect(cudaStream_t s);
+    // diagnostics
+    int energy_now(double *out, cudaStream_t s);
+};
+
+}  // namespace s3
+}  // namespace pamo

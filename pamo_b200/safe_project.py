@@ -1,0 +1,220 @@
+"""Stage 3 (safe projection) host side; mirrors pamo_safe_project
+(simp_cuda/safe_project/src/pamo_safe_project): ``Stage3Config``,
+``Stage3System`` and ``process(gt_V, gt_F, V, F, n_iters, system, config)``.
+
+The host does what the reference does on the CPU before its GPU loop: the
+normalisation by the ground truth (processing.py:15-20,57-59) in float64, the
+unique edges, the hinges (one per interior edge, hinge_energy.py:21-57), the
+Voronoi vertex areas (the mixed areas of Meyer et al. 2003, which
+igl.massmatrix(VORONOI) computes, system.py:223-225) and the small-angle guard
+(system.py:217-221).  Everything after that -- closest points on the ground
+truth, contact detection, energies, Jacobi-PCG, CCD, line search -- runs in
+libpamo_b200.so (csrc/stage3.cu) through pamo_safe_project().
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import Context, check
+
+
+class pamo_s3_config(ctypes.Structure):
+    _fields_ = [("n_newton_iters", ctypes.c_int), ("n_cg_iters", ctypes.c_int), ("n_line_search_iters", ctypes.c_int),
+                ("ccd_max_iters", ctypes.c_int), ("spd_max_iters", ctypes.c_int), ("d_hat", ctypes.c_float),
+                ("coll_stiffness", ctypes.c_float), ("contact_detection_radius", ctypes.c_float),
+                ("ee_classify_thres", ctypes.c_float), ("ccd_slackness", ctypes.c_float),
+                ("ccd_thickness", ctypes.c_float), ("elas_young_modulus", ctypes.c_float),
+                ("elas_poisson_ratio", ctypes.c_float), ("hinge_stiffness", ctypes.c_float),
+                ("mesh2gt_dist_stiffness", ctypes.c_float), ("max_blocks", ctypes.c_longlong)]
+
+
+class Stage3Config:
+    """The reference's Stage3Config defaults (config.py:6-73) for the default
+    energy set (GT distance, membrane, bending, contact)."""
+
+    def __init__(self):
+        self.debug = False
+        self.seed = 0
+        self.max_particles = 1 << 20
+        self.max_blocks = 1 << 25
+        self.max_gt_particles = 1 << 24
+        self.max_gt_samples = 1 << 14
+        self.n_newton_iters = 10
+        self.n_cg_iters = 40
+        self.cg_precond = "jacobi"
+        self.use_cuda_graph = True
+        self.n_line_search_iters = 10
+        self.detect_contact_every = "newton"
+        self.system_scale = 1.0
+        self.d_hat = 1e-3
+        self.coll_stiffness = 1e2
+        self.contact_detection_radius = 1e-2
+        self.ee_classify_thres = 1e-3
+        self.ccd_slackness = 0.7
+        self.ccd_thickness = 1e-6
+        self.ccd_max_iters = 100
+        self.spd_max_iters = 3
+        self.elas_young_modulus = 1e-1
+        self.elas_poisson_ratio = 0.0
+        self.curv_stiffness = 1e-8
+        self.hinge_stiffness = 1e-2
+        self.mesh2gt_dist_stiffness = 1e3
+        self.gt2mesh_dist_stiffness = 1e3
+        self.min_angle_thres = 0.0
+
+    def to_c(self) -> pamo_s3_config:
+        if self.cg_precond != "jacobi" or self.detect_contact_every != "newton":
+            raise NotImplementedError("only the reference's default solver settings are supported")
+        c = pamo_s3_config()
+        for name, _ in pamo_s3_config._fields_:
+            setattr(c, name, getattr(self, name))
+        return c
+
+
+# ------------------------------------------------------------ host preprocessing
+def normalization(V):
+    """processing.py:15-20."""
+    center = np.mean(V, axis=0)
+    extents = np.max(V, axis=0) - np.min(V, axis=0)
+    scale = 1.0 / np.max(extents)
+    return scale, -center * scale
+
+
+def edges_unique(F):
+    e = np.sort(np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]]), axis=1)
+    return np.unique(e, axis=0)
+
+
+def hinges(F):
+    """(x0, x1, x2, x3) per interior edge: the face with directed edge x1->x2
+    (x1 < x2) and the face with x2->x1; x0 / x3 their opposite vertices."""
+    F = np.asarray(F, np.int64)
+    D = np.concatenate([np.stack([F[:, k], F[:, (k + 1) % 3], F[:, (k + 2) % 3]], 1) for k in range(3)])
+    n = int(F.max()) + 1 if len(F) else 1
+    fwd = D[D[:, 0] < D[:, 1]]
+    bwd = D[D[:, 0] > D[:, 1]]
+    kf = fwd[:, 0] * n + fwd[:, 1]
+    kb = bwd[:, 1] * n + bwd[:, 0]
+    ob = np.argsort(kb, kind="stable")
+    kbs = kb[ob]
+    pos = np.searchsorted(kbs, kf)
+    ok = (pos < len(kbs)) & (kbs[np.minimum(pos, max(len(kbs) - 1, 0))] == kf) if len(kbs) else np.zeros(len(kf), bool)
+    H = np.stack([fwd[ok, 2], fwd[ok, 0], fwd[ok, 1], bwd[ob][pos[ok], 2]], 1)
+    return H[np.lexsort((H[:, 2], H[:, 1]))]
+
+
+def voronoi_areas(V, F):
+    """Mixed Voronoi vertex areas (Meyer, Desbrun, Schroeder, Barr 2003)."""
+    a, b, c = V[F[:, 0]], V[F[:, 1]], V[F[:, 2]]
+    ea, eb, ec = c - b, a - c, b - a
+    la2, lb2, lc2 = (ea * ea).sum(1), (eb * eb).sum(1), (ec * ec).sum(1)
+    area = 0.5 * np.linalg.norm(np.cross(ec, -eb), axis=1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        cos_a = -(eb * ec).sum(1) / np.sqrt(lb2 * lc2)
+        cos_b = -(ec * ea).sum(1) / np.sqrt(lc2 * la2)
+        cos_c = -(ea * eb).sum(1) / np.sqrt(la2 * lb2)
+        cot = lambda cs: cs / np.sqrt(np.maximum(1 - cs * cs, 0))
+        ca, cb, cc = cot(cos_a), cot(cos_b), cot(cos_c)
+    vor = np.stack([(lb2 * cb + lc2 * cc) / 8, (lc2 * cc + la2 * ca) / 8, (la2 * ca + lb2 * cb) / 8], 1)
+    mix = np.stack([np.where(cos_a < 0, area / 2, area / 4), np.where(cos_b < 0, area / 2, area / 4),
+                    np.where(cos_c < 0, area / 2, area / 4)], 1)
+    obtuse = (cos_a < 0) | (cos_b < 0) | (cos_c < 0)
+    w = np.where(obtuse[:, None], mix, vor)
+    out = np.zeros(len(V))
+    for k in range(3):
+        np.add.at(out, F[:, k], w[:, k])
+    return out
+
+
+def min_internal_angle_deg(V, F):
+    a, b, c = V[F[:, 0]], V[F[:, 1]], V[F[:, 2]]
+    ang = []
+    for p, q, r in ((a, b, c), (b, c, a), (c, a, b)):
+        u, v = q - p, r - p
+        cs = (u * v).sum(1) / (np.linalg.norm(u, axis=1) * np.linalg.norm(v, axis=1))
+        ang.append(np.arccos(np.clip(cs, -1, 1)))
+    return float(np.min(ang) * 180 / np.pi) if len(F) else 180.0
+
+
+def merge_vertices(V, F, digits=8):
+    """trimesh.Trimesh(process=True) merging (PaMO.run's stage2_mesh,
+    pamo/__init__.py:194): vertices equal after rounding to `digits` decimals
+    become one; unreferenced vertices are kept in order like trimesh keeps them
+    after merging."""
+    V = np.asarray(V, np.float64)
+    key = np.round(V, digits)
+    _, first, inv = np.unique(key, axis=0, return_index=True, return_inverse=True)
+    order = np.argsort(first)
+    rank = np.empty_like(order)
+    rank[order] = np.arange(len(order))
+    newF = rank[inv.reshape(-1)][np.asarray(F)]
+    return V[first[order]], newF
+
+
+class Stage3System:
+    """Device state for stage 3 (one pamo_ctx)."""
+
+    def __init__(self, config: Stage3Config | None = None, device=0):
+        self.config = config or Stage3Config()
+        if isinstance(device, str):
+            device = int(device.split(":")[1]) if ":" in device else 0
+        self.device = device
+        self.ctx = Context(device)
+        self.last_stats = None
+
+    def clear(self):
+        self.last_stats = None
+
+    def project(self, gt_V, gt_F, V, F, n_steps):
+        """Normalised-frame arrays in, projected vertices (float32) out."""
+        import torch
+
+        c = self.config
+        dev = torch.device("cuda", self.device)
+        V64 = np.asarray(V, np.float64) * c.system_scale
+        gV = np.asarray(gt_V, np.float64) * c.system_scale
+        F = np.asarray(F, np.int64)
+        E = edges_unique(F)
+        H = hinges(F)
+        if len(H) != len(E):
+            raise ValueError(f"number of hinges {len(H)} != number of edges {len(E)} (mesh not closed 2-manifold)")
+        vor = voronoi_areas(V64, F)
+        do_nothing = min_internal_angle_deg(V64, F) <= c.min_angle_thres
+        t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
+        d_gv, d_gf = t(gV, np.float32), t(gt_F, np.int32)
+        d_v, d_f = t(V64, np.float32), t(F, np.int32)
+        d_e, d_h, d_w = t(E, np.int32), t(H, np.int32), t(vor, np.float32)
+        out = torch.empty((len(V64), 3), dtype=torch.float32, device=dev)
+        cfg = c.to_c()
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        check("pamo_safe_project", _lib.lib().pamo_safe_project(
+            self.ctx.handle, d_gv.data_ptr(), d_gf.data_ptr(), len(gV), len(d_gf), d_v.data_ptr(), d_f.data_ptr(),
+            len(V64), len(F), d_e.data_ptr(), len(E), d_h.data_ptr(), len(H), d_w.data_ptr(), int(n_steps),
+            int(do_nothing), ctypes.byref(cfg), stream, out.data_ptr()))
+        st = (ctypes.c_double * 3)()
+        _lib.lib().pamo_safe_project_stats(self.ctx.handle, st)
+        self.last_stats = {"energy": st[0], "contacts": int(st[1]), "newton_iters": int(st[2]),
+                           "do_nothing": bool(do_nothing)}
+        return out.cpu().numpy() / c.system_scale
+
+
+def process(gt_V, gt_F, stage2_V, stage2_F, n_iters, system: Stage3System | None = None,
+            config: Stage3Config | None = None, eval=False, return_curve=False):
+    """processing.py:23-108: normalise by the ground truth, project, undo the
+    normalisation.  Faces are returned unchanged."""
+    if system is None:
+        system = Stage3System(config or Stage3Config())
+    else:
+        system.clear()
+    scale, t = normalization(np.asarray(gt_V, np.float64))
+    gV = np.asarray(gt_V, np.float64) * scale + t
+    sV = np.asarray(stage2_V, np.float64) * scale + t
+    q = system.project(gV, gt_F, sV, stage2_F, n_iters).astype(np.float64)
+    return (q - t) / scale, np.asarray(stage2_F)
+
+
+def __getattr__(name):  # the reference exposes the defaults through .config / .system
+    raise AttributeError(name)
