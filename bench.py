@@ -164,10 +164,30 @@ def reference_arm(args):
     return 0
 
 
+def cpu_baseline_sample(args, V, F, ratio):
+    """The CPU restatement (oracle/, OpenMP on all host threads) on the first
+    `sample_rounds` rounds of the same run, extrapolated by face-rounds."""
+    from oracle import oracle as O
+
+    target = int(ratio * len(F))
+    tm = O.tris_mean(V, F)
+    Vc = (V - tm).astype(np.float32)
+    Fs = O.shuffle_faces(F)
+    o = O.Stage2Oracle()
+    t0 = time.perf_counter()
+    o.run(Vc, Fs, target, 4, 1e-3, args.sample_rounds)
+    t = time.perf_counter() - t0
+    frac = _sample_fraction(args, args.sample_rounds)
+    total = t / frac if frac else float("nan")
+    return {"value": len(F) / 1e6 / total, "unit": "Mfaces/s", "cores": O.lib().s2o_num_threads(), "kind": "port",
+            "sample": f"first {args.sample_rounds} rounds ({(frac or 0) * 100:.1f}% of the run's face-rounds, "
+                      f"{t:.1f} s), extrapolated by face-rounds"}
+
+
 def _sample_fraction(args, sample_rounds):
     """Share of face-rounds covered by the first `sample_rounds` rounds, from the
-    round sizes of a run of the same workload (cached under _cache/)."""
-    path = os.path.join(ROOT, "profiles", f"round_sizes_{args.workload}.json")
+    recorded round sizes of the same workload (tests/golden/<workload>_round_faces.json)."""
+    path = os.path.join(ROOT, "tests", "golden", f"{args.workload}_round_faces.json")
     try:
         sizes = json.load(open(path))["faces_in"]
     except Exception:
@@ -294,6 +314,9 @@ def product_arm(args):
     rounds = rr.value
     stats = (ctypes.c_longlong * 8)()
     L.pamo_stage2_last_round_stats(ctx.handle, stats)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args, V, F, ratio)
     if rank == 0:
         value = ws * nF / 1e6 / (ms_max / 1e3)
         e2e = ws * nF / 1e6 / (e2e_ms / 1e3)
@@ -309,6 +332,7 @@ def product_arm(args):
             "e2e": {"value": e2e, "unit": "Mfaces/s", "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
                     "d2h_bytes_per_step": int(d2h)},
             "clocks": clocks,
+            "cpu_baseline": cpu,
             "phases_ms": {k: round(v["ms"], 3) for k, v in phases.items()},
             "roofline": roofline_edge_cost(phases, round_faces, peaks),
             "round_faces": round_faces if args.dump_rounds else None,
@@ -327,7 +351,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2"])
-    ap.add_argument("--sample-rounds", type=int, default=3)
+    ap.add_argument("--sample-rounds", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dump-rounds", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
