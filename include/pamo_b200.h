@@ -183,6 +183,23 @@ int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int
 int pamo_safe_project_stats(pamo_ctx *ctx, double *h_out3);
 
 /*
+ * pamo_self_intersect without any allocation (no counterpart in the reference).
+ * For callers that may not allocate device memory themselves or have the
+ * library do it: a host application that owns all device memory through its own
+ * pool, or a latency-critical loop where cudaMalloc/cudaFree would synchronise
+ * the device and stall its other streams.  Same inputs and output as
+ * pamo_self_intersect, with no context.  All scratch lives in one ~11 MB
+ * file-scope device array that every GPU loading the library holds until the
+ * process exits.  Limits: n_tris <= 32768, n_pts <= 65536 and at most 24
+ * candidate pairs per face; larger inputs return PAMO_ERR_CAPACITY.  The first
+ * call on each device looks up the array's device address (do that first call
+ * before any stream capture).  Every call shares the array: calls that overlap
+ * on the GPU, on any stream, race and must be serialised by the caller.
+ */
+int pamo_self_intersect_noalloc(const float *d_points, const int *d_tris, int n_pts, int n_tris,
+                                unsigned char *d_out_flags, long long *out_n_pairs, void *stream);
+
+/*
  * Host-pointer simplifier.  Same signature and meaning as the reference's
  * Blender C ABI pamo_simplify (pamo_blender/cusimpinterface.cu:57): rounds until
  * four rounds without progress, output written to caller buffers sized like the

@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I", os.path.join(ROOT, "include")]
 # translation units whose arithmetic must round exactly like the reference
-NO_FMA = {"stage2.cu", "lbvh.cu", "scan.cu", "abi.cu", "shuffle.cu", "s2_noalloc.cu"}
+NO_FMA = {"stage2.cu", "lbvh.cu", "scan.cu", "abi.cu", "shuffle.cu", "noalloc.cu"}
 
 
 def sources():

@@ -1027,6 +1027,15 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     return PAMO_OK;
 }
 
+cudaError_t query_and_test_pairs(const BvhNode *nodes, const int *vals, const int *scene, const float4 *pts,
+                                 const int4 *tris, const uint8_t *active, int m, uint2 *pairs, long long cap_pairs,
+                                 RoundCounters *cnt, uint8_t *isect, cudaStream_t s)
+{
+    k_query<<<grid_for(m), kThreads, 0, s>>>(nodes, vals, scene, pts, tris, active, m, pairs, cap_pairs, cnt);
+    k_pairs<<<grid_for(cap_pairs), kThreads, 0, s>>>(pairs, cnt, cap_pairs, pts, tris, isect, 1e-3f);
+    return cudaGetLastError();
+}
+
 int Stage2::self_intersect_all(int n, int m, cudaStream_t s)
 {
     // faces of opts/otris; every live face queries the hierarchy

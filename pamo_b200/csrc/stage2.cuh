@@ -128,4 +128,10 @@ struct Stage2 {
 
 int stage2_shuffle_faces(int4 *tris, int m, cudaStream_t s);  // reference init permutation
 
+// Hierarchy query of the faces flagged in `active` and the pair tests, on
+// caller-provided buffers (cnt->n_pairs / pair_overflow must be zero).
+cudaError_t query_and_test_pairs(const BvhNode *nodes, const int *vals, const int *scene, const float4 *pts,
+                                 const int4 *tris, const uint8_t *active, int m, uint2 *pairs, long long cap_pairs,
+                                 RoundCounters *cnt, uint8_t *isect, cudaStream_t s);
+
 }  // namespace pamo
