@@ -113,15 +113,14 @@ def workload(name):
 
 
 def dist_init(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from pamo_b200 import replicas
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch
 
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        torch.cuda.set_device(local)
+    ws, rank = replicas.init("nccl", timeout_s=600.0)
     return ws, rank, local
 
 
@@ -241,7 +240,7 @@ def product_arm(args):
 
     def run_resident():
         _lib.check("pamo_stage2_run", L.pamo_stage2_run(ctx.handle, Pd.data_ptr(), Fd.data_ptr(), len(V), nF, target,
-                                                        4, 1e-3, 1000000, sp, ctypes.byref(on), ctypes.byref(om),
+                                                        4, 1e-3, args.iters, sp, ctypes.byref(on), ctypes.byref(om),
                                                         ctypes.byref(rr)))
 
     # pinned host buffers for the end-to-end leg
@@ -256,7 +255,7 @@ def product_arm(args):
         Pe.copy_(Ph, non_blocking=True)
         Fe.copy_(Fh, non_blocking=True)
         _lib.check("pamo_stage2_run", L.pamo_stage2_run(ctx.handle, Pe.data_ptr(), Fe.data_ptr(), len(V), nF, target,
-                                                        4, 1e-3, 1000000, sp, ctypes.byref(on), ctypes.byref(om),
+                                                        4, 1e-3, args.iters, sp, ctypes.byref(on), ctypes.byref(om),
                                                         ctypes.byref(rr)))
         _lib.check("pamo_stage2_fetch", L.pamo_stage2_fetch(ctx.handle, out_v.data_ptr(), out_f.data_ptr(), 1, sp))
         return on.value * 12 + om.value * 12
@@ -276,11 +275,13 @@ def product_arm(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    launches0 = L.pamo_launch_count()
     ev0.record(s)
     for _ in range(args.steps):
         run_resident()
     ev1.record(s)
     torch.cuda.synchronize()
+    launches = L.pamo_launch_count() - launches0
     dev_ms = ev0.elapsed_time(ev1) / args.steps
     # end-to-end leg with host buffers, per-step latencies
     lat = []
@@ -291,6 +292,30 @@ def product_arm(args):
         d2h = run_e2e()
         torch.cuda.synchronize()
         lat.append(time.perf_counter() - t0)
+    stage3 = None
+    if args.stage3:
+        # PaMO.run with stage 3 (safe projection against the input, 5 steps), the
+        # public drop-in: host arrays in, host arrays out, stage 2 then stage 3
+        pm = pamo_b200.PaMO((V, F), use_stage1=False, use_stage3=True, device=local, verbose=False)
+        Ph3 = torch.from_numpy(V).pin_memory()
+        Fh3 = torch.from_numpy(F).pin_memory()
+        pm.run(Ph3.to(dev), Fh3.to(dev), ratio, min_verts=0)  # warm-up (allocations)
+        t3 = []
+        for _ in range(max(1, min(args.steps, 3))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            vv, ff = pm.run(Ph3.to(dev, non_blocking=True), Fh3.to(dev, non_blocking=True), ratio, min_verts=0)
+            torch.cuda.synchronize()
+            t3.append((time.perf_counter() - t0, dict(pm.timings)))
+        tt = float(np.median([x[0] for x in t3]))
+        stage3 = {"e2e_all_stages": {"value": nF / 1e6 / tt, "unit": "Mfaces/s", "ms": tt * 1e3,
+                                     "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
+                                     "d2h_bytes_per_step": int(vv.nbytes + ff.nbytes)},
+                  "stage2_ms": float(np.median([x[1]["stage2"] for x in t3])) * 1e3,
+                  "stage3_ms": float(np.median([x[1]["stage3"] for x in t3])) * 1e3,
+                  "stage3_stats": pm.system.last_stats,
+                  "what": "PaMO((V,F), use_stage1=False, use_stage3=True).run(V, F, ratio, min_verts=0) "
+                          "from pinned host tensors; stage 1 is not built"}
     clocks = clk.stop()
     # one more run with per-phase CUDA events (outside the timed region)
     L.pamo_profile_enable(ctx.handle, 1)
@@ -307,10 +332,9 @@ def product_arm(args):
     ms_max = dev_ms
     e2e_ms = float(np.mean(lat)) * 1e3
     if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([dev_ms, e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max, e2e_ms = float(t[0]), float(t[1])
+        from pamo_b200 import replicas
+
+        ms_max, e2e_ms = replicas.max_over_ranks([dev_ms, e2e_ms], device=dev)
     rounds = rr.value
     stats = (ctypes.c_longlong * 8)()
     L.pamo_stage2_last_round_stats(ctx.handle, stats)
@@ -326,8 +350,9 @@ def product_arm(args):
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "stages": "2 (stage-2 loop of PaMO.run)", "faces_out": om.value,
-                       "verts_out": on.value, "rounds": rounds, "l2": "inputs/working set > L2, no flush",
+                       "verts_out": on.value, "rounds": rounds, "iters": args.iters, "l2": "inputs/working set > L2, no flush",
                        "parallelism": f"replicas x{ws}"},
+            "gpu_launches": int(launches),
             "latency_ms": {"p50": float(np.percentile(lat, 50)) * 1e3, "p99": float(np.percentile(lat, 99)) * 1e3},
             "e2e": {"value": e2e, "unit": "Mfaces/s", "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
                     "d2h_bytes_per_step": int(d2h)},
@@ -336,11 +361,236 @@ def product_arm(args):
             "phases_ms": {k: round(v["ms"], 3) for k, v in phases.items()},
             "roofline": roofline_edge_cost(phases, round_faces, peaks),
             "round_faces": round_faces if args.dump_rounds else None,
+            "stage3": stage3,
         }
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+    return 0
+
+
+def _plain_runs(ctx, L, meshes, dev, sp, torch):
+    """The plain drop-in: one pamo_stage2_run per mesh, one after another, on
+    device-resident inputs; returns per-mesh completion times (s) from the start."""
+    done = []
+    on, om, rr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    from pamo_b200 import _lib
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for (Pd, Fd, target) in meshes:
+        _lib.check("pamo_stage2_run", L.pamo_stage2_run(ctx.handle, Pd.data_ptr(), Fd.data_ptr(), Pd.shape[0],
+                                                        Fd.shape[0], target, 4, 1e-3, 1000000, sp, ctypes.byref(on),
+                                                        ctypes.byref(om), ctypes.byref(rr)))
+        done.append(time.perf_counter() - t0)
+    torch.cuda.synchronize()
+    return done
+
+
+def batched_arm(args):
+    """256 meshes of uneven sizes (face counts log-uniform in [5k, 500k]; displaced
+    spheres, noisy tori, thin-shell pairs; ratios 0.001 / 0.01 / 0.05), simplified
+    (stage 2, PaMO.run's loop with min_verts 0) by the batch engine and by the
+    plain per-mesh drop-in one after another.  A step = the whole list."""
+    import torch
+
+    from pamo_b200 import _lib
+    from pamo_b200 import meshgen as mg
+    from pamo_b200.batch import BatchEngine, target_faces
+
+    ws, rank, local = dist_init(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    t_gen = time.perf_counter()
+    mix = mg.mixed_batch(args.n_meshes, seed=args.seed)
+    t_gen = time.perf_counter() - t_gen
+    total_faces = sum(len(F) for _, _, F, _ in mix)
+    targets = [target_faces(len(F), r, 0) for _, _, F, r in mix]
+    dmeshes = [(torch.from_numpy(V).to(dev), torch.from_numpy(F).to(dev), t) for (_, V, F, _), t in zip(mix, targets)]
+    hmeshes = [(torch.from_numpy(V).pin_memory(), torch.from_numpy(F).pin_memory(), t)
+               for (_, V, F, _), t in zip(mix, targets)]
+    max_v = sum(len(V) for _, V, _, _ in mix)
+    eng = BatchEngine(device=local, max_verts=max_v, max_faces=total_faces, max_meshes=len(mix))
+    L = _lib.lib()
+
+    def run_batch(host: bool):
+        """All meshes through the engine; returns (seconds, per-mesh completion
+        times, bytes copied in, bytes copied out)."""
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        src = hmeshes if host else dmeshes
+        jobs = []
+        for (P, F, t) in src:
+            jobs.append(eng.submit(P, F, target=t) if not host else
+                        eng.submit(P.numpy(), F.numpy(), target=t))
+        finish = {}
+        while True:
+            r, p = eng.step()
+            now = time.perf_counter() - t0
+            for j in jobs:
+                if j not in finish and eng.job(j)["state"] == 2:
+                    finish[j] = now
+            if r == 0 and p == 0:
+                break
+        out_bytes = 0
+        results = []
+        for j in jobs:
+            info = eng.job(j)
+            if host:
+                V, F = eng.result(j)
+                out_bytes += V.nbytes + F.nbytes
+            else:
+                V = torch.empty((info["n_pts"], 3), dtype=torch.float32, device=dev)
+                F = torch.empty((info["n_tris"], 3), dtype=torch.int32, device=dev)
+                _lib.check("pamo_batch_fetch", L.pamo_batch_fetch(eng.handle, j, V.data_ptr(), F.data_ptr(), 0))
+                eng.release(j)
+            results.append(info)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        in_bytes = sum(P.numel() * 4 + F.numel() * 4 for P, F, _ in src) if host else 0
+        return dt, [finish[j] for j in jobs], in_bytes, out_bytes, results
+
+    for _ in range(args.warmup):
+        run_batch(False)
+    clk = ClockSampler(local)
+    clk.start()
+    for _ in range(100):
+        if clk.samples or clk.error:
+            break
+        time.sleep(0.05)
+    launches0 = L.pamo_launch_count()
+    step_s, lat = [], []
+    for _ in range(args.steps):
+        dt, fin, _, _, res = run_batch(False)
+        step_s.append(dt)
+        lat.extend(fin)
+    launches = L.pamo_launch_count() - launches0
+    e2e_dt, _, bi, bo, _ = run_batch(True)
+    clocks = clk.stop()
+    # the plain per-mesh drop-in on the same meshes (same device, fresh context)
+    import pamo_b200
+
+    ctx = pamo_b200.Context(local)
+    sp = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    plain_done = _plain_runs(ctx, L, dmeshes, dev, sp, torch)
+    plain_s = plain_done[-1]
+    t = float(np.median(step_s))
+    faces_out = sum(r["n_tris"] for r in res)
+    if rank == 0:
+        line = {
+            "metric": "input Mfaces/s", "value": total_faces / 1e6 / t, "unit": "Mfaces/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched: {len(mix)} meshes, {total_faces:,} faces (log-uniform 5k..500k; "
+                                   f"spheres / tori / thin-shell pairs; ratios 0.001/0.01/0.05), stage 2, "
+                                   f"min_verts 0", "faces_out": faces_out, "engine": "pamo_batch (one packed round "
+                                   "per step for every running mesh)", "mesh_generation_s": round(t_gen, 1)},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)) * 1e3, "p99": float(np.percentile(lat, 99)) * 1e3,
+                           "what": "per mesh, submit of the whole list to its result"},
+            "plain": {"value": total_faces / 1e6 / plain_s, "unit": "Mfaces/s", "ms": plain_s * 1e3,
+                      "latency_ms": {"p50": float(np.percentile(plain_done, 50)) * 1e3,
+                                     "p99": float(np.percentile(plain_done, 99)) * 1e3},
+                      "what": "pamo_stage2_run per mesh, one after another, same inputs"},
+            "e2e": {"value": total_faces / 1e6 / e2e_dt, "unit": "Mfaces/s", "h2d_bytes_per_step": int(bi),
+                    "d2h_bytes_per_step": int(bo)},
+            "gpu_launches": int(launches), "clocks": clocks,
+        }
+        print(json.dumps(line))
+    eng.close()
+    return 0
+
+
+def serving_arm(args):
+    """Continuous batching under Poisson arrivals: requests (face counts
+    log-uniform in [10k, 2M], the same mesh families, ratios 0.001/0.01/0.05)
+    arrive at each swept rate; between collapse rounds the engine admits what
+    has arrived and fits, so new requests overlap the running ones.  Reported
+    per rate: throughput (input faces / makespan) and p50/p99 latency (arrival
+    to result on the host), beside the plain drop-in serving the same arrivals
+    one request at a time."""
+    import torch
+
+    import pamo_b200
+    from pamo_b200 import _lib
+    from pamo_b200 import meshgen as mg
+    from pamo_b200.batch import BatchEngine, target_faces
+
+    ws, rank, local = dist_init(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(args.seed)
+    # a pool of distinct request meshes; requests draw from it
+    pool = mg.mixed_batch(args.pool, fmin=10_000, fmax=2_000_000, seed=args.seed)
+    pool = [(V, F, r) for _, V, F, r in pool]
+    L = _lib.lib()
+    ctx = pamo_b200.Context(local)
+    sp = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    max_f = args.serve_max_faces
+    eng = BatchEngine(device=local, max_faces=max_f, max_meshes=args.n_meshes)
+    rates = [float(x) for x in args.rates.split(",")]
+    out = []
+    clk = ClockSampler(local)
+    clk.start()
+    for rate in rates:
+        n_req = args.requests
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+        picks = rng.integers(0, len(pool), n_req)
+        faces = sum(len(pool[k][1]) for k in picks)
+        # batched, continuous admission
+        t0 = time.perf_counter()
+        nxt, live, lat = 0, {}, []
+        while nxt < n_req or live:
+            now = time.perf_counter() - t0
+            while nxt < n_req and arrivals[nxt] <= now:
+                V, F, r = pool[picks[nxt]]
+                live[eng.submit(V, F, target=target_faces(len(F), r, 0))] = arrivals[nxt]
+                nxt += 1
+            if not live:
+                time.sleep(max(0.0, min(arrivals[nxt] - now, 0.01)))
+                continue
+            eng.step()
+            for j in list(live):
+                if eng.job(j)["state"] == 2:
+                    eng.result(j)
+                    lat.append(time.perf_counter() - t0 - live.pop(j))
+        span = time.perf_counter() - t0
+        # plain: the same arrivals served one at a time (host in, host out)
+        t0 = time.perf_counter()
+        plat = []
+        on, om, rr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        for k in range(n_req):
+            now = time.perf_counter() - t0
+            if arrivals[k] > now:
+                time.sleep(arrivals[k] - now)
+            V, F, r = pool[picks[k]]
+            Pd = torch.from_numpy(V).to(dev)
+            Fd = torch.from_numpy(F).to(dev)
+            _lib.check("pamo_stage2_run", L.pamo_stage2_run(
+                ctx.handle, Pd.data_ptr(), Fd.data_ptr(), len(V), len(F), target_faces(len(F), r, 0), 4, 1e-3,
+                1000000, sp, ctypes.byref(on), ctypes.byref(om), ctypes.byref(rr)))
+            ov = np.empty((on.value, 3), np.float32)
+            of = np.empty((om.value, 3), np.int32)
+            _lib.check("pamo_stage2_fetch", L.pamo_stage2_fetch(ctx.handle, ov.ctypes.data, of.ctypes.data, 1, sp))
+            plat.append(time.perf_counter() - t0 - arrivals[k])
+        pspan = time.perf_counter() - t0
+        out.append({"rate_req_s": rate, "requests": n_req, "input_faces": int(faces),
+                    "batched": {"Mfaces_s": faces / 1e6 / span, "p50_ms": float(np.percentile(lat, 50)) * 1e3,
+                                "p99_ms": float(np.percentile(lat, 99)) * 1e3, "makespan_s": span},
+                    "plain": {"Mfaces_s": faces / 1e6 / pspan, "p50_ms": float(np.percentile(plat, 50)) * 1e3,
+                              "p99_ms": float(np.percentile(plat, 99)) * 1e3, "makespan_s": pspan}})
+    clocks = clk.stop()
+    best = max(out, key=lambda o: o["batched"]["Mfaces_s"])
+    if rank == 0:
+        line = {"metric": "input Mfaces/s", "value": best["batched"]["Mfaces_s"], "unit": "Mfaces/s",
+                "n_gpus": ws, "steps": len(rates), "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"serving: Poisson arrivals, {args.requests} requests per rate drawn from "
+                                       f"{args.pool} meshes (faces log-uniform 10k..2M), ratios 0.001/0.01/0.05, "
+                                       f"stage 2, host in / host out", "engine_max_faces": max_f},
+                "rates": out, "clocks": clocks}
+        print(json.dumps(line))
+    eng.close()
     return 0
 
 
@@ -350,13 +600,27 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4", "c5"],
+                    help="c1/c2: one mesh (plain loop); c4: 256-mesh batch; c5: Poisson serving")
+    ap.add_argument("--stage3", action="store_true", help="c1/c2: also time PaMO.run with stage 3")
+    ap.add_argument("--n-meshes", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--pool", type=int, default=24, help="c5: distinct request meshes")
+    ap.add_argument("--requests", type=int, default=200, help="c5: requests per rate")
+    ap.add_argument("--rates", default="5,20,50,200", help="c5: arrival rates (requests/s)")
+    ap.add_argument("--serve-max-faces", type=int, default=16_000_000)
     ap.add_argument("--sample-rounds", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dump-rounds", action="store_true")
+    ap.add_argument("--iters", type=int, default=1000000,
+                    help="PaMO.run's iter: the most collapse rounds per simplification")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "c4":
+        return batched_arm(args)
+    if args.workload == "c5":
+        return serving_arm(args)
     return product_arm(args)
 
 

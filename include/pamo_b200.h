@@ -35,6 +35,11 @@ typedef struct pamo_ctx pamo_ctx;
 /* Library version (major*10000 + minor*100 + patch). */
 int pamo_version(void);
 
+/* Kernels this library has launched in this process, on every device and
+   stream (a running total; take the difference around a region of interest).
+   No counterpart in the reference. */
+long long pamo_launch_count(void);
+
 /* Human-readable name of a status code (static storage). */
 const char *pamo_status_string(int status);
 
@@ -212,6 +217,52 @@ void pamo_simplify(float *in_verts, int *in_tris, float *out_verts, int *out_tri
 /* pamo_simplify with an explicit context and a status code. */
 int pamo_simplify_ctx(pamo_ctx *ctx, const float *h_in_verts, const int *h_in_tris, float *h_out_verts,
                       int *h_out_tris, int *in_out_nv_ni, float threshold);
+
+/* ---------------------------------------------------------------------------
+ * Batched simplification (no counterpart in the reference, which runs one mesh
+ * per CUDSP_Free object).  Many meshes share every collapse round: they are
+ * packed one after another into one set of round buffers, each keeps its own
+ * parameters and the state the reference carries between rounds, and each ends
+ * by PaMO.run's own rules (target, tolerance, iteration cap), so its result is
+ * the one pamo_stage2_run gives for it on a fresh context.  Meshes submitted
+ * while others run join at the next round, when the packed capacity
+ * (max_verts / max_faces / max_meshes) and the device-memory budget allow.
+ * One engine per host thread; all work goes to `stream`. */
+typedef struct pamo_batch pamo_batch;
+
+#define PAMO_JOB_PENDING 0 /* submitted, waiting for room */
+#define PAMO_JOB_RUNNING 1
+#define PAMO_JOB_DONE 2 /* result ready for pamo_batch_fetch; a failed job reports -status */
+
+/* memory_budget: bytes of per-mesh device state (inputs waiting, per-mesh
+   round state, results not yet released) the engine may hold; 0 = no limit. */
+int pamo_batch_create(int device, long long max_verts, long long max_faces, int max_meshes,
+                      long long memory_budget, void *stream, pamo_batch **out);
+int pamo_batch_destroy(pamo_batch *b);
+
+/* Queues one mesh (points [n,3] f32, faces [m,3] i32, host or device memory;
+   host buffers may be reused on return).  target_faces / tolerance / threshold
+   / iters mean what they mean for pamo_stage2_run. */
+int pamo_batch_submit(pamo_batch *b, const float *points, const int *tris, int n_pts, int n_tris, int on_host,
+                      long long target_faces, int tolerance, float threshold, int iters, long long *out_job);
+
+/* Admits what fits, runs one collapse round over every running mesh and
+   retires the meshes whose loop ended.  Returns the running / pending counts. */
+int pamo_batch_step(pamo_batch *b, int *out_running, int *out_pending);
+
+/* State (PAMO_JOB_*), current (or final) sizes and rounds run of a job. */
+int pamo_batch_job(pamo_batch *b, long long job, int *state, int *n_pts, int *n_tris, int *rounds);
+
+/* Copies a finished job's result (points [n,3] with the centring undone, faces
+   [m,3]) to host (to_host=1) or device buffers of at least that size. */
+int pamo_batch_fetch(pamo_batch *b, long long job, float *out_points, int *out_tris, int to_host);
+
+/* Frees a finished or failed job's result. */
+int pamo_batch_release(pamo_batch *b, long long job);
+
+/* {running, pending, packed vertices, packed faces, bytes held, rounds run,
+    max_faces, memory budget} */
+int pamo_batch_stats(pamo_batch *b, long long *h_out8);
 
 #ifdef __cplusplus
 }

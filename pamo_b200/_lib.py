@@ -27,6 +27,15 @@ _vp, _i, _f, _ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_longl
 _ip = ctypes.POINTER(ctypes.c_int)
 SIGNATURES = {
     "pamo_version": (_i, []),
+    "pamo_launch_count": (_ll, []),
+    "pamo_batch_create": (_i, [_i, _ll, _ll, _i, _ll, _vp, ctypes.POINTER(_vp)]),
+    "pamo_batch_destroy": (_i, [_vp]),
+    "pamo_batch_submit": (_i, [_vp, _vp, _vp, _i, _i, _i, _ll, _i, _f, _i, ctypes.POINTER(_ll)]),
+    "pamo_batch_step": (_i, [_vp, _ip, _ip]),
+    "pamo_batch_job": (_i, [_vp, _ll, _ip, _ip, _ip, _ip]),
+    "pamo_batch_fetch": (_i, [_vp, _ll, _vp, _vp, _i]),
+    "pamo_batch_release": (_i, [_vp, _ll]),
+    "pamo_batch_stats": (_i, [_vp, ctypes.POINTER(_ll)]),
     "pamo_status_string": (ctypes.c_char_p, [_i]),
     "pamo_ctx_create": (_i, [_i, ctypes.POINTER(_vp)]),
     "pamo_ctx_destroy": (_i, [_vp]),

@@ -82,59 +82,62 @@ __global__ void k_face_means(const float *pts, const int *tris, int m, float *mx
 
 // numpy's .mean(axis=0) of a C-contiguous (F,3) float32 array adds the rows one
 // after another into a float32 accumulator (no pairwise split on this axis), then
-// divides by F.  That chain is inherently sequential.  One block: warps 1..31
-// stream the next chunk into shared memory while thread 0 runs the three
-// coordinate chains (interleaved, so the FADD latency is the bound) on the
-// current chunk.
+// divides by F.  Each coordinate's chain is inherently sequential, so the bound
+// is the latency of F dependent adds.  One block: lane 0 of warps 0, 1, 2 runs
+// the x, y, z chains (reading four values per shared-memory load) while warps
+// 3..31 stream the next chunk into the other shared buffer.
 constexpr int kMeanChunk = 4096;
+constexpr int kMeanLoadFirst = 3 * 32;
 
 __global__ void __launch_bounds__(1024) k_sequential_mean(const float *mx, const float *my, const float *mz, int m,
                                                           float *out)
 {
-    extern __shared__ float sm[];  // 2 buffers x 3 coordinates x kMeanChunk
+    extern __shared__ float4 sm4[];  // 2 buffers x 3 coordinates x kMeanChunk floats
+    float *sm = reinterpret_cast<float *>(sm4);
     if (m <= 0) return;
     const int n_chunks = (m + kMeanChunk - 1) / kMeanChunk;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     auto load = [&](int c, int buf) {
         float *dst = sm + buf * 3 * kMeanChunk;
         int base = c * kMeanChunk;
         int cnt = min(kMeanChunk, m - base);
-        for (int i = threadIdx.x - 32; i < cnt; i += blockDim.x - 32) {
+        for (int i = threadIdx.x - kMeanLoadFirst; i < cnt; i += blockDim.x - kMeanLoadFirst) {
             dst[i] = mx[base + i];
             dst[kMeanChunk + i] = my[base + i];
             dst[2 * kMeanChunk + i] = mz[base + i];
         }
     };
-    if (threadIdx.x >= 32) load(0, 0);
+    if (threadIdx.x >= kMeanLoadFirst) load(0, 0);
     __syncthreads();
-    float sx = 0.f, sy = 0.f, sz = 0.f;
+    float acc = 0.f;
     for (int c = 0; c < n_chunks; ++c) {
         const int buf = c & 1;
-        if (threadIdx.x >= 32) {
+        if (threadIdx.x >= kMeanLoadFirst) {
             if (c + 1 < n_chunks) load(c + 1, buf ^ 1);
-        } else if (threadIdx.x == 0) {
-            const float *b = sm + buf * 3 * kMeanChunk;
-            int cnt = min(kMeanChunk, m - c * kMeanChunk);
+        } else if (lane == 0) {
+            const float *bs = sm + (buf * 3 + warp) * kMeanChunk;
+            const float4 *b4 = reinterpret_cast<const float4 *>(bs);
+            const int cnt = min(kMeanChunk, m - c * kMeanChunk);
             int i = 0;
             if (c == 0) {  // the accumulator starts from the first row
-                sx = b[0];
-                sy = b[kMeanChunk];
-                sz = b[2 * kMeanChunk];
+                acc = bs[0];
                 i = 1;
             }
-#pragma unroll 8
-            for (; i < cnt; ++i) {
-                sx += b[i];
-                sy += b[kMeanChunk + i];
-                sz += b[2 * kMeanChunk + i];
+            for (; i < cnt && (i & 3); ++i) acc += bs[i];
+            const int n4 = cnt >> 2;
+#pragma unroll 4
+            for (int q = i >> 2; q < n4; ++q) {
+                float4 v = b4[q];
+                acc += v.x;
+                acc += v.y;
+                acc += v.z;
+                acc += v.w;
             }
+            for (i = max(i, n4 * 4); i < cnt; ++i) acc += bs[i];
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        out[0] = sx / (float)m;
-        out[1] = sy / (float)m;
-        out[2] = sz / (float)m;
-    }
+    if (threadIdx.x < kMeanLoadFirst && lane == 0) out[warp] = acc / (float)m;
 }
 
 __global__ void k_centre(const float *pts, int n, const float *mean, float4 *out, int *bounds)
@@ -237,6 +240,8 @@ extern "C" {
 
 int pamo_version(void) { return 100; }
 
+long long pamo_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
 const char *pamo_status_string(int status)
 {
     switch (status) {
@@ -296,13 +301,13 @@ int pamo_free_forward(pamo_ctx *ctx, const float *d_points, const int *d_tris, c
     RET_IF(S.ensure(n_pts, n_tris));
     if (n_verts_undo > S.cap_undo) return PAMO_ERR_CAPACITY;
     RET_IF(S.validate(d_tris, n_pts, n_tris, d_verts_undo, n_verts_undo, (int)S.cap_pts, s));
-    k_aos3_to_f4<<<grid_for(n_pts), kThreads, 0, s>>>(d_points, S.opts, n_pts);
-    k_aos3_to_i4<<<grid_for(n_tris), kThreads, 0, s>>>(d_tris, S.otris, n_tris);
+    launch(k_aos3_to_f4, grid_for(n_pts), kThreads, 0, s, d_points, S.opts, n_pts);
+    launch(k_aos3_to_i4, grid_for(n_tris), kThreads, 0, s, d_tris, S.otris, n_tris);
     if (init) RET_IF(stage2_shuffle_faces(S.otris, n_tris, s));
     int nvu = 0;
     RET_IF(S.round(n_pts, n_tris, scale, threshold, is_stuck != 0, d_verts_undo, n_verts_undo, &nvu, s));
-    if (d_out_points) k_f4_to_aos3<<<grid_for(n_pts), kThreads, 0, s>>>(S.pts, d_out_points, n_pts, 0, 0, 0, 0);
-    if (d_out_tris) k_i4_to_aos3<<<grid_for(n_tris), kThreads, 0, s>>>(S.tris, d_out_tris, n_tris);
+    if (d_out_points) launch(k_f4_to_aos3, grid_for(n_pts), kThreads, 0, s, S.pts, d_out_points, n_pts, 0, 0, 0, 0);
+    if (d_out_tris) launch(k_i4_to_aos3, grid_for(n_tris), kThreads, 0, s, S.tris, d_out_tris, n_tris);
     if (d_out_occ && n_pts) CU_RET(cudaMemcpyAsync(d_out_occ, S.occ, (size_t)n_pts * 4, cudaMemcpyDeviceToDevice, s));
     if (d_out_map && n_pts)
         CU_RET(cudaMemcpyAsync(d_out_map, S.pts_map, (size_t)n_pts * 4, cudaMemcpyDeviceToDevice, s));
@@ -339,17 +344,17 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
     float *mean_dev = reinterpret_cast<float *>(S.dev_misc);
     int *bounds = S.dev_misc + 8;
     float *bounds_f = reinterpret_cast<float *>(S.dev_misc + 16);
-    k_face_means<<<grid_for(n_tris), kThreads, 0, s>>>(d_points, d_tris, n_tris, mxyz, mxyz + n_tris,
+    launch(k_face_means, grid_for(n_tris), kThreads, 0, s, d_points, d_tris, n_tris, mxyz, mxyz + n_tris,
                                                        mxyz + 2LL * n_tris);
     {
         const int smem = 2 * 3 * kMeanChunk * (int)sizeof(float);
         CU_RET(cudaFuncSetAttribute(k_sequential_mean, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        k_sequential_mean<<<1, 1024, smem, s>>>(mxyz, mxyz + n_tris, mxyz + 2LL * n_tris, n_tris, mean_dev);
+        launch(k_sequential_mean, 1, 1024, smem, s, mxyz, mxyz + n_tris, mxyz + 2LL * n_tris, n_tris, mean_dev);
     }
-    k_bounds_init<<<1, 32, 0, s>>>(bounds);
-    k_centre<<<grid_for(n_pts), kThreads, 0, s>>>(d_points, n_pts, mean_dev, S.opts, bounds);
-    k_bounds_to_float<<<1, 32, 0, s>>>(bounds, bounds_f);
-    k_aos3_to_i4<<<grid_for(n_tris), kThreads, 0, s>>>(d_tris, S.otris, n_tris);
+    launch(k_bounds_init, 1, 32, 0, s, bounds);
+    launch(k_centre, grid_for(n_pts), kThreads, 0, s, d_points, n_pts, mean_dev, S.opts, bounds);
+    launch(k_bounds_to_float, 1, 32, 0, s, bounds, bounds_f);
+    launch(k_aos3_to_i4, grid_for(n_tris), kThreads, 0, s, d_tris, S.otris, n_tris);
     RET_IF(stage2_shuffle_faces(S.otris, n_tris, s));
     CU_RET(cudaMemcpyAsync(S.h_scalars, mean_dev, 3 * 4, cudaMemcpyDeviceToHost, s));
     CU_RET(cudaMemcpyAsync(S.h_scalars + 4, bounds_f, 6 * 4, cudaMemcpyDeviceToHost, s));
@@ -367,7 +372,7 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
         int prev = m;
         S.round_faces.push_back(m);
         int nvu = 0;
-        RET_IF(S.round(n, m, scale, threshold, stuck, n_undo ? ctx->undo_prev : nullptr, n_undo, &nvu, s));
+        RET_IF(S.round(n, m, scale, threshold, stuck, n_undo ? ctx->undo_prev : nullptr, n_undo, &nvu, s, it > 0));
         rounds++;
         if (nvu > ctx->undo_prev_cap) return PAMO_ERR_CAPACITY;
         if (nvu) CU_RET(cudaMemcpyAsync(ctx->undo_prev, S.undo_list, (size_t)nvu * 4, cudaMemcpyDeviceToDevice, s));
@@ -403,13 +408,13 @@ int pamo_stage2_fetch(pamo_ctx *ctx, float *out_points, int *out_tris, int to_ho
     int n = S.res_n_pts, m = S.res_n_tris;
     if (to_host) {
         RET_IF(ensure_stage(ctx, 3LL * n + 3, 3LL * m + 3));
-        k_f4_to_aos3<<<grid_for(n), kThreads, 0, s>>>(S.opts, ctx->stage, n, S.offset[0], S.offset[1], S.offset[2], 1);
-        k_i4_to_aos3<<<grid_for(m), kThreads, 0, s>>>(S.otris, ctx->istage, m);
+        launch(k_f4_to_aos3, grid_for(n), kThreads, 0, s, S.opts, ctx->stage, n, S.offset[0], S.offset[1], S.offset[2], 1);
+        launch(k_i4_to_aos3, grid_for(m), kThreads, 0, s, S.otris, ctx->istage, m);
         CU_RET(cudaMemcpyAsync(out_points, ctx->stage, (size_t)n * 12, cudaMemcpyDeviceToHost, s));
         CU_RET(cudaMemcpyAsync(out_tris, ctx->istage, (size_t)m * 12, cudaMemcpyDeviceToHost, s));
     } else {
-        k_f4_to_aos3<<<grid_for(n), kThreads, 0, s>>>(S.opts, out_points, n, S.offset[0], S.offset[1], S.offset[2], 1);
-        k_i4_to_aos3<<<grid_for(m), kThreads, 0, s>>>(S.otris, out_tris, m);
+        launch(k_f4_to_aos3, grid_for(n), kThreads, 0, s, S.opts, out_points, n, S.offset[0], S.offset[1], S.offset[2], 1);
+        launch(k_i4_to_aos3, grid_for(m), kThreads, 0, s, S.otris, out_tris, m);
     }
     CU_RET(cudaGetLastError());
     CU_RET(cudaStreamSynchronize(s));
@@ -439,8 +444,8 @@ int pamo_self_intersect(pamo_ctx *ctx, const float *d_points, const int *d_tris,
     Stage2 &S = ctx->s2;
     RET_IF(S.ensure(n_pts, n_tris));
     RET_IF(S.validate(d_tris, n_pts, n_tris, nullptr, 0, 0, s));
-    k_aos3_to_f4<<<grid_for(n_pts), kThreads, 0, s>>>(d_points, S.opts, n_pts);
-    k_aos3_to_i4<<<grid_for(n_tris), kThreads, 0, s>>>(d_tris, S.otris, n_tris);
+    launch(k_aos3_to_f4, grid_for(n_pts), kThreads, 0, s, d_points, S.opts, n_pts);
+    launch(k_aos3_to_i4, grid_for(n_tris), kThreads, 0, s, d_tris, S.otris, n_tris);
     RET_IF(S.self_intersect_all(n_pts, n_tris, s));
     if (n_tris) CU_RET(cudaMemcpyAsync(d_out_flags, S.isect, (size_t)n_tris, cudaMemcpyDeviceToDevice, s));
     CU_RET(cudaStreamSynchronize(s));
@@ -568,8 +573,8 @@ int pamo_simplify_ctx(pamo_ctx *ctx, const float *h_in_verts, const int *h_in_tr
     CU_RET(cudaMemcpyAsync(ctx->stage, h_in_verts, (size_t)n * 12, cudaMemcpyHostToDevice, s));
     CU_RET(cudaMemcpyAsync(ctx->istage, h_in_tris, (size_t)m * 12, cudaMemcpyHostToDevice, s));
     RET_IF(S.validate(ctx->istage, n, m, nullptr, 0, 0, s));
-    k_aos3_to_f4<<<grid_for(n), kThreads, 0, s>>>(ctx->stage, S.opts, n);
-    k_aos3_to_i4<<<grid_for(m), kThreads, 0, s>>>(ctx->istage, S.otris, m);
+    launch(k_aos3_to_f4, grid_for(n), kThreads, 0, s, ctx->stage, S.opts, n);
+    launch(k_aos3_to_i4, grid_for(m), kThreads, 0, s, ctx->istage, S.otris, m);
     const int tolerance = 4;
     int same = 0, n_undo = 0;
     bool stuck = false, init = true;
@@ -578,7 +583,7 @@ int pamo_simplify_ctx(pamo_ctx *ctx, const float *h_in_verts, const int *h_in_tr
         init = false;
         int nvu = 0;
         // the reference passes its own undo list back in (cusimpinterface.cu:103-105)
-        RET_IF(S.round(n, m, scale, threshold, stuck, n_undo ? S.undo_list : nullptr, n_undo, &nvu, s));
+        RET_IF(S.round(n, m, scale, threshold, stuck, n_undo ? S.undo_list : nullptr, n_undo, &nvu, s, it > 0));
         n_undo = nvu;
         RET_IF(S.compact(n, m, s));
         int old_m = m;
@@ -594,8 +599,8 @@ int pamo_simplify_ctx(pamo_ctx *ctx, const float *h_in_verts, const int *h_in_tr
         if (same >= 2) stuck = true;
         if (same >= tolerance) break;
     }
-    k_f4_to_aos3<<<grid_for(n), kThreads, 0, s>>>(S.opts, ctx->stage, n, 0, 0, 0, 0);
-    k_i4_to_aos3<<<grid_for(m), kThreads, 0, s>>>(S.otris, ctx->istage, m);
+    launch(k_f4_to_aos3, grid_for(n), kThreads, 0, s, S.opts, ctx->stage, n, 0, 0, 0, 0);
+    launch(k_i4_to_aos3, grid_for(m), kThreads, 0, s, S.otris, ctx->istage, m);
     CU_RET(cudaMemcpyAsync(h_out_verts, ctx->stage, (size_t)n * 12, cudaMemcpyDeviceToHost, s));
     CU_RET(cudaMemcpyAsync(h_out_tris, ctx->istage, (size_t)m * 12, cudaMemcpyDeviceToHost, s));
     CU_RET(cudaStreamSynchronize(s));
@@ -611,6 +616,532 @@ void pamo_simplify(float *in_verts, int *in_tris, float *out_verts, int *out_tri
     }
     int rc = pamo_simplify_ctx(g_ctx, in_verts, in_tris, out_verts, out_tris, in_out_nv_ni, threshold);
     if (rc != PAMO_OK) fprintf(stderr, "pamo_simplify: %s\n", pamo_status_string(rc));
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched simplification engine (pamo_batch_*): many meshes of any sizes are
+// packed into the rounds of one Stage2 (see SlotInfo), admitted while the packed
+// capacity and the device-memory budget allow, and retired as soon as their own
+// loop (PaMO.run's termination rules) ends, so new meshes join between rounds.
+
+namespace pamo {
+namespace {
+
+struct JobHeader {  // device scalars of one mesh
+    float mean[4];    // centring offset (numpy's tris mean)
+    float scale;      // max bounding-box extent after centring
+    float pad[3];
+    int bounds[8];    // ordered-int box of the centred points
+};
+
+__global__ void k_scale_from_bounds(JobHeader *h)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    float b[6];
+    for (int k = 0; k < 6; ++k) b[k] = ordered_to_float(h->bounds[k]);
+    float sx = b[3] - b[0], sy = b[4] - b[1], sz = b[5] - b[2];
+    float scale = sy > sx ? sy : sx;  // Python max() keeps the first maximal argument
+    h->scale = sz > scale ? sz : scale;
+}
+
+__global__ void k_aos3_to_i4_off(const int *in, int4 *out, int n, int off)
+{
+    PAMO_GRID_STRIDE(i, n) out[i] = make_int4(in[3 * i] + off, in[3 * i + 1] + off, in[3 * i + 2] + off, 0);
+}
+
+// a finished mesh out of the packed arrays: points + centring offset, faces rebased
+__global__ void k_b_extract(const float4 *opts, const int4 *otris, int voff, int n, int foff, int m,
+                            const JobHeader *h, float *out_p, int *out_t)
+{
+    const float ox = h->mean[0], oy = h->mean[1], oz = h->mean[2];
+    PAMO_GRID_STRIDE(i, (long long)(n > m ? n : m))
+    {
+        if (i < n) {
+            float4 p = opts[voff + i];
+            out_p[3 * i] = p.x + ox;
+            out_p[3 * i + 1] = p.y + oy;
+            out_p[3 * i + 2] = p.z + oz;
+        }
+        if (i < m) {
+            int4 t = otris[foff + i];
+            out_t[3 * i] = t.x - voff;
+            out_t[3 * i + 1] = t.y - voff;
+            out_t[3 * i + 2] = t.z - voff;
+        }
+    }
+}
+
+struct Move {
+    int src_v, dst_v, n, src_f, dst_f, m;
+};
+
+// kept meshes moved down to close the gaps of retired ones (into the other buffer)
+__global__ void k_b_repack(const Move *moves, const float4 *src_p, const int4 *src_t, float4 *dst_p, int4 *dst_t)
+{
+    const Move mv = moves[blockIdx.y];
+    const int shift = mv.src_v - mv.dst_v;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (mv.n > mv.m ? mv.n : mv.m);
+         i += (long long)blockDim.x * gridDim.x) {
+        if (i < mv.n) dst_p[mv.dst_v + i] = src_p[mv.src_v + i];
+        if (i < mv.m) {
+            int4 t = src_t[mv.src_f + i];
+            dst_t[mv.dst_f + i] = make_int4(t.x - shift, t.y - shift, t.z - shift, 0);
+        }
+    }
+}
+
+struct BatchJob {
+    long long id = 0;
+    int state = PAMO_JOB_PENDING;
+    int n0 = 0, m0 = 0;
+    float *raw_p = nullptr;  // device copy of the input until admission
+    int *raw_t = nullptr;
+    long long target = 0;
+    int tolerance = 4, iters = 1000000;
+    float threshold = 1e-3f;
+    uint32_t collapse_t = 0;
+    // while running
+    int n = 0, m = 0, vert_off = 0, face_off = 0;
+    int rounds = 0, count = 0, n_undo = 0;
+    bool stuck = false;
+    unsigned char *region = nullptr;
+    long long region_bytes = 0;
+    SlotInfo tmpl{};
+    JobHeader *hdr = nullptr;
+    // finished
+    float *out_p = nullptr;
+    int *out_t = nullptr;
+    int n_out = 0, m_out = 0;
+};
+
+long long region_bytes_for(long long n0, long long m0, long long *cap_undo)
+{
+    long long cu = 16 * (n0 + 1) + 6 * m0 + 16;
+    *cap_undo = cu;
+    auto al = [](long long b) { return (b + 255) / 256 * 256; };
+    return al(sizeof(JobHeader)) + al((3 * m0 + 1) * 4) + al((n0 + 1) * 4) + 3 * al(cu * 4) + al(n0 + 1);
+}
+
+}  // namespace
+}  // namespace pamo
+
+struct pamo_batch {
+    int device = 0;
+    cudaStream_t s = nullptr;
+    pamo::Stage2 S;
+    long long cap_v = 0, cap_f = 0, budget = 0, in_use = 0;
+    int max_meshes = 0;
+    int n_packed = 0, m_packed = 0;
+    long long next_id = 1;
+    std::vector<pamo::BatchJob *> pending, running;
+    std::vector<pamo::BatchJob *> all;  // every job not yet released
+    pamo::Move *d_moves = nullptr;
+    pamo::Move *h_moves = nullptr;
+    std::vector<int> nvu;
+    long long rounds_run = 0;
+};
+
+namespace pamo {
+namespace {
+
+BatchJob *find_job(pamo_batch *b, long long id)
+{
+    for (BatchJob *j : b->all)
+        if (j->id == id) return j;
+    return nullptr;
+}
+
+int batch_admit(pamo_batch *b, BatchJob *j)
+{
+    cudaStream_t s = b->s;
+    Stage2 &S = b->S;
+    long long cu = 0;
+    j->region_bytes = region_bytes_for(j->n0, j->m0, &cu);
+    CU_RET(cudaMallocAsync((void **)&j->region, (size_t)j->region_bytes, s));
+    CU_RET(cudaMemsetAsync(j->region, 0, (size_t)j->region_bytes, s));
+    auto al = [](long long x) { return (x + 255) / 256 * 256; };
+    unsigned char *p = j->region;
+    j->hdr = reinterpret_cast<JobHeader *>(p);
+    p += al(sizeof(JobHeader));
+    SlotInfo &t = j->tmpl;
+    t = SlotInfo{};
+    t.edge_cost = reinterpret_cast<uint32_t *>(p);
+    p += al((3LL * j->m0 + 1) * 4);
+    t.pts_map = reinterpret_cast<int *>(p);
+    p += al((j->n0 + 1LL) * 4);
+    t.undo_list = reinterpret_cast<int *>(p);
+    p += al(cu * 4);
+    t.tmp_undo = reinterpret_cast<int *>(p);
+    p += al(cu * 4);
+    t.undo_prev = reinterpret_cast<int *>(p);
+    p += al(cu * 4);
+    t.invalid = p;
+    t.cap_v = j->n0 + 1;
+    t.cap_undo = cu;
+    t.scale = &j->hdr->scale;
+    t.collapse_t = j->collapse_t;
+    t.tres = j->threshold;
+    // centring and scale as the single-mesh loop does, written at the packed tail
+    const int voff = b->n_packed, foff = b->m_packed, n = j->n0, m = j->m0;
+    float *mxyz = reinterpret_cast<float *>(S.plane);  // 3*m floats of scratch
+    launch(k_face_means, grid_for(m), kThreads, 0, s, (const float *)j->raw_p, (const int *)j->raw_t, m, mxyz,
+           mxyz + m, mxyz + 2LL * m);
+    const int smem = 2 * 3 * kMeanChunk * (int)sizeof(float);
+    CU_RET(cudaFuncSetAttribute(k_sequential_mean, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    launch(k_sequential_mean, 1, 1024, smem, s, (const float *)mxyz, (const float *)(mxyz + m),
+           (const float *)(mxyz + 2LL * m), m, j->hdr->mean);
+    launch(k_bounds_init, 1, 32, 0, s, j->hdr->bounds);
+    launch(k_centre, grid_for(n), kThreads, 0, s, (const float *)j->raw_p, n, (const float *)j->hdr->mean,
+           S.opts + voff, j->hdr->bounds);
+    launch(k_scale_from_bounds, 1, 32, 0, s, j->hdr);
+    launch(k_aos3_to_i4_off, grid_for(m), kThreads, 0, s, (const int *)j->raw_t, S.otris + foff, m, voff);
+    RET_IF(stage2_shuffle_faces(S.otris + foff, m, s));
+    CU_RET(cudaFreeAsync(j->raw_p, s));
+    CU_RET(cudaFreeAsync(j->raw_t, s));
+    j->raw_p = nullptr;
+    j->raw_t = nullptr;
+    b->in_use -= 12LL * (n + m);
+    b->in_use += j->region_bytes;
+    j->n = n;
+    j->m = m;
+    j->vert_off = voff;
+    j->face_off = foff;
+    j->state = PAMO_JOB_RUNNING;
+    b->n_packed += n;
+    b->m_packed += m;
+    CU_RET(cudaGetLastError());
+    return PAMO_OK;
+}
+
+int batch_finish(pamo_batch *b, BatchJob *j)
+{
+    cudaStream_t s = b->s;
+    CU_RET(cudaMallocAsync((void **)&j->out_p, (size_t)(j->n > 0 ? j->n : 1) * 12, s));
+    CU_RET(cudaMallocAsync((void **)&j->out_t, (size_t)(j->m > 0 ? j->m : 1) * 12, s));
+    launch(k_b_extract, grid_for(j->n > j->m ? j->n : j->m), kThreads, 0, s, (const float4 *)b->S.opts,
+           (const int4 *)b->S.otris, j->vert_off, j->n, j->face_off, j->m, (const JobHeader *)j->hdr, j->out_p,
+           j->out_t);
+    CU_RET(cudaFreeAsync(j->region, s));
+    b->in_use -= j->region_bytes;
+    b->in_use += 12LL * (j->n + j->m);
+    j->region = nullptr;
+    j->hdr = nullptr;
+    j->n_out = j->n;
+    j->m_out = j->m;
+    j->state = PAMO_JOB_DONE;
+    CU_RET(cudaGetLastError());
+    return PAMO_OK;
+}
+
+void batch_fail(pamo_batch *b, BatchJob *j, int rc)
+{
+    if (j->region) cudaFreeAsync(j->region, b->s);
+    if (j->raw_p) cudaFreeAsync(j->raw_p, b->s);
+    if (j->raw_t) cudaFreeAsync(j->raw_t, b->s);
+    j->region = nullptr;
+    j->raw_p = nullptr;
+    j->raw_t = nullptr;
+    j->state = -rc;
+}
+
+}  // namespace
+}  // namespace pamo
+
+extern "C" {
+
+int pamo_batch_create(int device, long long max_verts, long long max_faces, int max_meshes,
+                      long long memory_budget, void *stream, pamo_batch **out)
+{
+    if (!out || max_verts <= 0 || max_faces <= 0 || max_meshes <= 0 || memory_budget < 0) return PAMO_ERR_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return PAMO_ERR_NO_DEVICE;
+    if (device < 0 || device >= count) return PAMO_ERR_INVALID_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return PAMO_ERR_DEVICE;
+    pamo_batch *b = new (std::nothrow) pamo_batch();
+    if (!b) return PAMO_ERR_OOM;
+    b->device = device;
+    b->s = (cudaStream_t)stream;
+    b->cap_v = max_verts;
+    b->cap_f = max_faces;
+    b->max_meshes = max_meshes;
+    b->budget = memory_budget;
+    int rc = b->S.ensure(max_verts, max_faces);
+    if (!rc) rc = b->S.ensure_batch(max_meshes);
+    if (!rc && (cudaMalloc((void **)&b->d_moves, (size_t)max_meshes * sizeof(Move)) != cudaSuccess ||
+                cudaMallocHost((void **)&b->h_moves, (size_t)max_meshes * sizeof(Move)) != cudaSuccess))
+        rc = PAMO_ERR_OOM;
+    if (rc) {
+        pamo_batch_destroy(b);
+        return rc;
+    }
+    b->nvu.resize(max_meshes);
+    *out = b;
+    return PAMO_OK;
+}
+
+int pamo_batch_destroy(pamo_batch *b)
+{
+    if (!b) return PAMO_ERR_INVALID_ARG;
+    cudaSetDevice(b->device);
+    if (b->s) cudaStreamSynchronize(b->s);
+    for (BatchJob *j : b->all) {
+        if (j->raw_p) cudaFree(j->raw_p);
+        if (j->raw_t) cudaFree(j->raw_t);
+        if (j->region) cudaFree(j->region);
+        if (j->out_p) cudaFree(j->out_p);
+        if (j->out_t) cudaFree(j->out_t);
+        delete j;
+    }
+    b->S.release();
+    if (b->S.slots) cudaFree(b->S.slots);
+    if (b->S.scnt) cudaFree(b->S.scnt);
+    if (b->S.roots) cudaFree(b->S.roots);
+    if (b->S.vslot) cudaFree(b->S.vslot);
+    if (b->S.gmap) cudaFree(b->S.gmap);
+    if (b->S.line_list) cudaFree(b->S.line_list);
+    if (b->S.cand) cudaFree(b->S.cand);
+    if (b->S.hslots) cudaFreeHost(b->S.hslots);
+    if (b->S.hscnt) cudaFreeHost(b->S.hscnt);
+    if (b->d_moves) cudaFree(b->d_moves);
+    if (b->h_moves) cudaFreeHost(b->h_moves);
+    delete b;
+    return PAMO_OK;
+}
+
+int pamo_batch_submit(pamo_batch *b, const float *points, const int *tris, int n_pts, int n_tris, int on_host,
+                      long long target_faces, int tolerance, float threshold, int iters, long long *out_job)
+{
+    if (!b || !points || !tris || n_pts <= 0 || n_tris <= 0 || !out_job || iters < 0) return PAMO_ERR_INVALID_ARG;
+    if (n_pts > b->cap_v || n_tris > b->cap_f) return PAMO_ERR_CAPACITY;
+    if (cudaSetDevice(b->device) != cudaSuccess) return PAMO_ERR_DEVICE;
+    cudaStream_t s = b->s;
+    if (on_host) {  // reject faces with indices outside [0, n) before anything reaches the device
+        for (long long i = 0; i < 3LL * n_tris; ++i)
+            if (tris[i] < 0 || tris[i] >= n_pts) return PAMO_ERR_INVALID_ARG;
+    }
+    BatchJob *j = new (std::nothrow) BatchJob();
+    if (!j) return PAMO_ERR_OOM;
+    j->n0 = n_pts;
+    j->m0 = n_tris;
+    j->target = target_faces;
+    j->tolerance = tolerance;
+    j->threshold = threshold;
+    j->iters = iters;
+    float ct = (0.0f > threshold) ? 0.0f : threshold;
+    ct = (ct < 10.0f) ? ct : 10.0f;
+    j->collapse_t = (uint32_t)(unsigned long long)(ct / 10.0f * 4294967296.0f);
+    if (cudaMallocAsync((void **)&j->raw_p, (size_t)n_pts * 12, s) != cudaSuccess ||
+        cudaMallocAsync((void **)&j->raw_t, (size_t)n_tris * 12, s) != cudaSuccess) {
+        batch_fail(b, j, PAMO_ERR_OOM);
+        delete j;
+        return PAMO_ERR_OOM;
+    }
+    cudaMemcpyKind kind = on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (cudaMemcpyAsync(j->raw_p, points, (size_t)n_pts * 12, kind, s) != cudaSuccess ||
+        cudaMemcpyAsync(j->raw_t, tris, (size_t)n_tris * 12, kind, s) != cudaSuccess) {
+        batch_fail(b, j, PAMO_ERR_DEVICE);
+        delete j;
+        return PAMO_ERR_DEVICE;
+    }
+    if (!on_host) {  // device input: check the indices on the device before admitting
+        int rc = b->S.validate(j->raw_t, n_pts, n_tris, nullptr, 0, 0, s);
+        if (rc) {
+            batch_fail(b, j, rc);
+            delete j;
+            return rc;
+        }
+    } else if (cudaStreamSynchronize(s) != cudaSuccess) {  // the caller may reuse its host buffers now
+        batch_fail(b, j, PAMO_ERR_DEVICE);
+        delete j;
+        return PAMO_ERR_DEVICE;
+    }
+    b->in_use += 12LL * (n_pts + n_tris);
+    j->id = b->next_id++;
+    b->pending.push_back(j);
+    b->all.push_back(j);
+    *out_job = j->id;
+    return PAMO_OK;
+}
+
+int pamo_batch_step(pamo_batch *b, int *out_running, int *out_pending)
+{
+    if (!b) return PAMO_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return PAMO_ERR_DEVICE;
+    cudaStream_t s = b->s;
+    Stage2 &S = b->S;
+    // admission: every pending mesh that fits the packed capacity, the mesh
+    // count and the memory budget, in submission order
+    for (size_t k = 0; k < b->pending.size();) {
+        BatchJob *j = b->pending[k];
+        long long cu = 0;
+        long long need = region_bytes_for(j->n0, j->m0, &cu);
+        bool fits = b->n_packed + (long long)j->n0 <= b->cap_v && b->m_packed + (long long)j->m0 <= b->cap_f &&
+                    (int)b->running.size() < b->max_meshes &&
+                    (b->budget == 0 || b->in_use + need - 12LL * (j->n0 + j->m0) <= b->budget);
+        if (!fits) {
+            ++k;
+            continue;
+        }
+        int rc = batch_admit(b, j);
+        b->pending.erase(b->pending.begin() + k);
+        if (rc) {
+            batch_fail(b, j, rc);
+            continue;
+        }
+        if (j->iters == 0) {  // no round: the centred, permuted input comes back, as from the plain loop
+            rc = batch_finish(b, j);
+            if (rc) batch_fail(b, j, rc);
+            b->n_packed -= j->n0;  // it was the last one packed
+            b->m_packed -= j->m0;
+            continue;
+        }
+        b->running.push_back(j);
+    }
+    const int K = (int)b->running.size();
+    if (K > 0) {
+        for (int r = 0; r < K; ++r) {
+            BatchJob *j = b->running[r];
+            SlotInfo &h = S.hslots[r];
+            h = j->tmpl;
+            h.vert_off = j->vert_off;
+            h.n = j->n;
+            h.face_off = j->face_off;
+            h.m = j->m;
+            h.is_stuck = j->stuck ? 1 : 0;
+            h.n_undo_in = j->n_undo;
+            h.clear_invalid = (!j->stuck && j->n_undo != 0) ? 1 : 0;
+        }
+        int rc = S.round_batch(b->n_packed, b->m_packed, K, b->nvu.data(), s);
+        if (!rc) rc = S.compact_batch(b->n_packed, b->m_packed, K, s);
+        if (rc) {  // a device or capacity error fails every mesh of the round
+            for (BatchJob *j : b->running) batch_fail(b, j, rc);
+            b->running.clear();
+            b->n_packed = b->m_packed = 0;
+            return rc;
+        }
+        b->rounds_run++;
+        // PaMO.run's loop per mesh (simp_cuda/pamo/__init__.py:169-185)
+        std::vector<BatchJob *> keep;
+        int n_moves = 0, dst_v = 0, dst_f = 0;
+        bool moved = false;
+        for (int r = 0; r < K; ++r) {
+            BatchJob *j = b->running[r];
+            const SlotCounters &c = S.hscnt[r];
+            const int prev = j->m;
+            j->rounds++;
+            j->n_undo = b->nvu[r];
+            j->n = c.n_next;
+            j->m = c.m_next;
+            j->vert_off = c.vert_off_next;
+            j->face_off = c.face_off_next;
+            bool done = (long long)j->m <= j->target || j->m <= 10;
+            if (!done) {
+                if (j->m == prev) j->count++;
+                else {
+                    j->count = 0;
+                    j->stuck = false;
+                }
+                if (j->count >= 2) j->stuck = true;
+                if (j->count == j->tolerance) done = true;
+            }
+            if (j->rounds >= j->iters) done = true;
+            if (done) {
+                int frc = batch_finish(b, j);
+                if (frc) batch_fail(b, j, frc);
+                moved = true;
+                continue;
+            }
+            if (j->vert_off != dst_v || j->face_off != dst_f) moved = true;
+            b->h_moves[n_moves++] = Move{j->vert_off, dst_v, j->n, j->face_off, dst_f, j->m};
+            j->vert_off = dst_v;
+            j->face_off = dst_f;
+            dst_v += j->n;
+            dst_f += j->m;
+            keep.push_back(j);
+        }
+        if (moved && n_moves > 0) {
+            int max_len = 0;
+            for (int k = 0; k < n_moves; ++k) {
+                int l = b->h_moves[k].n > b->h_moves[k].m ? b->h_moves[k].n : b->h_moves[k].m;
+                max_len = l > max_len ? l : max_len;
+            }
+            CU_RET(cudaMemcpyAsync(b->d_moves, b->h_moves, (size_t)n_moves * sizeof(Move), cudaMemcpyHostToDevice, s));
+            long long gx = (max_len + kThreads - 1) / kThreads;
+            gx = gx < 1 ? 1 : (gx > 64 ? 64 : gx);
+            launch(k_b_repack, dim3((unsigned)gx, (unsigned)n_moves), kThreads, 0, s, (const Move *)b->d_moves,
+                   (const float4 *)S.opts, (const int4 *)S.otris, S.pts, S.tris);
+            std::swap(S.opts, S.pts);
+            std::swap(S.otris, S.tris);
+            CU_RET(cudaGetLastError());
+            CU_RET(cudaStreamSynchronize(s));  // h_moves is rewritten by the next step
+        }
+        b->running.swap(keep);
+        b->n_packed = dst_v;
+        b->m_packed = dst_f;
+    }
+    if (out_running) *out_running = (int)b->running.size();
+    if (out_pending) *out_pending = (int)b->pending.size();
+    return PAMO_OK;
+}
+
+int pamo_batch_job(pamo_batch *b, long long job, int *state, int *n_pts, int *n_tris, int *rounds)
+{
+    if (!b) return PAMO_ERR_INVALID_ARG;
+    BatchJob *j = find_job(b, job);
+    if (!j) return PAMO_ERR_INVALID_ARG;
+    if (state) *state = j->state;
+    if (n_pts) *n_pts = j->state == PAMO_JOB_DONE ? j->n_out : j->n;
+    if (n_tris) *n_tris = j->state == PAMO_JOB_DONE ? j->m_out : j->m;
+    if (rounds) *rounds = j->rounds;
+    return PAMO_OK;
+}
+
+int pamo_batch_fetch(pamo_batch *b, long long job, float *out_points, int *out_tris, int to_host)
+{
+    if (!b || !out_points || !out_tris) return PAMO_ERR_INVALID_ARG;
+    BatchJob *j = find_job(b, job);
+    if (!j || j->state != PAMO_JOB_DONE) return PAMO_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return PAMO_ERR_DEVICE;
+    cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    CU_RET(cudaMemcpyAsync(out_points, j->out_p, (size_t)j->n_out * 12, kind, b->s));
+    CU_RET(cudaMemcpyAsync(out_tris, j->out_t, (size_t)j->m_out * 12, kind, b->s));
+    CU_RET(cudaStreamSynchronize(b->s));
+    return PAMO_OK;
+}
+
+int pamo_batch_release(pamo_batch *b, long long job)
+{
+    if (!b) return PAMO_ERR_INVALID_ARG;
+    for (size_t k = 0; k < b->all.size(); ++k) {
+        BatchJob *j = b->all[k];
+        if (j->id != job) continue;
+        if (j->state == PAMO_JOB_PENDING || j->state == PAMO_JOB_RUNNING) return PAMO_ERR_INVALID_ARG;
+        cudaSetDevice(b->device);
+        if (j->out_p) cudaFreeAsync(j->out_p, b->s);
+        if (j->out_t) cudaFreeAsync(j->out_t, b->s);
+        b->in_use -= 12LL * (j->n_out + j->m_out);
+        b->all.erase(b->all.begin() + k);
+        delete j;
+        return PAMO_OK;
+    }
+    return PAMO_ERR_INVALID_ARG;
+}
+
+int pamo_batch_stats(pamo_batch *b, long long *h_out8)
+{
+    if (!b || !h_out8) return PAMO_ERR_INVALID_ARG;
+    h_out8[0] = (long long)b->running.size();
+    h_out8[1] = (long long)b->pending.size();
+    h_out8[2] = b->n_packed;
+    h_out8[3] = b->m_packed;
+    h_out8[4] = b->in_use;
+    h_out8[5] = b->rounds_run;
+    h_out8[6] = b->cap_f;
+    h_out8[7] = b->budget;
+    return PAMO_OK;
 }
 
 }  // extern "C"

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/pamo_b200.h"
 
 namespace pamo {
@@ -18,6 +20,17 @@ inline int grid_for(long long n, int threads = kThreads)
     long long cap = (long long)kNumSMs * 8;
     if (b < 1) b = 1;
     return (int)(b < cap ? b : cap);
+}
+
+// Every kernel this library starts goes through launch(): it counts the launches
+// (pamo_launch_count) and then issues the launch on the given stream.
+inline std::atomic<long long> g_launches{0};
+
+template <typename... KArgs, typename... Args>
+inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args)
+{
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    kernel<<<grid, block, smem, s>>>(args...);
 }
 
 #define PAMO_CUDA_TRY(expr)                                      \

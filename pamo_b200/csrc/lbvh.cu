@@ -66,9 +66,13 @@ __global__ void __launch_bounds__(kThreads) k_scene_bounds(const float4 *pts, co
     }
 }
 
+// Sort key of each face: the Morton code of its box centre over the scene box.
+// With vslot (a batch of meshes) the key is rank << 3*bits | Morton code with
+// `bits` bits per axis, so each mesh's faces are contiguous and form a subtree.
 __global__ void __launch_bounds__(kThreads) k_morton(const float4 *pts, const int4 *tris, int m, const int *scene,
-                                                     uint32_t *keys, int *vals)
+                                                     uint32_t *keys, int *vals, const int *vslot, int bits)
 {
+    const float res = (float)(1 << bits);
     float slo[3], ext[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -87,11 +91,12 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *pts, const in
             uint32_t q[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                float u = (c[k] - slo[k]) / ext[k] * 1024.0f;
-                u = fminf(fmaxf(u, 0.0f), 1023.0f);
+                float u = (c[k] - slo[k]) / ext[k] * res;
+                u = fminf(fmaxf(u, 0.0f), res - 1.0f);
                 q[k] = expand10((uint32_t)u);
             }
             key = q[0] * 4 + q[1] * 2 + q[2];
+            if (vslot) key |= (uint32_t)vslot[t.x] << (3 * bits);
         }
         keys[f] = key;
         vals[f] = (int)f;
@@ -167,8 +172,12 @@ __device__ __forceinline__ int delta(const uint32_t *keys, int L, int i, int j)
 }
 
 // Karras (2012) hierarchy construction, one thread per internal node.
+// roots (batch of meshes, rank in the key bits above `rank_shift`): the child
+// of a node spanning several ranks that holds one rank only is that rank's
+// whole subtree (keys of one rank are contiguous and share every bit above the
+// split), recorded as the start node of the rank's queries.
 __global__ void __launch_bounds__(kThreads) k_karras(const uint32_t *keys, const int *scene, BvhNode *nodes,
-                                                     int *parent)
+                                                     int *parent, int *roots, int rank_shift)
 {
     const int L = scene[7];
     PAMO_GRID_STRIDE(ii, (long long)L - 1)
@@ -200,6 +209,13 @@ __global__ void __launch_bounds__(kThreads) k_karras(const uint32_t *keys, const
         parent[lid] = (i << 1) | 0;
         parent[rid] = (i << 1) | 1;
         if (i == 0) parent[0] = -1;
+        if (roots) {
+            const uint32_t rlo = keys[lo] >> rank_shift, rhi = keys[hi] >> rank_shift;
+            if (rlo != rhi) {
+                if (rlo == (keys[gamma] >> rank_shift)) roots[rlo] = left;
+                if (rhi == (keys[gamma + 1] >> rank_shift)) roots[rhi] = right;
+            }
+        }
     }
 }
 
@@ -231,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) k_refit(const float4 *pts, const int
     PAMO_GRID_STRIDE(p, L)
     {
         int f = vals[p];
-        int4 t = tris[f];
+        int4 t = f >= 0 ? tris[f] : make_int4(-1, -1, -1, 0);
         float3 lo, hi;
         if (face_dead(t)) {
             lo = make_float3(INFINITY, INFINITY, INFINITY);
@@ -308,40 +324,54 @@ void Lbvh::release()
     nodes = nullptr;
     parent = flags = leaf_of_face = scene = nullptr;
     cap = 0;
+    leaves_built = 0;
 }
 
-cudaError_t lbvh_build(Lbvh &b, const float4 *pts, const int4 *tris, int m, cudaStream_t s)
+cudaError_t lbvh_build(Lbvh &b, const float4 *pts, const int4 *tris, int m, cudaStream_t s, const int *vslot,
+                       int n_ranks, int *roots)
 {
     cudaError_t e = b.ensure(m);
     if (e != cudaSuccess) return e;
-    k_scene_init<<<1, 32, 0, s>>>(b.scene);
+    b.leaves_built = m;
+    launch(k_scene_init, 1, 32, 0, s, b.scene);
     if (m == 0) return cudaGetLastError();
-    k_scene_bounds<<<grid_for(m), kThreads, 0, s>>>(pts, tris, m, b.scene);
-    k_morton<<<grid_for(m), kThreads, 0, s>>>(pts, tris, m, b.scene, b.keys, b.vals);
+    launch(k_scene_bounds, grid_for(m), kThreads, 0, s, pts, tris, m, b.scene);
+    // Morton bits per axis: 10, or fewer to leave room for the rank (keys of live
+    // faces stay below 2^31, under the key of removed faces)
+    int rank_bits = 0;
+    while (vslot && (1 << rank_bits) < n_ranks) ++rank_bits;
+    const int bits = vslot ? (31 - rank_bits) / 3 : 10;
+    if (roots) {
+        e = cudaMemsetAsync(roots, 0, (size_t)n_ranks * 4, s);  // one rank: the whole tree
+        if (e != cudaSuccess) return e;
+    }
+    launch(k_morton, grid_for(m), kThreads, 0, s, pts, tris, m, b.scene, b.keys, b.vals, vslot, bits);
     int tiles = (m + kSortTile - 1) / kSortTile;
     uint32_t *k_in = b.keys, *k_out = b.keys2;
     int *v_in = b.vals, *v_out = b.vals2;
     for (int shift = 0; shift < 32; shift += 8) {
-        k_radix_hist<<<tiles, kSortThreads, 0, s>>>(k_in, m, shift, tiles, b.hist);
+        launch(k_radix_hist, tiles, kSortThreads, 0, s, k_in, m, shift, tiles, b.hist);
         e = exclusive_scan(b.hist, b.hist, (long long)256 * tiles, nullptr, b.hist_scratch, nullptr, s);
         if (e != cudaSuccess) return e;
-        k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(k_in, v_in, m, shift, tiles, b.hist, k_out, v_out);
+        launch(k_radix_scatter, tiles, kSortThreads, 0, s, k_in, v_in, m, shift, tiles, b.hist, k_out, v_out);
         uint32_t *tk = k_in; k_in = k_out; k_out = tk;
         int *tv = v_in; v_in = v_out; v_out = tv;
     }
     // after an even number of passes the sorted data is back in keys/vals
-    k_count_leaves<<<1, 1, 0, s>>>(m, b.scene);
-    k_karras<<<grid_for(m), kThreads, 0, s>>>(b.keys, b.scene, b.nodes, b.parent);
-    k_leaf_map<<<grid_for(m), kThreads, 0, s>>>(b.vals, b.scene, b.leaf_of_face, m);
+    launch(k_count_leaves, 1, 1, 0, s, m, b.scene);
+    launch(k_karras, grid_for(m), kThreads, 0, s, b.keys, b.scene, b.nodes, b.parent, vslot ? roots : nullptr,
+           3 * bits);
+    launch(k_leaf_map, grid_for(m), kThreads, 0, s, b.vals, b.scene, b.leaf_of_face, m);
     return cudaGetLastError();
 }
 
 cudaError_t lbvh_refit(Lbvh &b, const float4 *pts, const int4 *tris, int m, cudaStream_t s)
 {
-    if (m < 2) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(b.flags, 0, (size_t)m * 4, s);
+    const long long L = b.leaves_built > m ? b.leaves_built : m;
+    if (L < 2) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(b.flags, 0, (size_t)L * 4, s);
     if (e != cudaSuccess) return e;
-    k_refit<<<grid_for(m), kThreads, 0, s>>>(pts, tris, b.vals, b.scene, b.parent, b.nodes, b.flags);
+    launch(k_refit, grid_for(m), kThreads, 0, s, pts, tris, b.vals, b.scene, b.parent, b.nodes, b.flags);
     return cudaGetLastError();
 }
 

@@ -95,7 +95,7 @@ extern "C" int pamo_self_intersect_noalloc(const float *d_points, const int *d_t
     int *bad = reinterpret_cast<int *>(base + kOffBad);
     int h_bad = 0;
     if (cudaMemsetAsync(bad, 0, sizeof(int), s) != cudaSuccess) return PAMO_ERR_DEVICE;
-    k_na_validate<<<grid_for(n_tris), kThreads, 0, s>>>(d_tris, n_tris, n_pts, bad);
+    launch(k_na_validate, grid_for(n_tris), kThreads, 0, s, d_tris, n_tris, n_pts, bad);
     if (cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PAMO_ERR_DEVICE;
     if (cudaStreamSynchronize(s) != cudaSuccess) return PAMO_ERR_DEVICE;
     if (h_bad) return PAMO_ERR_INVALID_ARG;
@@ -121,7 +121,7 @@ extern "C" int pamo_self_intersect_noalloc(const float *d_points, const int *d_t
     b.scene = reinterpret_cast<int *>(base + kOffScene);
 
     // the array keeps the previous call's contents: reset what must start at zero
-    k_na_convert<<<grid_for(n_pts > n_tris ? n_pts : n_tris), kThreads, 0, s>>>(d_points, n_pts, d_tris, n_tris, p4,
+    launch(k_na_convert, grid_for(n_pts > n_tris ? n_pts : n_tris), kThreads, 0, s, d_points, n_pts, d_tris, n_tris, p4,
                                                                                t4);
     if (cudaMemsetAsync(active, 1, (size_t)n_tris, s) != cudaSuccess) return PAMO_ERR_DEVICE;
     if (cudaMemsetAsync(cnt, 0, sizeof(RoundCounters), s) != cudaSuccess) return PAMO_ERR_DEVICE;

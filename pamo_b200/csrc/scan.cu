@@ -105,13 +105,13 @@ cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *
         return cudaSuccess;
     }
     if (n_max <= (long long)kSingleThreads * kSingleItems) {
-        k_scan_single<<<1, kSingleThreads, 0, s>>>(in, out, n_max, d_n, d_total);
+        launch(k_scan_single, 1, kSingleThreads, 0, s, in, out, n_max, d_n, d_total);
         return cudaGetLastError();
     }
     long long tiles = (n_max + kScanTile - 1) / kScanTile;
-    k_scan_reduce<<<(unsigned)tiles, kScanThreads, 0, s>>>(in, n_max, d_n, scratch);
-    k_scan_tile_sums<<<1, 1024, 0, s>>>(scratch, tiles, n_max, d_n, d_total);
-    k_scan_down<<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n_max, d_n, scratch);
+    launch(k_scan_reduce, (unsigned)tiles, kScanThreads, 0, s, in, n_max, d_n, scratch);
+    launch(k_scan_tile_sums, 1, 1024, 0, s, scratch, tiles, n_max, d_n, d_total);
+    launch(k_scan_down, (unsigned)tiles, kScanThreads, 0, s, in, out, n_max, d_n, scratch);
     return cudaGetLastError();
 }
 

@@ -45,6 +45,7 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr float kCostRange = 10.0f;
+constexpr double kRebuildFraction = 0.6;
 
 __device__ __forceinline__ uint32_t quantise_cost(float c)
 {
@@ -189,16 +190,21 @@ struct CostArgs {
     unsigned long long *vmin;
     float tres, edge_s;
     int is_stuck;
+    // batch mode (null otherwise): per-mesh parameters and stale state
+    const SlotInfo *slots;
+    const SlotCounters *scnt;
+    const int *vslot;
 };
 
 // Returns true when the reference writes a new cost for the edge.
-__device__ bool edge_cost_value(const CostArgs &A, int u, int v, uint32_t &out)
+__device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, bool inv_v, float tres, float edge_s,
+                                int is_stuck, uint32_t &out)
 {
-    if (A.invalid[u] && A.invalid[v]) {
+    if (inv_u && inv_v) {
         out = 0xFFFFFFFFu;
         return true;
     }
-    if (A.is_stuck) return false;
+    if (is_stuck) return false;
     const int ua = A.first_near[u], ub = A.first_near[u + 1];
     const int va = A.first_near[v], vb = A.first_near[v + 1];
     int dup = 0;
@@ -229,8 +235,8 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, uint32_t &out)
         }
     }
     V3 v0 = v3(A.pts[u]), v1 = v3(A.pts[v]);
-    elen = elen / (float)nedge / A.edge_s * A.tres;
-    elen = elen + vnorm(vsub(v0, v1)) / A.edge_s * A.tres;
+    elen = elen / (float)nedge / edge_s * tres;
+    elen = elen + vnorm(vsub(v0, v1)) / edge_s * tres;
     V3 mid = vmid(v0, v1);
 
     float Qa = 0.0f;
@@ -270,30 +276,70 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, uint32_t &out)
     float r2 = m02 * x + m12 * y + m22 * z + m23 * w;
     float r3 = m03 * x + m13 * y + m23 * z + m33 * w;
     float qe = r0 * x + r1 * y + r2 * z + r3 * w;
-    float cost = qe / (A.edge_s * A.edge_s);
-    out = quantise_cost(cost + elen + Qa / (float)ntri * A.tres);
+    float cost = qe / (edge_s * edge_s);
+    out = quantise_cost(cost + elen + Qa / (float)ntri * tres);
     return true;
 }
 
-// Threads walk the faces in the hierarchy's leaf (Morton) order and handle each
-// face's edges, so neighbouring lanes gather neighbouring vertices; the results
-// are indexed by edge, so the order of work does not change them.
+// Edge passes run in the hierarchy's leaf (Morton) order: a block takes
+// kChunkFaces consecutive leaves, lists their faces' edges in shared memory
+// (each face owns its 0-3 descending edges) and its threads take the list in
+// turn, so neighbouring lanes gather neighbouring vertices and every lane has an
+// edge.  Results are indexed by edge and winners never share a face, so the
+// order of work does not change them.
+constexpr int kChunkFaces = 2 * kThreads;
+constexpr int kChunkEdges = 3 * kChunkFaces;
+
+__device__ __forceinline__ int chunk_edges(const int *order, const int *first_edge, int L, long long base,
+                                           int *s_list)
+{
+    int fe[2], c[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        long long p = base + 2 * threadIdx.x + k;
+        int f = p < L ? order[p] : -1;  // -1: past the end, or a face removed since the build
+        fe[k] = f >= 0 ? first_edge[f] : 0;
+        c[k] = f >= 0 ? first_edge[f + 1] - fe[k] : 0;
+    }
+    int total;
+    int off = block_excl_scan<kThreads>(c[0] + c[1], total);
+    for (int j = 0; j < c[0]; ++j) s_list[off + j] = fe[0] + j;
+    for (int j = 0; j < c[1]; ++j) s_list[off + c[0] + j] = fe[1] + j;
+    __syncthreads();
+    return total;
+}
+
 __global__ void __launch_bounds__(kThreads) k_edge_cost(CostArgs A, const int *order, const int *scene,
                                                         const int *first_edge)
 {
+    __shared__ int s_list[kChunkEdges];
     const int L = scene[7];
-    PAMO_GRID_STRIDE(pp, L)
-    {
-        const int f = order[pp];
-        for (int e = first_edge[f]; e < first_edge[f + 1]; ++e) {
+    for (long long base = (long long)blockIdx.x * kChunkFaces; base < L; base += (long long)gridDim.x * kChunkFaces) {
+        const int total = chunk_edges(order, first_edge, L, base, s_list);
+        for (int q = threadIdx.x; q < total; q += kThreads) {
+            const int e = s_list[q];
             int2 ed = A.edges[e];
             uint32_t c;
-            if (edge_cost_value(A, ed.x, ed.y, c)) A.edge_cost[e] = c;
-            else c = A.edge_cost[e];  // the reference keeps the previous round's value
+            if (!A.slots) {
+                if (edge_cost_value(A, ed.x, ed.y, A.invalid[ed.x], A.invalid[ed.y], A.tres, A.edge_s, A.is_stuck, c))
+                    A.edge_cost[e] = c;
+                else
+                    c = A.edge_cost[e];  // the reference keeps the previous round's value
+            } else {  // the mesh's own parameters, invalid table and stale costs (mesh-local numbers)
+                const int r = A.vslot[ed.x];
+                const SlotInfo &S = A.slots[r];
+                const int el = e - A.scnt[r].edge_off;
+                if (edge_cost_value(A, ed.x, ed.y, S.invalid[ed.x - S.vert_off], S.invalid[ed.y - S.vert_off], S.tres,
+                                    *S.scale, S.is_stuck, c))
+                    S.edge_cost[el] = c;
+                else
+                    c = S.edge_cost[el];
+            }
             unsigned long long key = ((unsigned long long)c << 32) | (unsigned)e;
             atomicMin(&A.vmin[ed.x], key);
             atomicMin(&A.vmin[ed.y], key);
         }
+        __syncthreads();
     }
 }
 
@@ -322,6 +368,9 @@ struct CollapseArgs {
     int *occ;
     int *eflag;
     uint32_t collapse_t;
+    const SlotInfo *slots;  // batch mode (null otherwise)
+    const SlotCounters *scnt;
+    const int *vslot;
 };
 
 __device__ __forceinline__ bool faces_min_ok(const CollapseArgs &A, int lo, int hi, unsigned long long key)
@@ -336,14 +385,23 @@ __device__ __forceinline__ bool faces_min_ok(const CollapseArgs &A, int lo, int 
 __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A, const int *order, const int *scene,
                                                        const int *first_edge)
 {
+    __shared__ int s_list[kChunkEdges];
     const int L = scene[7];
-    PAMO_GRID_STRIDE(pp, L)
-    {
-      const int f = order[pp];
-      for (int e = first_edge[f]; e < first_edge[f + 1]; ++e) {
+    for (long long base = (long long)blockIdx.x * kChunkFaces; base < L; base += (long long)gridDim.x * kChunkFaces) {
+      const int total = chunk_edges(order, first_edge, L, base, s_list);
+      for (int q = threadIdx.x; q < total; q += kThreads) {
+        const int e = s_list[q];
         int win = 0;
-        uint32_t c = A.edge_cost[e];
-        if (c <= A.collapse_t) {
+        uint32_t c, collapse_t;
+        if (!A.slots) {
+            c = A.edge_cost[e];
+            collapse_t = A.collapse_t;
+        } else {
+            const int r = A.vslot[A.edges[e].x];
+            c = A.slots[r].edge_cost[e - A.scnt[r].edge_off];
+            collapse_t = A.slots[r].collapse_t;
+        }
+        if (c <= collapse_t) {
             int2 ed = A.edges[e];
             const int u = ed.x, v = ed.y;
             unsigned long long key = ((unsigned long long)c << 32) | (unsigned)e;
@@ -393,6 +451,7 @@ __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A, const int
         }
         A.eflag[e] = win;
       }
+      __syncthreads();
     }
 }
 
@@ -433,37 +492,69 @@ __global__ void k_line_flags(const int2 *edges, const int *n_edges, const float4
 }
 
 // Coincident-endpoint collapses: positions were read (k_line_flags) before any
-// write; the writes are applied here in edge order by one thread.  Runs only
-// when at least one edge was flagged (rare: needs exactly equal coordinates).
-__global__ void k_line_apply(const int2 *edges, const int *n_edges, const int *eflag, const int *first_near,
-                             const int *near_tris, float4 *pts, int4 *tris, int *occ, int *collapsed,
-                             RoundCounters *cnt)
+// write; the writes are applied in edge order by one thread.  Flagged edges are
+// rare (exactly equal coordinates), so one block of kLineThreads finds them
+// chunk by chunk and its thread 0 applies each chunk's edges in order.
+constexpr int kLineThreads = 1024;
+constexpr int kLinePerThread = 8;
+
+__device__ __forceinline__ void line_collapse(int u, int v, const int *first_near, const int *near_tris, float4 *pts,
+                                              int4 *tris, int *occ)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    pts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+    occ[v] = 0;
+    for (int a = first_near[u]; a < first_near[u + 1]; ++a) {
+        int f = near_tris[a];
+        if (face_has(tris[f], v)) tris[f] = make_int4(-1, -1, -1, 0);
+    }
+    for (int a = first_near[v]; a < first_near[v + 1]; ++a) {
+        int f = near_tris[a];
+        int4 t = tris[f];
+        if (face_has(t, u)) t = make_int4(-1, -1, -1, 0);
+        else if (t.x == v) t.x = u;
+        else if (t.y == v) t.y = u;
+        else if (t.z == v) t.z = u;
+        tris[f] = t;
+    }
+}
+
+// Calls on_edge(e) on thread 0 for every flagged e < E, in ascending order.
+template <typename OnEdge>
+__device__ __forceinline__ void for_flagged_in_order(const int *eflag, int E, OnEdge on_edge)
+{
+    __shared__ int s_idx[kLineThreads * kLinePerThread];
+    for (long long base = 0; base < E; base += kLineThreads * kLinePerThread) {
+        int local[kLinePerThread];
+        int c = 0;
+#pragma unroll
+        for (int k = 0; k < kLinePerThread; ++k) {
+            long long e = base + (long long)threadIdx.x * kLinePerThread + k;
+            if (e < E && eflag[e]) local[c++] = (int)e;
+        }
+        int total;
+        int off = block_excl_scan<kLineThreads>(c, total);
+        for (int k = 0; k < c; ++k) s_idx[off + k] = local[k];
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int i = 0; i < total; ++i) on_edge(s_idx[i]);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kLineThreads) k_line_apply(const int2 *edges, const int *n_edges, const int *eflag,
+                                                             const int *first_near, const int *near_tris, float4 *pts,
+                                                             int4 *tris, int *occ, int *collapsed, RoundCounters *cnt)
+{
     const int E = *n_edges;
-    int nm = cnt->n_main, k = 0;
-    if (cnt->n_line > 0) {
-        for (int e = 0; e < E; ++e) {
-            if (!eflag[e]) continue;
+    const int nm = cnt->n_main;
+    int k = 0;
+    if (cnt->n_line > 0)
+        for_flagged_in_order(eflag, E, [&](int e) {
             int u = edges[e].x, v = edges[e].y;
             collapsed[nm + k++] = e;
-            pts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
-            occ[v] = 0;
-            for (int a = first_near[u]; a < first_near[u + 1]; ++a) {
-                int f = near_tris[a];
-                if (face_has(tris[f], v)) tris[f] = make_int4(-1, -1, -1, 0);
-            }
-            for (int a = first_near[v]; a < first_near[v + 1]; ++a) {
-                int f = near_tris[a];
-                int4 t = tris[f];
-                if (face_has(t, u)) t = make_int4(-1, -1, -1, 0);
-                else if (t.x == v) t.x = u;
-                else if (t.y == v) t.y = u;
-                else if (t.z == v) t.z = u;
-                tris[f] = t;
-            }
-        }
-    }
+            line_collapse(u, v, first_near, near_tris, pts, tris, occ);
+        });
+    if (threadIdx.x != 0) return;
     cnt->n_line = k;
     cnt->n_total = nm + k;
     int window = ((nm + 511) / 512) * 512;  // grid of the reference's undo-candidate launch
@@ -495,6 +586,26 @@ __device__ __forceinline__ int shared_indices(int4 a, int4 b)
            (a.z == b.x) + (a.z == b.y) + (a.z == b.z);
 }
 
+// The active live faces in leaf (Morton) order, appended a warp at a time, so
+// the query threads that follow all have a face and neighbouring lanes walk
+// neighbouring paths.
+__global__ void k_active_list(const int *__restrict__ vals, const int *scene, const uint8_t *__restrict__ active,
+                              const int4 *__restrict__ tris, int *qlist, RoundCounters *cnt)
+{
+    const int L = scene[7];
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < L; base += (long long)blockDim.x * gridDim.x) {
+        const long long p = base + threadIdx.x;
+        int f = p < L ? vals[p] : -1;
+        bool ok = f >= 0 && active[f] && tris[f].x != -1;
+        unsigned ball = __ballot_sync(0xffffffffu, ok);
+        int first = 0;
+        if (lane == 0 && ball) first = atomicAdd(&cnt->n_query, __popc(ball));
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (ok) qlist[first + __popc(ball & ((1u << lane) - 1u))] = f;
+    }
+}
+
 // For each active live face, enumerate overlapping leaves and append candidate
 // pairs.  A pair of two active faces is emitted once (by the lower index);
 // pairs sharing two or more vertex indices are never reported by the reference
@@ -502,22 +613,28 @@ __device__ __forceinline__ int shared_indices(int4 a, int4 b)
 __global__ void __launch_bounds__(kThreads) k_query(const BvhNode *__restrict__ nodes, const int *__restrict__ vals,
                                                     const int *scene, const float4 *__restrict__ pts,
                                                     const int4 *__restrict__ tris, const uint8_t *__restrict__ active,
-                                                    int m, uint2 *pairs, long long cap_pairs, RoundCounters *cnt)
+                                                    int m, uint2 *pairs, long long cap_pairs, RoundCounters *cnt,
+                                                    const int *roots, const int *vslot, const int *qlist)
 {
     const int L = scene[7];
     int stack[kStack];
-    // queries in leaf (Morton) order: neighbouring lanes walk neighbouring paths
-    PAMO_GRID_STRIDE(pp, L)
+    // queries from the list of active faces (k_active_list), or every leaf in
+    // leaf order with the inactive ones skipped
+    const int N = qlist ? cnt->n_query : L;
+    PAMO_GRID_STRIDE(pp, N)
     {
-        const int f = vals[pp];
-        if (!active[f] || L < 2) continue;
+        const int f = qlist ? qlist[pp] : vals[pp];
+        if (f < 0 || !active[f] || L < 2) continue;
         int4 t = tris[f];
         if (t.x == -1) continue;
         float4 a = pts[t.x], b = pts[t.y], c = pts[t.z];
         float3 qlo = make_float3(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)));
         float3 qhi = make_float3(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)));
+        // a batch starts at the face's own mesh subtree (a leaf: a one-face mesh)
+        const int start = roots ? roots[vslot[t.x]] : 0;
+        if (start < 0) continue;
         int sp = 0;
-        stack[sp++] = 0;
+        stack[sp++] = start;
         // a tree visits each of its L-1 inner nodes at most once per query; the
         // bound only guards against a corrupted hierarchy
         int budget = 2 * L + 16;
@@ -535,7 +652,7 @@ __global__ void __launch_bounds__(kThreads) k_query(const BvhNode *__restrict__ 
                 int child = __float_as_int(lo.w);
                 if (child < 0) {
                     int g = vals[~child];
-                    if (g == f) continue;
+                    if (g < 0 || g == f) continue;  // empty leaves have empty boxes; guard anyway
                     if (active[g] && g < f) continue;
                     int4 tg = tris[g];
                     if (shared_indices(t, tg) >= 2) continue;
@@ -667,6 +784,17 @@ __global__ void k_compact(const float4 *pts, const int *occ, const int *pts_map,
     }
 }
 
+// After compaction: leaf p's face gets its compacted index, or -1 if removed.
+__global__ void k_remap_leaves(int *vals, const int *scene, const int *fflag, const int *fpos)
+{
+    const int L = scene[7];
+    PAMO_GRID_STRIDE(p, L)
+    {
+        int f = vals[p];
+        vals[p] = (f >= 0 && fflag[f]) ? fpos[f] : -1;
+    }
+}
+
 __global__ void k_validate_faces(const int *tris, int m, int n, int *bad)
 {
     int local = 0;
@@ -685,6 +813,193 @@ __global__ void k_validate_range(const int *v, int count, int hi, int *bad)
     int local = 0;
     PAMO_GRID_STRIDE(i, count) local += (v[i] < 0 || v[i] > hi);
     if (local) atomicAdd(bad, local);
+}
+
+// ---------------------------------------------------------------------------
+// Batch kernels.  Per-mesh loops use blockIdx.y = the mesh's rank and stride
+// over the mesh's range with blockIdx.x.
+#define SLOT_STRIDE(j, count) \
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < (long long)(count); j += (long long)blockDim.x * gridDim.x)
+
+// Before the round, per mesh, as the single-mesh round does (cusimp_free.cu:899-916):
+// stuck: the undo list starts with the previous one mapped through the previous
+// vertex map; not stuck with a non-empty list: the invalid table is cleared.
+__global__ void k_b_pre_copy(const SlotInfo *slots)
+{
+    const SlotInfo S = slots[blockIdx.y];
+    if (S.is_stuck) {
+        SLOT_STRIDE(j, S.n_undo_in)
+        {
+            int x = S.undo_prev[j];
+            S.tmp_undo[j] = x;
+            S.undo_list[j] = S.pts_map[x];
+        }
+    } else if (S.clear_invalid) {
+        SLOT_STRIDE(j, S.cap_v) S.invalid[j] = 0;
+    }
+}
+
+__global__ void k_b_pre_mark(const SlotInfo *slots)
+{
+    const SlotInfo S = slots[blockIdx.y];
+    SLOT_STRIDE(j, S.n_undo_in) S.invalid[S.undo_prev[j]] = 1;
+}
+
+__global__ void k_b_vslot(const SlotInfo *slots, int *vslot)
+{
+    const SlotInfo S = slots[blockIdx.y];
+    SLOT_STRIDE(j, S.n) vslot[S.vert_off + j] = (int)blockIdx.y;
+}
+
+// first packed edge and edge count of each mesh (first_edge has m + 1 entries)
+__global__ void k_b_edge_off(const SlotInfo *slots, const int *first_edge, SlotCounters *scnt, int K)
+{
+    PAMO_GRID_STRIDE(r, K)
+    {
+        const SlotInfo &S = slots[r];
+        scnt[r].edge_off = first_edge[S.face_off];
+        scnt[r].n_edges = first_edge[S.face_off + S.m] - first_edge[S.face_off];
+    }
+}
+
+// pos = exclusive scan over the packed edges of a flag, total = its sum:
+// each mesh's first entry and count in the compacted list.
+__device__ __forceinline__ void seg_of_scan(const int *pos, int total, int n_all, int first, int count, int &off,
+                                            int &cnt)
+{
+    off = first < n_all ? pos[first] : total;
+    int end = first + count < n_all ? pos[first + count] : total;
+    cnt = end - off;
+}
+
+__global__ void k_b_main(const int *pos, const RoundCounters *cnt, SlotCounters *scnt, int K)
+{
+    PAMO_GRID_STRIDE(r, K)
+    {
+        int off, c;
+        seg_of_scan(pos, cnt->n_main, cnt->n_edges, scnt[r].edge_off, scnt[r].n_edges, off, c);
+        scnt[r].main_off = off;
+        scnt[r].n_main = c;
+    }
+}
+
+// Coincident-endpoint collapses over the whole batch (the single-mesh version's
+// order: positions read before any write, writes in edge order), and each
+// mesh's undo-candidate window: its collapsed edges then its coincident ones,
+// cut at the reference's launch-grid roundup of its own collapsed count.
+__global__ void __launch_bounds__(kLineThreads) k_b_line_apply(const int2 *edges, const int *n_edges,
+                                                               const int *eflag, const int *first_near,
+                                                               const int *near_tris, float4 *pts, int4 *tris, int *occ,
+                                                               int *line_list, const int *vslot, RoundCounters *cnt,
+                                                               SlotCounters *scnt, int K)
+{
+    const int E = *n_edges;
+    for (int r = threadIdx.x; r < K; r += blockDim.x) scnt[r].n_line = 0;
+    __syncthreads();
+    int k = 0;
+    if (cnt->n_line > 0)
+        for_flagged_in_order(eflag, E, [&](int e) {
+            int u = edges[e].x, v = edges[e].y;
+            line_list[k++] = e;
+            scnt[vslot[u]].n_line++;
+            line_collapse(u, v, first_near, near_tris, pts, tris, occ);
+        });
+    if (threadIdx.x != 0) return;
+    cnt->n_line = k;
+    cnt->n_total = cnt->n_main + k;
+    int line_off = 0, cand_off = 0;
+    for (int r = 0; r < K; ++r) {
+        SlotCounters &c = scnt[r];
+        c.line_off = line_off;
+        line_off += c.n_line;
+        int total = c.n_main + c.n_line;
+        int window = ((c.n_main + 511) / 512) * 512;
+        c.n_considered = total < window ? total : window;
+        c.cand_off = cand_off;
+        cand_off += c.n_considered;
+    }
+    cnt->n_considered = cand_off;
+}
+
+__global__ void k_b_cand_fill(const int *collapsed, const int *line_list, const int2 *edges, const int *vslot,
+                              const RoundCounters *cnt, const SlotCounters *scnt, int *cand)
+{
+    const int nm = cnt->n_main, nl = cnt->n_line;
+    PAMO_GRID_STRIDE(p, (long long)nm + nl)
+    {
+        int e, r, k;
+        if (p < nm) {
+            e = collapsed[p];
+            r = vslot[edges[e].x];
+            k = (int)p - scnt[r].main_off;
+        } else {
+            int q = (int)p - nm;
+            e = line_list[q];
+            r = vslot[edges[e].x];
+            k = scnt[r].n_main + q - scnt[r].line_off;
+        }
+        if (k < scnt[r].n_considered) cand[scnt[r].cand_off + k] = e;
+    }
+}
+
+__global__ void k_b_undo_counts(const int *upos, const RoundCounters *cnt, SlotCounters *scnt, int K)
+{
+    PAMO_GRID_STRIDE(r, K)
+    {
+        int off, c;
+        seg_of_scan(upos, cnt->n_undo, cnt->n_considered, scnt[r].cand_off, scnt[r].n_considered, off, c);
+        scnt[r].undo_off = off;
+        scnt[r].n_undo = c;
+    }
+}
+
+// undo edges (packed) and each mesh's undo vertices (mesh-local numbers)
+__global__ void k_b_undo_scatter(const int *uflag, const int *upos, const RoundCounters *cnt, const int *cand,
+                                 const int2 *edges, const int *vslot, const SlotInfo *slots,
+                                 const SlotCounters *scnt, int *undo_edges)
+{
+    const int N = cnt->n_considered;
+    PAMO_GRID_STRIDE(p, N)
+    {
+        if (!uflag[p]) continue;
+        int k = upos[p];
+        int e = cand[p];
+        int2 ed = edges[e];
+        undo_edges[k] = e;
+        int r = vslot[ed.x];
+        const SlotInfo &S = slots[r];
+        int j = k - scnt[r].undo_off;
+        S.tmp_undo[2 * j] = ed.x - S.vert_off;
+        S.tmp_undo[2 * j + 1] = ed.y - S.vert_off;
+    }
+}
+
+// undo_list[first + j] = pts_map[tmp_undo[j]] per mesh (the previous round's map)
+__global__ void k_b_rearrange(const SlotInfo *slots)
+{
+    const SlotInfo S = slots[blockIdx.y];
+    SLOT_STRIDE(j, S.pass_count) S.undo_list[S.pass_first + j] = S.pts_map[S.tmp_undo[j]];
+}
+
+// each mesh's vertex map in its own numbers, and the copy of its undo list
+__global__ void k_b_local_map(const SlotInfo *slots, const int *gmap)
+{
+    const SlotInfo S = slots[blockIdx.y];
+    const int base = gmap[S.vert_off];
+    SLOT_STRIDE(j, (long long)S.n + 1) S.pts_map[j] = gmap[S.vert_off + j] - base;
+    SLOT_STRIDE(j, S.nvu) S.undo_prev[j] = S.undo_list[j];
+}
+
+__global__ void k_b_next(const SlotInfo *slots, const int *gmap, const int *fpos, SlotCounters *scnt, int K)
+{
+    PAMO_GRID_STRIDE(r, K)
+    {
+        const SlotInfo &S = slots[r];
+        scnt[r].vert_off_next = gmap[S.vert_off];
+        scnt[r].n_next = gmap[S.vert_off + S.n] - gmap[S.vert_off];
+        scnt[r].face_off_next = fpos[S.face_off];
+        scnt[r].m_next = fpos[S.face_off + S.m] - fpos[S.face_off];
+    }
 }
 
 }  // namespace
@@ -748,8 +1063,8 @@ int Stage2::validate(const int *d_tris, int n, int m, const int *d_undo, int n_u
 {
     int *bad = dev_misc + 32;
     S2_TRY_EARLY(cudaMemsetAsync(bad, 0, 4, s));
-    if (m > 0) k_validate_faces<<<grid_for(m), kThreads, 0, s>>>(d_tris, m, n, bad);
-    if (n_undo > 0) k_validate_range<<<grid_for(n_undo), kThreads, 0, s>>>(d_undo, n_undo, undo_hi, bad);
+    if (m > 0) launch(k_validate_faces, grid_for(m), kThreads, 0, s, d_tris, m, n, bad);
+    if (n_undo > 0) launch(k_validate_range, grid_for(n_undo), kThreads, 0, s, d_undo, n_undo, undo_hi, bad);
     S2_TRY_EARLY(cudaMemcpyAsync(hcnt, bad, 4, cudaMemcpyDeviceToHost, s));
     S2_TRY_EARLY(cudaStreamSynchronize(s));
     return hcnt->n_main == 0 ? PAMO_OK : PAMO_ERR_INVALID_ARG;
@@ -775,6 +1090,8 @@ void Stage2::release()
     vmin = nullptr; eflag = collapsed = nullptr; active = isect = nullptr; uflag = undo_edges = fflag = nullptr;
     pairs = nullptr; scan_scratch = nullptr; dev_misc = nullptr; dcnt = nullptr; hcnt = nullptr; h_scalars = nullptr;
     bvh.release();
+    bvh_carried = false;
+    bvh_leaves = 0;
     cap_pts = cap_tris = cap_edges = cap_undo = cap_pairs = 0;
 }
 
@@ -883,10 +1200,15 @@ static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s)
     S.prof.begin(PH_REFIT, s);
     if ((e = lbvh_refit(S.bvh, S.pts, S.tris, m, s)) != cudaSuccess) return e;
     S.prof.begin(PH_QUERY, s);
-    k_query<<<grid_for(m), kThreads, 0, s>>>(S.bvh.nodes, S.bvh.vals, S.bvh.scene, S.pts, S.tris, S.active, m,
-                                             S.pairs, S.cap_pairs, S.dcnt);
+    const bool batch = S.n_slots > 0;
+    if ((e = cudaMemsetAsync(&S.dcnt->n_query, 0, sizeof(int), s)) != cudaSuccess) return e;
+    launch(k_active_list, grid_for(m), kThreads, 0, s, (const int *)S.bvh.vals, (const int *)S.bvh.scene,
+           (const uint8_t *)S.active, (const int4 *)S.tris, S.fflag, S.dcnt);
+    launch(k_query, grid_for(m), kThreads, 0, s, S.bvh.nodes, S.bvh.vals, S.bvh.scene, S.pts, S.tris, S.active, m,
+                                             S.pairs, S.cap_pairs, S.dcnt, batch ? (const int *)S.roots : nullptr,
+                                             batch ? (const int *)S.vslot : nullptr, (const int *)S.fflag);
     S.prof.begin(PH_PAIRS, s);
-    k_pairs<<<grid_for(S.cap_pairs), kThreads, 0, s>>>(S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris, S.isect, 1e-3f);
+    launch(k_pairs, grid_for(S.cap_pairs), kThreads, 0, s, S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris, S.isect, 1e-3f);
     S.prof.end(s);
     return cudaGetLastError();
 }
@@ -895,33 +1217,33 @@ static cudaError_t undo_check(Stage2 &S, cudaStream_t s)
 {
     S.prof.begin(PH_UNDO, s);
     const long long NC = S.cap_edges;
-    k_undo_flags<<<grid_for(NC), kThreads, 0, s>>>(S.collapsed, S.dcnt, S.edges, S.first_near, S.near_tris, S.isect,
+    launch(k_undo_flags, grid_for(NC), kThreads, 0, s, S.collapsed, S.dcnt, S.edges, S.first_near, S.near_tris, S.isect,
                                                    S.uflag);
     // positions of the flagged entries (in collapsed-list order)
     cudaError_t e = exclusive_scan(S.uflag, S.eflag, NC, &S.dcnt->n_considered, S.scan_scratch, &S.dcnt->n_undo, s);
     if (e != cudaSuccess) return e;
-    k_undo_scatter<<<grid_for(NC), kThreads, 0, s>>>(S.uflag, S.eflag, S.dcnt, S.collapsed, S.edges, S.undo_edges,
+    launch(k_undo_scatter, grid_for(NC), kThreads, 0, s, S.uflag, S.eflag, S.dcnt, S.collapsed, S.edges, S.undo_edges,
                                                      S.tmp_undo);
     S.prof.end(s);
     return cudaGetLastError();
 }
 
 int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, const int *d_undo_in, int n_undo_in,
-                  int *n_undo_out, cudaStream_t s)
+                  int *n_undo_out, cudaStream_t s, bool keep_bvh)
 {
     int nvu = 0, first = 0;
     S2_TRY(cudaMemsetAsync(dcnt, 0, sizeof(RoundCounters), s));
     if (is_stuck) {
         if (n_undo_in > 0) {
             S2_TRY(cudaMemcpyAsync(tmp_undo, d_undo_in, (size_t)n_undo_in * 4, cudaMemcpyDeviceToDevice, s));
-            k_rearrange<<<grid_for(n_undo_in), kThreads, 0, s>>>(tmp_undo, pts_map, undo_list, 0, n_undo_in);
+            launch(k_rearrange, grid_for(n_undo_in), kThreads, 0, s, tmp_undo, pts_map, undo_list, 0, n_undo_in);
         }
         nvu += n_undo_in;
         first += n_undo_in;
     } else if (n_undo_in != 0) {
         S2_TRY(cudaMemsetAsync(invalid_table, 0, (size_t)cap_pts + 1, s));
     }
-    if (n_undo_in > 0) k_mark_invalid<<<grid_for(n_undo_in), kThreads, 0, s>>>(d_undo_in, n_undo_in, invalid_table);
+    if (n_undo_in > 0) launch(k_mark_invalid, grid_for(n_undo_in), kThreads, 0, s, d_undo_in, n_undo_in, invalid_table);
 
     const float tres = threshold, edge_s = scale;
     // host-side conversion as in the reference (cusimp_free.cu:923): the
@@ -931,37 +1253,46 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     const uint32_t collapse_t = (uint32_t)(unsigned long long)(ct / kCostRange * 4294967296.0f);
 
     prof.begin(PH_SETUP, s);
-    k_round_init<<<grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s>>>(opts, otris, pts, tris, occ, first_near,
+    launch(k_round_init, grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s, opts, otris, pts, tris, occ, first_near,
                                                                        cursor, vmin, n, m);
-    k_face_a<<<grid_for(m), kThreads, 0, s>>>(pts, tris, m, first_near, first_edge, plane, elen4);
+    launch(k_face_a, grid_for(m), kThreads, 0, s, pts, tris, m, first_near, first_edge, plane, elen4);
     if (m > 0) S2_TRY(cudaMemsetAsync(first_edge + m, 0, 4, s));
     S2_TRY(exclusive_scan(first_near, first_near, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
     S2_TRY(exclusive_scan(first_edge, first_edge, (long long)m + 1, nullptr, scan_scratch, &dcnt->n_edges, s));
     const int *d_n_edges = &dcnt->n_edges;
-    k_face_b<<<grid_for(m), kThreads, 0, s>>>(tris, m, first_near, cursor, near_tris, first_edge, edges);
-    k_vertex_quadric<<<grid_for(n), kThreads, 0, s>>>(first_near, near_tris, plane, tris, quad, nxt, n);
-    // the hierarchy only depends on the round input: build it now
+    launch(k_face_b, grid_for(m), kThreads, 0, s, tris, m, first_near, cursor, near_tris, first_edge, edges);
+    launch(k_vertex_quadric, grid_for(n), kThreads, 0, s, first_near, near_tris, plane, tris, quad, nxt, n);
+    // The hierarchy only needs the round input's faces as leaves: build it, or
+    // keep the previous round's (leaves renumbered by compact(), removed faces
+    // as empty leaves) while at least kRebuildFraction of its leaves are faces.
+    // Queries find every overlapping leaf whatever the tree, so the pairs found
+    // do not depend on this choice; the refit before each query sets the boxes.
     prof.begin(PH_LBVH_BUILD, s);
-    S2_TRY(lbvh_build(bvh, pts, tris, m, s));
+    if (!(keep_bvh && bvh_carried && m <= bvh_leaves && (double)m >= kRebuildFraction * (double)bvh_leaves)) {
+        S2_TRY(lbvh_build(bvh, pts, tris, m, s));
+        bvh_leaves = m;
+    }
+    bvh_carried = false;
 
     const long long EMAX = 3LL * m;
     prof.begin(PH_EDGE_COST, s);
     CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, nxt, plane, elen4, quad, invalid_table,
-                edge_cost, vmin, tres, edge_s, is_stuck ? 1 : 0};
-    k_edge_cost<<<grid_for(m), kThreads, 0, s>>>(ca, bvh.vals, bvh.scene, first_edge);
+                edge_cost, vmin, tres, edge_s, is_stuck ? 1 : 0, nullptr, nullptr, nullptr};
+    launch(k_edge_cost, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
     CollapseArgs cl{edges, d_n_edges, edge_cost, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
-                    collapse_t};
+                    collapse_t, nullptr, nullptr, nullptr};
     prof.begin(PH_COLLAPSE, s);
-    k_collapse<<<grid_for(m), kThreads, 0, s>>>(cl, bvh.vals, bvh.scene, first_edge);
+    launch(k_collapse, grid_for(m, kChunkFaces), kThreads, 0, s, cl, bvh.vals, bvh.scene, first_edge);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
-    k_scatter_flagged<<<grid_for(EMAX), kThreads, 0, s>>>(eflag, uflag, d_n_edges, collapsed, 0);
+    launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
     prof.begin(PH_CLEANUP, s);
-    k_remove_invalid_faces<<<grid_for(m), kThreads, 0, s>>>(tris, m);
-    k_line_flags<<<grid_for(EMAX), kThreads, 0, s>>>(edges, d_n_edges, pts, eflag, &dcnt->n_line);
-    k_line_apply<<<1, 32, 0, s>>>(edges, d_n_edges, eflag, first_near, near_tris, pts, tris, occ, collapsed, dcnt);
+    launch(k_remove_invalid_faces, grid_for(m), kThreads, 0, s, tris, m);
+    launch(k_line_flags, grid_for(EMAX), kThreads, 0, s, edges, d_n_edges, pts, eflag, &dcnt->n_line);
+    launch(k_line_apply, 1, kLineThreads, 0, s, edges, d_n_edges, eflag, first_near, near_tris, pts, tris, occ, collapsed,
+           dcnt);
 
     S2_TRY(cudaMemsetAsync(active, 0, (size_t)m, s));
-    k_mark_active<<<grid_for(EMAX), kThreads, 0, s>>>(collapsed, dcnt, edges, first_near, near_tris, active);
+    launch(k_mark_active, grid_for(EMAX), kThreads, 0, s, collapsed, dcnt, edges, first_near, near_tris, active);
     S2_TRY(isect_pass(*this, m, s));
     S2_TRY(undo_check(*this, s));
     S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
@@ -991,10 +1322,10 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     while (cnt_undo != 0) {
         it++;
         prof.begin(PH_UNDO, s);
-        k_undo_apply<<<grid_for(cnt_undo), kThreads, 0, s>>>(undo_edges, dcnt, edges, first_near, near_tris, opts,
+        launch(k_undo_apply, grid_for(cnt_undo), kThreads, 0, s, undo_edges, dcnt, edges, first_near, near_tris, opts,
                                                               otris, pts, tris, occ);
         if (nvu - first > 0)
-            k_rearrange<<<grid_for(nvu - first), kThreads, 0, s>>>(tmp_undo, pts_map, undo_list, first, nvu - first);
+            launch(k_rearrange, grid_for(nvu - first), kThreads, 0, s, tmp_undo, pts_map, undo_list, first, nvu - first);
         first += 2 * cnt_undo;
         S2_TRY(isect_pass(*this, m, s));
         S2_TRY(undo_check(*this, s));
@@ -1031,15 +1362,18 @@ cudaError_t query_and_test_pairs(const BvhNode *nodes, const int *vals, const in
                                  const int4 *tris, const uint8_t *active, int m, uint2 *pairs, long long cap_pairs,
                                  RoundCounters *cnt, uint8_t *isect, cudaStream_t s)
 {
-    k_query<<<grid_for(m), kThreads, 0, s>>>(nodes, vals, scene, pts, tris, active, m, pairs, cap_pairs, cnt);
-    k_pairs<<<grid_for(cap_pairs), kThreads, 0, s>>>(pairs, cnt, cap_pairs, pts, tris, isect, 1e-3f);
+    launch(k_query, grid_for(m), kThreads, 0, s, nodes, vals, scene, pts, tris, active, m, pairs, cap_pairs, cnt,
+           (const int *)nullptr, (const int *)nullptr, (const int *)nullptr);
+    launch(k_pairs, grid_for(cap_pairs), kThreads, 0, s, pairs, cnt, cap_pairs, pts, tris, isect, 1e-3f);
     return cudaGetLastError();
 }
 
 int Stage2::self_intersect_all(int n, int m, cudaStream_t s)
 {
+    bvh_carried = false;
+    bvh_leaves = 0;
     // faces of opts/otris; every live face queries the hierarchy
-    k_round_init<<<grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s>>>(opts, otris, pts, tris, occ, first_near,
+    launch(k_round_init, grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s, opts, otris, pts, tris, occ, first_near,
                                                                        cursor, vmin, n, m);
     S2_TRY(cudaMemsetAsync(dcnt, 0, sizeof(RoundCounters), s));
     S2_TRY(cudaMemsetAsync(active, 1, (size_t)m, s));
@@ -1063,12 +1397,228 @@ int Stage2::self_intersect_all(int n, int m, cudaStream_t s)
 int Stage2::compact(int n, int m, cudaStream_t s)
 {
     prof.begin(PH_COMPACT, s);
-    k_face_live_flags<<<grid_for(m), kThreads, 0, s>>>(tris, m, fflag);
+    launch(k_face_live_flags, grid_for(m), kThreads, 0, s, tris, m, fflag);
     S2_TRY(exclusive_scan(fflag, uflag, m, nullptr, scan_scratch, nullptr, s));
-    k_compact<<<grid_for(n > m ? n : m), kThreads, 0, s>>>(pts, occ, pts_map, n, tris, fflag, uflag, m, opts, otris,
+    launch(k_compact, grid_for(n > m ? n : m), kThreads, 0, s, pts, occ, pts_map, n, tris, fflag, uflag, m, opts, otris,
                                                            dcnt);
+    if (bvh_leaves > 0 && bvh_leaves >= m) {
+        launch(k_remap_leaves, grid_for(bvh_leaves), kThreads, 0, s, bvh.vals, bvh.scene, fflag, uflag);
+        bvh_carried = true;
+    }
     prof.end(s);
     S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+    S2_TRY(cudaStreamSynchronize(s));
+    prof.collect();
+    return PAMO_OK;
+}
+
+}  // namespace pamo
+
+// ---------------------------------------------------------------------------
+// batch rounds
+
+namespace pamo {
+
+int Stage2::ensure_batch(int K)
+{
+    if (K <= cap_slots && slots) return PAMO_OK;
+    if (cap_pts <= 0 || cap_tris <= 0) return PAMO_ERR_INVALID_ARG;  // ensure() first
+    if (slots) cudaFree(slots);
+    if (scnt) cudaFree(scnt);
+    if (roots) cudaFree(roots);
+    if (hslots) cudaFreeHost(hslots);
+    if (hscnt) cudaFreeHost(hscnt);
+    slots = nullptr; scnt = nullptr; roots = nullptr; hslots = nullptr; hscnt = nullptr;
+    cap_slots = 0;
+    int c = K > 16 ? K : 16;
+    if (cudaMalloc((void **)&slots, (size_t)c * sizeof(SlotInfo)) != cudaSuccess ||
+        cudaMalloc((void **)&scnt, (size_t)c * sizeof(SlotCounters)) != cudaSuccess ||
+        cudaMalloc((void **)&roots, (size_t)c * 4) != cudaSuccess ||
+        cudaMallocHost((void **)&hslots, (size_t)c * sizeof(SlotInfo)) != cudaSuccess ||
+        cudaMallocHost((void **)&hscnt, (size_t)c * sizeof(SlotCounters)) != cudaSuccess)
+        return PAMO_ERR_OOM;
+    if (!vslot && cudaMalloc((void **)&vslot, (size_t)(cap_pts + 1) * 4) != cudaSuccess) return PAMO_ERR_OOM;
+    if (!gmap && cudaMalloc((void **)&gmap, (size_t)(cap_pts + 1) * 4) != cudaSuccess) return PAMO_ERR_OOM;
+    if (!line_list && cudaMalloc((void **)&line_list, (size_t)(cap_edges + 1) * 4) != cudaSuccess) return PAMO_ERR_OOM;
+    if (!cand && cudaMalloc((void **)&cand, (size_t)(cap_edges + 1) * 4) != cudaSuccess) return PAMO_ERR_OOM;
+    cap_slots = c;
+    return PAMO_OK;
+}
+
+static cudaError_t undo_check_batch(Stage2 &S, int K, cudaStream_t s)
+{
+    S.prof.begin(PH_UNDO, s);
+    const long long NC = S.cap_edges;
+    launch(k_undo_flags, grid_for(NC), kThreads, 0, s, S.cand, S.dcnt, S.edges, S.first_near, S.near_tris, S.isect,
+           S.uflag);
+    cudaError_t e = exclusive_scan(S.uflag, S.eflag, NC, &S.dcnt->n_considered, S.scan_scratch, &S.dcnt->n_undo, s);
+    if (e != cudaSuccess) return e;
+    launch(k_b_undo_counts, grid_for(K), kThreads, 0, s, S.eflag, S.dcnt, S.scnt, K);
+    launch(k_b_undo_scatter, grid_for(NC), kThreads, 0, s, S.uflag, S.eflag, S.dcnt, S.cand, S.edges, S.vslot,
+           S.slots, S.scnt, S.undo_edges);
+    S.prof.end(s);
+    return cudaGetLastError();
+}
+
+static dim3 slot_grid(int K, long long per_slot_max)
+{
+    long long x = (per_slot_max + kThreads - 1) / kThreads;
+    x = x < 1 ? 1 : (x > 64 ? 64 : x);
+    return dim3((unsigned)x, (unsigned)K);
+}
+
+int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
+{
+    if (K <= 0 || K > cap_slots) return PAMO_ERR_INVALID_ARG;
+    n_slots = K;
+    bvh_carried = false;
+    std::vector<int> nvu(K), first(K), cnt_undo(K);
+    long long max_n = 0, max_undo_in = 0, max_cap_v = 0;
+    for (int r = 0; r < K; ++r) {
+        SlotInfo &h = hslots[r];
+        nvu[r] = first[r] = h.is_stuck ? h.n_undo_in : 0;
+        h.pass_first = h.pass_count = 0;
+        h.nvu = 0;
+        max_n = h.n > max_n ? h.n : max_n;
+        max_undo_in = h.n_undo_in > max_undo_in ? h.n_undo_in : max_undo_in;
+        max_cap_v = h.cap_v > max_cap_v ? h.cap_v : max_cap_v;
+    }
+    S2_TRY(cudaMemsetAsync(dcnt, 0, sizeof(RoundCounters), s));
+    S2_TRY(cudaMemsetAsync(scnt, 0, (size_t)K * sizeof(SlotCounters), s));
+    S2_TRY(cudaMemcpyAsync(slots, hslots, (size_t)K * sizeof(SlotInfo), cudaMemcpyHostToDevice, s));
+    launch(k_b_pre_copy, slot_grid(K, max_undo_in > max_cap_v ? max_undo_in : max_cap_v), kThreads, 0, s,
+           (const SlotInfo *)slots);
+    launch(k_b_pre_mark, slot_grid(K, max_undo_in), kThreads, 0, s, (const SlotInfo *)slots);
+    launch(k_b_vslot, slot_grid(K, max_n), kThreads, 0, s, (const SlotInfo *)slots, vslot);
+
+    prof.begin(PH_SETUP, s);
+    launch(k_round_init, grid_for((n + 1 > m ? n + 1 : m)), kThreads, 0, s, opts, otris, pts, tris, occ, first_near,
+           cursor, vmin, n, m);
+    launch(k_face_a, grid_for(m), kThreads, 0, s, pts, tris, m, first_near, first_edge, plane, elen4);
+    S2_TRY(cudaMemsetAsync(first_edge + m, 0, 4, s));
+    S2_TRY(exclusive_scan(first_near, first_near, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
+    S2_TRY(exclusive_scan(first_edge, first_edge, (long long)m + 1, nullptr, scan_scratch, &dcnt->n_edges, s));
+    const int *d_n_edges = &dcnt->n_edges;
+    launch(k_face_b, grid_for(m), kThreads, 0, s, tris, m, first_near, cursor, near_tris, first_edge, edges);
+    launch(k_vertex_quadric, grid_for(n), kThreads, 0, s, first_near, near_tris, plane, tris, quad, nxt, n);
+    launch(k_b_edge_off, grid_for(K), kThreads, 0, s, (const SlotInfo *)slots, (const int *)first_edge, scnt, K);
+    prof.begin(PH_LBVH_BUILD, s);
+    S2_TRY(lbvh_build(bvh, pts, tris, m, s, vslot, K, roots));
+    bvh_leaves = m;
+
+    const long long EMAX = 3LL * m;
+    prof.begin(PH_EDGE_COST, s);
+    CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, nxt, plane, elen4, quad, nullptr,
+                nullptr, vmin, 0.f, 1.f, 0, slots, scnt, vslot};
+    launch(k_edge_cost, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
+    CollapseArgs cl{edges, d_n_edges, nullptr, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
+                    0u, slots, scnt, vslot};
+    prof.begin(PH_COLLAPSE, s);
+    launch(k_collapse, grid_for(m, kChunkFaces), kThreads, 0, s, cl, bvh.vals, bvh.scene, first_edge);
+    S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
+    launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
+    launch(k_b_main, grid_for(K), kThreads, 0, s, (const int *)uflag, (const RoundCounters *)dcnt, scnt, K);
+    prof.begin(PH_CLEANUP, s);
+    launch(k_remove_invalid_faces, grid_for(m), kThreads, 0, s, tris, m);
+    launch(k_line_flags, grid_for(EMAX), kThreads, 0, s, edges, d_n_edges, pts, eflag, &dcnt->n_line);
+    launch(k_b_line_apply, 1, kLineThreads, 0, s, edges, d_n_edges, eflag, first_near, near_tris, pts, tris, occ,
+           line_list, (const int *)vslot, dcnt, scnt, K);
+    launch(k_b_cand_fill, grid_for(EMAX), kThreads, 0, s, (const int *)collapsed, (const int *)line_list, edges,
+           (const int *)vslot, (const RoundCounters *)dcnt, (const SlotCounters *)scnt, cand);
+
+    S2_TRY(cudaMemsetAsync(active, 0, (size_t)m, s));
+    launch(k_mark_active, grid_for(EMAX), kThreads, 0, s, cand, dcnt, edges, first_near, near_tris, active);
+    auto pass = [&]() -> int {
+        S2_TRY(isect_pass(*this, m, s));
+        S2_TRY(undo_check_batch(*this, K, s));
+        S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+        S2_TRY(cudaMemcpyAsync(hscnt, scnt, (size_t)K * sizeof(SlotCounters), cudaMemcpyDeviceToHost, s));
+        S2_TRY(cudaStreamSynchronize(s));
+        prof.collect();
+        if (hcnt->pair_overflow > 0) {
+            long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
+            int rc = ensure_pairs(need);
+            if (rc) return rc;
+            S2_TRY(isect_pass(*this, m, s));
+            S2_TRY(undo_check_batch(*this, K, s));
+            S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+            S2_TRY(cudaMemcpyAsync(hscnt, scnt, (size_t)K * sizeof(SlotCounters), cudaMemcpyDeviceToHost, s));
+            S2_TRY(cudaStreamSynchronize(s));
+            if (hcnt->pair_overflow > 0) return PAMO_ERR_CAPACITY;
+        }
+        if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
+        return PAMO_OK;
+    };
+    int rc = pass();
+    if (rc) return rc;
+    last_stats[0] = hcnt->n_edges;
+    last_stats[1] = hcnt->n_main;
+    last_stats[2] = hcnt->n_total;
+    last_stats[5] = hcnt->n_pairs;
+    last_stats[6] = m;
+    bool any = false;
+    for (int r = 0; r < K; ++r) {
+        cnt_undo[r] = hscnt[r].n_undo;
+        nvu[r] += 2 * cnt_undo[r];
+        if (nvu[r] > hslots[r].cap_undo) return PAMO_ERR_CAPACITY;
+        any = any || cnt_undo[r] != 0;
+    }
+    int it = 0;
+    while (any) {
+        it++;
+        prof.begin(PH_UNDO, s);
+        launch(k_undo_apply, grid_for(hcnt->n_undo), kThreads, 0, s, undo_edges, dcnt, edges, first_near, near_tris,
+               opts, otris, pts, tris, occ);
+        long long max_cnt = 0;
+        for (int r = 0; r < K; ++r) {
+            hslots[r].pass_first = first[r];
+            hslots[r].pass_count = nvu[r] - first[r];
+            max_cnt = hslots[r].pass_count > max_cnt ? hslots[r].pass_count : max_cnt;
+            first[r] += 2 * cnt_undo[r];
+        }
+        S2_TRY(cudaMemcpyAsync(slots, hslots, (size_t)K * sizeof(SlotInfo), cudaMemcpyHostToDevice, s));
+        if (max_cnt > 0) launch(k_b_rearrange, slot_grid(K, max_cnt), kThreads, 0, s, (const SlotInfo *)slots);
+        rc = pass();
+        if (rc) return rc;
+        any = false;
+        for (int r = 0; r < K; ++r) {
+            cnt_undo[r] = hscnt[r].n_undo;
+            nvu[r] += 2 * cnt_undo[r];
+            if (nvu[r] > hslots[r].cap_undo) return PAMO_ERR_CAPACITY;
+            any = any || cnt_undo[r] != 0;
+        }
+        if (it == 5) break;
+    }
+    last_stats[3] = it;
+    // the packed vertex map, each mesh's own map and undo-list copy
+    prof.begin(PH_COMPACT, s);
+    S2_TRY(exclusive_scan(occ, gmap, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
+    long long max_nvu = 0;
+    for (int r = 0; r < K; ++r) {
+        hslots[r].nvu = nvu[r];
+        max_nvu = nvu[r] > max_nvu ? nvu[r] : max_nvu;
+        nvu_out[r] = nvu[r];
+    }
+    S2_TRY(cudaMemcpyAsync(slots, hslots, (size_t)K * sizeof(SlotInfo), cudaMemcpyHostToDevice, s));
+    launch(k_b_local_map, slot_grid(K, (max_n + 1 > max_nvu ? max_n + 1 : max_nvu)), kThreads, 0, s,
+           (const SlotInfo *)slots, (const int *)gmap);
+    prof.end(s);
+    return PAMO_OK;
+}
+
+int Stage2::compact_batch(int n, int m, int K, cudaStream_t s)
+{
+    prof.begin(PH_COMPACT, s);
+    launch(k_face_live_flags, grid_for(m), kThreads, 0, s, tris, m, fflag);
+    S2_TRY(cudaMemsetAsync(fflag + m, 0, 4, s));
+    S2_TRY(exclusive_scan(fflag, uflag, (long long)m + 1, nullptr, scan_scratch, nullptr, s));
+    launch(k_compact, grid_for(n > m ? n : m), kThreads, 0, s, pts, occ, gmap, n, tris, fflag, uflag, m, opts, otris,
+           dcnt);
+    launch(k_b_next, grid_for(K), kThreads, 0, s, (const SlotInfo *)slots, (const int *)gmap, (const int *)uflag, scnt,
+           K);
+    prof.end(s);
+    S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
+    S2_TRY(cudaMemcpyAsync(hscnt, scnt, (size_t)K * sizeof(SlotCounters), cudaMemcpyDeviceToHost, s));
     S2_TRY(cudaStreamSynchronize(s));
     prof.collect();
     return PAMO_OK;

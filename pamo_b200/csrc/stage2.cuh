@@ -21,7 +21,55 @@ struct RoundCounters {
     int n_pts_next;      // compaction result
     int n_tris_next;
     int n_edges;
-    int pad[5];
+    int n_query;         // faces in this pass's query list
+    int pad[4];
+};
+
+// ---------------------------------------------------------------------------
+// Batches: several meshes packed into one round.
+//
+// The meshes of a batch sit one after another in the packed round arrays
+// (vertices, faces, and so the edges emitted per face, keep their order), so
+// every per-vertex, per-face and per-edge kernel runs unchanged over the packed
+// arrays: a mesh never shares a vertex with another one, and the independent
+// set, the collapses and the cleanup only look at one-rings.  What the
+// reference keeps per simplifier is kept per mesh: the state it reads stale
+// from earlier rounds (edge costs, the previous vertex map, the undo lists, the
+// invalid-vertex table) lives in a region of the mesh's own (`SlotInfo`
+// pointers, indexed by mesh-local numbers), the parameters (scale, threshold,
+// stuck mode) are per mesh, the undo check's collapsed-list window is per mesh,
+// and the hierarchy keeps each mesh in its own subtree (the mesh's rank is the
+// top of the sort key), which each query starts from.
+struct SlotInfo {        // uploaded by the host before each round, indexed by rank
+    int vert_off, n;     // packed vertex range of the mesh
+    int face_off, m;     // packed face range
+    int is_stuck;
+    int n_undo_in;       // entries of undo_prev from the previous round
+    int clear_invalid;   // clear the invalid table before marking (not stuck, list non-empty)
+    uint32_t collapse_t;
+    float tres;          // threshold
+    int pass_first, pass_count;  // undo pass: rearrangement window of the undo list
+    int nvu;             // undo-list length at the end of the round
+    const float *scale;  // device scalar: the mesh's scale (max bbox extent)
+    uint32_t *edge_cost; // [3 m0 + 1] edge costs (stale between rounds)
+    int *pts_map;        // [n0 + 1] the previous round's vertex map
+    int *undo_list;      // [cap_undo]
+    int *tmp_undo;       // [cap_undo]
+    int *undo_prev;      // [cap_undo] copy of the previous round's undo list
+    uint8_t *invalid;    // [n0 + 1] invalid-vertex table
+    long long cap_v;     // n0 + 1
+    long long cap_undo;  // entries of each undo region
+};
+
+struct SlotCounters {    // written on the device during a round, read by the host
+    int edge_off, n_edges;
+    int main_off, n_main;
+    int line_off, n_line;
+    int cand_off, n_considered;
+    int undo_off, n_undo;
+    int vert_off_next, n_next;
+    int face_off_next, m_next;
+    int pad[2];
 };
 
 // Optional per-phase device timing (CUDA events on the round's stream, read at
@@ -98,6 +146,22 @@ struct Stage2 {
     RoundCounters *hcnt = nullptr;  // pinned
     float *h_scalars = nullptr;     // pinned: [0..2] offset, [3] scale
     Lbvh bvh;
+    // The hierarchy of the previous round, its leaves renumbered by compact():
+    // reused (refit only) while enough of its leaves are still faces.
+    bool bvh_carried = false;
+    long long bvh_leaves = 0;  // faces the hierarchy was built over
+
+    // batch mode (see SlotInfo); unused by the single-mesh rounds
+    int n_slots = 0, cap_slots = 0;
+    SlotInfo *slots = nullptr;       // device [cap_slots]
+    SlotInfo *hslots = nullptr;      // pinned host copy
+    SlotCounters *scnt = nullptr;    // device [cap_slots]
+    SlotCounters *hscnt = nullptr;   // pinned host copy
+    int *vslot = nullptr;            // device [cap_pts + 1]: rank of each packed vertex
+    int *roots = nullptr;            // device [cap_slots]: subtree of each rank in the hierarchy
+    int *line_list = nullptr;        // device [cap_edges + 1]
+    int *cand = nullptr;             // device [cap_edges + 1]: per-mesh undo-candidate windows
+    int *gmap = nullptr;             // device [cap_pts + 1]: packed vertex map
 
     // input staging for the per-round ABI ([n,3] layouts)
     // results of the device loop
@@ -114,15 +178,26 @@ struct Stage2 {
 
     // One round on opts/otris (already holding the input; init shuffle applied
     // by the caller).  d_undo_in: device list of n_undo_in entries.
+    // keep_bvh: opts/otris are this context's own compact() output, so the
+    // hierarchy carried over from the previous round may be reused.
     int round(int n, int m, float scale, float threshold, bool is_stuck, const int *d_undo_in, int n_undo_in,
-              int *n_undo_out, cudaStream_t s);
+              int *n_undo_out, cudaStream_t s, bool keep_bvh = false);
+
+    // Batch mode: buffers for up to n_slots meshes (after ensure()).
+    int ensure_batch(int n_slots);
+    // One round over the packed meshes in opts/otris described by hslots[0..K)
+    // (uploaded here).  Per-mesh undo-list lengths come back in nvu_out[K].
+    int round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s);
+    // Compaction of a batch round; per-mesh next sizes and offsets in hscnt.
+    int compact_batch(int n, int m, int K, cudaStream_t s);
 
     // Whole-mesh self-intersection of opts/otris: isect[f] = 1 for every face of
     // a pair the reference's selfx::self_intersect reports (all pairs, no cap).
     int self_intersect_all(int n, int m, cudaStream_t s);
 
     // compaction of the round's output into opts/otris for the next round;
-    // returns new sizes through hcnt (after a sync).
+    // returns new sizes through hcnt (after a sync).  The hierarchy's leaves
+    // are renumbered to the compacted faces (removed faces become empty leaves).
     int compact(int n, int m, cudaStream_t s);
 };
 

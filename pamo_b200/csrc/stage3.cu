@@ -1015,17 +1015,17 @@ int Stage3::register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, in
     if (rc) return rc;
     np = n_v; nt = n_f; ne = n_e; nh = n_h; ngp = n_gt_v; ngt = n_gt_f;
     radius = cfg.contact_detection_radius;
-    k_aos_to_f4<<<grid_for(np), kThreads, 0, s>>>(d_v, q, q_prev, np);
-    k_aos_to_i4<<<grid_for(nt), kThreads, 0, s>>>(d_f, tris, nt, 3, 0);
-    k_aos_to_i4<<<grid_for(ne), kThreads, 0, s>>>(d_e, edges4, ne, 2, 1);
-    k_aos_to_i4<<<grid_for(nh), kThreads, 0, s>>>(d_h, hinges, nh, 4, 0);
-    k_aos_to_f4<<<grid_for(ngp), kThreads, 0, s>>>(d_gt_v, gt_pts, nullptr, ngp);
-    k_aos_to_i4<<<grid_for(ngt), kThreads, 0, s>>>(d_gt_f, gt_tris, ngt, 3, 0);
+    launch(k_aos_to_f4, grid_for(np), kThreads, 0, s, d_v, q, q_prev, np);
+    launch(k_aos_to_i4, grid_for(nt), kThreads, 0, s, d_f, tris, nt, 3, 0);
+    launch(k_aos_to_i4, grid_for(ne), kThreads, 0, s, d_e, edges4, ne, 2, 1);
+    launch(k_aos_to_i4, grid_for(nh), kThreads, 0, s, d_h, hinges, nh, 4, 0);
+    launch(k_aos_to_f4, grid_for(ngp), kThreads, 0, s, d_gt_v, gt_pts, nullptr, ngp);
+    launch(k_aos_to_i4, grid_for(ngt), kThreads, 0, s, d_gt_f, gt_tris, ngt, 3, 0);
     // Voronoi areas x GT-distance stiffness
     S3_TRY(cudaMemcpyAsync(wk, d_vor, (size_t)np * 4, cudaMemcpyDeviceToDevice, s));
-    k_scale<<<grid_for(np), kThreads, 0, s>>>(wk, np, cfg.mesh2gt_dist_stiffness);
-    k_elastic_pre<<<grid_for(nt), kThreads, 0, s>>>(q, tris, nt, area, inv_dm);
-    k_hinge_pre<<<grid_for(nh), kThreads, 0, s>>>(q, hinges, nh, rest_angle, rest_elen);
+    launch(k_scale, grid_for(np), kThreads, 0, s, wk, np, cfg.mesh2gt_dist_stiffness);
+    launch(k_elastic_pre, grid_for(nt), kThreads, 0, s, q, tris, nt, area, inv_dm);
+    launch(k_hinge_pre, grid_for(nh), kThreads, 0, s, q, hinges, nh, rest_angle, rest_elen);
     S3_TRY(lbvh_build(gt_bvh, gt_pts, gt_tris, ngt, s));
     S3_TRY(lbvh_refit(gt_bvh, gt_pts, gt_tris, ngt, s));
     S3_TRY(lbvh_build(tri_bvh, q, tris, nt, s));
@@ -1043,9 +1043,9 @@ int Stage3::detect(cudaStream_t s)
     for (int attempt = 0; attempt < 64; ++attempt) {
         const float thr = 2.f * radius + cfg.d_hat;
         S3_TRY(cudaMemsetAsync(iscal, 0, 3 * sizeof(int), s));
-        k_detect_pt<<<grid_for(np), kThreads, 0, s>>>(q, np, tris, tri_bvh.nodes, tri_bvh.vals, tri_bvh.scene, thr,
+        launch(k_detect_pt, grid_for(np), kThreads, 0, s, q, np, tris, tri_bvh.nodes, tri_bvh.vals, tri_bvh.scene, thr,
                                                       iscal, cap_b, bidx, bkind);
-        k_detect_ee<<<grid_for(ne), kThreads, 0, s>>>(q, ne, edges4, edge_bvh.nodes, edge_bvh.vals, edge_bvh.scene, thr,
+        launch(k_detect_ee, grid_for(ne), kThreads, 0, s, q, ne, edges4, edge_bvh.nodes, edge_bvh.vals, edge_bvh.scene, thr,
                                                       cfg.ee_classify_thres, iscal, cap_b, bidx, bkind);
         S3_TRY(cudaMemcpyAsync(h_iscal, iscal, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
         S3_TRY(cudaStreamSynchronize(s));
@@ -1073,20 +1073,20 @@ static int energy_pass(Stage3 &S, cudaStream_t s)
                 ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
             S.hinges, S.rest_angle, S.rest_elen, S.cfg.hinge_stiffness, S.bidx, S.bkind, S.bsub, S.bd, S.iscal, S.cap_b,
             S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials};
-    k_energy<<<kRedBlocks, kThreads, 0, s>>>(e);
-    k_finish_sum<<<1, 32, 0, s>>>(S.partials, kRedBlocks, S.dscal + D_ENERGY);
+    launch(k_energy, kRedBlocks, kThreads, 0, s, e);
+    launch(k_finish_sum, 1, 32, 0, s, S.partials, kRedBlocks, S.dscal + D_ENERGY);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
 static int hess_dx(Stage3 &S, const float4 *dx, float4 *out, cudaStream_t s)
 {
-    k_hess_vertex<<<grid_for(S.np), kThreads, 0, s>>>(S.wk, S.np, dx, out);
+    launch(k_hess_vertex, grid_for(S.np), kThreads, 0, s, S.wk, S.np, dx, out);
     HArgs h{S.q, S.wk, S.np, S.nt, S.nh, S.tris, S.area, S.inv_dm,
             S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
             S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
                 ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
             S.hinges, S.hblk, S.bidx, S.bg, S.bb2, S.iscal, S.cap_b, dx, out};
-    k_hess_elements<<<grid_for((long long)S.nt + S.nh + S.cap_b), kThreads, 0, s>>>(h);
+    launch(k_hess_elements, grid_for((long long)S.nt + S.nh + S.cap_b), kThreads, 0, s, h);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
@@ -1098,33 +1098,33 @@ int Stage3::newton(cudaStream_t s)
     S3_TRY(cudaMemcpyAsync(q_det, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
     if ((rc = energy_pass(*this, s))) return rc;
     // gradient (coefficient -1) and diagonal
-    k_diff_vertex<<<grid_for(np), kThreads, 0, s>>>(q, target, wk, np, grad, diag);
+    launch(k_diff_vertex, grid_for(np), kThreads, 0, s, q, target, wk, np, grad, diag);
     DArgs d{q, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
             cfg.elas_young_modulus * cfg.elas_poisson_ratio /
                 ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
             hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, hblk, bidx, bkind, bsub, bd, bg, bb2,
             iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag};
-    k_diff_elements<<<grid_for((long long)nt + nh + cap_b, 128), 128, 0, s>>>(d);
+    launch(k_diff_elements, grid_for((long long)nt + nh + cap_b, 128), 128, 0, s, d);
     // Jacobi-preconditioned CG (cg_solver.py:96-158)
-    k_cg_init<<<kRedBlocks, kThreads, 0, s>>>(grad, diag, np, p, r, z, v, partials);
-    k_finish_sum<<<1, 32, 0, s>>>(partials, kRedBlocks, dscal + D_ZR);
+    launch(k_cg_init, kRedBlocks, kThreads, 0, s, grad, diag, np, p, r, z, v, partials);
+    launch(k_finish_sum, 1, 32, 0, s, partials, kRedBlocks, dscal + D_ZR);
     for (int it = 0; it < cfg.n_cg_iters; ++it) {
         if ((rc = hess_dx(*this, v, Av, s))) return rc;
-        k_dot<<<kRedBlocks, kThreads, 0, s>>>(v, Av, np, partials);
-        k_finish_sum<<<1, 32, 0, s>>>(partials, kRedBlocks, dscal + D_VAV);
-        k_shift_zr<<<1, 1, 0, s>>>(dscal);
-        k_cg_update<<<kRedBlocks, kThreads, 0, s>>>(v, Av, diag, dscal, np, p, r, z, partials);
-        k_finish_sum<<<1, 32, 0, s>>>(partials, kRedBlocks, dscal + D_ZR);
-        k_cg_v<<<grid_for(np), kThreads, 0, s>>>(z, dscal, np, v);
+        launch(k_dot, kRedBlocks, kThreads, 0, s, v, Av, np, partials);
+        launch(k_finish_sum, 1, 32, 0, s, partials, kRedBlocks, dscal + D_VAV);
+        launch(k_shift_zr, 1, 1, 0, s, dscal);
+        launch(k_cg_update, kRedBlocks, kThreads, 0, s, v, Av, diag, dscal, np, p, r, z, partials);
+        launch(k_finish_sum, 1, 32, 0, s, partials, kRedBlocks, dscal + D_ZR);
+        launch(k_cg_v, grid_for(np), kThreads, 0, s, z, dscal, np, v);
     }
-    k_clamp<<<grid_for(np), kThreads, 0, s>>>(p, q_prev, q_det, np, cfg.contact_detection_radius);
-    k_set_float<<<1, 1, 0, s>>>(fscal, 1.0f);
-    k_accd<<<grid_for(cap_b, 128), 128, 0, s>>>(q, p, bidx, bkind, iscal, cap_b, cfg.ccd_slackness, cfg.ccd_thickness,
+    launch(k_clamp, grid_for(np), kThreads, 0, s, p, q_prev, q_det, np, cfg.contact_detection_radius);
+    launch(k_set_float, 1, 1, 0, s, fscal, 1.0f);
+    launch(k_accd, grid_for(cap_b, 128), 128, 0, s, q, p, bidx, bkind, iscal, cap_b, cfg.ccd_slackness, cfg.ccd_thickness,
                                                 cfg.ccd_max_iters, cfg.ee_classify_thres, fscal);
     // line search (system.py:393-409)
-    k_copy_energy_prev<<<1, 1, 0, s>>>(dscal);
+    launch(k_copy_energy_prev, 1, 1, 0, s, dscal);
     for (int nh_ = 0; nh_ < cfg.n_line_search_iters; ++nh_) {
-        k_line_search<<<grid_for(np), kThreads, 0, s>>>(q_prev, p, fscal, nh_, dscal, np, q);
+        launch(k_line_search, grid_for(np), kThreads, 0, s, q_prev, p, fscal, nh_, dscal, np, q);
         if ((rc = energy_pass(*this, s))) return rc;
     }
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
@@ -1134,7 +1134,7 @@ int Stage3::step(cudaStream_t s)
 {
     if (do_nothing) return PAMO_OK;
     S3_TRY(cudaMemsetAsync(iscal + I_STACK, 0, 4, s));
-    k_closest<<<grid_for(np), kThreads, 0, s>>>(q, np, gt_bvh.nodes, gt_bvh.vals, gt_bvh.scene, gt_pts, gt_tris, target,
+    launch(k_closest, grid_for(np), kThreads, 0, s, q, np, gt_bvh.nodes, gt_bvh.vals, gt_bvh.scene, gt_pts, gt_tris, target,
                                                 iscal);
     for (int it = 0; it < cfg.n_newton_iters; ++it) {
         int rc = newton(s);
@@ -1159,7 +1159,7 @@ int s3_validate(const int *a, long long count, int hi, int *d_bad, int *h_bad, c
 {
     if (count <= 0) return PAMO_OK;
     if (cudaMemsetAsync(d_bad, 0, 4, st) != cudaSuccess) return PAMO_ERR_DEVICE;
-    s3::k_validate_idx<<<grid_for(count), kThreads, 0, st>>>(a, count, hi, d_bad);
+    launch(s3::k_validate_idx, grid_for(count), kThreads, 0, st, a, count, hi, d_bad);
     if (cudaMemcpyAsync(h_bad, d_bad, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PAMO_ERR_DEVICE;
     if (cudaStreamSynchronize(st) != cudaSuccess) return PAMO_ERR_DEVICE;
     return *h_bad == 0 ? PAMO_OK : PAMO_ERR_INVALID_ARG;
@@ -1167,7 +1167,7 @@ int s3_validate(const int *a, long long count, int hi, int *d_bad, int *h_bad, c
 
 int s3_fetch(const float4 *q, float *out, int n, cudaStream_t st)
 {
-    s3::k_f4_to_aos<<<grid_for(n), kThreads, 0, st>>>(q, out, n);
+    launch(s3::k_f4_to_aos, grid_for(n), kThreads, 0, st, q, out, n);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 

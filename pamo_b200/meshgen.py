@@ -198,60 +198,59 @@ def noisy_torus(nu: int = 1024, nv: int = 1024, seed: int = 0, R: float = 1.0, r
 
 
 def geodesic_sphere(freq: int):
-    """Class-I geodesic sphere: each icosahedron face split into freq^2 triangles.
-    Shared edge points are generated once from the canonical (low->high) edge."""
-    freq = max(1, int(freq))
+    """Class-I geodesic sphere: each icosahedron face split into freq^2 triangles,
+    points pushed out to the unit sphere.  Vertices: the 12 corners, then the
+    freq-1 points of each of the 30 edges (walking from its lower corner), then
+    each face's interior points row by row; a point shared by faces is computed
+    once, from its edge."""
+    f_ = max(1, int(freq))
     cv, cf = icosahedron()
-    verts = [p for p in cv]
-    edge_pts = {}
+    cv = np.asarray(cv, np.float64)
+    cf = np.asarray(cf, np.int64)
+    ne = f_ - 1
+    edges = sorted({(min(a, b), max(a, b)) for t in cf for a, b in ((t[0], t[1]), (t[1], t[2]), (t[2], t[0]))})
+    eid = {e: k for k, e in enumerate(edges)}
+    e_lo = cv[[e[0] for e in edges]]
+    e_hi = cv[[e[1] for e in edges]]
+    st = (np.arange(1, f_) / f_)[None, :, None]
+    ep = (e_lo[:, None, :] + (e_hi - e_lo)[:, None, :] * st).reshape(-1, 3)
+    # interior grid points (i, j) with i, j, k = freq - i - j all >= 1, row-major
+    I, J = np.meshgrid(np.arange(f_ + 1), np.arange(f_ + 1), indexing="ij")
+    K = f_ - I - J
+    inner = (I >= 1) & (J >= 1) & (K >= 1)
+    ii, jj, kk = I[inner], J[inner], K[inner]
+    n_in = len(ii)
+    A, B, C = cv[cf[:, 0]], cv[cf[:, 1]], cv[cf[:, 2]]
+    ip = (A[:, None, :] * (kk / f_)[None, :, None] + B[:, None, :] * (ii / f_)[None, :, None] +
+          C[:, None, :] * (jj / f_)[None, :, None]).reshape(-1, 3)
+    pos = np.concatenate([cv, ep, ip], axis=0)
+    pos = pos / np.sqrt((pos * pos).sum(axis=1))[:, None]
+    base_e, base_i = 12, 12 + 30 * ne
 
-    def edge_point(a, b, t):
-        # t-th interior point walking from a to b (1..freq-1)
-        if a < b:
-            key, tt = (a, b), t
-        else:
-            key, tt = (b, a), freq - t
-        lst = edge_pts.get(key)
-        if lst is None:
-            lo, hi = cv[key[0]], cv[key[1]]
-            lst = []
-            for s in range(1, freq):
-                p = lo + (hi - lo) * (s / freq)
-                lst.append(len(verts))
-                verts.append(p / np.linalg.norm(p))
-            edge_pts[key] = lst
-        return lst[tt - 1]
+    def edge_ids(x, y, t):  # t-th point (1..freq-1) walking from corner x to corner y
+        if x < y:
+            return base_e + eid[(x, y)] * ne + (t - 1)
+        return base_e + eid[(y, x)] * ne + (f_ - t - 1)
 
+    inner_pos = np.full((f_ + 1, f_ + 1), -1, np.int64)
+    inner_pos[inner] = np.arange(n_in)
     faces = []
-    for (a, b, c) in cf:
-        A, B, C = cv[a], cv[b], cv[c]
-        idx = {}
-        for i in range(freq + 1):          # steps from A towards B
-            for j in range(freq + 1 - i):  # steps from A towards C
-                k = freq - i - j
-                if i == 0 and j == 0:
-                    vid = a
-                elif i == freq:
-                    vid = b
-                elif j == freq:
-                    vid = c
-                elif j == 0:
-                    vid = edge_point(a, b, i)
-                elif i == 0:
-                    vid = edge_point(a, c, j)
-                elif k == 0:
-                    vid = edge_point(b, c, j)
-                else:
-                    p = A * (k / freq) + B * (i / freq) + C * (j / freq)
-                    vid = len(verts)
-                    verts.append(p / np.linalg.norm(p))
-                idx[(i, j)] = vid
-        for i in range(freq):
-            for j in range(freq - i):
-                faces.append((idx[(i, j)], idx[(i + 1, j)], idx[(i, j + 1)]))
-                if i + j + 2 <= freq:
-                    faces.append((idx[(i + 1, j)], idx[(i + 1, j + 1)], idx[(i, j + 1)]))
-    return np.asarray(verts, dtype=np.float64), np.asarray(faces, dtype=np.int64)
+    valid = K >= 0
+    for fi, (a, b, c) in enumerate(cf):
+        idx = np.full((f_ + 1, f_ + 1), -1, np.int64)
+        idx[inner] = base_i + fi * n_in + inner_pos[inner]
+        idx[0, 0], idx[f_, 0], idx[0, f_] = a, b, c
+        t = np.arange(1, f_)
+        if ne:
+            idx[t, 0] = edge_ids(a, b, t)          # j = 0: from a towards b
+            idx[0, t] = edge_ids(a, c, t)          # i = 0: from a towards c
+            idx[f_ - t, t] = edge_ids(b, c, t)     # k = 0: from b towards c
+        i0, j0 = np.nonzero(valid & (I < f_) & (J < f_ - I))
+        faces.append(np.stack([idx[i0, j0], idx[i0 + 1, j0], idx[i0, j0 + 1]], 1))
+        i1, j1 = np.nonzero(valid & (I + J + 2 <= f_))
+        faces.append(np.stack([idx[i1 + 1, j1], idx[i1 + 1, j1 + 1], idx[i1, j1 + 1]], 1))
+    F = np.concatenate(faces, axis=0)
+    return pos, F
 
 
 def displaced_geodesic(n_faces: int, seed: int = 0, amplitude: float = 0.1, radius: float = 1.0):
