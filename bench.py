@@ -1,29 +1,33 @@
-"""Benchmark: PaMO stage-2 simplification on one B200.
+"""Benchmark: PaMO on one B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
-                    [--workload c2|c1] [--no-cpu-baseline]
+                    [--workload c2|c1|c4|c5] [--stages 23|2] [--no-cpu-baseline]
 
-Workload (default "c2"): 1024x1024 noisy torus (1,048,576 verts / 2,097,152
-faces, fp32/int32, seeded) simplified with ratio 0.01 (~20,971 faces) by the
-stage-2 loop of PaMO.run (centring, init permutation, collapse rounds with the
-self-intersection undo, compaction) -- the path this library implements.
+Default workload "c2" (config 2): a 1024x1024 noisy torus (1,048,576 verts /
+2,097,152 faces, fp32/int32, seeded) through PaMO(mesh, use_stage1=False,
+use_stage3=True).run(points, triangles, 0.01, min_verts=0): the stage-2
+simplification loop (centring, init permutation, collapse rounds with the
+self-intersection undo, compaction) to ~20,971 faces, then stage 3 (safe
+projection against the input, 5 steps of 10 Newton iterations).  Stage 1 is
+not built.  "c1" is config 1 (level-5 displaced icosphere, ratio 0.05).
 
-One step = one whole simplification of the mesh.  `value` = input Mfaces/s with
-the inputs already resident in HBM (device-timed with CUDA events around the
-steps); `e2e` = the same metric through the public C ABI entry points with host
-buffers: pinned host -> device copy of the mesh, the run, device -> host copy of
-the result, all inside the timed region.  The working set per round is far
-larger than the 126 MB L2 at 2M faces (several hundred MB), so no explicit L2
-flush is done between steps.
+One step = one whole PaMO.run.  `value` = input Mfaces/s with the inputs
+resident in device memory (CUDA events around the steps; PaMO.run returns host
+arrays, as the reference's does); `e2e` = the same from pinned host tensors,
+the host -> device copy inside the timed region.  The working set is far larger
+than the 126 MB L2 at 2M faces, so no explicit L2 flush is done between steps.
+`stage2_device` is the stage-2 device loop alone (pamo_stage2_run).
 
-`--impl reference` times the reference's algorithm on the host cores (the CPU
-restatement under oracle/, all threads) on a bounded sample of the same workload:
-the first rounds of the same run, extrapolated to the whole run by the face
-counts of the rounds (identical to the device run's rounds).
+`--impl reference` and the line's `cpu_baseline` time the reference's
+algorithm on the host cores (the CPU restatement under oracle/) on bounded
+samples of the same workload (see cpu_sample).
 
-With --gpus N > 1 (torchrun, one rank per GPU) every rank simplifies its own
-copy of the mesh (replicas; there is no data exchange), timed as the max over
-ranks; value = N * faces / time.
+"c4" runs 256 meshes of uneven sizes through the batch engine and through the
+plain per-mesh loop; "c5" serves Poisson arrivals with continuous batching.
+
+With --gpus N > 1 (torchrun, one rank per GPU) every rank runs its own copy
+(replicas; no data exchange), timed as the max over ranks; value = N * faces /
+time.
 """
 from __future__ import annotations
 
@@ -124,48 +128,23 @@ def dist_init(args):
     return ws, rank, local
 
 
-def reference_arm(args):
-    """CPU restatement of the reference's stage 2 on the host cores."""
-    ws, rank, _ = dist_init(args)
-    if rank != 0:
-        return 0
-    from oracle import oracle as O
+def stage3_stand_in(name):
+    """A mesh of the family and size of the stage-2 output (the input of stage 3)
+    for the CPU sample: 20,604 faces for config 2, ~1k for config 1."""
+    from pamo_b200 import meshgen as mg
 
-    V, F, ratio, desc = workload(args.workload)
-    target = int(ratio * len(F))
-    tm = O.tris_mean(V, F)
-    Vc = (V - tm).astype(np.float32)
-    Fs = O.shuffle_faces(F)
-    # bounded sample: the first rounds of the run
-    sample_rounds = args.sample_rounds
-    step_s = []
-    face_rounds = None
-    for _ in range(args.warmup + args.steps):
-        o = O.Stage2Oracle()
-        t0 = time.perf_counter()
-        v, f, rounds = o.run(Vc, Fs, target, 4, 1e-3, sample_rounds)
-        step_s.append(time.perf_counter() - t0)
-    t = float(np.median(step_s[args.warmup:]))
-    # faces entering each round of the full run, to extrapolate the sample
-    frac = _sample_fraction(args, sample_rounds)
-    total_s = t / frac if frac else float("nan")
-    value = len(F) / 1e6 / total_s
-    cores = O.lib().s2o_num_threads()
-    line = {"metric": "input Mfaces/s", "value": value, "unit": "Mfaces/s", "impl": "reference", "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc},
-            "cpu_baseline": {"value": value, "unit": "Mfaces/s", "cores": cores, "kind": "port",
-                             "sample": f"first {sample_rounds} rounds ({frac * 100:.1f}% of the run's face-rounds), "
-                                       f"extrapolated by face-rounds"},
-            "e2e": {"value": value, "unit": "Mfaces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
-    return 0
+    if name == "c1":
+        return mg.displaced_geodesic(980, 1)
+    return mg.noisy_torus(101, 102, 1)
 
 
-def cpu_baseline_sample(args, V, F, ratio):
-    """The CPU restatement (oracle/, OpenMP on all host threads) on the first
-    `sample_rounds` rounds of the same run, extrapolated by face-rounds."""
+def cpu_sample(args, V, F, ratio):
+    """The CPU restatement (oracle/) timed on the host cores, on bounded samples:
+    stage 2 = its first `sample_rounds` rounds (C, OpenMP on all host threads),
+    extrapolated by the face-rounds of the whole run; stage 3 = one Newton
+    iteration of the FP64 numpy restatement on a stand-in of the stage-2 output,
+    extrapolated to PaMO.run's 5 steps x 10 Newton iterations (plus its setup).
+    Returns (seconds for the whole workload, sample description, threads)."""
     from oracle import oracle as O
 
     target = int(ratio * len(F))
@@ -173,14 +152,66 @@ def cpu_baseline_sample(args, V, F, ratio):
     Vc = (V - tm).astype(np.float32)
     Fs = O.shuffle_faces(F)
     o = O.Stage2Oracle()
-    t0 = time.perf_counter()
-    o.run(Vc, Fs, target, 4, 1e-3, args.sample_rounds)
-    t = time.perf_counter() - t0
     frac = _sample_fraction(args, args.sample_rounds)
-    total = t / frac if frac else float("nan")
-    return {"value": len(F) / 1e6 / total, "unit": "Mfaces/s", "cores": O.lib().s2o_num_threads(), "kind": "port",
-            "sample": f"first {args.sample_rounds} rounds ({(frac or 0) * 100:.1f}% of the run's face-rounds, "
-                      f"{t:.1f} s), extrapolated by face-rounds"}
+    t0 = time.perf_counter()
+    o.run(Vc, Fs, target, 4, 1e-3, args.sample_rounds if frac else 1000000)
+    t2 = time.perf_counter() - t0
+    if frac:
+        total = t2 / frac
+        desc = (f"stage 2: first {args.sample_rounds} rounds ({frac * 100:.1f}% of the run's face-rounds, "
+                f"{t2:.1f} s) extrapolated by face-rounds")
+    else:  # no recorded round sizes for this workload: the whole loop
+        total = t2
+        desc = f"stage 2: the whole loop ({t2:.1f} s)"
+    if args.stages == "23":
+        from oracle import s3_oracle as S3  # numpy FP64 restatement
+
+        v, f = stage3_stand_in(args.workload)
+        scale, t = S3.normalization(np.asarray(V, np.float64))
+        gV = np.asarray(V, np.float64) * scale + t
+        sV = np.asarray(v, np.float64) * scale + t
+        s3 = S3.Stage3Oracle()
+        t0 = time.perf_counter()
+        s3.register(gV, F, sV, f)
+        t_reg = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        s3.update_target()
+        t_tgt = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        s3.newton()
+        t_newton = time.perf_counter() - t0
+        n_newton = 5 * s3.c.n_newton_iters
+        total += t_reg + 5 * t_tgt + n_newton * t_newton
+        desc += (f"; stage 3: one Newton iteration on a {len(f):,}-face stand-in of the stage-2 output "
+                 f"({t_newton:.1f} s, {len(s3.blocks):,} contact blocks) x {n_newton} + setup")
+    return total, desc, O.lib().s2o_num_threads()
+
+
+def reference_arm(args):
+    """The reference's algorithm on the host cores: the CPU restatement under
+    oracle/ (the reference has no CPU path for stage 2, and its stage-3 CPU
+    device, Warp, is absent), bounded samples of the same workload."""
+    ws, rank, _ = dist_init(args)
+    if rank != 0:
+        return 0
+    V, F, ratio, desc = workload(args.workload)
+    secs = []
+    for _ in range(args.warmup + args.steps):
+        total, sample, cores = cpu_sample(args, V, F, ratio)
+        secs.append(total)
+    total_s = float(np.median(secs[args.warmup:]))
+    value = len(F) / 1e6 / total_s
+    line = {"metric": "input Mfaces/s", "value": value, "unit": "Mfaces/s", "impl": "reference", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "stages": STAGES[args.stages]},
+            "cpu_baseline": {"value": value, "unit": "Mfaces/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "Mfaces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+STAGES = {"23": "stages 2 + 3 of PaMO.run (stage 1 is not built)", "2": "stage 2 of PaMO.run"}
 
 
 def _sample_fraction(args, sample_rounds):
@@ -203,7 +234,9 @@ def roofline_edge_cost(phases, round_faces, peaks):
     cost write 4 B/edge, CSR offsets 4 B/vertex, CSR entries 12 B/face, faces
     (int4) 16 B/face, points (float4) 16 B/vertex, quadrics 48 B/vertex,
     invalid flags 1 B/vertex, per-vertex key minimum read+write 16 B/vertex:
-    12 E + 85 V + 28 F = 88.5 B/face."""
+    12 E + 85 V + 28 F = 88.5 B/face.  Traffic: DRAM bytes per face of the
+    round-0 launch on config 2 (ncu, profiles/k_edge_cost_c2_round0.txt),
+    times the average faces per launch."""
     ph = phases.get("edge_cost")
     if not ph or not ph["ms"] or not round_faces:
         return None
@@ -211,11 +244,19 @@ def roofline_edge_cost(phases, round_faces, peaks):
     t = ph["ms"] / 1e3
     achieved = total_bytes / t / 1e9
     peak = peaks.get("hbm_gbs") or 6650.0
+    avg_faces = sum(round_faces) / max(len(round_faces), 1)
     return {"bound": "hbm", "kernel": "k_edge_cost", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "launches": ph["calls"],
-            "avg_launch_ms": ph["ms"] / max(ph["calls"], 1),
+            "frac": achieved / peak,
+            "traffic": EDGE_COST_DRAM_BYTES_PER_FACE * avg_faces if EDGE_COST_DRAM_BYTES_PER_FACE else None,
+            "launches": ph["calls"], "avg_launch_ms": ph["ms"] / max(ph["calls"], 1),
             "bytes_per_launch_avg": total_bytes / max(ph["calls"], 1),
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs") else "fallback"}
+
+
+# DRAM read + write of k_edge_cost per input face of the launch, from an ncu
+# capture of round 0 of config 2 (2,097,152 faces: 915.6 MB read + 60.0 MB
+# written); profiles/stage2_kernels_c2_round0.txt.
+EDGE_COST_DRAM_BYTES_PER_FACE = 465.2
 
 
 def product_arm(args):
@@ -230,35 +271,24 @@ def product_arm(args):
     V, F, ratio, desc = workload(args.workload)
     target = int(ratio * len(F))
     nF = len(F)
-    ctx = pamo_b200.Context(local)
     L = _lib.lib()
     s = torch.cuda.current_stream(dev)
     sp = ctypes.c_void_p(s.cuda_stream)
     Pd = torch.from_numpy(V).to(dev)
     Fd = torch.from_numpy(F).to(dev)
-    on, om, rr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-
-    def run_resident():
-        _lib.check("pamo_stage2_run", L.pamo_stage2_run(ctx.handle, Pd.data_ptr(), Fd.data_ptr(), len(V), nF, target,
-                                                        4, 1e-3, args.iters, sp, ctypes.byref(on), ctypes.byref(om),
-                                                        ctypes.byref(rr)))
-
-    # pinned host buffers for the end-to-end leg
     Ph = torch.from_numpy(V).pin_memory()
     Fh = torch.from_numpy(F).pin_memory()
-    Pe = torch.empty_like(Pd)
-    Fe = torch.empty_like(Fd)
-    out_v = torch.empty((len(V), 3), dtype=torch.float32).pin_memory()
-    out_f = torch.empty((nF, 3), dtype=torch.int32).pin_memory()
+    pm = pamo_b200.PaMO((V, F), use_stage1=False, use_stage3=args.stages == "23", device=local, verbose=False)
+
+    def run_resident():
+        """One PaMO.run from device-resident inputs to its host (verts, faces)."""
+        return pm.run(Pd, Fd, ratio, iter=args.iters, min_verts=0)
 
     def run_e2e():
-        Pe.copy_(Ph, non_blocking=True)
-        Fe.copy_(Fh, non_blocking=True)
-        _lib.check("pamo_stage2_run", L.pamo_stage2_run(ctx.handle, Pe.data_ptr(), Fe.data_ptr(), len(V), nF, target,
-                                                        4, 1e-3, args.iters, sp, ctypes.byref(on), ctypes.byref(om),
-                                                        ctypes.byref(rr)))
-        _lib.check("pamo_stage2_fetch", L.pamo_stage2_fetch(ctx.handle, out_v.data_ptr(), out_f.data_ptr(), 1, sp))
-        return on.value * 12 + om.value * 12
+        """The same from pinned host tensors (host -> device copy inside)."""
+        v, f = pm.run(Ph.to(dev, non_blocking=True), Fh.to(dev, non_blocking=True), ratio, iter=args.iters,
+                      min_verts=0)
+        return v.nbytes + f.nbytes
 
     for _ in range(args.warmup):
         run_resident()
@@ -283,7 +313,8 @@ def product_arm(args):
     torch.cuda.synchronize()
     launches = L.pamo_launch_count() - launches0
     dev_ms = ev0.elapsed_time(ev1) / args.steps
-    # end-to-end leg with host buffers, per-step latencies
+    timings = dict(pm.timings)
+    rounds = pm.last_rounds
     lat = []
     d2h = 0
     for _ in range(max(args.steps, 3)):
@@ -292,42 +323,35 @@ def product_arm(args):
         d2h = run_e2e()
         torch.cuda.synchronize()
         lat.append(time.perf_counter() - t0)
-    stage3 = None
-    if args.stage3:
-        # PaMO.run with stage 3 (safe projection against the input, 5 steps), the
-        # public drop-in: host arrays in, host arrays out, stage 2 then stage 3
-        pm = pamo_b200.PaMO((V, F), use_stage1=False, use_stage3=True, device=local, verbose=False)
-        Ph3 = torch.from_numpy(V).pin_memory()
-        Fh3 = torch.from_numpy(F).pin_memory()
-        pm.run(Ph3.to(dev), Fh3.to(dev), ratio, min_verts=0)  # warm-up (allocations)
-        t3 = []
-        for _ in range(max(1, min(args.steps, 3))):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            vv, ff = pm.run(Ph3.to(dev, non_blocking=True), Fh3.to(dev, non_blocking=True), ratio, min_verts=0)
-            torch.cuda.synchronize()
-            t3.append((time.perf_counter() - t0, dict(pm.timings)))
-        tt = float(np.median([x[0] for x in t3]))
-        stage3 = {"e2e_all_stages": {"value": nF / 1e6 / tt, "unit": "Mfaces/s", "ms": tt * 1e3,
-                                     "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
-                                     "d2h_bytes_per_step": int(vv.nbytes + ff.nbytes)},
-                  "stage2_ms": float(np.median([x[1]["stage2"] for x in t3])) * 1e3,
-                  "stage3_ms": float(np.median([x[1]["stage3"] for x in t3])) * 1e3,
-                  "stage3_stats": pm.system.last_stats,
-                  "what": "PaMO((V,F), use_stage1=False, use_stage3=True).run(V, F, ratio, min_verts=0) "
-                          "from pinned host tensors; stage 1 is not built"}
+    # stage 2 alone on the device (the device loop, no host copies), for reference
+    on, om, rr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    ev0.record(s)
+    n_s2 = max(args.steps, 3)
+    for _ in range(n_s2):
+        _lib.check("pamo_stage2_run", L.pamo_stage2_run(pm.ctx.handle, Pd.data_ptr(), Fd.data_ptr(), len(V), nF,
+                                                        target, 4, 1e-3, args.iters, sp, ctypes.byref(on),
+                                                        ctypes.byref(om), ctypes.byref(rr)))
+    ev1.record(s)
+    torch.cuda.synchronize()
+    s2_ms = ev0.elapsed_time(ev1) / n_s2
     clocks = clk.stop()
-    # one more run with per-phase CUDA events (outside the timed region)
-    L.pamo_profile_enable(ctx.handle, 1)
+    # one more run with per-phase CUDA events on both stages (outside the timed region)
+    handles = [pm.ctx.handle] + ([pm.system.ctx.handle] if args.stages == "23" else [])
+    for h in handles:
+        L.pamo_profile_enable(h, 1)
     run_resident()
     torch.cuda.synchronize()
-    ph_ms = (ctypes.c_double * 16)()
-    ph_calls = (ctypes.c_longlong * 16)()
-    nph = L.pamo_profile_read(ctx.handle, ph_ms, ph_calls, 16)
-    L.pamo_profile_enable(ctx.handle, 0)
-    phases = {_lib.PHASES[i]: {"ms": ph_ms[i], "calls": ph_calls[i]} for i in range(min(nph, len(_lib.PHASES)))}
+    phases = {}
+    for h in handles:
+        ph_ms = (ctypes.c_double * 16)()
+        ph_calls = (ctypes.c_longlong * 16)()
+        nph = L.pamo_profile_read(h, ph_ms, ph_calls, 16)
+        L.pamo_profile_enable(h, 0)
+        for i in range(min(nph, len(_lib.PHASES))):
+            if ph_calls[i]:
+                phases[_lib.PHASES[i]] = {"ms": ph_ms[i], "calls": ph_calls[i]}
     sizes = (ctypes.c_int * 4096)()
-    nr = L.pamo_stage2_round_sizes(ctx.handle, sizes, 4096)
+    nr = L.pamo_stage2_round_sizes(pm.ctx.handle, sizes, 4096)
     round_faces = [sizes[i] for i in range(min(nr, 4096))]
     ms_max = dev_ms
     e2e_ms = float(np.mean(lat)) * 1e3
@@ -335,12 +359,10 @@ def product_arm(args):
         from pamo_b200 import replicas
 
         ms_max, e2e_ms = replicas.max_over_ranks([dev_ms, e2e_ms], device=dev)
-    rounds = rr.value
-    stats = (ctypes.c_longlong * 8)()
-    L.pamo_stage2_last_round_stats(ctx.handle, stats)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(args, V, F, ratio)
+        total, sample, cores = cpu_sample(args, V, F, ratio)
+        cpu = {"value": nF / 1e6 / total, "unit": "Mfaces/s", "cores": cores, "kind": "port", "sample": sample}
     if rank == 0:
         value = ws * nF / 1e6 / (ms_max / 1e3)
         e2e = ws * nF / 1e6 / (e2e_ms / 1e3)
@@ -349,24 +371,27 @@ def product_arm(args):
             "metric": "input Mfaces/s", "value": value, "unit": "Mfaces/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "stages": "2 (stage-2 loop of PaMO.run)", "faces_out": om.value,
-                       "verts_out": on.value, "rounds": rounds, "iters": args.iters, "l2": "inputs/working set > L2, no flush",
-                       "parallelism": f"replicas x{ws}"},
+            "config": {"workload": desc, "stages": STAGES[args.stages], "faces_out": om.value, "verts_out": on.value,
+                       "rounds": rounds, "iters": args.iters, "l2": "inputs/working set > L2, no flush",
+                       "parallelism": f"replicas x{ws}", "api": "PaMO(mesh, use_stage1=False, use_stage3).run"},
             "gpu_launches": int(launches),
             "latency_ms": {"p50": float(np.percentile(lat, 50)) * 1e3, "p99": float(np.percentile(lat, 99)) * 1e3},
             "e2e": {"value": e2e, "unit": "Mfaces/s", "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
                     "d2h_bytes_per_step": int(d2h)},
+            "stage_ms": {k: round(v * 1e3, 3) for k, v in timings.items()},
+            "stage2_device": {"value": nF / 1e6 / (s2_ms / 1e3), "unit": "Mfaces/s", "ms": s2_ms,
+                              "what": "pamo_stage2_run alone, device-resident in and out"},
             "clocks": clocks,
             "cpu_baseline": cpu,
             "phases_ms": {k: round(v["ms"], 3) for k, v in phases.items()},
             "roofline": roofline_edge_cost(phases, round_faces, peaks),
             "round_faces": round_faces if args.dump_rounds else None,
-            "stage3": stage3,
         }
         print(json.dumps(line))
     if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+        from pamo_b200 import replicas
+
+        replicas.finalize()
     return 0
 
 
@@ -468,6 +493,14 @@ def batched_arm(args):
     launches = L.pamo_launch_count() - launches0
     e2e_dt, _, bi, bo, _ = run_batch(True)
     clocks = clk.stop()
+    # one more batch with per-phase CUDA events (outside the timed region)
+    L.pamo_batch_profile(eng.handle, 1, None, None, 0)
+    run_batch(False)
+    p_ms = (ctypes.c_double * 16)()
+    p_calls = (ctypes.c_longlong * 16)()
+    n_ph = L.pamo_batch_profile(eng.handle, 0, p_ms, p_calls, 16)
+    batch_phases = {_lib.PHASES[i]: round(p_ms[i], 3) for i in range(min(n_ph, len(_lib.PHASES))) if p_calls[i]}
+    rounds_run = eng.stats()["rounds_run"]
     # the plain per-mesh drop-in on the same meshes (same device, fresh context)
     import pamo_b200
 
@@ -494,7 +527,8 @@ def batched_arm(args):
                       "what": "pamo_stage2_run per mesh, one after another, same inputs"},
             "e2e": {"value": total_faces / 1e6 / e2e_dt, "unit": "Mfaces/s", "h2d_bytes_per_step": int(bi),
                     "d2h_bytes_per_step": int(bo)},
-            "gpu_launches": int(launches), "clocks": clocks,
+            "gpu_launches": int(launches), "clocks": clocks, "phases_ms": batch_phases,
+            "rounds_per_step": rounds_run // (args.warmup + args.steps + 2),
         }
         print(json.dumps(line))
     eng.close()
@@ -602,7 +636,8 @@ def main():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4", "c5"],
                     help="c1/c2: one mesh (plain loop); c4: 256-mesh batch; c5: Poisson serving")
-    ap.add_argument("--stage3", action="store_true", help="c1/c2: also time PaMO.run with stage 3")
+    ap.add_argument("--stages", default="23", choices=["23", "2"],
+                    help="c1/c2: PaMO.run with stage 3 (default) or stage 2 alone")
     ap.add_argument("--n-meshes", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--pool", type=int, default=24, help="c5: distinct request meshes")

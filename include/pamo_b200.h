@@ -180,6 +180,18 @@ int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int
                       int n_h, const float *d_vor, int n_steps, int do_nothing, const pamo_s3_config *cfg,
                       void *stream, float *d_out_v);
 
+/* Mean (double, a fixed-order sum) and bounding-box extent of points [n,3] on
+   the device: h_out6 = {mean x, y, z, extent x, y, z} (host memory).  Stage 3's
+   normalisation takes these for the ground truth (processing.py:15-20). */
+int pamo_point_stats(const float *d_pts, int n, double *h_out6, void *stream);
+
+/* Stage-3 input normalisation on the device (processing.py:57-59 applies it
+   to the ground truth on the host): out[i] = float((in[i] * scale + t) * post)
+   per coordinate of n points [n,3], each step in double with one rounding, so
+   the result equals the host float64 computation cast to float32. */
+int pamo_affine_points(const float *d_in, int n, double scale, double tx, double ty, double tz, double post,
+                       float *d_out, void *stream);
+
 /*
  * Diagnostics of the last pamo_safe_project call (no reference counterpart):
  * h_out[0] total energy at the end, [1] contact blocks of the last detection,
@@ -259,6 +271,12 @@ int pamo_batch_fetch(pamo_batch *b, long long job, float *out_points, int *out_t
 
 /* Frees a finished or failed job's result. */
 int pamo_batch_release(pamo_batch *b, long long job);
+
+/* Per-phase device times (ms) and call counts accumulated since the timer was
+   last switched (same phases as pamo_profile_read); then enable (1) or disable
+   (0) the timer and reset it, or leave it as it is (-1).  Returns the number of
+   phases. */
+int pamo_batch_profile(pamo_batch *b, int enable, double *h_ms, long long *h_calls, int cap);
 
 /* {running, pending, packed vertices, packed faces, bytes held, rounds run,
     max_faces, memory budget} */

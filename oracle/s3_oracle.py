@@ -74,6 +74,20 @@ def edges_unique(F):
     return np.unique(e, axis=0)
 
 
+
+def _scatter_add(out, idx, vals):
+    """out[idx[k]] += vals[k] for every k (np.add.at, through bincount per column)."""
+    idx = np.asarray(idx).ravel()
+    vals = np.asarray(vals, dtype=out.dtype)
+    n = out.shape[0]
+    if out.ndim == 1:
+        out += np.bincount(idx, weights=vals.ravel(), minlength=n)[:n]
+    else:
+        v2 = vals.reshape(len(idx), -1)
+        o2 = out.reshape(n, -1)
+        for c in range(o2.shape[1]):
+            o2[:, c] += np.bincount(idx, weights=v2[:, c], minlength=n)[:n]
+
 def voronoi_areas(V, F):
     """Mixed Voronoi vertex areas (Meyer, Desbrun, Schroeder, Barr 2003): for a
     non-obtuse triangle each corner gets (|e_ij|^2 cot + |e_ik|^2 cot)/8; for an
@@ -96,7 +110,7 @@ def voronoi_areas(V, F):
                     np.where(cos_c < 0, area / 2, area / 4)], 1)
     w = np.where(obtuse[:, None], mix, vor)
     for k in range(3):
-        np.add.at(out, F[:, k], w[:, k])
+        _scatter_add(out, F[:, k], w[:, k])
     return out
 
 
@@ -592,12 +606,12 @@ class Stage3Oracle:
         f2 = Hm[:, 0, 1, None] * b1 + Hm[:, 1, 1, None] * b2
         f0 = -f1 - f2
         for k, f in ((0, f0), (1, f1), (2, f2)):
-            np.add.at(g, self.F[:, k], f)
+            _scatter_add(g, self.F[:, k], f)
         # hinge
         Hb, gh = self._hinge_blocks(q)
         for k in range(4):
-            np.add.at(g, self.H[:, k], -gh[:, k])
-            np.add.at(dg, self.H[:, k], np.stack([Hb[:, k, k, i, i] for i in range(3)], 1))
+            _scatter_add(g, self.H[:, k], -gh[:, k])
+            _scatter_add(dg, self.H[:, k], np.stack([Hb[:, k, k, i, i] for i in range(3)], 1))
         self.hinge_blocks = spd_project(Hb, c.spd_max_iters)
         # collision (Gauss-Newton)
         self.coll = None
@@ -611,8 +625,8 @@ class Stage3Oracle:
             b1c = np.where(act, b1c, 0.0)
             b2c = np.where(act, b2c, 0.0)
             for k in range(4):
-                np.add.at(g, self.blocks[:, k], -G[:, k] * b1c[:, None])
-                np.add.at(dg, self.blocks[:, k], b2c[:, None] * G[:, k] ** 2)
+                _scatter_add(g, self.blocks[:, k], -G[:, k] * b1c[:, None])
+                _scatter_add(dg, self.blocks[:, k], b2c[:, None] * G[:, k] ** 2)
             self.coll = (G, b2c)
         return g, dg
 
@@ -708,19 +722,19 @@ class Stage3Oracle:
         df2 = dH[:, 0, 1, None] * b1 + dH[:, 1, 1, None] * b2
         df0 = -df1 - df2
         for k, f in ((0, df0), (1, df1), (2, df2)):
-            np.add.at(out, F[:, k], f)
+            _scatter_add(out, F[:, k], f)
         # hinge blocks
         Hb = self.hinge_blocks
         dxh = dx[self.H]  # [nh,4,3]
         contrib = np.einsum("hijab,hjb->hia", Hb, dxh)
         for k in range(4):
-            np.add.at(out, self.H[:, k], contrib[:, k])
+            _scatter_add(out, self.H[:, k], contrib[:, k])
         # collision Gauss-Newton
         if self.coll is not None:
             G, b2c = self.coll
             s = np.einsum("hjb,hjb->h", G, dx[self.blocks])
             for k in range(4):
-                np.add.at(out, self.blocks[:, k], G[:, k] * (b2c * s)[:, None])
+                _scatter_add(out, self.blocks[:, k], G[:, k] * (b2c * s)[:, None])
         return out
 
     # ---------------------------------------------------------------- solver
@@ -755,51 +769,60 @@ class Stage3Oracle:
         return p
 
     def accd(self, p):
-        """Additive CCD step bound over all blocks (ccd_kernels.py:8-110)."""
+        """Additive CCD step bound over all blocks (ccd_kernels.py:8-110), every
+        block advanced together (each block's loop is the reference's; blocks
+        leave the set as their own loops end)."""
         c = self.c
-        if not len(self.blocks):
+        nb = len(self.blocks)
+        if not nb:
             return 1.0
+        idx = np.asarray(self.blocks)
+        kinds = np.asarray(self.kinds)
+        x = self.q[idx].copy()
+        v = p[idx].copy()
+        v = v - v.mean(1, keepdims=True)
+        nv = np.sqrt((v * v).sum(2))
+        is_pt = kinds == BLOCK_PT
+        lv = np.where(is_pt, nv[:, 0] + nv[:, 1:].max(1), nv[:, :2].max(1) + nv[:, 2:].max(1))
+
+        def dist(X, K):
+            ty = np.empty(len(X), np.int64)
+            m = K == BLOCK_PT
+            if m.any():
+                ty[m] = pt_classify(X[m, 0], X[m, 1], X[m, 2], X[m, 3])
+            if (~m).any():
+                ty[~m] = ee_classify(X[~m, 0], X[~m, 1], X[~m, 2], X[~m, 3], c.ee_classify_thres)
+            d, _ = pair_distance_grad(X, K, ty)
+            return d
+
+        def dminus(d):
+            return np.maximum((d * d - c.ccd_thickness ** 2) / (d + c.ccd_thickness), 0.0)
+
+        act = lv >= 1e-12
         step = 1.0
-        q = self.q
-        for b in range(len(self.blocks)):
-            idx = self.blocks[b]
-            x = q[idx].copy()
-            v = p[idx].copy()
-            v = v - v.mean(0)
-            if self.kinds[b] == BLOCK_PT:
-                lv = _norm(v[0]) + max(_norm(v[1]), _norm(v[2]), _norm(v[3]))
-            else:
-                lv = max(_norm(v[0]), _norm(v[1])) + max(_norm(v[2]), _norm(v[3]))
-            if lv < 1e-12:
-                continue
-
-            def dist(x):
-                X = x[None]
-                if self.kinds[b] == BLOCK_PT:
-                    ty = pt_classify(X[:, 0], X[:, 1], X[:, 2], X[:, 3])
-                else:
-                    ty = ee_classify(X[:, 0], X[:, 1], X[:, 2], X[:, 3], c.ee_classify_thres)
-                d, _ = pair_distance_grad(X, self.kinds[b:b + 1], ty)
-                return float(d[0])
-
-            d = dist(x)
-            dmt = max((d * d - c.ccd_thickness ** 2) / (d + c.ccd_thickness), 0.0)
-            gap = (1 - c.ccd_slackness) * dmt
-            t = 0.0
-            tl = c.ccd_slackness * dmt / lv
-            i = 0
-            while True:
-                x = x + tl * v
-                d = dist(x)
-                dmt = max((d * d - c.ccd_thickness ** 2) / (d + c.ccd_thickness), 0.0)
-                if (i > 0 and dmt <= gap) or i >= c.ccd_max_iters:
-                    step = min(step, t)
-                    break
-                t = t + tl
-                if t > 1.0:
-                    break
-                tl = 0.8 * dmt / lv
-                i += 1
+        d = np.zeros(nb)
+        d[act] = dist(x[act], kinds[act])
+        dmt = dminus(d)
+        gap = (1 - c.ccd_slackness) * dmt
+        t = np.zeros(nb)
+        tl = np.where(act, c.ccd_slackness * dmt / np.where(act, lv, 1.0), 0.0)
+        i = 0
+        while act.any():
+            a = np.nonzero(act)[0]
+            x[a] = x[a] + tl[a, None, None] * v[a]
+            d[a] = dist(x[a], kinds[a])
+            dmt[a] = dminus(d[a])
+            done = ((i > 0) & (dmt[a] <= gap[a])) | (i >= c.ccd_max_iters)
+            if done.any():
+                step = min(step, float(t[a[done]].min()))
+                act[a[done]] = False
+            a = a[~done]
+            t[a] = t[a] + tl[a]
+            over = t[a] > 1.0
+            act[a[over]] = False
+            a = a[~over]
+            tl[a] = 0.8 * dmt[a] / lv[a]
+            i += 1
         return step
 
     def newton(self):

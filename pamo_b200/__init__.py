@@ -146,6 +146,10 @@ class PaMO:
         V, F = _mesh_arrays(input_mesh)
         self.bbox = np.stack([V.min(0), V.max(0)]) if len(V) else np.zeros((2, 3))
         self.gt_mesh = (copy.deepcopy(V), copy.deepcopy(F))
+        # a float32 input is kept as such too, so stage 3 can normalise it on the device
+        V_in = input_mesh[0] if isinstance(input_mesh, (tuple, list)) else getattr(input_mesh, "vertices", None)
+        self._gt_f32 = np.array(V_in, dtype=np.float32) if getattr(V_in, "dtype", None) == np.float32 else None
+        self._gt_f32_pinned = None
         self.ctx = Context(device)
         self.device = device
         self.target_faces = None
@@ -187,7 +191,13 @@ class PaMO:
             # the reference wraps the stage-2 result in trimesh.Trimesh(process=True),
             # which merges coincident vertices (pamo/__init__.py:193-203)
             v2, f2 = merge_vertices(verts.astype(np.float64), faces)
-            verts, faces = process(self.gt_mesh[0], self.gt_mesh[1], v2, f2, 5, system=self.system,
-                                   config=self.config)
+            gt_v = self.gt_mesh[0]
+            if self._gt_f32 is not None:
+                if self._gt_f32_pinned is None:  # page-locked host copies of the ground truth
+                    self._gt_f32_pinned = torch.from_numpy(self._gt_f32).pin_memory()
+                    self._gt_f_pinned = torch.from_numpy(self.gt_mesh[1].astype(np.int32)).pin_memory()
+                gt_v = self._gt_f32_pinned
+            gt_f = self._gt_f_pinned if self._gt_f32 is not None else self.gt_mesh[1]
+            verts, faces = process(gt_v, gt_f, v2, f2, 5, system=self.system, config=self.config)
             self.timings["stage3"] = time.time() - t0
         return verts, faces

@@ -28,6 +28,9 @@ _ip = ctypes.POINTER(ctypes.c_int)
 SIGNATURES = {
     "pamo_version": (_i, []),
     "pamo_launch_count": (_ll, []),
+    "pamo_point_stats": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_double), _vp]),
+    "pamo_affine_points": (_i, [_vp, _i, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                ctypes.c_double, _vp, _vp]),
     "pamo_batch_create": (_i, [_i, _ll, _ll, _i, _ll, _vp, ctypes.POINTER(_vp)]),
     "pamo_batch_destroy": (_i, [_vp]),
     "pamo_batch_submit": (_i, [_vp, _vp, _vp, _i, _i, _i, _ll, _i, _f, _i, ctypes.POINTER(_ll)]),
@@ -36,6 +39,7 @@ SIGNATURES = {
     "pamo_batch_fetch": (_i, [_vp, _ll, _vp, _vp, _i]),
     "pamo_batch_release": (_i, [_vp, _ll]),
     "pamo_batch_stats": (_i, [_vp, ctypes.POINTER(_ll)]),
+    "pamo_batch_profile": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_ll), _i]),
     "pamo_status_string": (ctypes.c_char_p, [_i]),
     "pamo_ctx_create": (_i, [_i, ctypes.POINTER(_vp)]),
     "pamo_ctx_destroy": (_i, [_vp]),
@@ -88,7 +92,7 @@ def check(fn: str, code: int):
 
 
 PHASES = ["setup", "lbvh_build", "edge_cost", "collapse", "cleanup", "refit", "query", "pair_tests", "undo",
-          "compact"]
+          "compact", "s3_closest", "s3_detect", "s3_diff", "s3_cg", "s3_ccd", "s3_line"]
 
 
 class Context:

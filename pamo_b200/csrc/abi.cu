@@ -86,7 +86,7 @@ __global__ void k_face_means(const float *pts, const int *tris, int m, float *mx
 // is the latency of F dependent adds.  One block: lane 0 of warps 0, 1, 2 runs
 // the x, y, z chains (reading four values per shared-memory load) while warps
 // 3..31 stream the next chunk into the other shared buffer.
-constexpr int kMeanChunk = 4096;
+constexpr int kMeanChunk = 8192;
 constexpr int kMeanLoadFirst = 3 * 32;
 
 __global__ void __launch_bounds__(1024) k_sequential_mean(const float *mx, const float *my, const float *mz, int m,
@@ -164,6 +164,82 @@ __global__ void k_centre(const float *pts, int n, const float *mean, float4 *out
             atomicMin(&bounds[k], float_to_ordered(lo[k]));
             atomicMax(&bounds[3 + k], float_to_ordered(hi[k]));
         }
+}
+
+// Per-block partial sums (double) and exact min / max of points [n,3]; a fixed
+// grid and a fixed final order make the sums deterministic.
+constexpr int kStatBlocks = 296;
+
+__global__ void __launch_bounds__(256) k_point_stats(const float *pts, int n, double *part)
+{
+    double s[3] = {0.0, 0.0, 0.0};
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    PAMO_GRID_STRIDE(i, n)
+    {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float x = pts[3 * i + k];
+            s[k] += (double)x;
+            lo[k] = fminf(lo[k], x);
+            hi[k] = fmaxf(hi[k], x);
+        }
+    }
+    __shared__ double ss[3][8];
+    __shared__ float sl[3][8], sh[3][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        for (int o = 16; o > 0; o >>= 1) {
+            s[k] += __shfl_down_sync(0xffffffffu, s[k], o);
+            lo[k] = fminf(lo[k], __shfl_down_sync(0xffffffffu, lo[k], o));
+            hi[k] = fmaxf(hi[k], __shfl_down_sync(0xffffffffu, hi[k], o));
+        }
+        if (lane == 0) {
+            ss[k][w] = s[k];
+            sl[k][w] = lo[k];
+            sh[k][w] = hi[k];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        const int k = threadIdx.x;
+        double a = 0.0;
+        float l = INFINITY, h = -INFINITY;
+        for (int j = 0; j < (int)(blockDim.x >> 5); ++j) {
+            a += ss[k][j];
+            l = fminf(l, sl[k][j]);
+            h = fmaxf(h, sh[k][j]);
+        }
+        part[9 * blockIdx.x + k] = a;
+        part[9 * blockIdx.x + 3 + k] = (double)l;
+        part[9 * blockIdx.x + 6 + k] = (double)h;
+    }
+}
+
+__global__ void k_point_stats_finish(const double *part, int nblocks, int n, double *out)
+{
+    if (threadIdx.x >= 3) return;
+    const int k = threadIdx.x;
+    double a = 0.0, l = INFINITY, h = -INFINITY;
+    for (int b = 0; b < nblocks; ++b) {
+        a += part[9 * b + k];
+        l = fmin(l, part[9 * b + 3 + k]);
+        h = fmax(h, part[9 * b + 6 + k]);
+    }
+    out[k] = a / (double)n;  // mean
+    out[3 + k] = h - l;      // extent
+}
+
+// out = float((in * scale + t) * post), each step one double rounding
+__global__ void k_affine_points(const float *in, int n, double scale, double tx, double ty, double tz, double post,
+                                float *out)
+{
+    PAMO_GRID_STRIDE(i, 3LL * n)
+    {
+        const int k = (int)(i % 3);
+        const double t = k == 0 ? tx : (k == 1 ? ty : tz);
+        out[i] = (float)__dmul_rn(__dadd_rn(__dmul_rn((double)in[i], scale), t), post);
+    }
 }
 
 __global__ void k_bounds_init(int *b)
@@ -264,6 +340,7 @@ int pamo_ctx_create(int device, pamo_ctx **out)
     if (!c) return PAMO_ERR_OOM;
     c->device = device;
     c->s2.device = device;
+    c->s3.prof = &c->s2.prof;  // one phase timer for both stages
     int rc = set_device(c);
     if (rc) {
         delete c;
@@ -524,6 +601,15 @@ int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int
     RET_IF(s3_validate(d_h, 4LL * n_h, n_v, bad, S.h_iscal, s));
     RET_IF(s3_validate(d_gt_f, 3LL * n_gt_f, n_gt_v, bad, S.h_iscal, s));
     S.do_nothing = do_nothing != 0;
+    // the solve runs on the context's own stream, ordered after the caller's
+    // stream and before whatever the caller queues next
+    if (!S.work) CU_RET(cudaStreamCreateWithFlags(&S.work, cudaStreamNonBlocking));
+    if (!S.ev_in) CU_RET(cudaEventCreateWithFlags(&S.ev_in, cudaEventDisableTiming));
+    if (!S.ev_out) CU_RET(cudaEventCreateWithFlags(&S.ev_out, cudaEventDisableTiming));
+    CU_RET(cudaEventRecord(S.ev_in, s));
+    CU_RET(cudaStreamWaitEvent(S.work, S.ev_in, 0));
+    cudaStream_t caller = s;
+    s = S.work;
     RET_IF(S.register_mesh(d_gt_v, d_gt_f, n_gt_v, n_gt_f, d_v, d_f, n_v, n_f, d_e, n_e, d_h, n_h, d_vor, s));
     int newton = 0;
     for (int k = 0; k < n_steps; ++k) {
@@ -535,9 +621,37 @@ int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int
     RET_IF(S.energy_now(&e, s));
     CU_RET(cudaMemcpyAsync(S.h_iscal, S.iscal, 4, cudaMemcpyDeviceToHost, s));
     CU_RET(cudaStreamSynchronize(s));
+    CU_RET(cudaEventRecord(S.ev_out, s));
+    CU_RET(cudaStreamWaitEvent(caller, S.ev_out, 0));
     ctx->s3_stats[0] = e;
     ctx->s3_stats[1] = S.h_iscal[0];
     ctx->s3_stats[2] = newton;
+    return PAMO_OK;
+}
+
+int pamo_point_stats(const float *d_pts, int n, double *h_out6, void *stream)
+{
+    if (n <= 0 || !d_pts || !h_out6) return PAMO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    double *scratch = nullptr;
+    CU_RET(cudaMallocAsync((void **)&scratch, (9 * kStatBlocks + 8) * sizeof(double), s));
+    launch(k_point_stats, kStatBlocks, 256, 0, s, d_pts, n, scratch);
+    launch(k_point_stats_finish, 1, 32, 0, s, (const double *)scratch, kStatBlocks, n, scratch + 9 * kStatBlocks);
+    cudaError_t e = cudaMemcpyAsync(h_out6, scratch + 9 * kStatBlocks, 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    CU_RET(e);
+    return PAMO_OK;
+}
+
+int pamo_affine_points(const float *d_in, int n, double scale, double tx, double ty, double tz, double post,
+                       float *d_out, void *stream)
+{
+    if (n < 0 || (n && (!d_in || !d_out))) return PAMO_ERR_INVALID_ARG;
+    if (n == 0) return PAMO_OK;
+    launch(k_affine_points, grid_for(3LL * n), kThreads, 0, (cudaStream_t)stream, d_in, n, scale, tx, ty, tz, post,
+           d_out);
+    CU_RET(cudaGetLastError());
     return PAMO_OK;
 }
 
@@ -1128,6 +1242,22 @@ int pamo_batch_release(pamo_batch *b, long long job)
         return PAMO_OK;
     }
     return PAMO_ERR_INVALID_ARG;
+}
+
+int pamo_batch_profile(pamo_batch *b, int enable, double *h_ms, long long *h_calls, int cap)
+{
+    if (!b || cap < 0) return -PAMO_ERR_INVALID_ARG;
+    Profiler &P = b->S.prof;
+    int n = cap < PH_COUNT ? cap : PH_COUNT;
+    for (int i = 0; i < n; ++i) {
+        if (h_ms) h_ms[i] = P.ms[i];
+        if (h_calls) h_calls[i] = P.calls[i];
+    }
+    if (enable >= 0) {
+        P.on = enable != 0;
+        P.reset();
+    }
+    return PH_COUNT;
 }
 
 int pamo_batch_stats(pamo_batch *b, long long *h_out8)

@@ -281,6 +281,54 @@ __global__ void __launch_bounds__(kThreads) k_refit(const float4 *pts, const int
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_refit_dirty(const float4 *pts, const int4 *tris, const int *vals,
+                                                          int *scene, const int *parent, BvhNode *nodes, int *claim,
+                                                          int *dmask, int *dcount, const int *dlist)
+{
+    const int L = scene[7];
+    const int n = scene[9];
+    PAMO_GRID_STRIDE(k, n)
+    {
+        const int p = dlist[k];
+        claim[p] = 0;
+        const int f = vals[p];
+        int4 t = f >= 0 ? tris[f] : make_int4(-1, -1, -1, 0);
+        float3 lo, hi;
+        if (face_dead(t)) {
+            lo = make_float3(INFINITY, INFINITY, INFINITY);
+            hi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+        } else {
+            face_box(pts, t, lo, hi);
+        }
+        int code = parent[(L - 1) + p];
+        store_child_box(nodes, code, ~p, lo, hi);
+        int node = code >> 1;
+        for (int depth = 0;; ++depth) {
+            if (depth > 256) {
+                atomicExch(&scene[8], 1);
+                break;
+            }
+            // the marks were set by an earlier kernel; read them before arriving,
+            // since the last child to arrive clears them
+            const int need = __popc(__ldcg(&dmask[node]));
+            __threadfence();
+            const int old = atomicAdd(&dcount[node], 1);
+            if (old + 1 < need) break;  // the other dirty child merges this node
+            __threadfence();
+            float4 a = __ldcg(&nodes[node].llo), b = __ldcg(&nodes[node].lhi);
+            float4 c = __ldcg(&nodes[node].rlo), d = __ldcg(&nodes[node].rhi);
+            lo = make_float3(fminf(a.x, c.x), fminf(a.y, c.y), fminf(a.z, c.z));
+            hi = make_float3(fmaxf(b.x, d.x), fmaxf(b.y, d.y), fmaxf(b.z, d.z));
+            dmask[node] = 0;
+            dcount[node] = 0;
+            const int pc = parent[node];
+            if (pc < 0) break;  // root
+            store_child_box(nodes, pc, node, lo, hi);
+            node = pc >> 1;
+        }
+    }
+}
+
 __global__ void k_count_leaves(int m, int *scene) { scene[7] = m - scene[6]; }
 
 }  // namespace
@@ -308,14 +356,24 @@ cudaError_t Lbvh::ensure(long long n)
     ALLOC(flags, c * 4);
     ALLOC(leaf_of_face, c * 4);
     ALLOC(scene, 64);
+    ALLOC(claim, c * 4);
+    ALLOC(dmask, c * 4);
+    ALLOC(dcount, c * 4);
+    ALLOC(dlist, c * 4);
 #undef ALLOC
+    if ((e = cudaMemset(claim, 0, c * 4)) != cudaSuccess || (e = cudaMemset(dmask, 0, c * 4)) != cudaSuccess ||
+        (e = cudaMemset(dcount, 0, c * 4)) != cudaSuccess) {
+        release();
+        return e;
+    }
     cap = c;
     return cudaSuccess;
 }
 
 void Lbvh::release()
 {
-    void *p[] = {keys, keys2, vals, vals2, hist, hist_scratch, nodes, parent, flags, leaf_of_face, scene};
+    void *p[] = {keys, keys2, vals, vals2, hist, hist_scratch, nodes, parent, flags, leaf_of_face, scene, claim, dmask,
+                 dcount, dlist};
     for (void *q : p)
         if (q) cudaFree(q);
     keys = keys2 = nullptr;
@@ -323,6 +381,7 @@ void Lbvh::release()
     hist = hist_scratch = nullptr;
     nodes = nullptr;
     parent = flags = leaf_of_face = scene = nullptr;
+    claim = dmask = dcount = dlist = nullptr;
     cap = 0;
     leaves_built = 0;
 }
@@ -362,6 +421,14 @@ cudaError_t lbvh_build(Lbvh &b, const float4 *pts, const int4 *tris, int m, cuda
     launch(k_karras, grid_for(m), kThreads, 0, s, b.keys, b.scene, b.nodes, b.parent, vslot ? roots : nullptr,
            3 * bits);
     launch(k_leaf_map, grid_for(m), kThreads, 0, s, b.vals, b.scene, b.leaf_of_face, m);
+    return cudaGetLastError();
+}
+
+cudaError_t lbvh_refit_dirty(Lbvh &b, const float4 *pts, const int4 *tris, long long max_dirty, cudaStream_t s)
+{
+    if (b.leaves_built < 2 || max_dirty <= 0) return cudaSuccess;
+    launch(k_refit_dirty, grid_for(max_dirty), kThreads, 0, s, pts, tris, (const int *)b.vals, b.scene,
+           (const int *)b.parent, b.nodes, b.claim, b.dmask, b.dcount, (const int *)b.dlist);
     return cudaGetLastError();
 }
 

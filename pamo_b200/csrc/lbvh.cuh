@@ -14,6 +14,8 @@
 // hierarchy.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace pamo {
@@ -40,6 +42,11 @@ struct Lbvh {
     int *scene = nullptr;       // 6 ordered ints + n_dead + n_leaves
     int sort_tiles = 0;
     long long leaves_built = 0;  // faces of the last build: bound on the leaf count
+    // incremental refit (lbvh_mark_dirty_leaf / lbvh_refit_dirty); all zero between refits
+    int *claim = nullptr;   // [cap] leaf listed as dirty
+    int *dmask = nullptr;   // [cap] per inner node: which children hold a dirty leaf (bit 0 left, 1 right)
+    int *dcount = nullptr;  // [cap] per inner node: dirty children merged so far
+    int *dlist = nullptr;   // [cap] dirty leaves; their count is scene[9]
 
     cudaError_t ensure(long long n_faces);
     void release();
@@ -56,5 +63,32 @@ cudaError_t lbvh_build(Lbvh &b, const float4 *pts, const int4 *tris, int m, cuda
 // Recomputes all boxes from the current geometry (pts, tris).  A leaf whose face
 // index is negative (a face removed after the build) gets the empty box.
 cudaError_t lbvh_refit(Lbvh &b, const float4 *pts, const int4 *tris, int m, cudaStream_t s);
+
+// Incremental refit, for boxes that were all up to date before some faces
+// changed: the caller lists the changed faces' leaves with lbvh_mark_dirty_leaf
+// (in a kernel, after zeroing scene[9]); lbvh_refit_dirty then recomputes those
+// leaves and, bottom-up, exactly the inner nodes above them (a node is merged by
+// the last of its dirty children to arrive).  Leaves the marks zero again.
+__device__ __forceinline__ void lbvh_mark_dirty_leaf(int p, int L, const int *parent, int *claim, int *dmask,
+                                                     int *dlist, int *scene)
+{
+    if (atomicExch(&claim[p], 1) != 0) return;  // listed already
+    {  // one counter atomic per group of lanes listing together
+        cooperative_groups::coalesced_group g = cooperative_groups::coalesced_threads();
+        int base = 0;
+        if (g.thread_rank() == 0) base = atomicAdd(&scene[9], (int)g.size());
+        dlist[g.shfl(base, 0) + (int)g.thread_rank()] = p;
+    }
+    int code = parent[(L - 1) + p];
+    // mark the path to the root; a node already marked has its path marked (or
+    // being marked) by the leaf that got there first
+    for (int depth = 0; depth < 256 && code >= 0; ++depth) {
+        const int node = code >> 1;
+        if (atomicOr(&dmask[node], 1 << (code & 1)) != 0) break;
+        code = parent[node];
+    }
+}
+
+cudaError_t lbvh_refit_dirty(Lbvh &b, const float4 *pts, const int4 *tris, long long max_dirty, cudaStream_t s);
 
 }  // namespace pamo

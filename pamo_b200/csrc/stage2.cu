@@ -169,6 +169,30 @@ __device__ __forceinline__ float skinny_term(V3 n0, V3 n1, V3 n2)
     // the squares and the sum after the fp32 numerator are doubles, rounded once
     const float c4s3 = 4.0f * sqrtf(3.0f);
     float num = c4s3 * area;
+    // Shortcut: every term is non-negative, so the same sum in fp32 (five
+    // roundings, relative error < 4e-7 while l01^2 is a normal float; an fp32
+    // overflow to +inf only happens when the double sum is far above 1) bounds
+    // the double sum from below within 4e-7.  At or above 1 + 2^-18 the double
+    // sum is above 1, its float rounding is >= 1, and the clamped penalty is
+    // exactly 0 -- the value the double path returns.  Well-shaped triangles
+    // (sum near 3) take this path; NaN and near-1 sums fall through.
+    const float q01 = l01 * l01;
+    if (q01 >= 1.17549435e-38f) {
+        float ef = num / q01 + l12 * l12 + l20 * l20 + 0.0000001f;
+        if (ef >= 1.0f + 0x1p-18f) return 0.0f;
+    }
+    // Second shortcut: CUDA's double pow(x, 2.0) is within one double ulp of the
+    // exact square x*x for every float x (an exhaustive check over all finite
+    // floats on a B200; it differs for ~6% of them).  The same sum with exact
+    // squares therefore lies within 8 ulp of the one with pow (each term is
+    // non-negative); when a 16-ulp neighbourhood of it rounds to one float, that
+    // float is the reference's.  Otherwise (NaN, inf, or a sum next to a float
+    // rounding boundary) the pow form is evaluated as the reference writes it.
+    const double sq = (double)num / ((double)l01 * (double)l01) + (double)l12 * (double)l12 +
+                      (double)l20 * (double)l20 + (double)0.0000001f;
+    const double margin = sq * 0x1p-48;
+    const float fq = (float)sq;
+    if (fq == (float)(sq - margin) && fq == (float)(sq + margin)) return 1.0f - tclamp(fq, 0.0f, 1.0f);
     double e = (double)num / pow((double)l01, 2.0) + pow((double)l12, 2.0) + pow((double)l20, 2.0) +
                (double)0.0000001f;
     return 1.0f - tclamp((float)e, 0.0f, 1.0f);
@@ -281,30 +305,24 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, boo
     return true;
 }
 
-// Edge passes run in the hierarchy's leaf (Morton) order: a block takes
+// The edge-cost pass runs in the hierarchy's leaf (Morton) order: a block takes
 // kChunkFaces consecutive leaves, lists their faces' edges in shared memory
-// (each face owns its 0-3 descending edges) and its threads take the list in
+// (each face owns its 0-2 descending edges) and its threads take the list in
 // turn, so neighbouring lanes gather neighbouring vertices and every lane has an
-// edge.  Results are indexed by edge and winners never share a face, so the
-// order of work does not change them.
-constexpr int kChunkFaces = 2 * kThreads;
+// edge.  Costs are indexed by edge, so the order of work does not change them.
+constexpr int kChunkFaces = kThreads;
 constexpr int kChunkEdges = 3 * kChunkFaces;
 
 __device__ __forceinline__ int chunk_edges(const int *order, const int *first_edge, int L, long long base,
                                            int *s_list)
 {
-    int fe[2], c[2];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        long long p = base + 2 * threadIdx.x + k;
-        int f = p < L ? order[p] : -1;  // -1: past the end, or a face removed since the build
-        fe[k] = f >= 0 ? first_edge[f] : 0;
-        c[k] = f >= 0 ? first_edge[f + 1] - fe[k] : 0;
-    }
+    long long p = base + threadIdx.x;
+    int f = p < L ? order[p] : -1;  // -1: past the end, or a face removed since the build
+    int fe = f >= 0 ? first_edge[f] : 0;
+    int c = f >= 0 ? first_edge[f + 1] - fe : 0;
     int total;
-    int off = block_excl_scan<kThreads>(c[0] + c[1], total);
-    for (int j = 0; j < c[0]; ++j) s_list[off + j] = fe[0] + j;
-    for (int j = 0; j < c[1]; ++j) s_list[off + c[0] + j] = fe[1] + j;
+    int off = block_excl_scan<kThreads>(c, total);
+    for (int j = 0; j < c; ++j) s_list[off + j] = fe + j;
     __syncthreads();
     return total;
 }
@@ -382,15 +400,14 @@ __device__ __forceinline__ bool faces_min_ok(const CollapseArgs &A, int lo, int 
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A, const int *order, const int *scene,
-                                                       const int *first_edge)
+// One thread per edge: most edges fail the threshold or the key test at once,
+// and a winner's collapse is long, so no block-wide step waits on it.
+__global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
 {
-    __shared__ int s_list[kChunkEdges];
-    const int L = scene[7];
-    for (long long base = (long long)blockIdx.x * kChunkFaces; base < L; base += (long long)gridDim.x * kChunkFaces) {
-      const int total = chunk_edges(order, first_edge, L, base, s_list);
-      for (int q = threadIdx.x; q < total; q += kThreads) {
-        const int e = s_list[q];
+    const int E = *A.n_edges;
+    PAMO_GRID_STRIDE(ee, E)
+    {
+        const int e = (int)ee;
         int win = 0;
         uint32_t c, collapse_t;
         if (!A.slots) {
@@ -450,8 +467,6 @@ __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A, const int
             }
         }
         A.eflag[e] = win;
-      }
-      __syncthreads();
     }
 }
 
@@ -784,14 +799,40 @@ __global__ void k_compact(const float4 *pts, const int *occ, const int *pts_map,
     }
 }
 
-// After compaction: leaf p's face gets its compacted index, or -1 if removed.
-__global__ void k_remap_leaves(int *vals, const int *scene, const int *fflag, const int *fpos)
+// After compaction: leaf p's face gets its compacted index, or -1 if removed
+// (every surviving face is a leaf, so leaf_of_face is complete again).
+__global__ void k_remap_leaves(int *vals, const int *scene, const int *fflag, const int *fpos, int *leaf_of_face)
 {
     const int L = scene[7];
     PAMO_GRID_STRIDE(p, L)
     {
         int f = vals[p];
-        vals[p] = (f >= 0 && fflag[f]) ? fpos[f] : -1;
+        int nf = (f >= 0 && fflag[f]) ? fpos[f] : -1;
+        vals[p] = nf;
+        if (nf >= 0) leaf_of_face[nf] = (int)p;
+    }
+}
+
+// Leaves whose boxes changed since the last refit: the faces of the one-rings of
+// the listed edges (collapses, coincident-endpoint collapses and undos only
+// change those faces and their vertices).
+__global__ void k_mark_dirty(const int *elist, const int *n_list, const int2 *edges, const int *first_near,
+                             const int *near_tris, const int *leaf_of_face, const int *parent, int *claim,
+                             int *dmask, int *dlist, int *scene)
+{
+    const int N = *n_list;
+    const int L = scene[7];
+    if (L < 2) return;
+    PAMO_GRID_STRIDE(k, N)
+    {
+        const int2 ed = edges[elist[k]];
+        for (int side = 0; side < 2; ++side) {
+            const int w = side ? ed.y : ed.x;
+            for (int a = first_near[w]; a < first_near[w + 1]; ++a) {
+                const int p = leaf_of_face[near_tris[a]];
+                if (p >= 0) lbvh_mark_dirty_leaf(p, L, parent, claim, dmask, dlist, scene);
+            }
+        }
     }
 }
 
@@ -1036,8 +1077,20 @@ void Profiler::collect()
             calls[marks[i][0]]++;
         }
     }
+    if (open_phase >= 0) {  // a phase still open keeps its start event, moved to slot 0
+        const int slot = marks[n_marks][1];
+        cudaEvent_t a = ev[0], b = ev[1];
+        ev[0] = ev[slot];
+        ev[1] = ev[slot + 1];
+        ev[slot] = a;
+        ev[slot + 1] = b;
+        marks[0][0] = marks[n_marks][0];
+        marks[0][1] = 0;
+        used = 2;
+    } else {
+        used = 0;
+    }
     n_marks = 0;
-    used = 0;
 }
 
 void Profiler::reset()
@@ -1092,6 +1145,7 @@ void Stage2::release()
     bvh.release();
     bvh_carried = false;
     bvh_leaves = 0;
+    bvh_boxes_valid = false;
     cap_pts = cap_tris = cap_edges = cap_undo = cap_pairs = 0;
 }
 
@@ -1192,13 +1246,26 @@ int Stage2::ensure_pairs(long long n)
         if (_e != cudaSuccess) return map_cuda_error(_e); \
     } while (0)
 
-static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s)
+// dirty_edges / n_dirty: when the boxes were up to date before this round's
+// changes, the edges whose one-rings changed since (incremental refit);
+// otherwise null (full refit).
+static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s, const int *dirty_edges = nullptr,
+                              const int *n_dirty = nullptr)
 {
     cudaError_t e;
     if ((e = cudaMemsetAsync(S.isect, 0, (size_t)m, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&S.dcnt->n_pairs, 0, 2 * sizeof(int), s)) != cudaSuccess) return e;  // n_pairs, overflow
     S.prof.begin(PH_REFIT, s);
-    if ((e = lbvh_refit(S.bvh, S.pts, S.tris, m, s)) != cudaSuccess) return e;
+    if (dirty_edges && S.bvh_boxes_valid && S.bvh.leaves_built >= 2) {
+        if ((e = cudaMemsetAsync(S.bvh.scene + 9, 0, sizeof(int), s)) != cudaSuccess) return e;
+        launch(k_mark_dirty, grid_for(3LL * m), kThreads, 0, s, dirty_edges, n_dirty, (const int2 *)S.edges,
+               (const int *)S.first_near, (const int *)S.near_tris, (const int *)S.bvh.leaf_of_face,
+               (const int *)S.bvh.parent, S.bvh.claim, S.bvh.dmask, S.bvh.dlist, S.bvh.scene);
+        if ((e = lbvh_refit_dirty(S.bvh, S.pts, S.tris, S.bvh.leaves_built, s)) != cudaSuccess) return e;
+    } else {
+        if ((e = lbvh_refit(S.bvh, S.pts, S.tris, m, s)) != cudaSuccess) return e;
+    }
+    S.bvh_boxes_valid = true;
     S.prof.begin(PH_QUERY, s);
     const bool batch = S.n_slots > 0;
     if ((e = cudaMemsetAsync(&S.dcnt->n_query, 0, sizeof(int), s)) != cudaSuccess) return e;
@@ -1271,6 +1338,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     if (!(keep_bvh && bvh_carried && m <= bvh_leaves && (double)m >= kRebuildFraction * (double)bvh_leaves)) {
         S2_TRY(lbvh_build(bvh, pts, tris, m, s));
         bvh_leaves = m;
+        bvh_boxes_valid = false;
     }
     bvh_carried = false;
 
@@ -1282,7 +1350,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     CollapseArgs cl{edges, d_n_edges, edge_cost, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
                     collapse_t, nullptr, nullptr, nullptr};
     prof.begin(PH_COLLAPSE, s);
-    launch(k_collapse, grid_for(m, kChunkFaces), kThreads, 0, s, cl, bvh.vals, bvh.scene, first_edge);
+    launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
     launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
     prof.begin(PH_CLEANUP, s);
@@ -1293,7 +1361,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
 
     S2_TRY(cudaMemsetAsync(active, 0, (size_t)m, s));
     launch(k_mark_active, grid_for(EMAX), kThreads, 0, s, collapsed, dcnt, edges, first_near, near_tris, active);
-    S2_TRY(isect_pass(*this, m, s));
+    S2_TRY(isect_pass(*this, m, s, collapsed, &dcnt->n_total));  // only the collapses' one-rings changed
     S2_TRY(undo_check(*this, s));
     S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
     S2_TRY(cudaStreamSynchronize(s));
@@ -1303,7 +1371,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
         long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
         int rc = ensure_pairs(need);
         if (rc) return rc;
-        S2_TRY(isect_pass(*this, m, s));
+        S2_TRY(isect_pass(*this, m, s, collapsed, &dcnt->n_total));
         S2_TRY(undo_check(*this, s));
         S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
         S2_TRY(cudaStreamSynchronize(s));
@@ -1327,7 +1395,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
         if (nvu - first > 0)
             launch(k_rearrange, grid_for(nvu - first), kThreads, 0, s, tmp_undo, pts_map, undo_list, first, nvu - first);
         first += 2 * cnt_undo;
-        S2_TRY(isect_pass(*this, m, s));
+        S2_TRY(isect_pass(*this, m, s, undo_edges, &dcnt->n_undo));  // only the undone one-rings changed
         S2_TRY(undo_check(*this, s));
         S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
         S2_TRY(cudaStreamSynchronize(s));
@@ -1336,7 +1404,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
             long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
             int rc = ensure_pairs(need);
             if (rc) return rc;
-            S2_TRY(isect_pass(*this, m, s));
+            S2_TRY(isect_pass(*this, m, s, undo_edges, &dcnt->n_undo));
             S2_TRY(undo_check(*this, s));
             S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
             S2_TRY(cudaStreamSynchronize(s));
@@ -1378,6 +1446,7 @@ int Stage2::self_intersect_all(int n, int m, cudaStream_t s)
     S2_TRY(cudaMemsetAsync(dcnt, 0, sizeof(RoundCounters), s));
     S2_TRY(cudaMemsetAsync(active, 1, (size_t)m, s));
     S2_TRY(lbvh_build(bvh, pts, tris, m, s));
+    bvh_boxes_valid = false;
     S2_TRY(isect_pass(*this, m, s));
     S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
     S2_TRY(cudaStreamSynchronize(s));
@@ -1402,7 +1471,8 @@ int Stage2::compact(int n, int m, cudaStream_t s)
     launch(k_compact, grid_for(n > m ? n : m), kThreads, 0, s, pts, occ, pts_map, n, tris, fflag, uflag, m, opts, otris,
                                                            dcnt);
     if (bvh_leaves > 0 && bvh_leaves >= m) {
-        launch(k_remap_leaves, grid_for(bvh_leaves), kThreads, 0, s, bvh.vals, bvh.scene, fflag, uflag);
+        launch(k_remap_leaves, grid_for(bvh_leaves), kThreads, 0, s, bvh.vals, (const int *)bvh.scene,
+               (const int *)fflag, (const int *)uflag, bvh.leaf_of_face);
         bvh_carried = true;
     }
     prof.end(s);
@@ -1504,6 +1574,7 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
     launch(k_b_edge_off, grid_for(K), kThreads, 0, s, (const SlotInfo *)slots, (const int *)first_edge, scnt, K);
     prof.begin(PH_LBVH_BUILD, s);
     S2_TRY(lbvh_build(bvh, pts, tris, m, s, vslot, K, roots));
+    bvh_boxes_valid = false;
     bvh_leaves = m;
 
     const long long EMAX = 3LL * m;
@@ -1514,7 +1585,7 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
     CollapseArgs cl{edges, d_n_edges, nullptr, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
                     0u, slots, scnt, vslot};
     prof.begin(PH_COLLAPSE, s);
-    launch(k_collapse, grid_for(m, kChunkFaces), kThreads, 0, s, cl, bvh.vals, bvh.scene, first_edge);
+    launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
     launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
     launch(k_b_main, grid_for(K), kThreads, 0, s, (const int *)uflag, (const RoundCounters *)dcnt, scnt, K);

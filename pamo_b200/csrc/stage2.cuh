@@ -85,6 +85,12 @@ enum Phase {
     PH_PAIRS,       // triangle-pair tests
     PH_UNDO,        // undo candidates, restore, list rearrangement
     PH_COMPACT,     // pts_map scan + compaction for the next round
+    PH_S3_CLOSEST,  // stage 3: closest points on the ground truth
+    PH_S3_DETECT,   // stage 3: hierarchy refits + contact detection (with its sync)
+    PH_S3_DIFF,     // stage 3: energy, gradient, diagonal, hinge / contact blocks
+    PH_S3_CG,       // stage 3: Jacobi-PCG iterations
+    PH_S3_CCD,      // stage 3: clamp + additive CCD
+    PH_S3_LINE,     // stage 3: line-search energies
     PH_COUNT
 };
 
@@ -150,6 +156,7 @@ struct Stage2 {
     // reused (refit only) while enough of its leaves are still faces.
     bool bvh_carried = false;
     long long bvh_leaves = 0;  // faces the hierarchy was built over
+    bool bvh_boxes_valid = false;  // every box matches the geometry of the last refit
 
     // batch mode (see SlotInfo); unused by the single-mesh rounds
     int n_slots = 0, cap_slots = 0;

@@ -31,7 +31,8 @@ constexpr int kRedBlocks = 296;  // fixed grid for deterministic reductions (2 x
 constexpr int kStack = 96;
 
 enum { D_ENERGY = 0, D_ENERGY_PREV, D_ZR, D_ZR_LAST, D_VAV };
-enum { I_NB = 0, I_OVERFLOW, I_STACK };
+enum { I_NB = 0, I_OVERFLOW, I_STACK, I_NACT, I_NCAND_PT, I_NCAND_EE, I_TICKET, I_DISP, I_BAR_ERR, I_BAR_COUNT,
+       I_BAR_GEN };
 
 __device__ __forceinline__ F3 ld(const float4 *a, int i) { return f3(a[i]); }
 __device__ __forceinline__ void st(float4 *a, int i, F3 v) { a[i] = make_float4(v.x, v.y, v.z, 0.f); }
@@ -246,10 +247,27 @@ __device__ __forceinline__ void append_block(int4 idx, int kind, int *iscal, lon
     }
 }
 
+// Detection runs in two passes.  The traversals (one thread per vertex or edge,
+// few threads for a small mesh) only emit candidate pairs whose boxes overlap
+// with a margin; the classification and distance test then runs one thread per
+// candidate, and a pair is kept when its classified distance is within thr, as
+// in contact_detection.py.  The candidates are gathered with thr + extra and
+// kept: while no vertex has moved more than extra / 2 since, every pair within
+// thr is among them (each of its two primitives moved at most extra / 2), so
+// later detections only rerun the test.
+__device__ __forceinline__ void append_pair(int a, int b, int *counter, long long cap, int2 *out)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
+    int pos = g.shfl(base, 0) + (int)g.thread_rank();
+    if (pos < cap) out[pos] = make_int2(a, b);
+}
+
 // point-triangle candidates (contact_detection.py:120-164)
 __global__ void __launch_bounds__(kThreads) k_detect_pt(const float4 *q, int np, const int4 *tris, const BvhNode *nodes,
                                                         const int *vals, const int *scene, float thr, int *iscal,
-                                                        long long cap, int4 *bidx, int *bkind)
+                                                        long long cap_c, int2 *cand)
 {
     const int L = scene[7];
     int stack[kStack];
@@ -263,9 +281,9 @@ __global__ void __launch_bounds__(kThreads) k_detect_pt(const float4 *q, int np,
         if (L > 1) stack[sp++] = 0;
         int budget = 2 * L + 16;
         while (sp > 0 || leaf_only) {
-            int cand[2] = {-1, -1};
+            int c2[2] = {-1, -1};
             if (leaf_only) {
-                cand[0] = vals[0];
+                c2[0] = vals[0];
                 leaf_only = 0;
             } else {
                 if (--budget < 0) {
@@ -277,30 +295,52 @@ __global__ void __launch_bounds__(kThreads) k_detect_pt(const float4 *q, int np,
                     float4 lo = side ? nd.rlo : nd.llo, hi = side ? nd.rhi : nd.lhi;
                     if (!overlap(lo, hi, qlo, qhi)) continue;
                     int child = __float_as_int(lo.w);
-                    if (child < 0) cand[side] = vals[~child];
+                    if (child < 0) c2[side] = vals[~child];
                     else if (sp < kStack) stack[sp++] = child;
                     else atomicAdd(&iscal[I_STACK], 1);
                 }
             }
             for (int k = 0; k < 2; ++k) {
-                int f = cand[k];
+                int f = c2[k];
                 if (f < 0) continue;
                 int4 t = tris[f];
                 if (t.x == i || t.y == i || t.z == i) continue;
-                F3 x[4] = {x0, ld(q, t.x), ld(q, t.y), ld(q, t.z)};
-                int ty = pt_classify(x[0], x[1], x[2], x[3]);
-                float d = classified_distance(KIND_PT, ty, x);
-                if (d <= thr) append_block(make_int4(i, t.x, t.y, t.z), KIND_PT, iscal, cap, bidx, bkind);
+                append_pair(i, f, &iscal[I_NCAND_PT], cap_c, cand);
             }
         }
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_test_pt(const float4 *q, const int4 *tris, const int2 *cand,
+                                                      long long cap_c, float thr, int *iscal, long long cap,
+                                                      int4 *bidx, int *bkind)
+{
+    const long long n = min((long long)iscal[I_NCAND_PT], cap_c);
+    PAMO_GRID_STRIDE(k, n)
+    {
+        int2 c = cand[k];
+        int4 t = tris[c.y];
+        F3 x[4] = {ld(q, c.x), ld(q, t.x), ld(q, t.y), ld(q, t.z)};
+        int ty = pt_classify(x[0], x[1], x[2], x[3]);
+        float d = classified_distance(KIND_PT, ty, x);
+        if (d <= thr) append_block(make_int4(c.x, t.x, t.y, t.z), KIND_PT, iscal, cap, bidx, bkind);
+    }
+}
+
+// largest displacement of a vertex since the candidates were gathered (float
+// bits of a non-negative value order like ints)
+__global__ void k_max_disp(const float4 *q, const float4 *q_gather, int np, int *iscal)
+{
+    float m = 0.f;
+    PAMO_GRID_STRIDE(i, np) m = fmaxf(m, len(ld(q, (int)i) - ld(q_gather, (int)i)));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(&iscal[I_DISP], __float_as_int(m));
+}
+
 // edge-edge candidates (contact_detection.py:168-216)
 __global__ void __launch_bounds__(kThreads) k_detect_ee(const float4 *q, int ne, const int4 *edges4,
                                                         const BvhNode *nodes, const int *vals, const int *scene,
-                                                        float thr, float ee_thres, int *iscal, long long cap,
-                                                        int4 *bidx, int *bkind)
+                                                        float thr, int *iscal, long long cap_c, int2 *cand)
 {
     const int L = scene[7];
     int stack[kStack];
@@ -334,12 +374,25 @@ __global__ void __launch_bounds__(kThreads) k_detect_ee(const float4 *q, int ne,
                 if (e1 <= e0) continue;
                 int4 b = edges4[e1];
                 if (a.x == b.x || a.x == b.y || a.y == b.x || a.y == b.y) continue;
-                F3 x[4] = {x0, x1, ld(q, b.x), ld(q, b.y)};
-                int ty = ee_classify(x[0], x[1], x[2], x[3], ee_thres);
-                float d = classified_distance(KIND_EE, ty, x);
-                if (d <= thr) append_block(make_int4(a.x, a.y, b.x, b.y), KIND_EE, iscal, cap, bidx, bkind);
+                append_pair(e0, e1, &iscal[I_NCAND_EE], cap_c, cand);
             }
         }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_test_ee(const float4 *q, const int4 *edges4, const int2 *cand,
+                                                      long long cap_c, float thr, float ee_thres, int *iscal,
+                                                      long long cap, int4 *bidx, int *bkind)
+{
+    const long long n = min((long long)iscal[I_NCAND_EE], cap_c);
+    PAMO_GRID_STRIDE(k, n)
+    {
+        int2 c = cand[k];
+        int4 a = edges4[c.x], b = edges4[c.y];
+        F3 x[4] = {ld(q, a.x), ld(q, a.y), ld(q, b.x), ld(q, b.y)};
+        int ty = ee_classify(x[0], x[1], x[2], x[3], ee_thres);
+        float d = classified_distance(KIND_EE, ty, x);
+        if (d <= thr) append_block(make_int4(a.x, a.y, b.x, b.y), KIND_EE, iscal, cap, bidx, bkind);
     }
 }
 
@@ -363,6 +416,10 @@ struct EArgs {
     long long cap_b;
     float d_hat, kappa, ee_thres;
     double *partials;
+    // line search: halving n_halves > 0 is skipped once a trial was accepted
+    // (energy below the start's), as the reference's loop stops there
+    int n_halves;
+    const double *dscal;
 };
 
 __device__ __forceinline__ void elastic_F(const float4 *q, int4 f, float4 im, F3 &b1, F3 &b2, float F[4])
@@ -379,6 +436,8 @@ __device__ __forceinline__ void elastic_F(const float4 *q, int4 f, float4 im, F3
 
 __global__ void __launch_bounds__(kThreads) k_energy(EArgs A)
 {
+    // the partials then still hold the accepted trial's energy
+    if (A.n_halves > 0 && A.dscal[D_ENERGY] < A.dscal[D_ENERGY_PREV]) return;
     const long long nb = min((long long)A.iscal[I_NB], A.cap_b);
     const long long total = (long long)A.np + A.nt + A.nh + nb;
     double acc = 0.0;
@@ -595,10 +654,11 @@ struct DArgs {
     const float *bd;
     float4 *bg;
     float *bb2;
-    const int *iscal;
+    int *iscal;
     long long cap_b;
     float d_hat, kappa;
     float4 *grad, *diag;
+    int *bact;  // contact blocks with d < d_hat, appended here for the CG products
 };
 
 __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
@@ -669,6 +729,10 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
                 atomic_add3(A.diag, idx[a], mk(b2f * g[a].x * g[a].x, b2f * g[a].y * g[a].y, b2f * g[a].z * g[a].z));
             }
             A.bb2[b] = b2f;
+            cg::coalesced_group grp = cg::coalesced_threads();
+            int base = 0;
+            if (grp.thread_rank() == 0) base = atomicAdd(&A.iscal[I_NACT], (int)grp.size());
+            A.bact[grp.shfl(base, 0) + (int)grp.thread_rank()] = b;
         }
     }
 }
@@ -691,18 +755,17 @@ struct HArgs {
     long long cap_b;
     const float4 *dx;
     float4 *out;
+    const int *bact;
 };
 
-__global__ void k_hess_vertex(const float *wk, int np, const float4 *dx, float4 *out)
+// Element terms of H dx added into out (atomics): membrane, hinges, and the
+// contact blocks with d < d_hat (listed by k_diff_elements; the others have no
+// Gauss-Newton term).  `first` / `stride` spread the elements over the threads.
+__device__ __forceinline__ void hess_elements_range(const HArgs &A, long long first, long long stride)
 {
-    PAMO_GRID_STRIDE(i, np) st(out, (int)i, wk[i] * ld(dx, (int)i));
-}
-
-__global__ void __launch_bounds__(kThreads) k_hess_elements(HArgs A)
-{
-    const long long nb = min((long long)A.iscal[I_NB], A.cap_b);
+    const long long nb = min((long long)A.iscal[I_NACT], A.cap_b);
     const long long total = (long long)A.nt + A.nh + nb;
-    PAMO_GRID_STRIDE(k, total)
+    for (long long k = first; k < total; k += stride)
     {
         if (k < A.nt) {
             int t = (int)k;
@@ -754,7 +817,7 @@ __global__ void __launch_bounds__(kThreads) k_hess_elements(HArgs A)
                 atomic_add3(A.out, idx[a], s);
             }
         } else {
-            int b = (int)(k - A.nt - A.nh);
+            int b = A.bact[k - A.nt - A.nh];
             float c = A.bb2[b];
             if (c == 0.f) continue;
             int4 i = A.bidx[b];
@@ -770,9 +833,42 @@ __global__ void __launch_bounds__(kThreads) k_hess_elements(HArgs A)
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_hess_elements(HArgs A)
+{
+    hess_elements_range(A, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)blockDim.x * gridDim.x);
+}
+
 // -------------------------------------------------------------------- CG
+// Each reduction kernel writes one partial per block; the last block to finish
+// (a ticket counter, no waiting) adds the partials in a fixed order -- the order
+// k_finish_sum uses -- so the sums are deterministic and a separate finishing
+// launch is not needed.  Returns true in the last block (all its threads).
+__device__ __forceinline__ bool last_block_sum(double block_total, double *partials, int *ticket, double *dst)
+{
+    __shared__ bool s_last;
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = block_total;
+        __threadfence();
+        s_last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) v += __ldcg(&partials[i]);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) {
+            *dst = v;
+            *ticket = 0;
+        }
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(kThreads) k_cg_init(const float4 *grad, const float4 *diag, int np, float4 *p,
-                                                      float4 *r, float4 *z, float4 *v, double *partials)
+                                                      float4 *r, float4 *z, float4 *v, double *partials, int *ticket,
+                                                      double *dscal)
 {
     double acc = 0.0;
     PAMO_GRID_STRIDE(i, np)
@@ -786,23 +882,40 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(const float4 *grad, const 
         acc += (double)dot(zz, g);
     }
     double s = block_sum<kThreads>(acc);
-    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+    last_block_sum(s, partials, ticket, dscal + D_ZR);
 }
 
-__global__ void __launch_bounds__(kThreads) k_dot(const float4 *a, const float4 *b, int np, double *partials)
+// v^T A v, then zr_last = zr
+__global__ void __launch_bounds__(kThreads) k_cg_dot(const float4 *a, const float4 *b, int np, double *partials,
+                                                     int *ticket, double *dscal)
 {
     double acc = 0.0;
     PAMO_GRID_STRIDE(i, np) acc += (double)dot(ld(a, (int)i), ld(b, (int)i));
     double s = block_sum<kThreads>(acc);
-    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+    if (last_block_sum(s, partials, ticket, dscal + D_VAV) && threadIdx.x == 0) dscal[D_ZR_LAST] = dscal[D_ZR];
 }
 
-__global__ void k_shift_zr(double *dscal) { dscal[D_ZR_LAST] = dscal[D_ZR]; }
+// start of a CG iteration: v = z + beta v (not in the first), Av = w v (the
+// vertex term of the Hessian; the element terms are added by k_hess_elements)
+__global__ void k_cg_pre(const float4 *z, const double *dscal, const float *wk, int np, int first, float4 *v,
+                         float4 *Av)
+{
+    const float beta = first ? 0.f : (float)(dscal[D_ZR] / dscal[D_ZR_LAST]);
+    PAMO_GRID_STRIDE(i, np)
+    {
+        F3 vv = ld(v, (int)i);
+        if (!first) {
+            vv = ld(z, (int)i) + beta * vv;
+            st(v, (int)i, vv);
+        }
+        st(Av, (int)i, wk[i] * vv);
+    }
+}
 
 // p += alpha v, r -= alpha Av (if v^T A v > 1e-16); z = r / diag; partial z.r
 __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const float4 *Av, const float4 *diag,
-                                                        const double *dscal, int np, float4 *p, float4 *r, float4 *z,
-                                                        double *partials)
+                                                        double *dscal, int np, float4 *p, float4 *r, float4 *z,
+                                                        double *partials, int *ticket)
 {
     const double vav = dscal[D_VAV];
     const bool upd = vav > 1e-16;
@@ -822,13 +935,132 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const f
         acc += (double)dot(zz, rr);
     }
     double s = block_sum<kThreads>(acc);
-    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+    last_block_sum(s, partials, ticket, dscal + D_ZR);
 }
 
-__global__ void k_cg_v(const float4 *z, const double *dscal, int np, float4 *v)
+// The whole Jacobi-PCG solve of a Newton iteration (the 40 iterations of
+// cg_solver.py:96-158) in one cooperative launch: the phases that the separate
+// kernels above run one launch each are separated by a grid barrier instead.
+// Every block keeps the same grid-stride ranges and adds the per-block partials
+// in the same fixed order as k_finish_sum, so the sums equal the multi-launch
+// solve's.  The barrier spins with a limit; on timeout it records the error and
+// the kernel returns.
+struct CGArgs {
+    HArgs h;
+    const float4 *grad, *diag;
+    const float *wk;
+    float4 *p, *r, *z, *v, *Av;
+    double *partials;
+    double *dscal;
+    int *iscal;
+    int np, n_iters;
+};
+
+__device__ __forceinline__ bool grid_barrier(int *iscal)
 {
-    const float beta = (float)(dscal[D_ZR] / dscal[D_ZR_LAST]);
-    PAMO_GRID_STRIDE(i, np) st(v, (int)i, ld(z, (int)i) + beta * ld(v, (int)i));
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile int *vgen = iscal + I_BAR_GEN;
+        const int gen = *vgen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(iscal + I_BAR_COUNT, 1) == (int)gridDim.x - 1) {
+            iscal[I_BAR_COUNT] = 0;
+            __threadfence();
+            atomicAdd(iscal + I_BAR_GEN, 1);
+        } else {
+            for (long long spins = 0; *vgen == gen; ++spins) {
+                if (spins > (1LL << 24)) {  // ~ seconds: a block never arrived
+                    atomicExch(iscal + I_BAR_ERR, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// sum of the blocks' partials in k_finish_sum's order, in every block
+__device__ __forceinline__ double all_blocks_sum(const double *partials)
+{
+    __shared__ double s_sum;
+    if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) v += __ldcg(&partials[i]);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) s_sum = v;
+    }
+    __syncthreads();
+    double r = s_sum;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kThreads, 2) k_cg_solve(CGArgs A)
+{
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long gs = (long long)blockDim.x * gridDim.x;
+    // r = g, z = v = g / (diag + 1e-6), p = 0
+    double acc = 0.0;
+    for (long long i = t0; i < A.np; i += gs) {
+        F3 g = ld(A.grad, (int)i), d = ld(A.diag, (int)i);
+        F3 zz = mk(g.x / (d.x + 1e-6f), g.y / (d.y + 1e-6f), g.z / (d.z + 1e-6f));
+        A.p[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        st(A.r, (int)i, g);
+        st(A.z, (int)i, zz);
+        st(A.v, (int)i, zz);
+        acc += (double)dot(zz, g);
+    }
+    double bs = block_sum<kThreads>(acc);
+    if (threadIdx.x == 0) A.partials[blockIdx.x] = bs;
+    if (!grid_barrier(A.iscal)) return;
+    double zr = all_blocks_sum(A.partials), zr_last = zr;
+    for (int it = 0; it < A.n_iters; ++it) {
+        const float beta = it == 0 ? 0.f : (float)(zr / zr_last);
+        for (long long i = t0; i < A.np; i += gs) {
+            F3 vv = ld(A.v, (int)i);
+            if (it > 0) {
+                vv = ld(A.z, (int)i) + beta * vv;
+                st(A.v, (int)i, vv);
+            }
+            st(A.Av, (int)i, A.wk[i] * vv);
+        }
+        if (!grid_barrier(A.iscal)) return;
+        hess_elements_range(A.h, t0, gs);
+        if (!grid_barrier(A.iscal)) return;
+        acc = 0.0;
+        for (long long i = t0; i < A.np; i += gs) acc += (double)dot(ld(A.v, (int)i), ld(A.Av, (int)i));
+        bs = block_sum<kThreads>(acc);
+        if (threadIdx.x == 0) A.partials[blockIdx.x] = bs;
+        if (!grid_barrier(A.iscal)) return;
+        const double vav = all_blocks_sum(A.partials);
+        zr_last = zr;
+        const bool upd = vav > 1e-16;
+        const float alpha = upd ? (float)(zr_last / vav) : 0.f;
+        acc = 0.0;
+        for (long long i = t0; i < A.np; i += gs) {
+            F3 rr = ld(A.r, (int)i);
+            if (upd) {
+                st(A.p, (int)i, ld(A.p, (int)i) + alpha * ld(A.v, (int)i));
+                rr = rr - alpha * ld(A.Av, (int)i);
+                st(A.r, (int)i, rr);
+            }
+            F3 d = ld(A.diag, (int)i);
+            F3 zz = mk(rr.x / d.x, rr.y / d.y, rr.z / d.z);
+            st(A.z, (int)i, zz);
+            acc += (double)dot(zz, rr);
+        }
+        bs = block_sum<kThreads>(acc);
+        if (threadIdx.x == 0) A.partials[blockIdx.x] = bs;
+        if (!grid_barrier(A.iscal)) return;
+        zr = all_blocks_sum(A.partials);
+    }
 }
 
 // ---------------------------------------------------------- clamp, CCD, line search
@@ -934,17 +1166,28 @@ __global__ void k_f4_to_aos(const float4 *in, float *out, int n)
 
 void Stage3::release()
 {
-    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, Av, wk, tris, area, inv_dm, edges4, hinges,
-                    rest_angle, rest_elen, hblk, bidx, bkind, bsub, bd, bb2, bg, gt_pts, gt_tris, dscal, fscal, iscal,
-                    partials};
+    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, Av, q_gather, wk, tris, area, inv_dm, edges4, hinges,
+                    rest_angle, rest_elen, hblk, bidx, bkind, bsub, bd, bb2, bg, bact, gt_pts, gt_tris, dscal, fscal,
+                    iscal, partials};
+    drop_graph();
+    if (cand_pt) cudaFree(cand_pt);
+    if (cand_ee) cudaFree(cand_ee);
+    cand_pt = cand_ee = nullptr;
+    cap_c = 0;
+    if (work) cudaStreamDestroy(work);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    work = nullptr;
+    ev_in = ev_out = nullptr;
     for (void *x : ptrs)
         if (x) cudaFree(x);
     if (h_iscal) cudaFreeHost(h_iscal);
     if (h_dscal) cudaFreeHost(h_dscal);
-    q = q_prev = q_det = p = grad = diag = target = r = z = v = Av = nullptr;
+    q = q_prev = q_det = p = grad = diag = target = r = z = v = Av = q_gather = nullptr;
+    gathered = false;
     wk = nullptr; tris = nullptr; area = nullptr; inv_dm = nullptr; edges4 = nullptr; hinges = nullptr;
     rest_angle = rest_elen = hblk = nullptr; bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr;
-    bg = nullptr; gt_pts = nullptr; gt_tris = nullptr; dscal = nullptr; fscal = nullptr; iscal = nullptr;
+    bg = nullptr; bact = nullptr; gt_pts = nullptr; gt_tris = nullptr; dscal = nullptr; fscal = nullptr; iscal = nullptr;
     partials = nullptr; h_iscal = nullptr; h_dscal = nullptr;
     tri_bvh.release();
     edge_bvh.release();
@@ -971,6 +1214,7 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
     } while (0)
     A3(q, cp * 16); A3(q_prev, cp * 16); A3(q_det, cp * 16); A3(p, cp * 16); A3(grad, cp * 16);
     A3(diag, cp * 16); A3(target, cp * 16); A3(r, cp * 16); A3(z, cp * 16); A3(v, cp * 16); A3(Av, cp * 16);
+    A3(q_gather, cp * 16);
     A3(wk, cp * 4);
     A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16);
     A3(edges4, ce * 16);
@@ -991,17 +1235,32 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
     return ensure_blocks(cb > 0 ? cb : 8 * cp + 1024);
 }
 
+int Stage3::ensure_cands(long long n)
+{
+    if (n <= cap_c && cand_pt) return PAMO_OK;
+    if (cand_pt) cudaFree(cand_pt);
+    if (cand_ee) cudaFree(cand_ee);
+    cand_pt = cand_ee = nullptr;
+    cap_c = 0;
+    if (cudaMalloc((void **)&cand_pt, n * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc((void **)&cand_ee, n * sizeof(int2)) != cudaSuccess)
+        return PAMO_ERR_OOM;
+    cap_c = n;
+    return PAMO_OK;
+}
+
 int Stage3::ensure_blocks(long long nb)
 {
     if (nb <= cap_b && bidx) return PAMO_OK;
-    void *ptrs[] = {bidx, bkind, bsub, bd, bb2, bg};
+    void *ptrs[] = {bidx, bkind, bsub, bd, bb2, bg, bact};
     for (void *x : ptrs)
         if (x) cudaFree(x);
-    bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr; bg = nullptr;
+    bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr; bg = nullptr; bact = nullptr;
     cap_b = 0;
     if (cudaMalloc((void **)&bidx, nb * 16) != cudaSuccess || cudaMalloc((void **)&bkind, nb * 4) != cudaSuccess ||
         cudaMalloc((void **)&bsub, nb * 4) != cudaSuccess || cudaMalloc((void **)&bd, nb * 4) != cudaSuccess ||
-        cudaMalloc((void **)&bb2, nb * 4) != cudaSuccess || cudaMalloc((void **)&bg, nb * 64) != cudaSuccess)
+        cudaMalloc((void **)&bb2, nb * 4) != cudaSuccess || cudaMalloc((void **)&bg, nb * 64) != cudaSuccess ||
+        cudaMalloc((void **)&bact, nb * 4) != cudaSuccess)
         return PAMO_ERR_OOM;
     cap_b = nb;
     return PAMO_OK;
@@ -1013,6 +1272,8 @@ int Stage3::register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, in
 {
     int rc = ensure(n_v, n_f, n_e, n_h, n_gt_v, n_gt_f);
     if (rc) return rc;
+    drop_graph();  // sizes and configuration are baked into the captured iteration
+    gathered = false;  // new geometry: contact candidates are gathered again
     np = n_v; nt = n_f; ne = n_e; nh = n_h; ngp = n_gt_v; ngt = n_gt_f;
     radius = cfg.contact_detection_radius;
     launch(k_aos_to_f4, grid_for(np), kThreads, 0, s, d_v, q, q_prev, np);
@@ -1037,19 +1298,56 @@ int Stage3::register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, in
 
 int Stage3::detect(cudaStream_t s)
 {
-    // refit the hierarchies built at registration (system.py:121-152)
-    S3_TRY(lbvh_refit(tri_bvh, q, tris, nt, s));
-    S3_TRY(lbvh_refit(edge_bvh, q, edges4, ne, s));
+    if (!cand_pt) {
+        int rc = ensure_cands(32LL * (np + ne) + 4096);
+        if (rc) return rc;
+    }
     for (int attempt = 0; attempt < 64; ++attempt) {
         const float thr = 2.f * radius + cfg.d_hat;
-        S3_TRY(cudaMemsetAsync(iscal, 0, 3 * sizeof(int), s));
-        launch(k_detect_pt, grid_for(np), kThreads, 0, s, q, np, tris, tri_bvh.nodes, tri_bvh.vals, tri_bvh.scene, thr,
-                                                      iscal, cap_b, bidx, bkind);
-        launch(k_detect_ee, grid_for(ne), kThreads, 0, s, q, ne, edges4, edge_bvh.nodes, edge_bvh.vals, edge_bvh.scene, thr,
-                                                      cfg.ee_classify_thres, iscal, cap_b, bidx, bkind);
-        S3_TRY(cudaMemcpyAsync(h_iscal, iscal, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        const float extra = 0.25f * thr;
+        bool gather = !gathered || thr > gather_thr;
+        if (gather) {
+            // refit the hierarchies built at registration (system.py:121-152) and
+            // collect the pairs within thr + extra
+            S3_TRY(lbvh_refit(tri_bvh, q, tris, nt, s));
+            S3_TRY(lbvh_refit(edge_bvh, q, edges4, ne, s));
+            S3_TRY(cudaMemsetAsync(iscal, 0, 6 * sizeof(int), s));
+            launch(k_detect_pt, grid_for(np), kThreads, 0, s, q, np, tris, tri_bvh.nodes, tri_bvh.vals, tri_bvh.scene,
+                   thr + extra, iscal, cap_c, cand_pt);
+            launch(k_detect_ee, grid_for(ne), kThreads, 0, s, q, ne, edges4, edge_bvh.nodes, edge_bvh.vals,
+                   edge_bvh.scene, thr + extra, iscal, cap_c, cand_ee);
+            S3_TRY(cudaMemcpyAsync(q_gather, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
+        } else {
+            S3_TRY(cudaMemsetAsync(iscal, 0, 3 * sizeof(int), s));
+        }
+        S3_TRY(cudaMemsetAsync(iscal + I_DISP, 0, sizeof(int), s));
+        launch(k_max_disp, grid_for(np), kThreads, 0, s, q, q_gather, np, iscal);
+        launch(k_test_pt, grid_for(cap_c), kThreads, 0, s, q, tris, cand_pt, cap_c, thr, iscal, cap_b, bidx, bkind);
+        launch(k_test_ee, grid_for(cap_c), kThreads, 0, s, q, edges4, cand_ee, cap_c, thr, cfg.ee_classify_thres,
+               iscal, cap_b, bidx, bkind);
+        S3_TRY(cudaMemcpyAsync(h_iscal, iscal, 12 * sizeof(int), cudaMemcpyDeviceToHost, s));
         S3_TRY(cudaStreamSynchronize(s));
+        if (prof) prof->collect();
+        if (h_iscal[I_BAR_ERR]) return PAMO_ERR_DEVICE;  // a solve's grid barrier timed out
         if (h_iscal[I_STACK] > 0) return PAMO_ERR_CAPACITY;
+        const long long nc = h_iscal[I_NCAND_PT] > h_iscal[I_NCAND_EE] ? h_iscal[I_NCAND_PT] : h_iscal[I_NCAND_EE];
+        if (nc > cap_c) {  // candidate buffers too small: grow and gather again
+            int rc = ensure_cands(nc + nc / 4 + 4096);
+            if (rc) return rc;
+            gathered = false;
+            continue;
+        }
+        float disp;
+        memcpy(&disp, &h_iscal[I_DISP], sizeof(float));
+        if (!gather && !(2.f * disp <= gather_thr - thr + extra_at_gather)) {
+            gathered = false;  // moved too far since the gathering: gather again
+            continue;
+        }
+        if (gather) {
+            gathered = true;
+            gather_thr = thr;
+            extra_at_gather = extra;
+        }
         long long n = h_iscal[I_NB];
         if (n > cfg.max_blocks) {  // the reference halves the radius and retries (energy.py:940-948)
             radius *= 0.5f;
@@ -1065,36 +1363,90 @@ int Stage3::detect(cudaStream_t s)
     return PAMO_ERR_CAPACITY;
 }
 
-static int energy_pass(Stage3 &S, cudaStream_t s)
+static int energy_pass(Stage3 &S, cudaStream_t s, int n_halves = -1)
 {
     EArgs e{S.q, S.target, S.wk, S.np, S.nt, S.nh, S.tris, S.area, S.inv_dm,
             S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
             S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
                 ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
             S.hinges, S.rest_angle, S.rest_elen, S.cfg.hinge_stiffness, S.bidx, S.bkind, S.bsub, S.bd, S.iscal, S.cap_b,
-            S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials};
+            S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials, n_halves, S.dscal};
     launch(k_energy, kRedBlocks, kThreads, 0, s, e);
     launch(k_finish_sum, 1, 32, 0, s, S.partials, kRedBlocks, S.dscal + D_ENERGY);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
-static int hess_dx(Stage3 &S, const float4 *dx, float4 *out, cudaStream_t s)
+static int hess_elements(Stage3 &S, const float4 *dx, float4 *out, cudaStream_t s)
 {
-    launch(k_hess_vertex, grid_for(S.np), kThreads, 0, s, S.wk, S.np, dx, out);
     HArgs h{S.q, S.wk, S.np, S.nt, S.nh, S.tris, S.area, S.inv_dm,
             S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
             S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
                 ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
-            S.hinges, S.hblk, S.bidx, S.bg, S.bb2, S.iscal, S.cap_b, dx, out};
+            S.hinges, S.hblk, S.bidx, S.bg, S.bb2, S.iscal, S.cap_b, dx, out, S.bact};
     launch(k_hess_elements, grid_for((long long)S.nt + S.nh + S.cap_b), kThreads, 0, s, h);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
+void Stage3::drop_graph()
+{
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    graph_cap_b = -1;
+    graph_kernels = 0;
+}
+
+// One Newton iteration (system.py:354-409).  Contact detection ends with a host
+// synchronisation (block count, buffer growth); everything after it has fixed
+// sizes and pointers and no host decision, so it is captured once as a CUDA
+// graph and replayed (recaptured when the contact buffer grows).  With the phase
+// timer on, the iteration runs eagerly so its events can be recorded.
 int Stage3::newton(cudaStream_t s)
 {
     S3_TRY(cudaMemcpyAsync(q_prev, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
+    if (prof) prof->begin(PH_S3_DETECT, s);
     int rc = detect(s);
     if (rc) return rc;
+    const bool timed = prof && prof->on;
+    if (timed || !use_graph) return newton_body(s);
+    if (!graph || graph_cap_b != cap_b) {
+        drop_graph();
+        const long long before = g_launches.load();
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();  // e.g. the legacy default stream: run the iteration directly
+            use_graph = false;
+            return newton_body(s);
+        }
+        rc = newton_body(s);
+        cudaError_t ce = cudaStreamEndCapture(s, &g);
+        graph_kernels = g_launches.load() - before;
+        g_launches.fetch_sub(graph_kernels);  // captured, not launched
+        if (rc || ce != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            if (rc) return rc;
+            use_graph = false;  // this stream cannot be captured: run the iteration directly
+            return newton_body(s);
+        }
+        ce = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+            graph = nullptr;
+            cudaGetLastError();
+            use_graph = false;
+            return newton_body(s);
+        }
+        graph_cap_b = cap_b;
+    }
+    S3_TRY(cudaGraphLaunch(graph, s));
+    g_launches.fetch_add(graph_kernels);
+    return PAMO_OK;
+}
+
+int Stage3::newton_body(cudaStream_t s)
+{
+    int rc;
+    if (prof) prof->begin(PH_S3_DIFF, s);
     S3_TRY(cudaMemcpyAsync(q_det, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
     if ((rc = energy_pass(*this, s))) return rc;
     // gradient (coefficient -1) and diagonal
@@ -1103,30 +1455,64 @@ int Stage3::newton(cudaStream_t s)
             cfg.elas_young_modulus * cfg.elas_poisson_ratio /
                 ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
             hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, hblk, bidx, bkind, bsub, bd, bg, bb2,
-            iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag};
+            iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag, bact};
+    S3_TRY(cudaMemsetAsync(iscal + I_NACT, 0, sizeof(int), s));
     launch(k_diff_elements, grid_for((long long)nt + nh + cap_b, 128), 128, 0, s, d);
     // Jacobi-preconditioned CG (cg_solver.py:96-158)
-    launch(k_cg_init, kRedBlocks, kThreads, 0, s, grad, diag, np, p, r, z, v, partials);
-    launch(k_finish_sum, 1, 32, 0, s, partials, kRedBlocks, dscal + D_ZR);
-    for (int it = 0; it < cfg.n_cg_iters; ++it) {
-        if ((rc = hess_dx(*this, v, Av, s))) return rc;
-        launch(k_dot, kRedBlocks, kThreads, 0, s, v, Av, np, partials);
-        launch(k_finish_sum, 1, 32, 0, s, partials, kRedBlocks, dscal + D_VAV);
-        launch(k_shift_zr, 1, 1, 0, s, dscal);
-        launch(k_cg_update, kRedBlocks, kThreads, 0, s, v, Av, diag, dscal, np, p, r, z, partials);
-        launch(k_finish_sum, 1, 32, 0, s, partials, kRedBlocks, dscal + D_ZR);
-        launch(k_cg_v, grid_for(np), kThreads, 0, s, z, dscal, np, v);
+    if (prof) prof->begin(PH_S3_CG, s);
+    if (cg_persistent < 0) {  // first use: can all blocks of the solve be resident at once?
+        int dev = 0, coop = 0, per_sm = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_solve, kThreads, 0);
+        cg_persistent = (coop && (long long)per_sm * sms >= kRedBlocks) ? 1 : 0;
+        cudaGetLastError();
     }
+    if (cg_persistent == 1) {
+        HArgs h{q, wk, np, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
+                cfg.elas_young_modulus * cfg.elas_poisson_ratio /
+                    ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
+                hinges, hblk, bidx, bg, bb2, iscal, cap_b, v, Av, bact};
+        CGArgs ca{h, grad, diag, wk, p, r, z, v, Av, partials, dscal, iscal, np, cfg.n_cg_iters};
+        S3_TRY(cudaMemsetAsync(iscal + I_BAR_COUNT, 0, sizeof(int), s));
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(kRedBlocks);
+        lc.blockDim = dim3(kThreads);
+        lc.dynamicSmemBytes = 0;
+        lc.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        S3_TRY(cudaLaunchKernelEx(&lc, k_cg_solve, ca));
+    } else {
+    int *ticket = iscal + I_TICKET;
+    launch(k_cg_init, kRedBlocks, kThreads, 0, s, grad, diag, np, p, r, z, v, partials, ticket, dscal);
+    for (int it = 0; it < cfg.n_cg_iters; ++it) {
+        launch(k_cg_pre, grid_for(np), kThreads, 0, s, (const float4 *)z, (const double *)dscal, (const float *)wk, np,
+               it == 0 ? 1 : 0, v, Av);
+        if ((rc = hess_elements(*this, v, Av, s))) return rc;
+        launch(k_cg_dot, kRedBlocks, kThreads, 0, s, (const float4 *)v, (const float4 *)Av, np, partials, ticket, dscal);
+        launch(k_cg_update, kRedBlocks, kThreads, 0, s, (const float4 *)v, (const float4 *)Av, (const float4 *)diag, dscal,
+               np, p, r, z, partials, ticket);
+    }
+    }
+    if (prof) prof->begin(PH_S3_CCD, s);
     launch(k_clamp, grid_for(np), kThreads, 0, s, p, q_prev, q_det, np, cfg.contact_detection_radius);
     launch(k_set_float, 1, 1, 0, s, fscal, 1.0f);
     launch(k_accd, grid_for(cap_b, 128), 128, 0, s, q, p, bidx, bkind, iscal, cap_b, cfg.ccd_slackness, cfg.ccd_thickness,
                                                 cfg.ccd_max_iters, cfg.ee_classify_thres, fscal);
     // line search (system.py:393-409)
+    if (prof) prof->begin(PH_S3_LINE, s);
     launch(k_copy_energy_prev, 1, 1, 0, s, dscal);
     for (int nh_ = 0; nh_ < cfg.n_line_search_iters; ++nh_) {
         launch(k_line_search, grid_for(np), kThreads, 0, s, q_prev, p, fscal, nh_, dscal, np, q);
-        if ((rc = energy_pass(*this, s))) return rc;
+        if ((rc = energy_pass(*this, s, nh_))) return rc;
     }
+    if (prof) prof->end(s);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
@@ -1134,6 +1520,7 @@ int Stage3::step(cudaStream_t s)
 {
     if (do_nothing) return PAMO_OK;
     S3_TRY(cudaMemsetAsync(iscal + I_STACK, 0, 4, s));
+    if (prof) prof->begin(PH_S3_CLOSEST, s);
     launch(k_closest, grid_for(np), kThreads, 0, s, q, np, gt_bvh.nodes, gt_bvh.vals, gt_bvh.scene, gt_pts, gt_tris, target,
                                                 iscal);
     for (int it = 0; it < cfg.n_newton_iters; ++it) {
@@ -1148,7 +1535,9 @@ int Stage3::energy_now(double *out, cudaStream_t s)
     int rc = energy_pass(*this, s);
     if (rc) return rc;
     S3_TRY(cudaMemcpyAsync(h_dscal, dscal, 8, cudaMemcpyDeviceToHost, s));
+    S3_TRY(cudaMemcpyAsync(h_iscal, iscal, 12 * sizeof(int), cudaMemcpyDeviceToHost, s));
     S3_TRY(cudaStreamSynchronize(s));
+    if (h_iscal[I_BAR_ERR]) return PAMO_ERR_DEVICE;  // a solve's grid barrier timed out
     *out = h_dscal[0];
     return PAMO_OK;
 }

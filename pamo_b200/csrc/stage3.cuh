@@ -11,6 +11,7 @@
 #include "../../include/pamo_b200.h"
 #include "common.cuh"
 #include "lbvh.cuh"
+#include "stage2.cuh"
 
 namespace pamo {
 namespace s3 {
@@ -40,6 +41,12 @@ struct Stage3 {
     int *bkind = nullptr, *bsub = nullptr;
     float *bd = nullptr, *bb2 = nullptr;
     float4 *bg = nullptr;  // 4 gradient vectors per block
+    int *bact = nullptr;   // blocks with d < d_hat (the CG operator's contact terms)
+    int2 *cand_pt = nullptr, *cand_ee = nullptr;  // detection: pairs whose boxes overlap
+    long long cap_c = 0;
+    float4 *q_gather = nullptr;  // positions when the candidates were gathered
+    bool gathered = false;
+    float gather_thr = 0.f, extra_at_gather = 0.f;
     // hierarchies
     Lbvh tri_bvh, edge_bvh, gt_bvh;
     float4 *gt_pts = nullptr;
@@ -51,9 +58,17 @@ struct Stage3 {
     double *partials = nullptr;
     int *h_iscal = nullptr;   // pinned
     double *h_dscal = nullptr;
+    Profiler *prof = nullptr;  // the context's phase timer (optional)
+    cudaGraphExec_t graph = nullptr;  // one Newton iteration after detection
+    long long graph_cap_b = -1, graph_kernels = 0;
+    bool use_graph = true;
+    int cg_persistent = -1;  // 1: one cooperative launch per solve; 0: one launch per phase; -1: not decided
+    cudaStream_t work = nullptr;  // the solve's own stream (graphs cannot be captured on the legacy stream)
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 
     int ensure(long long np_, long long nt_, long long ne_, long long nh_, long long ngp_, long long ngt_);
     int ensure_blocks(long long nb);
+    int ensure_cands(long long n);
     void release();
 
     // Inputs are device arrays in the normalised frame.
@@ -62,7 +77,9 @@ struct Stage3 {
                       const float *d_vor, cudaStream_t s);
     int step(cudaStream_t s);
     int newton(cudaStream_t s);
+    int newton_body(cudaStream_t s);
     int detect(cudaStream_t s);
+    void drop_graph();
     // diagnostics
     int energy_now(double *out, cudaStream_t s);
 };

@@ -76,16 +76,27 @@ class Stage3Config:
 
 # ------------------------------------------------------------ host preprocessing
 def normalization(V):
-    """processing.py:15-20."""
+    """processing.py:15-20.  The extents are exact whichever way they are
+    reduced; they are taken over a transposed copy, which numpy reduces much
+    faster than the (n, 3) columns."""
+    V = np.asarray(V, np.float64)
     center = np.mean(V, axis=0)
-    extents = np.max(V, axis=0) - np.min(V, axis=0)
+    Vt = np.ascontiguousarray(V.T)
+    extents = Vt.max(axis=1) - Vt.min(axis=1)
     scale = 1.0 / np.max(extents)
     return scale, -center * scale
 
 
 def edges_unique(F):
+    """Sorted unique edges (a < b), in the order np.unique(axis=0) gives, found as
+    unique 64-bit keys a * n + b."""
+    F = np.asarray(F, np.int64)
     e = np.sort(np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]]), axis=1)
-    return np.unique(e, axis=0)
+    if len(e) == 0:
+        return e.reshape(0, 2)
+    n = int(e.max()) + 1
+    k = np.unique(e[:, 0] * n + e[:, 1])
+    return np.stack([k // n, k % n], axis=1)
 
 
 def hinges(F):
@@ -168,14 +179,16 @@ class Stage3System:
     def clear(self):
         self.last_stats = None
 
-    def project(self, gt_V, gt_F, V, F, n_steps):
-        """Normalised-frame arrays in, projected vertices (float32) out."""
+    def project(self, gt_V, gt_F, V, F, n_steps, gt_affine=None):
+        """Normalised-frame arrays in, projected vertices (float32) out.  With
+        gt_affine = (scale, t), gt_V holds the raw ground-truth points and the
+        normalisation gt_V * scale + t is applied on the device (float64, then
+        rounded to float32 as the host path does)."""
         import torch
 
         c = self.config
         dev = torch.device("cuda", self.device)
         V64 = np.asarray(V, np.float64) * c.system_scale
-        gV = np.asarray(gt_V, np.float64) * c.system_scale
         F = np.asarray(F, np.int64)
         E = edges_unique(F)
         H = hinges(F)
@@ -184,14 +197,24 @@ class Stage3System:
         vor = voronoi_areas(V64, F)
         do_nothing = min_internal_angle_deg(V64, F) <= c.min_angle_thres
         t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
-        d_gv, d_gf = t(gV, np.float32), t(gt_F, np.int32)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        if gt_affine is None:
+            d_gv = t(np.asarray(gt_V, np.float64) * c.system_scale, np.float32)
+        else:
+            raw = gt_V if isinstance(gt_V, torch.Tensor) else t(gt_V, np.float32)
+            raw = raw.to(dev, torch.float32).contiguous()
+            d_gv = torch.empty_like(raw)
+            sc, tr = gt_affine
+            check("pamo_affine_points", _lib.lib().pamo_affine_points(
+                raw.data_ptr(), int(raw.shape[0]), float(sc), float(tr[0]), float(tr[1]), float(tr[2]),
+                float(c.system_scale), d_gv.data_ptr(), stream))
+        d_gf = gt_F.to(dev, torch.int32).contiguous() if isinstance(gt_F, torch.Tensor) else t(gt_F, np.int32)
         d_v, d_f = t(V64, np.float32), t(F, np.int32)
         d_e, d_h, d_w = t(E, np.int32), t(H, np.int32), t(vor, np.float32)
         out = torch.empty((len(V64), 3), dtype=torch.float32, device=dev)
         cfg = c.to_c()
-        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
         check("pamo_safe_project", _lib.lib().pamo_safe_project(
-            self.ctx.handle, d_gv.data_ptr(), d_gf.data_ptr(), len(gV), len(d_gf), d_v.data_ptr(), d_f.data_ptr(),
+            self.ctx.handle, d_gv.data_ptr(), d_gf.data_ptr(), len(d_gv), len(d_gf), d_v.data_ptr(), d_f.data_ptr(),
             len(V64), len(F), d_e.data_ptr(), len(E), d_h.data_ptr(), len(H), d_w.data_ptr(), int(n_steps),
             int(do_nothing), ctypes.byref(cfg), stream, out.data_ptr()))
         st = (ctypes.c_double * 3)()
@@ -209,11 +232,29 @@ def process(gt_V, gt_F, stage2_V, stage2_F, n_iters, system: Stage3System | None
         system = Stage3System(config or Stage3Config())
     else:
         system.clear()
-    scale, t = normalization(np.asarray(gt_V, np.float64))
-    gV = np.asarray(gt_V, np.float64) * scale + t
+    import torch
+
+    on_device = isinstance(gt_V, torch.Tensor) or np.asarray(gt_V).dtype == np.float32
+    if on_device:
+        # float32 ground truth: its mean and extents, the normalisation and the
+        # cast to float32 all run on the device (the mean is a fixed-order
+        # double sum, which rounds differently from numpy's by ~1e-16)
+        dev = torch.device("cuda", system.device)
+        d_gt = gt_V if isinstance(gt_V, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(gt_V))
+        d_gt = d_gt.to(dev, torch.float32, non_blocking=True).contiguous()
+        st = (ctypes.c_double * 6)()
+        check("pamo_point_stats", _lib.lib().pamo_point_stats(
+            d_gt.data_ptr(), int(d_gt.shape[0]), st, ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+        center = np.array(st[0:3])
+        scale = 1.0 / max(st[3], st[4], st[5])
+        t = -center * scale
+        gt_in = d_gt
+    else:  # float64 ground truth: normalised on the host, as processing.py does
+        scale, t = normalization(gt_V)
+        gt_in = np.asarray(gt_V, np.float64) * scale + t
     sV = np.asarray(stage2_V, np.float64) * scale + t
-    q = system.project(gV, gt_F, sV, stage2_F, n_iters).astype(np.float64)
-    return (q - t) / scale, np.asarray(stage2_F)
+    q = system.project(gt_in, gt_F, sV, stage2_F, n_iters, gt_affine=(scale, t) if on_device else None)
+    return (q.astype(np.float64) - t) / scale, np.asarray(stage2_F)
 
 
 def __getattr__(name):  # the reference exposes the defaults through .config / .system
