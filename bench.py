@@ -306,17 +306,20 @@ def product_arm(args):
     ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     launches0 = L.pamo_launch_count()
-    ev0.record(s)
-    for _ in range(args.steps):
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(s)
+    for k in range(args.steps):
         run_resident()
-    ev1.record(s)
+        evs[k + 1].record(s)
     torch.cuda.synchronize()
     launches = L.pamo_launch_count() - launches0
-    dev_ms = ev0.elapsed_time(ev1) / args.steps
+    dev_ms = evs[0].elapsed_time(evs[-1]) / args.steps
+    step_ms = [round(evs[k].elapsed_time(evs[k + 1]), 3) for k in range(args.steps)]
     timings = dict(pm.timings)
     rounds = pm.last_rounds
     lat = []
-    d2h = 0
+    d2h = run_e2e()  # one untimed run: the first host -> device copies allocate
+    torch.cuda.synchronize()
     for _ in range(max(args.steps, 3)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -375,6 +378,7 @@ def product_arm(args):
                        "rounds": rounds, "iters": args.iters, "l2": "inputs/working set > L2, no flush",
                        "parallelism": f"replicas x{ws}", "api": "PaMO(mesh, use_stage1=False, use_stage3).run"},
             "gpu_launches": int(launches),
+            "step_ms": step_ms,
             "latency_ms": {"p50": float(np.percentile(lat, 50)) * 1e3, "p99": float(np.percentile(lat, 99)) * 1e3},
             "e2e": {"value": e2e, "unit": "Mfaces/s", "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
                     "d2h_bytes_per_step": int(d2h)},
@@ -453,9 +457,8 @@ def batched_arm(args):
         while True:
             r, p = eng.step()
             now = time.perf_counter() - t0
-            for j in jobs:
-                if j not in finish and eng.job(j)["state"] == 2:
-                    finish[j] = now
+            for j in eng.finished():
+                finish[j] = now
             if r == 0 and p == 0:
                 break
         out_bytes = 0
@@ -584,10 +587,9 @@ def serving_arm(args):
                 time.sleep(max(0.0, min(arrivals[nxt] - now, 0.01)))
                 continue
             eng.step()
-            for j in list(live):
-                if eng.job(j)["state"] == 2:
-                    eng.result(j)
-                    lat.append(time.perf_counter() - t0 - live.pop(j))
+            for j in eng.finished():
+                eng.result(j)
+                lat.append(time.perf_counter() - t0 - live.pop(j))
         span = time.perf_counter() - t0
         # plain: the same arrivals served one at a time (host in, host out)
         t0 = time.perf_counter()
@@ -629,6 +631,9 @@ def serving_arm(args):
 
 
 def main():
+    import gc
+
+    gc.disable()  # no collector pauses inside the timed regions (the bench makes no reference cycles)
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)

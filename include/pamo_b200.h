@@ -262,6 +262,11 @@ int pamo_batch_submit(pamo_batch *b, const float *points, const int *tris, int n
    retires the meshes whose loop ended.  Returns the running / pending counts. */
 int pamo_batch_step(pamo_batch *b, int *out_running, int *out_pending);
 
+/* Jobs that finished (or failed) during the last pamo_batch_step: returns how
+   many, and writes up to cap of their ids to h_out, so a server need not poll
+   every job after every round. */
+int pamo_batch_finished(pamo_batch *b, long long *h_out, int cap);
+
 /* State (PAMO_JOB_*), current (or final) sizes and rounds run of a job. */
 int pamo_batch_job(pamo_batch *b, long long job, int *state, int *n_pts, int *n_tris, int *rounds);
 

@@ -36,6 +36,7 @@ SIGNATURES = {
     "pamo_batch_submit": (_i, [_vp, _vp, _vp, _i, _i, _i, _ll, _i, _f, _i, ctypes.POINTER(_ll)]),
     "pamo_batch_step": (_i, [_vp, _ip, _ip]),
     "pamo_batch_job": (_i, [_vp, _ll, _ip, _ip, _ip, _ip]),
+    "pamo_batch_finished": (_i, [_vp, ctypes.POINTER(_ll), _i]),
     "pamo_batch_fetch": (_i, [_vp, _ll, _vp, _vp, _i]),
     "pamo_batch_release": (_i, [_vp, _ll]),
     "pamo_batch_stats": (_i, [_vp, ctypes.POINTER(_ll)]),

@@ -106,6 +106,18 @@ class BatchEngine:
         check("pamo_batch_step", _lib.lib().pamo_batch_step(self.handle, ctypes.byref(r), ctypes.byref(p)))
         return r.value, p.value
 
+    def finished(self) -> list[int]:
+        """Jobs that finished (or failed) during the last step()."""
+        cap = 256
+        while True:
+            buf = (ctypes.c_longlong * cap)()
+            n = _lib.lib().pamo_batch_finished(self.handle, buf, cap)
+            if n < 0:
+                raise _lib.PamoError("pamo_batch_finished", -n)
+            if n <= cap:
+                return list(buf[:n])
+            cap = n
+
     def job(self, job: int) -> dict:
         st, n, m, rounds = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check("pamo_batch_job", _lib.lib().pamo_batch_job(self.handle, job, ctypes.byref(st), ctypes.byref(n),

@@ -855,6 +855,7 @@ struct pamo_batch {
     pamo::Move *h_moves = nullptr;
     std::vector<int> nvu;
     long long rounds_run = 0;
+    std::vector<long long> done_ids;  // jobs that finished or failed in the last step
 };
 
 namespace pamo {
@@ -1086,6 +1087,7 @@ int pamo_batch_step(pamo_batch *b, int *out_running, int *out_pending)
     if (cudaSetDevice(b->device) != cudaSuccess) return PAMO_ERR_DEVICE;
     cudaStream_t s = b->s;
     Stage2 &S = b->S;
+    b->done_ids.clear();
     // admission: every pending mesh that fits the packed capacity, the mesh
     // count and the memory budget, in submission order
     for (size_t k = 0; k < b->pending.size();) {
@@ -1103,11 +1105,13 @@ int pamo_batch_step(pamo_batch *b, int *out_running, int *out_pending)
         b->pending.erase(b->pending.begin() + k);
         if (rc) {
             batch_fail(b, j, rc);
+            b->done_ids.push_back(j->id);
             continue;
         }
         if (j->iters == 0) {  // no round: the centred, permuted input comes back, as from the plain loop
             rc = batch_finish(b, j);
             if (rc) batch_fail(b, j, rc);
+            b->done_ids.push_back(j->id);
             b->n_packed -= j->n0;  // it was the last one packed
             b->m_packed -= j->m0;
             continue;
@@ -1131,7 +1135,10 @@ int pamo_batch_step(pamo_batch *b, int *out_running, int *out_pending)
         int rc = S.round_batch(b->n_packed, b->m_packed, K, b->nvu.data(), s);
         if (!rc) rc = S.compact_batch(b->n_packed, b->m_packed, K, s);
         if (rc) {  // a device or capacity error fails every mesh of the round
-            for (BatchJob *j : b->running) batch_fail(b, j, rc);
+            for (BatchJob *j : b->running) {
+                batch_fail(b, j, rc);
+                b->done_ids.push_back(j->id);
+            }
             b->running.clear();
             b->n_packed = b->m_packed = 0;
             return rc;
@@ -1165,6 +1172,7 @@ int pamo_batch_step(pamo_batch *b, int *out_running, int *out_pending)
             if (done) {
                 int frc = batch_finish(b, j);
                 if (frc) batch_fail(b, j, frc);
+                b->done_ids.push_back(j->id);
                 moved = true;
                 continue;
             }
@@ -1199,6 +1207,14 @@ int pamo_batch_step(pamo_batch *b, int *out_running, int *out_pending)
     if (out_running) *out_running = (int)b->running.size();
     if (out_pending) *out_pending = (int)b->pending.size();
     return PAMO_OK;
+}
+
+int pamo_batch_finished(pamo_batch *b, long long *h_out, int cap)
+{
+    if (!b || cap < 0 || (cap && !h_out)) return -PAMO_ERR_INVALID_ARG;
+    const int n = (int)b->done_ids.size();
+    for (int i = 0; i < n && i < cap; ++i) h_out[i] = b->done_ids[i];
+    return n;
 }
 
 int pamo_batch_job(pamo_batch *b, long long job, int *state, int *n_pts, int *n_tris, int *rounds)

@@ -603,16 +603,23 @@ __device__ __forceinline__ int shared_indices(int4 a, int4 b)
 
 // The active live faces in leaf (Morton) order, appended a warp at a time, so
 // the query threads that follow all have a face and neighbouring lanes walk
-// neighbouring paths.
+// neighbouring paths.  In a batch, only the faces of meshes whose undo loop
+// still runs (a mesh whose last check found nothing would find nothing again
+// on its unchanged geometry, and pairs never cross meshes).
 __global__ void k_active_list(const int *__restrict__ vals, const int *scene, const uint8_t *__restrict__ active,
-                              const int4 *__restrict__ tris, int *qlist, RoundCounters *cnt)
+                              const int4 *__restrict__ tris, int *qlist, RoundCounters *cnt, const SlotInfo *slots,
+                              const int *vslot)
 {
     const int L = scene[7];
     const int lane = threadIdx.x & 31;
     for (long long base = (long long)blockIdx.x * blockDim.x; base < L; base += (long long)blockDim.x * gridDim.x) {
         const long long p = base + threadIdx.x;
         int f = p < L ? vals[p] : -1;
-        bool ok = f >= 0 && active[f] && tris[f].x != -1;
+        bool ok = f >= 0 && active[f];
+        if (ok) {
+            const int v0 = tris[f].x;
+            ok = v0 != -1 && (!slots || slots[vslot[v0]].in_undo);
+        }
         unsigned ball = __ballot_sync(0xffffffffu, ok);
         int first = 0;
         if (lane == 0 && ball) first = atomicAdd(&cnt->n_query, __popc(ball));
@@ -1270,7 +1277,8 @@ static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s, const int *dirty
     const bool batch = S.n_slots > 0;
     if ((e = cudaMemsetAsync(&S.dcnt->n_query, 0, sizeof(int), s)) != cudaSuccess) return e;
     launch(k_active_list, grid_for(m), kThreads, 0, s, (const int *)S.bvh.vals, (const int *)S.bvh.scene,
-           (const uint8_t *)S.active, (const int4 *)S.tris, S.fflag, S.dcnt);
+           (const uint8_t *)S.active, (const int4 *)S.tris, S.fflag, S.dcnt,
+           batch ? (const SlotInfo *)S.slots : nullptr, batch ? (const int *)S.vslot : nullptr);
     launch(k_query, grid_for(m), kThreads, 0, s, S.bvh.nodes, S.bvh.vals, S.bvh.scene, S.pts, S.tris, S.active, m,
                                              S.pairs, S.cap_pairs, S.dcnt, batch ? (const int *)S.roots : nullptr,
                                              batch ? (const int *)S.vslot : nullptr, (const int *)S.fflag);
@@ -1361,7 +1369,8 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
 
     S2_TRY(cudaMemsetAsync(active, 0, (size_t)m, s));
     launch(k_mark_active, grid_for(EMAX), kThreads, 0, s, collapsed, dcnt, edges, first_near, near_tris, active);
-    S2_TRY(isect_pass(*this, m, s, collapsed, &dcnt->n_total));  // only the collapses' one-rings changed
+    // a full refit: the collapses change too many leaves for the incremental one to pay
+    S2_TRY(isect_pass(*this, m, s));
     S2_TRY(undo_check(*this, s));
     S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
     S2_TRY(cudaStreamSynchronize(s));
@@ -1371,7 +1380,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
         long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
         int rc = ensure_pairs(need);
         if (rc) return rc;
-        S2_TRY(isect_pass(*this, m, s, collapsed, &dcnt->n_total));
+        S2_TRY(isect_pass(*this, m, s));
         S2_TRY(undo_check(*this, s));
         S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
         S2_TRY(cudaStreamSynchronize(s));
@@ -1549,6 +1558,7 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
         nvu[r] = first[r] = h.is_stuck ? h.n_undo_in : 0;
         h.pass_first = h.pass_count = 0;
         h.nvu = 0;
+        h.in_undo = 1;
         max_n = h.n > max_n ? h.n : max_n;
         max_undo_in = h.n_undo_in > max_undo_in ? h.n_undo_in : max_undo_in;
         max_cap_v = h.cap_v > max_cap_v ? h.cap_v : max_cap_v;
@@ -1599,8 +1609,10 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
 
     S2_TRY(cudaMemsetAsync(active, 0, (size_t)m, s));
     launch(k_mark_active, grid_for(EMAX), kThreads, 0, s, cand, dcnt, edges, first_near, near_tris, active);
-    auto pass = [&]() -> int {
-        S2_TRY(isect_pass(*this, m, s));
+    // the first pass refits the round's new hierarchy; the undo passes refit only
+    // the one-rings of the edges they undid
+    auto pass = [&](bool undo) -> int {
+        S2_TRY(isect_pass(*this, m, s, undo ? undo_edges : nullptr, undo ? &dcnt->n_undo : nullptr));
         S2_TRY(undo_check_batch(*this, K, s));
         S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
         S2_TRY(cudaMemcpyAsync(hscnt, scnt, (size_t)K * sizeof(SlotCounters), cudaMemcpyDeviceToHost, s));
@@ -1610,7 +1622,7 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
             long long need = (long long)hcnt->n_pairs + hcnt->n_pairs / 2 + 1024;
             int rc = ensure_pairs(need);
             if (rc) return rc;
-            S2_TRY(isect_pass(*this, m, s));
+            S2_TRY(isect_pass(*this, m, s, undo ? undo_edges : nullptr, undo ? &dcnt->n_undo : nullptr));
             S2_TRY(undo_check_batch(*this, K, s));
             S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
             S2_TRY(cudaMemcpyAsync(hscnt, scnt, (size_t)K * sizeof(SlotCounters), cudaMemcpyDeviceToHost, s));
@@ -1620,7 +1632,7 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
         if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
         return PAMO_OK;
     };
-    int rc = pass();
+    int rc = pass(false);
     if (rc) return rc;
     last_stats[0] = hcnt->n_edges;
     last_stats[1] = hcnt->n_main;
@@ -1644,12 +1656,13 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
         for (int r = 0; r < K; ++r) {
             hslots[r].pass_first = first[r];
             hslots[r].pass_count = nvu[r] - first[r];
+            hslots[r].in_undo = cnt_undo[r] != 0 ? 1 : 0;
             max_cnt = hslots[r].pass_count > max_cnt ? hslots[r].pass_count : max_cnt;
             first[r] += 2 * cnt_undo[r];
         }
         S2_TRY(cudaMemcpyAsync(slots, hslots, (size_t)K * sizeof(SlotInfo), cudaMemcpyHostToDevice, s));
         if (max_cnt > 0) launch(k_b_rearrange, slot_grid(K, max_cnt), kThreads, 0, s, (const SlotInfo *)slots);
-        rc = pass();
+        rc = pass(true);
         if (rc) return rc;
         any = false;
         for (int r = 0; r < K; ++r) {

@@ -50,6 +50,7 @@ struct SlotInfo {        // uploaded by the host before each round, indexed by r
     float tres;          // threshold
     int pass_first, pass_count;  // undo pass: rearrangement window of the undo list
     int nvu;             // undo-list length at the end of the round
+    int in_undo;         // the mesh's undo loop still runs: its faces are queried this pass
     const float *scale;  // device scalar: the mesh's scale (max bbox extent)
     uint32_t *edge_cost; // [3 m0 + 1] edge costs (stale between rounds)
     int *pts_map;        // [n0 + 1] the previous round's vertex map

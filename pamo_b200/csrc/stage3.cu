@@ -761,10 +761,15 @@ struct HArgs {
 // Element terms of H dx added into out (atomics): membrane, hinges, and the
 // contact blocks with d < d_hat (listed by k_diff_elements; the others have no
 // Gauss-Newton term).  `first` / `stride` spread the elements over the threads.
-__device__ __forceinline__ void hess_elements_range(const HArgs &A, long long first, long long stride)
+// Returns this thread's share of dx . (H_elements dx): each element's outputs
+// dotted with its own vertices' dx.
+__device__ __forceinline__ double hess_elements_range(const HArgs &A, long long first, long long stride)
 {
+    double dxh = 0.0;
+    // a hinge's four block rows go to four threads (one output vertex each)
     const long long nb = min((long long)A.iscal[I_NACT], A.cap_b);
-    const long long total = (long long)A.nt + A.nh + nb;
+    const long long nh4 = 4LL * A.nh;
+    const long long total = (long long)A.nt + nh4 + nb;
     for (long long k = first; k < total; k += stride)
     {
         if (k < A.nt) {
@@ -801,23 +806,23 @@ __device__ __forceinline__ void hess_elements_range(const HArgs &A, long long fi
             atomic_add3(A.out, f.x, f0);
             atomic_add3(A.out, f.y, f1);
             atomic_add3(A.out, f.z, f2);
-        } else if (k < (long long)A.nt + A.nh) {
-            int h = (int)(k - A.nt);
+            dxh += (double)dot(f0, ld(A.dx, f.x)) + (double)dot(f1, ld(A.dx, f.y)) + (double)dot(f2, ld(A.dx, f.z));
+        } else if (k < (long long)A.nt + nh4) {
+            const int h = (int)((k - A.nt) >> 2), a = (int)((k - A.nt) & 3);
             int4 i = A.hinges[h];
             int idx[4] = {i.x, i.y, i.z, i.w};
             F3 d[4] = {ld(A.dx, i.x), ld(A.dx, i.y), ld(A.dx, i.z), ld(A.dx, i.w)};
-            const float *B = A.hblk + (size_t)h * 144;
-            for (int a = 0; a < 4; ++a) {
-                F3 s = mk(0.f, 0.f, 0.f);
-                for (int b = 0; b < 4; ++b) {
-                    const float *m = B + (a * 4 + b) * 9;
-                    s = s + mk(m[0] * d[b].x + m[1] * d[b].y + m[2] * d[b].z, m[3] * d[b].x + m[4] * d[b].y + m[5] * d[b].z,
-                               m[6] * d[b].x + m[7] * d[b].y + m[8] * d[b].z);
-                }
-                atomic_add3(A.out, idx[a], s);
+            const float *B = A.hblk + (size_t)h * 144 + a * 36;  // block row a: blocks (a, 0..3)
+            F3 s = mk(0.f, 0.f, 0.f);
+            for (int b = 0; b < 4; ++b) {
+                const float *m = B + b * 9;
+                s = s + mk(m[0] * d[b].x + m[1] * d[b].y + m[2] * d[b].z, m[3] * d[b].x + m[4] * d[b].y + m[5] * d[b].z,
+                           m[6] * d[b].x + m[7] * d[b].y + m[8] * d[b].z);
             }
+            atomic_add3(A.out, idx[a], s);
+            dxh += (double)dot(s, d[a]);
         } else {
-            int b = A.bact[k - A.nt - A.nh];
+            int b = A.bact[k - A.nt - nh4];
             float c = A.bb2[b];
             if (c == 0.f) continue;
             int4 i = A.bidx[b];
@@ -829,8 +834,10 @@ __device__ __forceinline__ void hess_elements_range(const HArgs &A, long long fi
                 s += dot(g[a], ld(A.dx, idx[a]));
             }
             for (int a = 0; a < 4; ++a) atomic_add3(A.out, idx[a], (c * s) * g[a]);
+            dxh += (double)(c * s) * (double)s;
         }
     }
+    return dxh;
 }
 
 __global__ void __launch_bounds__(kThreads) k_hess_elements(HArgs A)
@@ -939,12 +946,15 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const f
 }
 
 // The whole Jacobi-PCG solve of a Newton iteration (the 40 iterations of
-// cg_solver.py:96-158) in one cooperative launch: the phases that the separate
-// kernels above run one launch each are separated by a grid barrier instead.
-// Every block keeps the same grid-stride ranges and adds the per-block partials
-// in the same fixed order as k_finish_sum, so the sums equal the multi-launch
-// solve's.  The barrier spins with a limit; on timeout it records the error and
-// the kernel returns.
+// cg_solver.py:96-158) in one cooperative launch, three grid barriers per
+// iteration: (A) v = z + beta v and the vertex term Av = w v, (B) the element
+// terms added into Av, with v . Av gathered on the way (each element's outputs
+// dotted with its own vertices' v, plus w |v|^2 from A), (D) the update of p, r
+// and z with z . r.  Per-block partials alternate between two buffers (a block
+// may write the next sum's partial while another still reads the last one) and
+// are added in a fixed order, so the sums do not depend on scheduling.  The
+// barrier spins with a limit; on timeout it records the error and the kernel
+// returns.
 struct CGArgs {
     HArgs h;
     const float4 *grad, *diag;
@@ -1006,6 +1016,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_cg_solve(CGArgs A)
 {
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long gs = (long long)blockDim.x * gridDim.x;
+    int buf = 0;  // partials buffer of the next reduction
+    auto reduce = [&](double acc) -> double {
+        double bs = block_sum<kThreads>(acc);
+        double *part = A.partials + (size_t)buf * gridDim.x;
+        buf ^= 1;
+        if (threadIdx.x == 0) part[blockIdx.x] = bs;
+        if (!grid_barrier(A.iscal)) return NAN;
+        return all_blocks_sum(part);
+    };
     // r = g, z = v = g / (diag + 1e-6), p = 0
     double acc = 0.0;
     for (long long i = t0; i < A.np; i += gs) {
@@ -1017,29 +1036,25 @@ __global__ void __launch_bounds__(kThreads, 2) k_cg_solve(CGArgs A)
         st(A.v, (int)i, zz);
         acc += (double)dot(zz, g);
     }
-    double bs = block_sum<kThreads>(acc);
-    if (threadIdx.x == 0) A.partials[blockIdx.x] = bs;
-    if (!grid_barrier(A.iscal)) return;
-    double zr = all_blocks_sum(A.partials), zr_last = zr;
+    double zr = reduce(acc), zr_last = zr;
+    if (A.iscal[I_BAR_ERR]) return;
     for (int it = 0; it < A.n_iters; ++it) {
         const float beta = it == 0 ? 0.f : (float)(zr / zr_last);
+        acc = 0.0;
         for (long long i = t0; i < A.np; i += gs) {
             F3 vv = ld(A.v, (int)i);
             if (it > 0) {
                 vv = ld(A.z, (int)i) + beta * vv;
                 st(A.v, (int)i, vv);
             }
-            st(A.Av, (int)i, A.wk[i] * vv);
+            const F3 wv = A.wk[i] * vv;
+            st(A.Av, (int)i, wv);
+            acc += (double)dot(vv, wv);
         }
         if (!grid_barrier(A.iscal)) return;
-        hess_elements_range(A.h, t0, gs);
-        if (!grid_barrier(A.iscal)) return;
-        acc = 0.0;
-        for (long long i = t0; i < A.np; i += gs) acc += (double)dot(ld(A.v, (int)i), ld(A.Av, (int)i));
-        bs = block_sum<kThreads>(acc);
-        if (threadIdx.x == 0) A.partials[blockIdx.x] = bs;
-        if (!grid_barrier(A.iscal)) return;
-        const double vav = all_blocks_sum(A.partials);
+        acc += hess_elements_range(A.h, t0, gs);
+        const double vav = reduce(acc);
+        if (A.iscal[I_BAR_ERR]) return;
         zr_last = zr;
         const bool upd = vav > 1e-16;
         const float alpha = upd ? (float)(zr_last / vav) : 0.f;
@@ -1056,10 +1071,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_cg_solve(CGArgs A)
             st(A.z, (int)i, zz);
             acc += (double)dot(zz, rr);
         }
-        bs = block_sum<kThreads>(acc);
-        if (threadIdx.x == 0) A.partials[blockIdx.x] = bs;
-        if (!grid_barrier(A.iscal)) return;
-        zr = all_blocks_sum(A.partials);
+        zr = reduce(acc);
+        if (A.iscal[I_BAR_ERR]) return;
     }
 }
 
@@ -1221,7 +1234,7 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
     A3(hinges, ch * 16); A3(rest_angle, ch * 4); A3(rest_elen, ch * 4); A3(hblk, ch * 144 * 4);
     A3(gt_pts, cgp * 16); A3(gt_tris, cgt * 16);
     A3(dscal, 64); A3(fscal, 64); A3(iscal, 64);
-    A3(partials, kRedBlocks * 8);
+    A3(partials, 2 * kRedBlocks * 8);  // two buffers for the persistent solve
 #undef A3
     if (cudaMallocHost((void **)&h_iscal, 64) != cudaSuccess || cudaMallocHost((void **)&h_dscal, 64) != cudaSuccess) {
         release();
@@ -1383,7 +1396,7 @@ static int hess_elements(Stage3 &S, const float4 *dx, float4 *out, cudaStream_t 
             S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
                 ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
             S.hinges, S.hblk, S.bidx, S.bg, S.bb2, S.iscal, S.cap_b, dx, out, S.bact};
-    launch(k_hess_elements, grid_for((long long)S.nt + S.nh + S.cap_b), kThreads, 0, s, h);
+    launch(k_hess_elements, grid_for((long long)S.nt + 4LL * S.nh + S.cap_b), kThreads, 0, s, h);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
