@@ -259,6 +259,18 @@ def roofline_edge_cost(phases, round_faces, peaks):
 EDGE_COST_DRAM_BYTES_PER_FACE = 465.2
 
 
+def count_intersections(ctx, V, F, dev):
+    """Faces of a result that the reference's pair predicate flags as
+    intersecting (pamo_self_intersect over the whole mesh)."""
+    import torch
+
+    import pamo_b200
+
+    flags, _ = pamo_b200.self_intersect(ctx, torch.from_numpy(np.ascontiguousarray(V, np.float32)).to(dev),
+                                        torch.from_numpy(np.ascontiguousarray(F, np.int32)).to(dev))
+    return int(flags.sum().item())
+
+
 def product_arm(args):
     import torch
 
@@ -342,8 +354,9 @@ def product_arm(args):
     handles = [pm.ctx.handle] + ([pm.system.ctx.handle] if args.stages == "23" else [])
     for h in handles:
         L.pamo_profile_enable(h, 1)
-    run_resident()
+    v_out, f_out = run_resident()
     torch.cuda.synchronize()
+    intersections = count_intersections(pamo_b200.Context(local), v_out, f_out, dev)
     phases = {}
     for h in handles:
         ph_ms = (ctypes.c_double * 16)()
@@ -387,6 +400,7 @@ def product_arm(args):
                               "what": "pamo_stage2_run alone, device-resident in and out"},
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "intersections": intersections,
             "phases_ms": {k: round(v["ms"], 3) for k, v in phases.items()},
             "roofline": roofline_edge_cost(phases, round_faces, peaks),
             "round_faces": round_faces if args.dump_rounds else None,
@@ -473,6 +487,7 @@ def batched_arm(args):
                 F = torch.empty((info["n_tris"], 3), dtype=torch.int32, device=dev)
                 _lib.check("pamo_batch_fetch", L.pamo_batch_fetch(eng.handle, j, V.data_ptr(), F.data_ptr(), 0))
                 eng.release(j)
+                info["out"] = (V, F)
             results.append(info)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
@@ -504,6 +519,13 @@ def batched_arm(args):
     n_ph = L.pamo_batch_profile(eng.handle, 0, p_ms, p_calls, 16)
     batch_phases = {_lib.PHASES[i]: round(p_ms[i], 3) for i in range(min(n_ph, len(_lib.PHASES))) if p_calls[i]}
     rounds_run = eng.stats()["rounds_run"]
+    import pamo_b200 as _pb
+
+    chk = _pb.Context(local)
+    intersections = 0
+    for info in res:
+        fl, _ = _pb.self_intersect(chk, *info.pop("out"))
+        intersections += int(fl.sum().item())
     # the plain per-mesh drop-in on the same meshes (same device, fresh context)
     import pamo_b200
 
@@ -531,6 +553,7 @@ def batched_arm(args):
             "e2e": {"value": total_faces / 1e6 / e2e_dt, "unit": "Mfaces/s", "h2d_bytes_per_step": int(bi),
                     "d2h_bytes_per_step": int(bo)},
             "gpu_launches": int(launches), "clocks": clocks, "phases_ms": batch_phases,
+            "intersections": intersections,
             "rounds_per_step": rounds_run // (args.warmup + args.steps + 2),
         }
         print(json.dumps(line))
@@ -636,7 +659,7 @@ def main():
     gc.disable()  # no collector pauses inside the timed regions (the bench makes no reference cycles)
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4", "c5"],

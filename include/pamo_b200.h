@@ -185,6 +185,14 @@ int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int
    normalisation takes these for the ground truth (processing.py:15-20). */
 int pamo_point_stats(const float *d_pts, int n, double *h_out6, void *stream);
 
+/* Stage-3 registration inputs on the device (system.py:217-225 computes them on
+   the host with libigl): the mixed Voronoi area of each vertex of the mesh
+   (double vertices [nv,3], faces [nf,3]; summed in double, stored as float32
+   in d_out[nv]) and the mesh's smallest corner angle in degrees (host; NaN if a
+   face is degenerate, 180 for no faces). */
+int pamo_voronoi_areas(const double *d_v, const int *d_f, int nv, int nf, float *d_out, double *h_min_angle_deg,
+                       void *stream);
+
 /* Stage-3 input normalisation on the device (processing.py:57-59 applies it
    to the ground truth on the host): out[i] = float((in[i] * scale + t) * post)
    per coordinate of n points [n,3], each step in double with one rounding, so

@@ -230,6 +230,88 @@ __global__ void k_point_stats_finish(const double *part, int nblocks, int n, dou
     out[3 + k] = h - l;      // extent
 }
 
+__global__ void k_f64_to_f32(const double *in, int n, float *out)
+{
+    PAMO_GRID_STRIDE(i, n) out[i] = (float)in[i];
+}
+
+// Mixed Voronoi vertex areas (Meyer, Desbrun, Schroeder, Barr 2003) in double
+// from double vertices [n,3], summed per vertex, and each face's largest
+// corner cosine (the smallest angle), for stage 3's registration.
+__global__ void k_voronoi(const double *v, const int *f, int nf, double *area, double *cmax_part)
+{
+    double cm = -2.0;
+    bool nan_seen = false;
+    PAMO_GRID_STRIDE(t, nf)
+    {
+        const int i0 = f[3 * t], i1 = f[3 * t + 1], i2 = f[3 * t + 2];
+        double a[3], b[3], c[3];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = v[3 * i0 + k];
+            b[k] = v[3 * i1 + k];
+            c[k] = v[3 * i2 + k];
+        }
+        double ea[3], eb[3], ec[3];
+        for (int k = 0; k < 3; ++k) {
+            ea[k] = c[k] - b[k];
+            eb[k] = a[k] - c[k];
+            ec[k] = b[k] - a[k];
+        }
+        auto dotd = [](const double *x, const double *y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+        const double la2 = dotd(ea, ea), lb2 = dotd(eb, eb), lc2 = dotd(ec, ec);
+        // cross(ec, -eb)
+        const double cx = -(ec[1] * eb[2] - ec[2] * eb[1]), cy = -(ec[2] * eb[0] - ec[0] * eb[2]),
+                     cz = -(ec[0] * eb[1] - ec[1] * eb[0]);
+        const double ar = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
+        const double cos_a = -dotd(eb, ec) / sqrt(lb2 * lc2);
+        const double cos_b = -dotd(ec, ea) / sqrt(lc2 * la2);
+        const double cos_c = -dotd(ea, eb) / sqrt(la2 * lb2);
+        auto cot = [](double cs) { return cs / sqrt(fmax(1.0 - cs * cs, 0.0)); };
+        const double ca = cot(cos_a), cb = cot(cos_b), cc = cot(cos_c);
+        double w0, w1, w2;
+        if (cos_a < 0 || cos_b < 0 || cos_c < 0) {
+            w0 = cos_a < 0 ? ar / 2 : ar / 4;
+            w1 = cos_b < 0 ? ar / 2 : ar / 4;
+            w2 = cos_c < 0 ? ar / 2 : ar / 4;
+        } else {
+            w0 = (lb2 * cb + lc2 * cc) / 8;
+            w1 = (lc2 * cc + la2 * ca) / 8;
+            w2 = (la2 * ca + lb2 * cb) / 8;
+        }
+        atomicAdd(&area[i0], w0);
+        atomicAdd(&area[i1], w1);
+        atomicAdd(&area[i2], w2);
+        // corner cosines for the smallest-angle test (at a, b, c; as vectors from the corner)
+        const double ka = dotd(ec, eb) * -1.0 / sqrt(lc2 * lb2), kb = -dotd(ea, ec) / sqrt(la2 * lc2),
+                     kc = -dotd(eb, ea) / sqrt(lb2 * la2);
+        for (double k : {ka, kb, kc}) {
+            if (k != k) nan_seen = true;
+            else cm = fmax(cm, k);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        cm = fmax(cm, __shfl_down_sync(0xffffffffu, cm, o));
+        nan_seen = __shfl_down_sync(0xffffffffu, (int)nan_seen, o) || nan_seen;
+    }
+    __shared__ double s_cm[32];
+    __shared__ int s_nan[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_cm[w] = cm;
+        s_nan[w] = nan_seen;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = -2.0;
+        int nn = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            r = fmax(r, s_cm[k]);
+            nn |= s_nan[k];
+        }
+        cmax_part[blockIdx.x] = nn ? NAN : r;
+    }
+}
+
 // out = float((in * scale + t) * post), each step one double rounding
 __global__ void k_affine_points(const float *in, int n, double scale, double tx, double ty, double tz, double post,
                                 float *out)
@@ -626,6 +708,37 @@ int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int
     ctx->s3_stats[0] = e;
     ctx->s3_stats[1] = S.h_iscal[0];
     ctx->s3_stats[2] = newton;
+    return PAMO_OK;
+}
+
+int pamo_voronoi_areas(const double *d_v, const int *d_f, int nv, int nf, float *d_out, double *h_min_angle_deg,
+                       void *stream)
+{
+    if (nv <= 0 || nf < 0 || !d_v || (nf && !d_f) || !d_out || !h_min_angle_deg) return PAMO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = 296;
+    double *scratch = nullptr;
+    CU_RET(cudaMallocAsync((void **)&scratch, ((size_t)nv + nb + 1) * sizeof(double), s));
+    cudaError_t e = cudaMemsetAsync(scratch, 0, (size_t)nv * sizeof(double), s);
+    if (e == cudaSuccess) {
+        if (nf) launch(k_voronoi, nb, 256, 0, s, d_v, d_f, nf, scratch, scratch + nv);
+        launch(k_f64_to_f32, grid_for(nv), kThreads, 0, s, (const double *)scratch, nv, d_out);
+        std::vector<double> host(nb, -2.0);
+        if (nf) e = cudaMemcpyAsync(host.data(), scratch + nv, nb * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        double cm = -2.0;
+        bool nan_seen = false;
+        for (double x : host) {
+            if (x != x) nan_seen = true;
+            else cm = std::max(cm, x);
+        }
+        if (!nf) *h_min_angle_deg = 180.0;
+        else if (nan_seen) *h_min_angle_deg = NAN;
+        else *h_min_angle_deg = std::acos(std::min(std::max(cm, -1.0), 1.0)) * 180.0 / M_PI;
+    }
+    cudaFreeAsync(scratch, s);
+    CU_RET(e);
+    CU_RET(cudaGetLastError());
     return PAMO_OK;
 }
 

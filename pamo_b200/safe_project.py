@@ -91,11 +91,12 @@ def edges_unique(F):
     """Sorted unique edges (a < b), in the order np.unique(axis=0) gives, found as
     unique 64-bit keys a * n + b."""
     F = np.asarray(F, np.int64)
-    e = np.sort(np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]]), axis=1)
-    if len(e) == 0:
-        return e.reshape(0, 2)
-    n = int(e.max()) + 1
-    k = np.unique(e[:, 0] * n + e[:, 1])
+    if len(F) == 0:
+        return np.zeros((0, 2), np.int64)
+    x = np.concatenate([F[:, 0], F[:, 1], F[:, 2]])
+    y = np.concatenate([F[:, 1], F[:, 2], F[:, 0]])
+    n = int(F.max()) + 1
+    k = np.unique(np.minimum(x, y) * n + np.maximum(x, y))
     return np.stack([k // n, k % n], axis=1)
 
 
@@ -134,20 +135,24 @@ def voronoi_areas(V, F):
                     np.where(cos_c < 0, area / 2, area / 4)], 1)
     obtuse = (cos_a < 0) | (cos_b < 0) | (cos_c < 0)
     w = np.where(obtuse[:, None], mix, vor)
-    out = np.zeros(len(V))
-    for k in range(3):
-        np.add.at(out, F[:, k], w[:, k])
-    return out
+    # per-vertex sums in face order (what np.add.at over the three corners does)
+    idx = np.asarray(F, np.int64).T.reshape(-1)
+    return np.bincount(idx, weights=w.T.reshape(-1), minlength=len(V))[:len(V)]
 
 
 def min_internal_angle_deg(V, F):
+    # the smallest angle has the largest cosine (arccos and the clip are monotone)
+    if not len(F):
+        return 180.0
     a, b, c = V[F[:, 0]], V[F[:, 1]], V[F[:, 2]]
-    ang = []
+    cmax = None
     for p, q, r in ((a, b, c), (b, c, a), (c, a, b)):
         u, v = q - p, r - p
-        cs = (u * v).sum(1) / (np.linalg.norm(u, axis=1) * np.linalg.norm(v, axis=1))
-        ang.append(np.arccos(np.clip(cs, -1, 1)))
-    return float(np.min(ang) * 180 / np.pi) if len(F) else 180.0
+        cs = (u * v).sum(1) / np.sqrt((u * u).sum(1) * (v * v).sum(1))
+        cmax = cs if cmax is None else np.fmax(cmax, cs)
+    if np.isnan(cmax).any():
+        return float("nan")
+    return float(np.arccos(np.clip(cmax.max(), -1, 1)) * 180 / np.pi)
 
 
 def merge_vertices(V, F, digits=8):
@@ -194,10 +199,16 @@ class Stage3System:
         H = hinges(F)
         if len(H) != len(E):
             raise ValueError(f"number of hinges {len(H)} != number of edges {len(E)} (mesh not closed 2-manifold)")
-        vor = voronoi_areas(V64, F)
-        do_nothing = min_internal_angle_deg(V64, F) <= c.min_angle_thres
         t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
         stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        # Voronoi areas and the smallest angle, on the device in double from the
+        # double vertices (voronoi_areas / min_internal_angle_deg are the host forms)
+        d_v64, d_f = t(V64, np.float64), t(F, np.int32)
+        d_w = torch.empty(len(V64), dtype=torch.float32, device=dev)
+        min_ang = ctypes.c_double()
+        check("pamo_voronoi_areas", _lib.lib().pamo_voronoi_areas(
+            d_v64.data_ptr(), d_f.data_ptr(), len(V64), len(F), d_w.data_ptr(), ctypes.byref(min_ang), stream))
+        do_nothing = min_ang.value <= c.min_angle_thres
         if gt_affine is None:
             d_gv = t(np.asarray(gt_V, np.float64) * c.system_scale, np.float32)
         else:
@@ -209,8 +220,8 @@ class Stage3System:
                 raw.data_ptr(), int(raw.shape[0]), float(sc), float(tr[0]), float(tr[1]), float(tr[2]),
                 float(c.system_scale), d_gv.data_ptr(), stream))
         d_gf = gt_F.to(dev, torch.int32).contiguous() if isinstance(gt_F, torch.Tensor) else t(gt_F, np.int32)
-        d_v, d_f = t(V64, np.float32), t(F, np.int32)
-        d_e, d_h, d_w = t(E, np.int32), t(H, np.int32), t(vor, np.float32)
+        d_v = d_v64.to(torch.float32)
+        d_e, d_h = t(E, np.int32), t(H, np.int32)
         out = torch.empty((len(V64), 3), dtype=torch.float32, device=dev)
         cfg = c.to_c()
         check("pamo_safe_project", _lib.lib().pamo_safe_project(
