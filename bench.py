@@ -320,9 +320,11 @@ def product_arm(args):
     launches0 = L.pamo_launch_count()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     evs[0].record(s)
+    stage_ms = []
     for k in range(args.steps):
         run_resident()
         evs[k + 1].record(s)
+        stage_ms.append([round(1e3 * pm.timings.get(key, 0.0), 1) for key in ("stage2", "stage3")])
     torch.cuda.synchronize()
     launches = L.pamo_launch_count() - launches0
     dev_ms = evs[0].elapsed_time(evs[-1]) / args.steps
@@ -392,6 +394,7 @@ def product_arm(args):
                        "parallelism": f"replicas x{ws}", "api": "PaMO(mesh, use_stage1=False, use_stage3).run"},
             "gpu_launches": int(launches),
             "step_ms": step_ms,
+            "step_stage_ms": stage_ms,
             "latency_ms": {"p50": float(np.percentile(lat, 50)) * 1e3, "p99": float(np.percentile(lat, 99)) * 1e3},
             "e2e": {"value": e2e, "unit": "Mfaces/s", "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
                     "d2h_bytes_per_step": int(d2h)},

@@ -718,6 +718,7 @@ int pamo_voronoi_areas(const double *d_v, const int *d_f, int nv, int nf, float 
     cudaStream_t s = (cudaStream_t)stream;
     const int nb = 296;
     double *scratch = nullptr;
+    CU_RET(retain_pool_memory());
     CU_RET(cudaMallocAsync((void **)&scratch, ((size_t)nv + nb + 1) * sizeof(double), s));
     cudaError_t e = cudaMemsetAsync(scratch, 0, (size_t)nv * sizeof(double), s);
     if (e == cudaSuccess) {
@@ -747,6 +748,7 @@ int pamo_point_stats(const float *d_pts, int n, double *h_out6, void *stream)
     if (n <= 0 || !d_pts || !h_out6) return PAMO_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     double *scratch = nullptr;
+    CU_RET(retain_pool_memory());
     CU_RET(cudaMallocAsync((void **)&scratch, (9 * kStatBlocks + 8) * sizeof(double), s));
     launch(k_point_stats, kStatBlocks, 256, 0, s, d_pts, n, scratch);
     launch(k_point_stats_finish, 1, 32, 0, s, (const double *)scratch, kStatBlocks, n, scratch + 9 * kStatBlocks);
@@ -1088,6 +1090,7 @@ int pamo_batch_create(int device, long long max_verts, long long max_faces, int 
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return PAMO_ERR_NO_DEVICE;
     if (device < 0 || device >= count) return PAMO_ERR_INVALID_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return PAMO_ERR_DEVICE;
+    if (retain_pool_memory() != cudaSuccess) return PAMO_ERR_DEVICE;
     pamo_batch *b = new (std::nothrow) pamo_batch();
     if (!b) return PAMO_ERR_OOM;
     b->device = device;

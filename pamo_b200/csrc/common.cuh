@@ -26,6 +26,30 @@ inline int grid_for(long long n, int threads = kThreads)
 // (pamo_launch_count) and then issues the launch on the given stream.
 inline std::atomic<long long> g_launches{0};
 
+// Per-call scratch comes from the device's default stream-ordered pool.  By
+// default the pool hands its memory back at every synchronisation, so each
+// call would map fresh memory; this keeps up to kPoolKeepBytes in the pool
+// (raising the threshold only, never lowering one set by the application).
+constexpr unsigned long long kPoolKeepBytes = 1ULL << 30;
+inline cudaError_t retain_pool_memory()
+{
+    static std::atomic<unsigned long long> done{0};  // one bit per device ordinal below 64
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && ((done.load() >> dev) & 1ULL)) return cudaSuccess;
+    cudaMemPool_t pool;
+    if ((e = cudaDeviceGetDefaultMemPool(&pool, dev)) != cudaSuccess) return e;
+    unsigned long long cur = 0;  // the attribute is a 64-bit unsigned value
+    if ((e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur)) != cudaSuccess) return e;
+    if (cur < kPoolKeepBytes) {
+        unsigned long long keep = kPoolKeepBytes;
+        if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    }
+    if (dev < 64) done.fetch_or(1ULL << dev);
+    return cudaSuccess;
+}
+
 template <typename... KArgs, typename... Args>
 inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args)
 {

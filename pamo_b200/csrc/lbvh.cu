@@ -206,8 +206,9 @@ __global__ void __launch_bounds__(kThreads) k_karras(const uint32_t *keys, const
         nodes[i].rlo.w = __int_as_float(right);
         int lid = left < 0 ? (L - 1) + gamma : gamma;
         int rid = right < 0 ? (L - 1) + gamma + 1 : gamma + 1;
-        parent[lid] = (i << 1) | 0;
-        parent[rid] = (i << 1) | 1;
+        const int tile = (lo >> kRefitTileShift) == (hi >> kRefitTileShift) ? 2 : 0;
+        parent[lid] = (i << 2) | tile | 0;
+        parent[rid] = (i << 2) | tile | 1;
         if (i == 0) parent[0] = -1;
         if (roots) {
             const uint32_t rlo = keys[lo] >> rank_shift, rhi = keys[hi] >> rank_shift;
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(kThreads) k_leaf_map(const int *vals, const in
 
 __device__ __forceinline__ void store_child_box(BvhNode *nodes, int code, int self, float3 lo, float3 hi)
 {
-    int par = code >> 1;
+    int par = code >> 2;
     if (code & 1) {
         nodes[par].rlo = make_float4(lo.x, lo.y, lo.z, __int_as_float(self));
         nodes[par].rhi = make_float4(hi.x, hi.y, hi.z, 0.0f);
@@ -237,47 +238,60 @@ __device__ __forceinline__ void store_child_box(BvhNode *nodes, int code, int se
     }
 }
 
-// Bottom-up refit: the second child to arrive at a node merges the two boxes.
-// No thread waits on another (the first arrival exits), so nothing spins.
-__global__ void __launch_bounds__(kThreads) k_refit(const float4 *pts, const int4 *tris, const int *vals,
-                                                    int *scene, const int *parent, BvhNode *nodes, int *flags)
+// Bottom-up refit, one thread per leaf: the second child to arrive at a node
+// merges the two boxes; the first arrival exits, so nothing waits.  A block
+// holds kRefitTile consecutive leaves; a node whose leaves all lie in the
+// block's run (the parent code's tile bit) only ever sees arrivals from this
+// block, so it counts them in shared memory with block-scope fences, and only
+// the few nodes above the runs use global counters and device-scope fences.
+// The node indices of one run's nodes lie in that run (a Karras node's index
+// is one end of its leaf range), so `node % kRefitTile` is a free slot.
+__global__ void __launch_bounds__(kRefitTile) k_refit(const float4 *pts, const int4 *tris, const int *vals,
+                                                      int *scene, const int *parent, BvhNode *nodes, int *flags)
 {
+    __shared__ int arrived[kRefitTile];
+    arrived[threadIdx.x] = 0;
+    __syncthreads();
     const int L = scene[7];
-    if (L < 2) return;
-    PAMO_GRID_STRIDE(p, L)
-    {
-        int f = vals[p];
-        int4 t = f >= 0 ? tris[f] : make_int4(-1, -1, -1, 0);
-        float3 lo, hi;
-        if (face_dead(t)) {
-            lo = make_float3(INFINITY, INFINITY, INFINITY);
-            hi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+    const long long p = (long long)blockIdx.x * kRefitTile + threadIdx.x;
+    if (L < 2 || p >= L) return;
+    int f = vals[p];
+    int4 t = f >= 0 ? tris[f] : make_int4(-1, -1, -1, 0);
+    float3 lo, hi;
+    if (face_dead(t)) {
+        lo = make_float3(INFINITY, INFINITY, INFINITY);
+        hi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+    } else {
+        face_box(pts, t, lo, hi);
+    }
+    int code = parent[(L - 1) + p];
+    store_child_box(nodes, code, ~(int)p, lo, hi);
+    // a valid hierarchy is at most 64 levels deep (unique 64-bit keys); the
+    // bound only guards against a corrupted parent chain
+    for (int depth = 0;; ++depth) {
+        if (depth > 256) {
+            atomicExch(&scene[8], 1);
+            break;
+        }
+        const int node = code >> 2;
+        float4 a, b, c, d;
+        if (code & 2) {
+            __threadfence_block();
+            if (atomicAdd(&arrived[node & (kRefitTile - 1)], 1) == 0) break;
+            __threadfence_block();
+            a = nodes[node].llo, b = nodes[node].lhi, c = nodes[node].rlo, d = nodes[node].rhi;
         } else {
-            face_box(pts, t, lo, hi);
-        }
-        int code = parent[(L - 1) + p];
-        store_child_box(nodes, code, ~(int)p, lo, hi);
-        int node = code >> 1;
-        // a valid hierarchy is at most 64 levels deep (unique 64-bit keys); the
-        // bound only guards against a corrupted parent chain
-        for (int depth = 0;; ++depth) {
-            if (depth > 256) {
-                atomicExch(&scene[8], 1);
-                break;
-            }
             __threadfence();
-            int old = atomicAdd(&flags[node], 1);
-            if (old == 0) break;
+            if (atomicAdd(&flags[node], 1) == 0) break;
             __threadfence();
-            float4 a = __ldcg(&nodes[node].llo), b = __ldcg(&nodes[node].lhi);
-            float4 c = __ldcg(&nodes[node].rlo), d = __ldcg(&nodes[node].rhi);
-            lo = make_float3(fminf(a.x, c.x), fminf(a.y, c.y), fminf(a.z, c.z));
-            hi = make_float3(fmaxf(b.x, d.x), fmaxf(b.y, d.y), fmaxf(b.z, d.z));
-            int pc = parent[node];
-            if (pc < 0) break;  // root
-            store_child_box(nodes, pc, node, lo, hi);
-            node = pc >> 1;
+            a = __ldcg(&nodes[node].llo), b = __ldcg(&nodes[node].lhi);
+            c = __ldcg(&nodes[node].rlo), d = __ldcg(&nodes[node].rhi);
         }
+        lo = make_float3(fminf(a.x, c.x), fminf(a.y, c.y), fminf(a.z, c.z));
+        hi = make_float3(fmaxf(b.x, d.x), fmaxf(b.y, d.y), fmaxf(b.z, d.z));
+        code = parent[node];
+        if (code < 0) break;  // root
+        store_child_box(nodes, code, node, lo, hi);
     }
 }
 
@@ -302,7 +316,7 @@ __global__ void __launch_bounds__(kThreads) k_refit_dirty(const float4 *pts, con
         }
         int code = parent[(L - 1) + p];
         store_child_box(nodes, code, ~p, lo, hi);
-        int node = code >> 1;
+        int node = code >> 2;
         for (int depth = 0;; ++depth) {
             if (depth > 256) {
                 atomicExch(&scene[8], 1);
@@ -324,7 +338,7 @@ __global__ void __launch_bounds__(kThreads) k_refit_dirty(const float4 *pts, con
             const int pc = parent[node];
             if (pc < 0) break;  // root
             store_child_box(nodes, pc, node, lo, hi);
-            node = pc >> 1;
+            node = pc >> 2;
         }
     }
 }
@@ -438,7 +452,8 @@ cudaError_t lbvh_refit(Lbvh &b, const float4 *pts, const int4 *tris, int m, cuda
     if (L < 2) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(b.flags, 0, (size_t)L * 4, s);
     if (e != cudaSuccess) return e;
-    launch(k_refit, grid_for(m), kThreads, 0, s, pts, tris, b.vals, b.scene, b.parent, b.nodes, b.flags);
+    launch(k_refit, (int)((L + kRefitTile - 1) / kRefitTile), kRefitTile, 0, s, pts, tris, b.vals, b.scene, b.parent,
+           b.nodes, b.flags);
     return cudaGetLastError();
 }
 

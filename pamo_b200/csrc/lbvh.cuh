@@ -20,6 +20,10 @@
 
 namespace pamo {
 
+constexpr int kRefitTile = 256;  // leaves per refit block
+constexpr int kRefitTileShift = 8;
+static_assert(kRefitTile == 1 << kRefitTileShift, "refit tile");
+
 struct __align__(16) BvhNode {
     float4 llo;  // .w = left child (int bits): >= 0 internal node, < 0 leaf ~position
     float4 lhi;
@@ -36,7 +40,10 @@ struct Lbvh {
     int *hist = nullptr;        // radix digit counts [256 * tiles]
     int *hist_scratch = nullptr;
     BvhNode *nodes = nullptr;   // [cap]
-    int *parent = nullptr;      // [2*cap]: internal nodes then leaves; (p<<1)|is_right, -1 for root
+    // [2*cap]: internal nodes then leaves; (p << 2) | tile << 1 | is_right, -1 for
+    // the root, where `tile` says that the parent's leaves all lie in one aligned
+    // run of kRefitTile leaves (merged in shared memory by k_refit)
+    int *parent = nullptr;
     int *flags = nullptr;       // [cap] refit arrival counters
     int *leaf_of_face = nullptr;  // [cap]: sorted position of each face, -1 if not a leaf
     int *scene = nullptr;       // 6 ordered ints + n_dead + n_leaves
@@ -83,7 +90,7 @@ __device__ __forceinline__ void lbvh_mark_dirty_leaf(int p, int L, const int *pa
     // mark the path to the root; a node already marked has its path marked (or
     // being marked) by the leaf that got there first
     for (int depth = 0; depth < 256 && code >= 0; ++depth) {
-        const int node = code >> 1;
+        const int node = code >> 2;
         if (atomicOr(&dmask[node], 1 << (code & 1)) != 0) break;
         code = parent[node];
     }

@@ -36,11 +36,10 @@ enum { I_NB = 0, I_OVERFLOW, I_STACK, I_NACT, I_NCAND_PT, I_NCAND_EE, I_TICKET, 
 
 __device__ __forceinline__ F3 ld(const float4 *a, int i) { return f3(a[i]); }
 __device__ __forceinline__ void st(float4 *a, int i, F3 v) { a[i] = make_float4(v.x, v.y, v.z, 0.f); }
+// one vector reduction (sm_90+, global memory) instead of three scalar ones
 __device__ __forceinline__ void atomic_add3(float4 *a, int i, F3 v)
 {
-    atomicAdd(&a[i].x, v.x);
-    atomicAdd(&a[i].y, v.y);
-    atomicAdd(&a[i].z, v.z);
+    atomicAdd(&a[i], make_float4(v.x, v.y, v.z, 0.f));
 }
 
 // ---------------------------------------------------------------- barrier (FP64)
@@ -659,6 +658,7 @@ struct DArgs {
     float d_hat, kappa;
     float4 *grad, *diag;
     int *bact;  // contact blocks with d < d_hat, appended here for the CG products
+    float4 *mcache;  // per triangle: frame, F and S at this Newton iteration's q (for the CG products)
 };
 
 __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
@@ -680,6 +680,10 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
             float tr = e00 + e11;
             // S = 2 mu E + la tr(E) I ; P = F S ; H = -W P inv_dm^T
             float s00 = 2.f * A.mu * e00 + A.la * tr, s01 = 2.f * A.mu * e01, s11 = 2.f * A.mu * e11 + A.la * tr;
+            A.mcache[4 * (size_t)t] = make_float4(b1.x, b1.y, b1.z, F[0]);
+            A.mcache[4 * (size_t)t + 1] = make_float4(b2.x, b2.y, b2.z, F[1]);
+            A.mcache[4 * (size_t)t + 2] = make_float4(F[2], F[3], s00, s01);
+            A.mcache[4 * (size_t)t + 3] = make_float4(s11, 0.f, 0.f, 0.f);
             float P00 = F[0] * s00 + F[1] * s01, P01 = F[0] * s01 + F[1] * s11;
             float P10 = F[2] * s00 + F[3] * s01, P11 = F[2] * s01 + F[3] * s11;
             float W = -A.area[t];
@@ -756,14 +760,16 @@ struct HArgs {
     const float4 *dx;
     float4 *out;
     const int *bact;
+    const float4 *mcache;  // written by k_diff_elements at the same q
 };
 
 // Element terms of H dx added into out (atomics): membrane, hinges, and the
 // contact blocks with d < d_hat (listed by k_diff_elements; the others have no
 // Gauss-Newton term).  `first` / `stride` spread the elements over the threads.
 // Returns this thread's share of dx . (H_elements dx): each element's outputs
-// dotted with its own vertices' dx.
-__device__ __forceinline__ double hess_elements_range(const HArgs &A, long long first, long long stride)
+// dotted with its own vertices' dx.  `ldx(j)` gives dx at vertex j.
+template <class LDX>
+__device__ __forceinline__ double hess_elements_range(const HArgs &A, long long first, long long stride, LDX ldx)
 {
     double dxh = 0.0;
     // a hinge's four block rows go to four threads (one output vertex each)
@@ -775,24 +781,22 @@ __device__ __forceinline__ double hess_elements_range(const HArgs &A, long long 
         if (k < A.nt) {
             int t = (int)k;
             int4 f = A.tris[t];
-            F3 b1, b2;
-            float F[4];
+            const float4 c0 = A.mcache[4 * (size_t)t], c1 = A.mcache[4 * (size_t)t + 1];
+            const float4 c2 = A.mcache[4 * (size_t)t + 2], c3 = A.mcache[4 * (size_t)t + 3];
+            const F3 b1 = mk(c0.x, c0.y, c0.z), b2 = mk(c1.x, c1.y, c1.z);
+            const float F[4] = {c0.w, c1.w, c2.x, c2.y};
             float4 im = A.inv_dm[t];
-            elastic_F(A.q, f, im, b1, b2, F);
-            F3 dx01 = ld(A.dx, f.y) - ld(A.dx, f.x), dx02 = ld(A.dx, f.z) - ld(A.dx, f.x);
+            const F3 x0 = ldx(f.x), x1 = ldx(f.y), x2 = ldx(f.z);
+            F3 dx01 = x1 - x0, dx02 = x2 - x0;
             float s00 = dot(b1, dx01), s01 = dot(b1, dx02), s10 = dot(b2, dx01), s11 = dot(b2, dx02);
             float dF[4] = {s00 * im.x + s01 * im.z, s00 * im.y + s01 * im.w, s10 * im.x + s11 * im.z,
                            s10 * im.y + s11 * im.w};
-            float e00 = 0.5f * (F[0] * F[0] + F[2] * F[2] - 1.f);
-            float e01 = 0.5f * (F[0] * F[1] + F[2] * F[3]);
-            float e11 = 0.5f * (F[1] * F[1] + F[3] * F[3] - 1.f);
-            float tr = e00 + e11;
             // dE = 0.5 (dF^T F + F^T dF)
             float de00 = dF[0] * F[0] + dF[2] * F[2];
             float de01 = 0.5f * (dF[0] * F[1] + dF[2] * F[3] + F[0] * dF[1] + F[2] * dF[3]);
             float de11 = dF[1] * F[1] + dF[3] * F[3];
             float trd = de00 + de11;
-            float S00 = 2.f * A.mu * e00 + A.la * tr, S01 = 2.f * A.mu * e01, S11 = 2.f * A.mu * e11 + A.la * tr;
+            const float S00 = c2.z, S01 = c2.w, S11 = c3.x;
             float T00 = 2.f * A.mu * de00 + A.la * trd, T01 = 2.f * A.mu * de01, T11 = 2.f * A.mu * de11 + A.la * trd;
             float dP00 = dF[0] * S00 + dF[1] * S01 + F[0] * T00 + F[1] * T01;
             float dP01 = dF[0] * S01 + dF[1] * S11 + F[0] * T01 + F[1] * T11;
@@ -806,12 +810,12 @@ __device__ __forceinline__ double hess_elements_range(const HArgs &A, long long 
             atomic_add3(A.out, f.x, f0);
             atomic_add3(A.out, f.y, f1);
             atomic_add3(A.out, f.z, f2);
-            dxh += (double)dot(f0, ld(A.dx, f.x)) + (double)dot(f1, ld(A.dx, f.y)) + (double)dot(f2, ld(A.dx, f.z));
+            dxh += (double)dot(f0, x0) + (double)dot(f1, x1) + (double)dot(f2, x2);
         } else if (k < (long long)A.nt + nh4) {
             const int h = (int)((k - A.nt) >> 2), a = (int)((k - A.nt) & 3);
             int4 i = A.hinges[h];
             int idx[4] = {i.x, i.y, i.z, i.w};
-            F3 d[4] = {ld(A.dx, i.x), ld(A.dx, i.y), ld(A.dx, i.z), ld(A.dx, i.w)};
+            F3 d[4] = {ldx(i.x), ldx(i.y), ldx(i.z), ldx(i.w)};
             const float *B = A.hblk + (size_t)h * 144 + a * 36;  // block row a: blocks (a, 0..3)
             F3 s = mk(0.f, 0.f, 0.f);
             for (int b = 0; b < 4; ++b) {
@@ -831,7 +835,7 @@ __device__ __forceinline__ double hess_elements_range(const HArgs &A, long long 
             float s = 0.f;
             for (int a = 0; a < 4; ++a) {
                 g[a] = f3(A.bg[4 * (size_t)b + a]);
-                s += dot(g[a], ld(A.dx, idx[a]));
+                s += dot(g[a], ldx(idx[a]));
             }
             for (int a = 0; a < 4; ++a) atomic_add3(A.out, idx[a], (c * s) * g[a]);
             dxh += (double)(c * s) * (double)s;
@@ -842,7 +846,8 @@ __device__ __forceinline__ double hess_elements_range(const HArgs &A, long long 
 
 __global__ void __launch_bounds__(kThreads) k_hess_elements(HArgs A)
 {
-    hess_elements_range(A, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)blockDim.x * gridDim.x);
+    hess_elements_range(A, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)blockDim.x * gridDim.x,
+                        [&](int j) { return ld(A.dx, j); });
 }
 
 // -------------------------------------------------------------------- CG
@@ -946,115 +951,116 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const f
 }
 
 // The whole Jacobi-PCG solve of a Newton iteration (the 40 iterations of
-// cg_solver.py:96-158) in one cooperative launch, three grid barriers per
-// iteration: (A) v = z + beta v and the vertex term Av = w v, (B) the element
-// terms added into Av, with v . Av gathered on the way (each element's outputs
-// dotted with its own vertices' v, plus w |v|^2 from A), (D) the update of p, r
-// and z with z . r.  Per-block partials alternate between two buffers (a block
-// may write the next sum's partial while another still reads the last one) and
-// are added in a fixed order, so the sums do not depend on scheduling.  The
-// barrier spins with a limit; on timeout it records the error and the kernel
-// returns.
+// cg_solver.py:96-158) in one cooperative launch, one block per SM and two
+// grid-wide sums per iteration:
+//   (B) the new direction v = z + beta v is formed where it is read -- every
+//       element computes it for its own vertices from z and the last direction
+//       (both final since the previous sum), and each vertex's owner stores it
+//       into the other direction buffer -- while the element terms of A v are
+//       added into Av (zeroed by the owner in the previous pass) and v . A v is
+//       gathered (each element's outputs dotted with its own vertices' v, plus
+//       the vertex term w |v|^2);
+//   (D) p += alpha v, r -= alpha (Av + w v), z = r / diag, Av = 0, and z . r.
+// A sum ends in a grid barrier whose last arriving block adds the per-block
+// partials in block order and publishes the total before releasing the
+// others, so the sums do not depend on scheduling and every block reads one
+// value.  The barrier spins with a limit; on timeout it records the error and
+// the kernel returns.
+constexpr int kCgThreads = 512;
+
 struct CGArgs {
     HArgs h;
     const float4 *grad, *diag;
     const float *wk;
-    float4 *p, *r, *z, *v, *Av;
-    double *partials;
-    double *dscal;
+    float4 *p, *r, *z, *v0, *v1, *Av;
+    double *partials;  // one per block
+    double *red;       // the published total
     int *iscal;
     int np, n_iters;
 };
 
-__device__ __forceinline__ bool grid_barrier(int *iscal)
+// Block sum of `acc`, then the grid-wide total (see above).  Returns false on
+// a barrier timeout.
+__device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, double &total)
 {
-    __shared__ int s_ok;
-    __syncthreads();
+    __shared__ int s_last, s_gen, s_ok;
+    __shared__ double s_val;
+    const double bs = block_sum<kCgThreads>(acc);
     if (threadIdx.x == 0) {
-        volatile int *vgen = iscal + I_BAR_GEN;
-        const int gen = *vgen;
+        A.partials[blockIdx.x] = bs;
+        s_gen = *(volatile int *)(A.iscal + I_BAR_GEN);
+        s_ok = 1;
         __threadfence();
-        int ok = 1;
-        if (atomicAdd(iscal + I_BAR_COUNT, 1) == (int)gridDim.x - 1) {
-            iscal[I_BAR_COUNT] = 0;
-            __threadfence();
-            atomicAdd(iscal + I_BAR_GEN, 1);
-        } else {
-            for (long long spins = 0; *vgen == gen; ++spins) {
-                if (spins > (1LL << 24)) {  // ~ seconds: a block never arrived
-                    atomicExch(iscal + I_BAR_ERR, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        s_ok = ok;
+        s_last = atomicAdd(A.iscal + I_BAR_COUNT, 1) == (int)gridDim.x - 1;
     }
     __syncthreads();
+    if (s_last) {
+        if (threadIdx.x < 32) {
+            __threadfence();
+            double v = 0.0;
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) v += __ldcg(&A.partials[i]);
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (threadIdx.x == 0) {
+                s_val = v;
+                *A.red = v;
+                A.iscal[I_BAR_COUNT] = 0;
+                __threadfence();
+                atomicAdd(A.iscal + I_BAR_GEN, 1);
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        volatile int *vgen = A.iscal + I_BAR_GEN;
+        for (long long spins = 0; *vgen == s_gen; ++spins) {
+            if (spins > (1LL << 24)) {  // ~ seconds: a block never arrived
+                atomicExch(A.iscal + I_BAR_ERR, 1);
+                s_ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        s_val = __ldcg(A.red);
+    }
+    __syncthreads();
+    total = s_val;
     return s_ok != 0;
 }
 
-// sum of the blocks' partials in k_finish_sum's order, in every block
-__device__ __forceinline__ double all_blocks_sum(const double *partials)
-{
-    __shared__ double s_sum;
-    if (threadIdx.x < 32) {
-        double v = 0.0;
-        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) v += __ldcg(&partials[i]);
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) s_sum = v;
-    }
-    __syncthreads();
-    double r = s_sum;
-    __syncthreads();
-    return r;
-}
-
-__global__ void __launch_bounds__(kThreads, 2) k_cg_solve(CGArgs A)
+__global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
 {
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long gs = (long long)blockDim.x * gridDim.x;
-    int buf = 0;  // partials buffer of the next reduction
-    auto reduce = [&](double acc) -> double {
-        double bs = block_sum<kThreads>(acc);
-        double *part = A.partials + (size_t)buf * gridDim.x;
-        buf ^= 1;
-        if (threadIdx.x == 0) part[blockIdx.x] = bs;
-        if (!grid_barrier(A.iscal)) return NAN;
-        return all_blocks_sum(part);
-    };
-    // r = g, z = v = g / (diag + 1e-6), p = 0
+    // r = g, z = g / (diag + 1e-6), p = 0, Av = 0
     double acc = 0.0;
     for (long long i = t0; i < A.np; i += gs) {
         F3 g = ld(A.grad, (int)i), d = ld(A.diag, (int)i);
         F3 zz = mk(g.x / (d.x + 1e-6f), g.y / (d.y + 1e-6f), g.z / (d.z + 1e-6f));
         A.p[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        A.Av[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         st(A.r, (int)i, g);
         st(A.z, (int)i, zz);
-        st(A.v, (int)i, zz);
         acc += (double)dot(zz, g);
     }
-    double zr = reduce(acc), zr_last = zr;
-    if (A.iscal[I_BAR_ERR]) return;
+    double zr, zr_last, vav;
+    if (!grid_sum(acc, A, zr)) return;
+    zr_last = zr;
     for (int it = 0; it < A.n_iters; ++it) {
         const float beta = it == 0 ? 0.f : (float)(zr / zr_last);
+        const float4 *vo = (it & 1) ? A.v1 : A.v0;  // last direction
+        float4 *vn = (it & 1) ? A.v0 : A.v1;        // this one
+        const float4 *z = A.z;
+        auto dir = [&](int j) -> F3 {
+            if (it == 0) return ld(z, j);
+            return ld(z, j) + beta * ld(vo, j);
+        };
         acc = 0.0;
         for (long long i = t0; i < A.np; i += gs) {
-            F3 vv = ld(A.v, (int)i);
-            if (it > 0) {
-                vv = ld(A.z, (int)i) + beta * vv;
-                st(A.v, (int)i, vv);
-            }
-            const F3 wv = A.wk[i] * vv;
-            st(A.Av, (int)i, wv);
-            acc += (double)dot(vv, wv);
+            const F3 vv = dir((int)i);
+            st(vn, (int)i, vv);
+            acc += (double)dot(vv, A.wk[i] * vv);
         }
-        if (!grid_barrier(A.iscal)) return;
-        acc += hess_elements_range(A.h, t0, gs);
-        const double vav = reduce(acc);
-        if (A.iscal[I_BAR_ERR]) return;
+        acc += hess_elements_range(A.h, t0, gs, dir);
+        if (!grid_sum(acc, A, vav)) return;
         zr_last = zr;
         const bool upd = vav > 1e-16;
         const float alpha = upd ? (float)(zr_last / vav) : 0.f;
@@ -1062,17 +1068,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_cg_solve(CGArgs A)
         for (long long i = t0; i < A.np; i += gs) {
             F3 rr = ld(A.r, (int)i);
             if (upd) {
-                st(A.p, (int)i, ld(A.p, (int)i) + alpha * ld(A.v, (int)i));
-                rr = rr - alpha * ld(A.Av, (int)i);
+                const F3 vv = ld(vn, (int)i);
+                st(A.p, (int)i, ld(A.p, (int)i) + alpha * vv);
+                rr = rr - alpha * (ld(A.Av, (int)i) + A.wk[i] * vv);
                 st(A.r, (int)i, rr);
             }
+            A.Av[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             F3 d = ld(A.diag, (int)i);
             F3 zz = mk(rr.x / d.x, rr.y / d.y, rr.z / d.z);
             st(A.z, (int)i, zz);
             acc += (double)dot(zz, rr);
         }
-        zr = reduce(acc);
-        if (A.iscal[I_BAR_ERR]) return;
+        if (!grid_sum(acc, A, zr)) return;
     }
 }
 
@@ -1179,7 +1186,7 @@ __global__ void k_f4_to_aos(const float4 *in, float *out, int n)
 
 void Stage3::release()
 {
-    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, Av, q_gather, wk, tris, area, inv_dm, edges4, hinges,
+    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, v2, Av, q_gather, wk, tris, area, inv_dm, mcache, edges4, hinges,
                     rest_angle, rest_elen, hblk, bidx, bkind, bsub, bd, bb2, bg, bact, gt_pts, gt_tris, dscal, fscal,
                     iscal, partials};
     drop_graph();
@@ -1196,9 +1203,9 @@ void Stage3::release()
         if (x) cudaFree(x);
     if (h_iscal) cudaFreeHost(h_iscal);
     if (h_dscal) cudaFreeHost(h_dscal);
-    q = q_prev = q_det = p = grad = diag = target = r = z = v = Av = q_gather = nullptr;
+    q = q_prev = q_det = p = grad = diag = target = r = z = v = v2 = Av = q_gather = nullptr;
     gathered = false;
-    wk = nullptr; tris = nullptr; area = nullptr; inv_dm = nullptr; edges4 = nullptr; hinges = nullptr;
+    wk = nullptr; tris = nullptr; area = nullptr; inv_dm = nullptr; mcache = nullptr; edges4 = nullptr; hinges = nullptr;
     rest_angle = rest_elen = hblk = nullptr; bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr;
     bg = nullptr; bact = nullptr; gt_pts = nullptr; gt_tris = nullptr; dscal = nullptr; fscal = nullptr; iscal = nullptr;
     partials = nullptr; h_iscal = nullptr; h_dscal = nullptr;
@@ -1226,10 +1233,10 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
         }                                                                \
     } while (0)
     A3(q, cp * 16); A3(q_prev, cp * 16); A3(q_det, cp * 16); A3(p, cp * 16); A3(grad, cp * 16);
-    A3(diag, cp * 16); A3(target, cp * 16); A3(r, cp * 16); A3(z, cp * 16); A3(v, cp * 16); A3(Av, cp * 16);
+    A3(diag, cp * 16); A3(target, cp * 16); A3(r, cp * 16); A3(z, cp * 16); A3(v, cp * 16); A3(v2, cp * 16); A3(Av, cp * 16);
     A3(q_gather, cp * 16);
     A3(wk, cp * 4);
-    A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16);
+    A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16); A3(mcache, ct * 64);
     A3(edges4, ce * 16);
     A3(hinges, ch * 16); A3(rest_angle, ch * 4); A3(rest_elen, ch * 4); A3(hblk, ch * 144 * 4);
     A3(gt_pts, cgp * 16); A3(gt_tris, cgt * 16);
@@ -1395,7 +1402,7 @@ static int hess_elements(Stage3 &S, const float4 *dx, float4 *out, cudaStream_t 
             S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
             S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
                 ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
-            S.hinges, S.hblk, S.bidx, S.bg, S.bb2, S.iscal, S.cap_b, dx, out, S.bact};
+            S.hinges, S.hblk, S.bidx, S.bg, S.bb2, S.iscal, S.cap_b, dx, out, S.bact, S.mcache};
     launch(k_hess_elements, grid_for((long long)S.nt + 4LL * S.nh + S.cap_b), kThreads, 0, s, h);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
@@ -1468,7 +1475,7 @@ int Stage3::newton_body(cudaStream_t s)
             cfg.elas_young_modulus * cfg.elas_poisson_ratio /
                 ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
             hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, hblk, bidx, bkind, bsub, bd, bg, bb2,
-            iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag, bact};
+            iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag, bact, mcache};
     S3_TRY(cudaMemsetAsync(iscal + I_NACT, 0, sizeof(int), s));
     launch(k_diff_elements, grid_for((long long)nt + nh + cap_b, 128), 128, 0, s, d);
     // Jacobi-preconditioned CG (cg_solver.py:96-158)
@@ -1478,20 +1485,22 @@ int Stage3::newton_body(cudaStream_t s)
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_solve, kThreads, 0);
-        cg_persistent = (coop && (long long)per_sm * sms >= kRedBlocks) ? 1 : 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_solve, kCgThreads, 0);
+        cg_persistent = (coop && per_sm >= 1 && sms >= 1) ? 1 : 0;
+        cg_blocks = sms < kRedBlocks ? sms : kRedBlocks;  // one block per SM, all resident
         cudaGetLastError();
     }
     if (cg_persistent == 1) {
         HArgs h{q, wk, np, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
                 cfg.elas_young_modulus * cfg.elas_poisson_ratio /
                     ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
-                hinges, hblk, bidx, bg, bb2, iscal, cap_b, v, Av, bact};
-        CGArgs ca{h, grad, diag, wk, p, r, z, v, Av, partials, dscal, iscal, np, cfg.n_cg_iters};
+                hinges, hblk, bidx, bg, bb2, iscal, cap_b, nullptr, Av, bact, mcache};
+        // partials: 2 x kRedBlocks doubles; the solve uses the first cg_blocks and publishes at kRedBlocks
+        CGArgs ca{h, grad, diag, wk, p, r, z, v, v2, Av, partials, partials + kRedBlocks, iscal, np, cfg.n_cg_iters};
         S3_TRY(cudaMemsetAsync(iscal + I_BAR_COUNT, 0, sizeof(int), s));
         cudaLaunchConfig_t lc = {};
-        lc.gridDim = dim3(kRedBlocks);
-        lc.blockDim = dim3(kThreads);
+        lc.gridDim = dim3(cg_blocks);
+        lc.blockDim = dim3(kCgThreads);
         lc.dynamicSmemBytes = 0;
         lc.stream = s;
         cudaLaunchAttribute attr[1];

@@ -26,12 +26,13 @@ struct Stage3 {
 
     // per vertex (xyz in float4, w unused)
     float4 *q = nullptr, *q_prev = nullptr, *q_det = nullptr, *p = nullptr, *grad = nullptr, *diag = nullptr;
-    float4 *target = nullptr, *r = nullptr, *z = nullptr, *v = nullptr, *Av = nullptr;
+    float4 *target = nullptr, *r = nullptr, *z = nullptr, *v = nullptr, *v2 = nullptr, *Av = nullptr;
     float *wk = nullptr;  // Voronoi area x GT-distance stiffness
     // per triangle / edge / hinge
     int4 *tris = nullptr;
     float *area = nullptr;
     float4 *inv_dm = nullptr;  // 2x2 row-major
+    float4 *mcache = nullptr;  // 4 per triangle: frame, F, S at the current Newton iteration
     int4 *edges4 = nullptr;    // (a, b, b, 0): a segment as a degenerate triangle for the LBVH
     int4 *hinges = nullptr;
     float *rest_angle = nullptr, *rest_elen = nullptr;
@@ -62,6 +63,7 @@ struct Stage3 {
     cudaGraphExec_t graph = nullptr;  // one Newton iteration after detection
     long long graph_cap_b = -1, graph_kernels = 0;
     bool use_graph = true;
+    int cg_blocks = 0;   // grid of the persistent solve
     int cg_persistent = -1;  // 1: one cooperative launch per solve; 0: one launch per phase; -1: not decided
     cudaStream_t work = nullptr;  // the solve's own stream (graphs cannot be captured on the legacy stream)
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
