@@ -125,9 +125,24 @@ __global__ void __launch_bounds__(1024) k_sequential_mean(const float *mx, const
             }
             for (; i < cnt && (i & 3); ++i) acc += bs[i];
             const int n4 = cnt >> 2;
-#pragma unroll 4
-            for (int q = i >> 2; q < n4; ++q) {
-                float4 v = b4[q];
+            int q = i >> 2;
+            // sixteen values per step, the next sixteen loaded while these are
+            // added (the clamped loads stay inside the buffer and are unused at
+            // the end), so the chain waits on the adds alone
+            if (q + 4 <= n4) {
+                float4 c0 = b4[q], c1 = b4[q + 1], c2 = b4[q + 2], c3 = b4[q + 3];
+                for (; q + 4 <= n4; q += 4) {
+                    const int nq = min(q + 4, n4 - 4);
+                    const float4 d0 = b4[nq], d1 = b4[nq + 1], d2 = b4[nq + 2], d3 = b4[nq + 3];
+                    acc += c0.x; acc += c0.y; acc += c0.z; acc += c0.w;
+                    acc += c1.x; acc += c1.y; acc += c1.z; acc += c1.w;
+                    acc += c2.x; acc += c2.y; acc += c2.z; acc += c2.w;
+                    acc += c3.x; acc += c3.y; acc += c3.z; acc += c3.w;
+                    c0 = d0; c1 = d1; c2 = d2; c3 = d3;
+                }
+            }
+            for (; q < n4; ++q) {
+                const float4 v = b4[q];
                 acc += v.x;
                 acc += v.y;
                 acc += v.z;

@@ -198,6 +198,23 @@ __device__ __forceinline__ float skinny_term(V3 n0, V3 n1, V3 n2)
     return 1.0f - tclamp((float)e, 0.0f, 1.0f);
 }
 
+// Whether the moved face's unit normal c / |c| points against `on`, i.e. the
+// reference's dot(on, c / |c|) < 0 with c normalised by three divisions.
+// Shortcut: with |c|^2 in the normal range and |on . c| well above the
+// rounding error of either dot product (1e-5 of sum |on_i c_i|, against a few
+// 2^-24 for both forms), the two dot products have the same, non-zero sign, and
+// dot(on, c) / |c| stays far from underflow (dc^2 > 1e-30 |c|^2).  Otherwise
+// the reference's expression is evaluated.
+__device__ __forceinline__ bool normal_flips(V3 on, V3 c)
+{
+    const float s2 = c.x * c.x + c.y * c.y + c.z * c.z;
+    const float dc = vdot(on, c);
+    const float mag = fabsf(on.x * c.x) + fabsf(on.y * c.y) + fabsf(on.z * c.z);
+    if (s2 > 1e-30f && s2 < 1e30f && fabsf(dc) > 1e-5f * mag && dc * dc > 1e-30f * s2) return dc < 0.f;
+    const V3 nn = vdivs(c, vnorm(c));
+    return vdot(on, nn) < 0;
+}
+
 struct CostArgs {
     const int2 *edges;
     const int *n_edges;
@@ -278,9 +295,8 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, boo
             V3 n2 = t.z == w ? mid : o2;
             // the unchanged face's unit normal is the face plane's (same expression)
             V3 on = v3(A.plane[f]);
-            V3 nn = vcross(vsub(n1, n0), vsub(n2, n0));
-            nn = vdivs(nn, vnorm(nn));
-            if (vdot(on, nn) < 0) {
+            const V3 c = vcross(vsub(n1, n0), vsub(n2, n0));
+            if (normal_flips(on, c)) {
                 out = 0xFFFFFFFFu;
                 return true;
             }

@@ -647,7 +647,8 @@ struct DArgs {
     const float *rest_angle, *rest_elen;
     float hinge_k;
     int spd_iters;
-    float *hblk;
+    float4 *kval;
+    const int *tri_slot, *hinge_slot;
     const int4 *bidx;
     const int *bkind, *bsub;
     const float *bd;
@@ -658,8 +659,38 @@ struct DArgs {
     float d_hat, kappa;
     float4 *grad, *diag;
     int *bact;  // contact blocks with d < d_hat, appended here for the CG products
-    float4 *mcache;  // per triangle: frame, F and S at this Newton iteration's q (for the CG products)
 };
+
+// one 3x3 block (row-major) added into the assembled Hessian
+__device__ __forceinline__ void add_block(float4 *kval, int slot, const float *m)
+{
+    atomicAdd(&kval[3 * (size_t)slot], make_float4(m[0], m[1], m[2], 0.f));
+    atomicAdd(&kval[3 * (size_t)slot + 1], make_float4(m[3], m[4], m[5], 0.f));
+    atomicAdd(&kval[3 * (size_t)slot + 2], make_float4(m[6], m[7], m[8], 0.f));
+}
+
+// The membrane Hessian's action on a displacement of the triangle's edge
+// vectors (dx01, dx02): dF, dE = (dF^T F + F^T dF) / 2, dS, dP = dF S + F dS,
+// and the forces on vertices 1 and 2 (vertex 0 gets minus their sum).
+__device__ __forceinline__ void membrane_apply(F3 b1, F3 b2, const float F[4], float S00, float S01, float S11,
+                                               float4 im, float W, float mu, float la, F3 dx01, F3 dx02, F3 &f1, F3 &f2)
+{
+    float s00 = dot(b1, dx01), s01 = dot(b1, dx02), s10 = dot(b2, dx01), s11 = dot(b2, dx02);
+    float dF[4] = {s00 * im.x + s01 * im.z, s00 * im.y + s01 * im.w, s10 * im.x + s11 * im.z, s10 * im.y + s11 * im.w};
+    float de00 = dF[0] * F[0] + dF[2] * F[2];
+    float de01 = 0.5f * (dF[0] * F[1] + dF[2] * F[3] + F[0] * dF[1] + F[2] * dF[3]);
+    float de11 = dF[1] * F[1] + dF[3] * F[3];
+    float trd = de00 + de11;
+    float T00 = 2.f * mu * de00 + la * trd, T01 = 2.f * mu * de01, T11 = 2.f * mu * de11 + la * trd;
+    float dP00 = dF[0] * S00 + dF[1] * S01 + F[0] * T00 + F[1] * T01;
+    float dP01 = dF[0] * S01 + dF[1] * S11 + F[0] * T01 + F[1] * T11;
+    float dP10 = dF[2] * S00 + dF[3] * S01 + F[2] * T00 + F[3] * T01;
+    float dP11 = dF[2] * S01 + dF[3] * S11 + F[2] * T01 + F[3] * T11;
+    float H00 = W * (dP00 * im.x + dP01 * im.y), H01 = W * (dP00 * im.z + dP01 * im.w);
+    float H10 = W * (dP10 * im.x + dP11 * im.y), H11 = W * (dP10 * im.z + dP11 * im.w);
+    f1 = H00 * b1 + H10 * b2;
+    f2 = H01 * b1 + H11 * b2;
+}
 
 __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
 {
@@ -680,10 +711,6 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
             float tr = e00 + e11;
             // S = 2 mu E + la tr(E) I ; P = F S ; H = -W P inv_dm^T
             float s00 = 2.f * A.mu * e00 + A.la * tr, s01 = 2.f * A.mu * e01, s11 = 2.f * A.mu * e11 + A.la * tr;
-            A.mcache[4 * (size_t)t] = make_float4(b1.x, b1.y, b1.z, F[0]);
-            A.mcache[4 * (size_t)t + 1] = make_float4(b2.x, b2.y, b2.z, F[1]);
-            A.mcache[4 * (size_t)t + 2] = make_float4(F[2], F[3], s00, s01);
-            A.mcache[4 * (size_t)t + 3] = make_float4(s11, 0.f, 0.f, 0.f);
             float P00 = F[0] * s00 + F[1] * s01, P01 = F[0] * s01 + F[1] * s11;
             float P10 = F[2] * s00 + F[3] * s01, P11 = F[2] * s01 + F[3] * s11;
             float W = -A.area[t];
@@ -694,6 +721,36 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
             atomic_add3(A.grad, f.x, f0);
             atomic_add3(A.grad, f.y, f1);
             atomic_add3(A.grad, f.z, f2);
+            // the membrane Hessian: the linear map (dx01, dx02) -> (force 1, force 2)
+            // on the six unit displacements gives M (6 x 6); vertex 0's rows and
+            // columns follow from dx01 = x1 - x0, dx02 = x2 - x0 and f0 = -f1 - f2
+            float M[6][6];  // M[row][col]: rows f1.xyz, f2.xyz; columns dx01.xyz, dx02.xyz
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                F3 e = mk(c % 3 == 0 ? 1.f : 0.f, c % 3 == 1 ? 1.f : 0.f, c % 3 == 2 ? 1.f : 0.f);
+                F3 z0 = mk(0.f, 0.f, 0.f), g1, g2;
+                membrane_apply(b1, b2, F, s00, s01, s11, im, A.area[t], A.mu, A.la, c < 3 ? e : z0, c < 3 ? z0 : e,
+                               g1, g2);
+                M[0][c] = g1.x; M[1][c] = g1.y; M[2][c] = g1.z;
+                M[3][c] = g2.x; M[4][c] = g2.y; M[5][c] = g2.z;
+            }
+            const int *slot = A.tri_slot + 9 * (size_t)t;
+            float blk[9];
+            // K_ab for a, b in {1, 2}: M's 3x3 sub-blocks; K_a0 = -(K_a1 + K_a2); K_0b = -(K_1b + K_2b)
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    for (int i = 0; i < 3; ++i)
+                        for (int j = 0; j < 3; ++j) {
+                            auto kk = [&](int aa, int bb) { return M[3 * (aa - 1) + i][3 * (bb - 1) + j]; };
+                            float val;
+                            if (a > 0 && b > 0) val = kk(a, b);
+                            else if (a > 0) val = -(kk(a, 1) + kk(a, 2));
+                            else if (b > 0) val = -(kk(1, b) + kk(2, b));
+                            else val = kk(1, 1) + kk(1, 2) + kk(2, 1) + kk(2, 2);
+                            blk[3 * i + j] = val;
+                        }
+                    add_block(A.kval, slot[3 * a + b], blk);
+                }
         } else if (k < (long long)A.nt + A.nh) {
             int h = (int)(k - A.nt);
             int4 i = A.hinges[h];
@@ -709,9 +766,8 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
                 atomic_add3(A.diag, idx[a], mk(B[a * 5][0], B[a * 5][4], B[a * 5][8]));
             }
             spd_project(B, A.spd_iters);
-            float *dst = A.hblk + (size_t)h * 144;
-            for (int b = 0; b < 16; ++b)
-                for (int e = 0; e < 9; ++e) dst[b * 9 + e] = B[b][e];
+            const int *slot = A.hinge_slot + 16 * (size_t)h;
+            for (int b = 0; b < 16; ++b) add_block(A.kval, slot[b], B[b]);
         } else {
             int b = (int)(k - A.nt - A.nh);
             float d = A.bd[b];
@@ -741,113 +797,239 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
     }
 }
 
-// ---------------------------------------------------------------- hess * dx
-struct HArgs {
-    const float4 *q;
-    const float *wk;
-    int np, nt, nh;
-    const int4 *tris;
-    const float *area;
-    const float4 *inv_dm;
-    float mu, la;
-    const int4 *hinges;
-    const float *hblk;
+// ---------------------------------------------------------------- A * dx
+// The operator of the CG: rows of the assembled block matrix (vertex term,
+// membrane, hinges) plus the rank-one Gauss-Newton terms of the contact blocks
+// with d < d_hat (listed by k_diff_elements).
+struct OpArgs {
+    int np;
+    const int *row_ptr, *col;
+    const float4 *kval;
     const int4 *bidx;
     const float4 *bg;
     const float *bb2;
+    const int *bact;
     const int *iscal;
     long long cap_b;
-    const float4 *dx;
-    float4 *out;
-    const int *bact;
-    const float4 *mcache;  // written by k_diff_elements at the same q
 };
 
-// Element terms of H dx added into out (atomics): membrane, hinges, and the
-// contact blocks with d < d_hat (listed by k_diff_elements; the others have no
-// Gauss-Newton term).  `first` / `stride` spread the elements over the threads.
-// Returns this thread's share of dx . (H_elements dx): each element's outputs
-// dotted with its own vertices' dx.  `ldx(j)` gives dx at vertex j.
+// Rows [first, ...) of K dx, eight rows per warp and four lanes per row (the
+// loop bounds are warp-uniform, so the shuffles see the whole warp).  `ldx(j)`
+// gives dx at vertex j; `row(i, (K dx)_i)` receives each finished row.
+template <class LDX, class ROW>
+__device__ __forceinline__ void op_rows(const OpArgs &A, long long warp0, long long nwarps, LDX ldx, ROW row)
+{
+    const int lane = threadIdx.x & 31, sub = lane & 3;
+    for (long long base = warp0 * 8; base < A.np; base += nwarps * 8) {
+        const long long i = base + (lane >> 2);
+        F3 acc = mk(0.f, 0.f, 0.f);
+        if (i < A.np) {
+            const int e = A.row_ptr[i + 1];
+            int s = A.row_ptr[i] + sub;
+            // a lane's first kRowBatch slots with every load issued before any
+            // use (the column, then dx there), so a row costs two round trips
+            constexpr int kRowBatch = 4;
+            int cidx[kRowBatch];
+#pragma unroll
+            for (int k = 0; k < kRowBatch; ++k) cidx[k] = s + 4 * k < e ? A.col[s + 4 * k] : -1;
+            F3 x[kRowBatch];
+#pragma unroll
+            for (int k = 0; k < kRowBatch; ++k) x[k] = cidx[k] >= 0 ? ldx(cidx[k]) : mk(0.f, 0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < kRowBatch; ++k) {
+                if (cidx[k] < 0) continue;
+                const size_t b = 3 * (size_t)(s + 4 * k);
+                const float4 k0 = A.kval[b], k1 = A.kval[b + 1], k2 = A.kval[b + 2];
+                acc = acc + mk(k0.x * x[k].x + k0.y * x[k].y + k0.z * x[k].z, k1.x * x[k].x + k1.y * x[k].y + k1.z * x[k].z,
+                               k2.x * x[k].x + k2.y * x[k].y + k2.z * x[k].z);
+            }
+            for (s += 4 * kRowBatch; s < e; s += 4) {  // rows longer than 4 x kRowBatch
+                const F3 xx = ldx(A.col[s]);
+                const float4 k0 = A.kval[3 * (size_t)s], k1 = A.kval[3 * (size_t)s + 1], k2 = A.kval[3 * (size_t)s + 2];
+                acc = acc + mk(k0.x * xx.x + k0.y * xx.y + k0.z * xx.z, k1.x * xx.x + k1.y * xx.y + k1.z * xx.z,
+                               k2.x * xx.x + k2.y * xx.y + k2.z * xx.z);
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+            acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
+        }
+        if (i < A.np && sub == 0) row((int)i, acc);
+    }
+}
+
+// The contact terms c (g . dx) g of blocks [first, ...), added into out with
+// atomics; returns this thread's share of dx . (their sum).
 template <class LDX>
-__device__ __forceinline__ double hess_elements_range(const HArgs &A, long long first, long long stride, LDX ldx)
+__device__ __forceinline__ double op_contacts(const OpArgs &A, long long first, long long stride, LDX ldx, float4 *out)
 {
     double dxh = 0.0;
-    // a hinge's four block rows go to four threads (one output vertex each)
     const long long nb = min((long long)A.iscal[I_NACT], A.cap_b);
-    const long long nh4 = 4LL * A.nh;
-    const long long total = (long long)A.nt + nh4 + nb;
-    for (long long k = first; k < total; k += stride)
-    {
-        if (k < A.nt) {
-            int t = (int)k;
-            int4 f = A.tris[t];
-            const float4 c0 = A.mcache[4 * (size_t)t], c1 = A.mcache[4 * (size_t)t + 1];
-            const float4 c2 = A.mcache[4 * (size_t)t + 2], c3 = A.mcache[4 * (size_t)t + 3];
-            const F3 b1 = mk(c0.x, c0.y, c0.z), b2 = mk(c1.x, c1.y, c1.z);
-            const float F[4] = {c0.w, c1.w, c2.x, c2.y};
-            float4 im = A.inv_dm[t];
-            const F3 x0 = ldx(f.x), x1 = ldx(f.y), x2 = ldx(f.z);
-            F3 dx01 = x1 - x0, dx02 = x2 - x0;
-            float s00 = dot(b1, dx01), s01 = dot(b1, dx02), s10 = dot(b2, dx01), s11 = dot(b2, dx02);
-            float dF[4] = {s00 * im.x + s01 * im.z, s00 * im.y + s01 * im.w, s10 * im.x + s11 * im.z,
-                           s10 * im.y + s11 * im.w};
-            // dE = 0.5 (dF^T F + F^T dF)
-            float de00 = dF[0] * F[0] + dF[2] * F[2];
-            float de01 = 0.5f * (dF[0] * F[1] + dF[2] * F[3] + F[0] * dF[1] + F[2] * dF[3]);
-            float de11 = dF[1] * F[1] + dF[3] * F[3];
-            float trd = de00 + de11;
-            const float S00 = c2.z, S01 = c2.w, S11 = c3.x;
-            float T00 = 2.f * A.mu * de00 + A.la * trd, T01 = 2.f * A.mu * de01, T11 = 2.f * A.mu * de11 + A.la * trd;
-            float dP00 = dF[0] * S00 + dF[1] * S01 + F[0] * T00 + F[1] * T01;
-            float dP01 = dF[0] * S01 + dF[1] * S11 + F[0] * T01 + F[1] * T11;
-            float dP10 = dF[2] * S00 + dF[3] * S01 + F[2] * T00 + F[3] * T01;
-            float dP11 = dF[2] * S01 + dF[3] * S11 + F[2] * T01 + F[3] * T11;
-            float W = A.area[t];
-            float H00 = W * (dP00 * im.x + dP01 * im.y), H01 = W * (dP00 * im.z + dP01 * im.w);
-            float H10 = W * (dP10 * im.x + dP11 * im.y), H11 = W * (dP10 * im.z + dP11 * im.w);
-            F3 f1 = H00 * b1 + H10 * b2, f2 = H01 * b1 + H11 * b2;
-            F3 f0 = mk(-f1.x - f2.x, -f1.y - f2.y, -f1.z - f2.z);
-            atomic_add3(A.out, f.x, f0);
-            atomic_add3(A.out, f.y, f1);
-            atomic_add3(A.out, f.z, f2);
-            dxh += (double)dot(f0, x0) + (double)dot(f1, x1) + (double)dot(f2, x2);
-        } else if (k < (long long)A.nt + nh4) {
-            const int h = (int)((k - A.nt) >> 2), a = (int)((k - A.nt) & 3);
-            int4 i = A.hinges[h];
-            int idx[4] = {i.x, i.y, i.z, i.w};
-            F3 d[4] = {ldx(i.x), ldx(i.y), ldx(i.z), ldx(i.w)};
-            const float *B = A.hblk + (size_t)h * 144 + a * 36;  // block row a: blocks (a, 0..3)
-            F3 s = mk(0.f, 0.f, 0.f);
-            for (int b = 0; b < 4; ++b) {
-                const float *m = B + b * 9;
-                s = s + mk(m[0] * d[b].x + m[1] * d[b].y + m[2] * d[b].z, m[3] * d[b].x + m[4] * d[b].y + m[5] * d[b].z,
-                           m[6] * d[b].x + m[7] * d[b].y + m[8] * d[b].z);
-            }
-            atomic_add3(A.out, idx[a], s);
-            dxh += (double)dot(s, d[a]);
-        } else {
-            int b = A.bact[k - A.nt - nh4];
-            float c = A.bb2[b];
-            if (c == 0.f) continue;
-            int4 i = A.bidx[b];
-            int idx[4] = {i.x, i.y, i.z, i.w};
-            F3 g[4];
-            float s = 0.f;
-            for (int a = 0; a < 4; ++a) {
-                g[a] = f3(A.bg[4 * (size_t)b + a]);
-                s += dot(g[a], ldx(idx[a]));
-            }
-            for (int a = 0; a < 4; ++a) atomic_add3(A.out, idx[a], (c * s) * g[a]);
-            dxh += (double)(c * s) * (double)s;
+    for (long long k = first; k < nb; k += stride) {
+        const int b = A.bact[k];
+        const float c = A.bb2[b];
+        if (c == 0.f) continue;
+        const int4 i = A.bidx[b];
+        const int idx[4] = {i.x, i.y, i.z, i.w};
+        F3 g[4];
+        float s = 0.f;
+        for (int a = 0; a < 4; ++a) {
+            g[a] = f3(A.bg[4 * (size_t)b + a]);
+            s += dot(g[a], ldx(idx[a]));
         }
+        for (int a = 0; a < 4; ++a) atomic_add3(out, idx[a], (c * s) * g[a]);
+        dxh += (double)(c * s) * (double)s;
     }
     return dxh;
 }
 
-__global__ void __launch_bounds__(kThreads) k_hess_elements(HArgs A)
+// out = K dx (rows), then the contact terms in a second launch
+__global__ void __launch_bounds__(kThreads) k_op_rows(OpArgs A, const float4 *dx, float4 *out)
 {
-    hess_elements_range(A, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)blockDim.x * gridDim.x,
-                        [&](int j) { return ld(A.dx, j); });
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    op_rows(A, t0 >> 5, ((long long)blockDim.x * gridDim.x) >> 5, [&](int j) { return ld(dx, j); },
+            [&](int i, F3 r) { st(out, i, r); });
+}
+
+__global__ void __launch_bounds__(kThreads) k_op_contacts(OpArgs A, const float4 *dx, float4 *out)
+{
+    op_contacts(A, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)blockDim.x * gridDim.x,
+                [&](int j) { return ld(dx, j); }, out);
+}
+
+// ------------------------------------------------------- the block pattern
+// Built once per registered mesh: every element's ordered vertex pairs (and
+// the diagonal) bucketed by row, each row sorted and deduplicated, then the
+// position of every element block in its row.
+__global__ void k_fill_int(int *a, long long n, int v)
+{
+    PAMO_GRID_STRIDE(i, n) a[i] = v;
+}
+
+__global__ void k_pat_count(const int4 *tris, int nt, const int4 *hinges, int nh, int *cnt)
+{
+    const long long total = (long long)nt + nh;
+    PAMO_GRID_STRIDE(k, total)
+    {
+        if (k < nt) {
+            const int4 t = tris[k];
+            atomicAdd(&cnt[t.x], 2);
+            atomicAdd(&cnt[t.y], 2);
+            atomicAdd(&cnt[t.z], 2);
+        } else {
+            const int4 h = hinges[k - nt];
+            atomicAdd(&cnt[h.x], 3);
+            atomicAdd(&cnt[h.y], 3);
+            atomicAdd(&cnt[h.z], 3);
+            atomicAdd(&cnt[h.w], 3);
+        }
+    }
+}
+
+__global__ void k_pat_fill(const int4 *tris, int nt, const int4 *hinges, int nh, int np, const int *off, int *cur,
+                           int *cand)
+{
+    const long long total = (long long)np + nt + nh;
+    auto put = [&](int r, int c) { cand[off[r] + atomicAdd(&cur[r], 1)] = c; };
+    PAMO_GRID_STRIDE(k, total)
+    {
+        if (k < np) {
+            put((int)k, (int)k);
+        } else if (k < (long long)np + nt) {
+            const int4 t = tris[k - np];
+            const int v[3] = {t.x, t.y, t.z};
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    if (a != b) put(v[a], v[b]);
+        } else {
+            const int4 h = hinges[k - np - nt];
+            const int v[4] = {h.x, h.y, h.z, h.w};
+            for (int a = 0; a < 4; ++a)
+                for (int b = 0; b < 4; ++b)
+                    if (a != b) put(v[a], v[b]);
+        }
+    }
+}
+
+__global__ void k_pat_sort(const int *off, int np, int *cand, int *ucnt)
+{
+    PAMO_GRID_STRIDE(v, np)
+    {
+        const int a = off[v], b = off[v + 1];
+        for (int i = a + 1; i < b; ++i) {
+            const int x = cand[i];
+            int j = i - 1;
+            while (j >= a && cand[j] > x) {
+                cand[j + 1] = cand[j];
+                --j;
+            }
+            cand[j + 1] = x;
+        }
+        int u = a;
+        for (int i = a; i < b; ++i)
+            if (u == a || cand[i] != cand[u - 1]) cand[u++] = cand[i];
+        ucnt[v] = u - a;
+    }
+}
+
+__global__ void k_pat_emit(const int *off, const int *row_ptr, const int *cand, int np, int *col)
+{
+    PAMO_GRID_STRIDE(v, np)
+    {
+        const int a = off[v], r = row_ptr[v], n = row_ptr[v + 1] - r;
+        for (int k = 0; k < n; ++k) col[r + k] = cand[a + k];
+    }
+}
+
+// position of column c in row r (present by construction)
+__device__ __forceinline__ int find_slot(const int *row_ptr, const int *col, int r, int c)
+{
+    int lo = row_ptr[r], hi = row_ptr[r + 1] - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (col[mid] < c) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_pat_slots(const int4 *tris, int nt, const int4 *hinges, int nh, int np, const int *row_ptr,
+                            const int *col, int *tri_slot, int *hinge_slot, int *diag_slot)
+{
+    const long long total = (long long)np + nt + nh;
+    PAMO_GRID_STRIDE(k, total)
+    {
+        if (k < np) {
+            diag_slot[k] = find_slot(row_ptr, col, (int)k, (int)k);
+        } else if (k < (long long)np + nt) {
+            const long long t = k - np;
+            const int4 f = tris[t];
+            const int v[3] = {f.x, f.y, f.z};
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) tri_slot[9 * t + 3 * a + b] = find_slot(row_ptr, col, v[a], v[b]);
+        } else {
+            const long long h = k - np - nt;
+            const int4 f = hinges[h];
+            const int v[4] = {f.x, f.y, f.z, f.w};
+            for (int a = 0; a < 4; ++a)
+                for (int b = 0; b < 4; ++b) hinge_slot[16 * h + 4 * a + b] = find_slot(row_ptr, col, v[a], v[b]);
+        }
+    }
+}
+
+// the vertex term w I on the diagonal blocks (kval zeroed before)
+__global__ void k_diag_term(const float *wk, const int *diag_slot, int np, float4 *kval)
+{
+    PAMO_GRID_STRIDE(i, np)
+    {
+        const float w = wk[i];
+        const size_t s = 3 * (size_t)diag_slot[i];
+        kval[s] = make_float4(w, 0.f, 0.f, 0.f);
+        kval[s + 1] = make_float4(0.f, w, 0.f, 0.f);
+        kval[s + 2] = make_float4(0.f, 0.f, w, 0.f);
+    }
 }
 
 // -------------------------------------------------------------------- CG
@@ -907,21 +1089,12 @@ __global__ void __launch_bounds__(kThreads) k_cg_dot(const float4 *a, const floa
     if (last_block_sum(s, partials, ticket, dscal + D_VAV) && threadIdx.x == 0) dscal[D_ZR_LAST] = dscal[D_ZR];
 }
 
-// start of a CG iteration: v = z + beta v (not in the first), Av = w v (the
-// vertex term of the Hessian; the element terms are added by k_hess_elements)
-__global__ void k_cg_pre(const float4 *z, const double *dscal, const float *wk, int np, int first, float4 *v,
-                         float4 *Av)
+// start of a CG iteration: v = z + beta v (not in the first)
+__global__ void k_cg_pre(const float4 *z, const double *dscal, int np, int first, float4 *v)
 {
-    const float beta = first ? 0.f : (float)(dscal[D_ZR] / dscal[D_ZR_LAST]);
-    PAMO_GRID_STRIDE(i, np)
-    {
-        F3 vv = ld(v, (int)i);
-        if (!first) {
-            vv = ld(z, (int)i) + beta * vv;
-            st(v, (int)i, vv);
-        }
-        st(Av, (int)i, wk[i] * vv);
-    }
+    if (first) return;
+    const float beta = (float)(dscal[D_ZR] / dscal[D_ZR_LAST]);
+    PAMO_GRID_STRIDE(i, np) st(v, (int)i, ld(z, (int)i) + beta * ld(v, (int)i));
 }
 
 // p += alpha v, r -= alpha Av (if v^T A v > 1e-16); z = r / diag; partial z.r
@@ -954,41 +1127,43 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const f
 // cg_solver.py:96-158) in one cooperative launch, one block per SM and two
 // grid-wide sums per iteration:
 //   (B) the new direction v = z + beta v is formed where it is read -- every
-//       element computes it for its own vertices from z and the last direction
-//       (both final since the previous sum), and each vertex's owner stores it
-//       into the other direction buffer -- while the element terms of A v are
-//       added into Av (zeroed by the owner in the previous pass) and v . A v is
-//       gathered (each element's outputs dotted with its own vertices' v, plus
-//       the vertex term w |v|^2);
-//   (D) p += alpha v, r -= alpha (Av + w v), z = r / diag, Av = 0, and z . r.
+//       row and contact block computes it for its own vertices from z and the
+//       last direction (both final since the previous sum), and each row's
+//       owner stores it into the other direction buffer -- while the rows of
+//       K v go to Av, the contact terms are added into Avc (zeroed by the owner
+//       in the previous pass), and v . A v is gathered;
+//   (D) p += alpha v, r -= alpha (Av + Avc), z = r / diag, Avc = 0, and z . r.
 // A sum ends in a grid barrier whose last arriving block adds the per-block
-// partials in block order and publishes the total before releasing the
-// others, so the sums do not depend on scheduling and every block reads one
-// value.  The barrier spins with a limit; on timeout it records the error and
-// the kernel returns.
+// partials in block order and publishes the total, so the sums do not depend
+// on scheduling.  The total itself is the release: sum k goes to slot k % 2,
+// which holds an all-ones bit pattern until then (a negative NaN that no sum
+// produces: sums and products give the positive canonical NaN), so a waiting
+// block reads the value in the load that sees the release.  The last block of
+// sum k resets slot (k - 1) % 2, which every block read before arriving.  The
+// wait spins with a limit; on timeout it records the error and the kernel
+// returns.
 constexpr int kCgThreads = 512;
+constexpr unsigned long long kSumPending = ~0ull;
 
 struct CGArgs {
-    HArgs h;
+    OpArgs op;
     const float4 *grad, *diag;
-    const float *wk;
-    float4 *p, *r, *z, *v0, *v1, *Av;
-    double *partials;  // one per block
-    double *red;       // the published total
+    float4 *p, *r, *z, *v0, *v1, *Av, *Avc;
+    double *partials;         // one per block
+    unsigned long long *red;  // two slots for the published totals (all ones before the solve)
     int *iscal;
     int np, n_iters;
 };
 
 // Block sum of `acc`, then the grid-wide total (see above).  Returns false on
 // a barrier timeout.
-__device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, double &total)
+__device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, int k, double &total)
 {
-    __shared__ int s_last, s_gen, s_ok;
+    __shared__ int s_last, s_ok;
     __shared__ double s_val;
     const double bs = block_sum<kCgThreads>(acc);
     if (threadIdx.x == 0) {
         A.partials[blockIdx.x] = bs;
-        s_gen = *(volatile int *)(A.iscal + I_BAR_GEN);
         s_ok = 1;
         __threadfence();
         s_last = atomicAdd(A.iscal + I_BAR_COUNT, 1) == (int)gridDim.x - 1;
@@ -1002,24 +1177,26 @@ __device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, double &to
             for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
             if (threadIdx.x == 0) {
                 s_val = v;
-                *A.red = v;
                 A.iscal[I_BAR_COUNT] = 0;
+                A.red[(k + 1) & 1] = kSumPending;
                 __threadfence();
-                atomicAdd(A.iscal + I_BAR_GEN, 1);
+                *(volatile unsigned long long *)(A.red + (k & 1)) = (unsigned long long)__double_as_longlong(v);
             }
         }
     } else if (threadIdx.x == 0) {
-        volatile int *vgen = A.iscal + I_BAR_GEN;
-        for (long long spins = 0; *vgen == s_gen; ++spins) {
+        volatile unsigned long long *slot = A.red + (k & 1);
+        unsigned long long bits = *slot;
+        for (long long spins = 0; bits == kSumPending; ++spins) {
             if (spins > (1LL << 24)) {  // ~ seconds: a block never arrived
                 atomicExch(A.iscal + I_BAR_ERR, 1);
                 s_ok = 0;
                 break;
             }
             __nanosleep(32);
+            bits = *slot;
         }
         __threadfence();
-        s_val = __ldcg(A.red);
+        s_val = __longlong_as_double((long long)bits);
     }
     __syncthreads();
     total = s_val;
@@ -1030,19 +1207,20 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
 {
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long gs = (long long)blockDim.x * gridDim.x;
-    // r = g, z = g / (diag + 1e-6), p = 0, Av = 0
+    // r = g, z = g / (diag + 1e-6), p = 0, Avc = 0
     double acc = 0.0;
     for (long long i = t0; i < A.np; i += gs) {
         F3 g = ld(A.grad, (int)i), d = ld(A.diag, (int)i);
         F3 zz = mk(g.x / (d.x + 1e-6f), g.y / (d.y + 1e-6f), g.z / (d.z + 1e-6f));
         A.p[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        A.Av[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        A.Avc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         st(A.r, (int)i, g);
         st(A.z, (int)i, zz);
         acc += (double)dot(zz, g);
     }
     double zr, zr_last, vav;
-    if (!grid_sum(acc, A, zr)) return;
+    int nsum = 0;
+    if (!grid_sum(acc, A, nsum++, zr)) return;
     zr_last = zr;
     for (int it = 0; it < A.n_iters; ++it) {
         const float beta = it == 0 ? 0.f : (float)(zr / zr_last);
@@ -1054,13 +1232,14 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
             return ld(z, j) + beta * ld(vo, j);
         };
         acc = 0.0;
-        for (long long i = t0; i < A.np; i += gs) {
-            const F3 vv = dir((int)i);
-            st(vn, (int)i, vv);
-            acc += (double)dot(vv, A.wk[i] * vv);
-        }
-        acc += hess_elements_range(A.h, t0, gs, dir);
-        if (!grid_sum(acc, A, vav)) return;
+        op_rows(A.op, t0 >> 5, gs >> 5, dir, [&](int i, F3 kv) {
+            const F3 vv = dir(i);
+            st(vn, i, vv);
+            st(A.Av, i, kv);
+            acc += (double)dot(vv, kv);
+        });
+        acc += op_contacts(A.op, t0, gs, dir, A.Avc);
+        if (!grid_sum(acc, A, nsum++, vav)) return;
         zr_last = zr;
         const bool upd = vav > 1e-16;
         const float alpha = upd ? (float)(zr_last / vav) : 0.f;
@@ -1068,18 +1247,17 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
         for (long long i = t0; i < A.np; i += gs) {
             F3 rr = ld(A.r, (int)i);
             if (upd) {
-                const F3 vv = ld(vn, (int)i);
-                st(A.p, (int)i, ld(A.p, (int)i) + alpha * vv);
-                rr = rr - alpha * (ld(A.Av, (int)i) + A.wk[i] * vv);
+                st(A.p, (int)i, ld(A.p, (int)i) + alpha * ld(vn, (int)i));
+                rr = rr - alpha * (ld(A.Av, (int)i) + ld(A.Avc, (int)i));
                 st(A.r, (int)i, rr);
             }
-            A.Av[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            A.Avc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             F3 d = ld(A.diag, (int)i);
             F3 zz = mk(rr.x / d.x, rr.y / d.y, rr.z / d.z);
             st(A.z, (int)i, zz);
             acc += (double)dot(zz, rr);
         }
-        if (!grid_sum(acc, A, zr)) return;
+        if (!grid_sum(acc, A, nsum++, zr)) return;
     }
 }
 
@@ -1123,6 +1301,9 @@ __global__ void __launch_bounds__(128) k_accd(const float4 *q, const float4 *pv,
         double dmt = fmax((d * d - th * th) / (sqrt(d * d) + th), 0.0);
         const double gap = (1.0 - slack) * dmt;
         double t = 0.0, tl = slack * dmt / lv;
+        // The first pass never records (it > 0 is needed, or max_iters == 0) and
+        // leaves with t = tl when tl > 1, so its distance evaluation is skipped.
+        if (max_iters > 0 && tl > 1.0) continue;
         for (int it = 0;; ++it) {
             for (int a = 0; a < 4; ++a) x[a] = x[a] + tl * v[a];
             ty = classify(kind, x, (double)ee_thres);
@@ -1186,8 +1367,9 @@ __global__ void k_f4_to_aos(const float4 *in, float *out, int n)
 
 void Stage3::release()
 {
-    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, v2, Av, q_gather, wk, tris, area, inv_dm, mcache, edges4, hinges,
-                    rest_angle, rest_elen, hblk, bidx, bkind, bsub, bd, bb2, bg, bact, gt_pts, gt_tris, dscal, fscal,
+    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, v2, Av, Avc, q_gather, wk, tris, area, inv_dm,
+                    edges4, hinges, rest_angle, rest_elen, row_ptr, col, kval, tri_slot, hinge_slot, diag_slot, pat_cnt,
+                    pat_cur, pat_off, pat_cand, pat_scan, bidx, bkind, bsub, bd, bb2, bg, bact, gt_pts, gt_tris, dscal, fscal,
                     iscal, partials};
     drop_graph();
     if (cand_pt) cudaFree(cand_pt);
@@ -1203,10 +1385,14 @@ void Stage3::release()
         if (x) cudaFree(x);
     if (h_iscal) cudaFreeHost(h_iscal);
     if (h_dscal) cudaFreeHost(h_dscal);
-    q = q_prev = q_det = p = grad = diag = target = r = z = v = v2 = Av = q_gather = nullptr;
+    q = q_prev = q_det = p = grad = diag = target = r = z = v = v2 = Av = Avc = q_gather = nullptr;
+    row_ptr = col = tri_slot = hinge_slot = diag_slot = nullptr;
+    pat_cnt = pat_cur = pat_off = pat_cand = pat_scan = nullptr;
+    kval = nullptr;
+    nnz = cap_nnz = cap_cand = 0;
     gathered = false;
-    wk = nullptr; tris = nullptr; area = nullptr; inv_dm = nullptr; mcache = nullptr; edges4 = nullptr; hinges = nullptr;
-    rest_angle = rest_elen = hblk = nullptr; bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr;
+    wk = nullptr; tris = nullptr; area = nullptr; inv_dm = nullptr; edges4 = nullptr; hinges = nullptr;
+    rest_angle = rest_elen = nullptr; bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr;
     bg = nullptr; bact = nullptr; gt_pts = nullptr; gt_tris = nullptr; dscal = nullptr; fscal = nullptr; iscal = nullptr;
     partials = nullptr; h_iscal = nullptr; h_dscal = nullptr;
     tri_bvh.release();
@@ -1233,12 +1419,14 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
         }                                                                \
     } while (0)
     A3(q, cp * 16); A3(q_prev, cp * 16); A3(q_det, cp * 16); A3(p, cp * 16); A3(grad, cp * 16);
-    A3(diag, cp * 16); A3(target, cp * 16); A3(r, cp * 16); A3(z, cp * 16); A3(v, cp * 16); A3(v2, cp * 16); A3(Av, cp * 16);
+    A3(diag, cp * 16); A3(target, cp * 16); A3(r, cp * 16); A3(z, cp * 16); A3(v, cp * 16); A3(v2, cp * 16); A3(Av, cp * 16); A3(Avc, cp * 16);
     A3(q_gather, cp * 16);
     A3(wk, cp * 4);
-    A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16); A3(mcache, ct * 64);
+    A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16); A3(tri_slot, ct * 36);
     A3(edges4, ce * 16);
-    A3(hinges, ch * 16); A3(rest_angle, ch * 4); A3(rest_elen, ch * 4); A3(hblk, ch * 144 * 4);
+    A3(hinges, ch * 16); A3(rest_angle, ch * 4); A3(rest_elen, ch * 4); A3(hinge_slot, ch * 64);
+    A3(row_ptr, (cp + 1) * 4); A3(diag_slot, cp * 4); A3(pat_cnt, (cp + 1) * 4); A3(pat_cur, cp * 4);
+    A3(pat_off, (cp + 1) * 4); A3(pat_scan, scan_scratch_ints(cp + 1) * 4);
     A3(gt_pts, cgp * 16); A3(gt_tris, cgt * 16);
     A3(dscal, 64); A3(fscal, 64); A3(iscal, 64);
     A3(partials, 2 * kRedBlocks * 8);  // two buffers for the persistent solve
@@ -1313,6 +1501,50 @@ int Stage3::register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, in
     S3_TRY(lbvh_build(edge_bvh, q, edges4, ne, s));
     S3_TRY(cudaMemsetAsync(iscal, 0, 64, s));
     S3_TRY(cudaMemsetAsync(dscal, 0, 64, s));
+    if ((rc = build_pattern(s))) return rc;
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+int Stage3::build_pattern(cudaStream_t s)
+{
+    const long long cand_n = (long long)np + 6LL * nt + 12LL * nh;
+    if (cand_n > cap_cand || !pat_cand) {
+        if (pat_cand) cudaFree(pat_cand);
+        pat_cand = nullptr;
+        cap_cand = 0;
+        if (cudaMalloc((void **)&pat_cand, (size_t)cand_n * 4) != cudaSuccess) return PAMO_ERR_OOM;
+        cap_cand = cand_n;
+    }
+    launch(k_fill_int, grid_for(np), kThreads, 0, s, pat_cnt, (long long)np, 1);  // the diagonal
+    S3_TRY(cudaMemsetAsync(pat_cnt + np, 0, 4, s));
+    launch(k_pat_count, grid_for((long long)nt + nh), kThreads, 0, s, (const int4 *)tris, nt, (const int4 *)hinges, nh,
+           pat_cnt);
+    S3_TRY(exclusive_scan(pat_cnt, pat_off, (long long)np + 1, nullptr, pat_scan, nullptr, s));
+    S3_TRY(cudaMemsetAsync(pat_cur, 0, (size_t)np * 4, s));
+    launch(k_pat_fill, grid_for((long long)np + nt + nh), kThreads, 0, s, (const int4 *)tris, nt, (const int4 *)hinges,
+           nh, np, (const int *)pat_off, pat_cur, pat_cand);
+    launch(k_pat_sort, grid_for(np), kThreads, 0, s, (const int *)pat_off, np, pat_cand, pat_cnt);
+    S3_TRY(exclusive_scan(pat_cnt, row_ptr, (long long)np + 1, nullptr, pat_scan, nullptr, s));
+    S3_TRY(cudaMemcpyAsync(h_iscal + 15, row_ptr + np, 4, cudaMemcpyDeviceToHost, s));
+    S3_TRY(cudaStreamSynchronize(s));
+    nnz = h_iscal[15];
+    if (nnz <= 0 || nnz > cand_n) return PAMO_ERR_DEVICE;
+    if (nnz > cap_nnz || !kval) {
+        if (col) cudaFree(col);
+        if (kval) cudaFree(kval);
+        col = nullptr;
+        kval = nullptr;
+        cap_nnz = 0;
+        const long long c = nnz + nnz / 8 + 64;
+        if (cudaMalloc((void **)&col, (size_t)c * 4) != cudaSuccess ||
+            cudaMalloc((void **)&kval, (size_t)c * 48) != cudaSuccess)
+            return PAMO_ERR_OOM;
+        cap_nnz = c;
+    }
+    launch(k_pat_emit, grid_for(np), kThreads, 0, s, (const int *)pat_off, (const int *)row_ptr,
+           (const int *)pat_cand, np, col);
+    launch(k_pat_slots, grid_for((long long)np + nt + nh), kThreads, 0, s, (const int4 *)tris, nt,
+           (const int4 *)hinges, nh, np, (const int *)row_ptr, (const int *)col, tri_slot, hinge_slot, diag_slot);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
@@ -1396,17 +1628,6 @@ static int energy_pass(Stage3 &S, cudaStream_t s, int n_halves = -1)
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
-static int hess_elements(Stage3 &S, const float4 *dx, float4 *out, cudaStream_t s)
-{
-    HArgs h{S.q, S.wk, S.np, S.nt, S.nh, S.tris, S.area, S.inv_dm,
-            S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
-            S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
-                ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
-            S.hinges, S.hblk, S.bidx, S.bg, S.bb2, S.iscal, S.cap_b, dx, out, S.bact, S.mcache};
-    launch(k_hess_elements, grid_for((long long)S.nt + 4LL * S.nh + S.cap_b), kThreads, 0, s, h);
-    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
-}
-
 void Stage3::drop_graph()
 {
     if (graph) cudaGraphExecDestroy(graph);
@@ -1474,8 +1695,11 @@ int Stage3::newton_body(cudaStream_t s)
     DArgs d{q, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
             cfg.elas_young_modulus * cfg.elas_poisson_ratio /
                 ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
-            hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, hblk, bidx, bkind, bsub, bd, bg, bb2,
-            iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag, bact, mcache};
+            hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, kval, tri_slot, hinge_slot, bidx,
+            bkind, bsub, bd, bg, bb2, iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag, bact};
+    // the Hessian's values: zero, the vertex term, then the elements (k_diff_elements)
+    S3_TRY(cudaMemsetAsync(kval, 0, (size_t)nnz * 48, s));
+    launch(k_diag_term, grid_for(np), kThreads, 0, s, (const float *)wk, (const int *)diag_slot, np, kval);
     S3_TRY(cudaMemsetAsync(iscal + I_NACT, 0, sizeof(int), s));
     launch(k_diff_elements, grid_for((long long)nt + nh + cap_b, 128), 128, 0, s, d);
     // Jacobi-preconditioned CG (cg_solver.py:96-158)
@@ -1490,14 +1714,14 @@ int Stage3::newton_body(cudaStream_t s)
         cg_blocks = sms < kRedBlocks ? sms : kRedBlocks;  // one block per SM, all resident
         cudaGetLastError();
     }
+    const OpArgs op{np, row_ptr, col, kval, bidx, bg, bb2, bact, iscal, cap_b};
     if (cg_persistent == 1) {
-        HArgs h{q, wk, np, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
-                cfg.elas_young_modulus * cfg.elas_poisson_ratio /
-                    ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
-                hinges, hblk, bidx, bg, bb2, iscal, cap_b, nullptr, Av, bact, mcache};
-        // partials: 2 x kRedBlocks doubles; the solve uses the first cg_blocks and publishes at kRedBlocks
-        CGArgs ca{h, grad, diag, wk, p, r, z, v, v2, Av, partials, partials + kRedBlocks, iscal, np, cfg.n_cg_iters};
+        // partials: 2 x kRedBlocks doubles; the solve uses the first cg_blocks, and
+        // the two published-total slots sit at kRedBlocks
+        unsigned long long *slots = reinterpret_cast<unsigned long long *>(partials + kRedBlocks);
+        CGArgs ca{op, grad, diag, p, r, z, v, v2, Av, Avc, partials, slots, iscal, np, cfg.n_cg_iters};
         S3_TRY(cudaMemsetAsync(iscal + I_BAR_COUNT, 0, sizeof(int), s));
+        S3_TRY(cudaMemsetAsync(slots, 0xFF, 2 * sizeof(unsigned long long), s));  // kSumPending
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(cg_blocks);
         lc.blockDim = dim3(kCgThreads);
@@ -1514,9 +1738,9 @@ int Stage3::newton_body(cudaStream_t s)
     int *ticket = iscal + I_TICKET;
     launch(k_cg_init, kRedBlocks, kThreads, 0, s, grad, diag, np, p, r, z, v, partials, ticket, dscal);
     for (int it = 0; it < cfg.n_cg_iters; ++it) {
-        launch(k_cg_pre, grid_for(np), kThreads, 0, s, (const float4 *)z, (const double *)dscal, (const float *)wk, np,
-               it == 0 ? 1 : 0, v, Av);
-        if ((rc = hess_elements(*this, v, Av, s))) return rc;
+        launch(k_cg_pre, grid_for(np), kThreads, 0, s, (const float4 *)z, (const double *)dscal, np, it == 0 ? 1 : 0, v);
+        launch(k_op_rows, grid_for(4LL * np), kThreads, 0, s, op, (const float4 *)v, Av);
+        launch(k_op_contacts, grid_for(cap_b), kThreads, 0, s, op, (const float4 *)v, Av);
         launch(k_cg_dot, kRedBlocks, kThreads, 0, s, (const float4 *)v, (const float4 *)Av, np, partials, ticket, dscal);
         launch(k_cg_update, kRedBlocks, kThreads, 0, s, (const float4 *)v, (const float4 *)Av, (const float4 *)diag, dscal,
                np, p, r, z, partials, ticket);

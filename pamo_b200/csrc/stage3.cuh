@@ -32,11 +32,23 @@ struct Stage3 {
     int4 *tris = nullptr;
     float *area = nullptr;
     float4 *inv_dm = nullptr;  // 2x2 row-major
-    float4 *mcache = nullptr;  // 4 per triangle: frame, F, S at the current Newton iteration
     int4 *edges4 = nullptr;    // (a, b, b, 0): a segment as a degenerate triangle for the LBVH
     int4 *hinges = nullptr;
     float *rest_angle = nullptr, *rest_elen = nullptr;
-    float *hblk = nullptr;  // 16 3x3 blocks per hinge (SPD-projected)
+    // The Hessian as 3x3 blocks in rows of vertices (BSR).  The pattern -- the
+    // diagonal, the mesh edges and the hinges' four-vertex couplings -- is fixed
+    // for a registered mesh; the values are assembled once per Newton iteration
+    // (vertex term, membrane, SPD-projected hinges).  The contact terms stay
+    // matrix-free (rank one per active block).
+    int *row_ptr = nullptr;     // [np + 1]
+    int *col = nullptr;         // [nnz], ascending in each row
+    float4 *kval = nullptr;     // [3 nnz]: the rows of each block (w unused)
+    int *tri_slot = nullptr;    // [9 nt]: block (a, b) of triangle t at 9 t + 3 a + b
+    int *hinge_slot = nullptr;  // [16 nh]: block (a, b) of hinge h at 16 h + 4 a + b
+    int *diag_slot = nullptr;   // [np]
+    int *pat_cnt = nullptr, *pat_cur = nullptr, *pat_off = nullptr, *pat_cand = nullptr, *pat_scan = nullptr;
+    long long nnz = 0, cap_nnz = 0, cap_cand = 0;
+    float4 *Avc = nullptr;      // contact terms of A v (the persistent solve)
     // contact blocks
     int4 *bidx = nullptr;
     int *bkind = nullptr, *bsub = nullptr;
@@ -71,6 +83,7 @@ struct Stage3 {
     int ensure(long long np_, long long nt_, long long ne_, long long nh_, long long ngp_, long long ngt_);
     int ensure_blocks(long long nb);
     int ensure_cands(long long n);
+    int build_pattern(cudaStream_t s);
     void release();
 
     // Inputs are device arrays in the normalised frame.
