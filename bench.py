@@ -235,7 +235,7 @@ def roofline_edge_cost(phases, round_faces, peaks):
     (int4) 16 B/face, points (float4) 16 B/vertex, quadrics 48 B/vertex,
     invalid flags 1 B/vertex, per-vertex key minimum read+write 16 B/vertex:
     12 E + 85 V + 28 F = 88.5 B/face.  Traffic: DRAM bytes per face of the
-    round-0 launch on config 2 (ncu, profiles/k_edge_cost_c2_round0.txt),
+    round-0 launch on config 2 (ncu, profiles/stage2_kernels_c2_round0.txt),
     times the average faces per launch."""
     ph = phases.get("edge_cost")
     if not ph or not ph["ms"] or not round_faces:
@@ -253,10 +253,39 @@ def roofline_edge_cost(phases, round_faces, peaks):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs") else "fallback"}
 
 
-# DRAM read + write of k_edge_cost per input face of the launch, from an ncu
-# capture of round 0 of config 2 (2,097,152 faces: 915.6 MB read + 60.0 MB
-# written); profiles/stage2_kernels_c2_round0.txt.
-EDGE_COST_DRAM_BYTES_PER_FACE = 465.2
+# DRAM read + write of k_edge_cost and k_query per input face of the launch,
+# from an ncu capture of round 0 of config 2 (2,097,152 faces): edge cost
+# 904.0 MB read + 57.0 MB written, query 254.9 MB read + 22.5 MB written;
+# profiles/stage2_kernels_c2_round0.txt.
+EDGE_COST_DRAM_BYTES_PER_FACE = 458.2
+QUERY_DRAM_BYTES_PER_FACE = 132.3
+
+
+def roofline_query(phases, round_faces, peaks):
+    """HBM roofline of the hierarchy query (k_query, the step's largest kernel
+    by device time; one launch per pass, the first pass of a round queries
+    every face whose one-ring changed).
+
+    Algorithmic bytes per pass over a round with F faces (L <= F leaves, V =
+    0.5 F), every array read or written once: inner nodes 64 B and leaf map
+    4 B per leaf, faces 16 B, active flags 1 B and query list 4 B per face,
+    points 16 B per vertex = 97 B/face, counted for the round's first pass
+    only (the undo passes query a few faces) and as if every face queried (about
+    85% do); candidate pairs (8 B each) are left out.  The phase time also
+    holds the active-list kernel, so `achieved` is a lower bound."""
+    ph = phases.get("query")
+    if not ph or not ph["ms"] or not round_faces:
+        return None
+    total_bytes = sum(97.0 * f for f in round_faces)
+    t = ph["ms"] / 1e3
+    achieved = total_bytes / t / 1e9
+    peak = peaks.get("hbm_gbs") or 6650.0
+    avg_faces = sum(round_faces) / max(len(round_faces), 1)
+    return {"bound": "hbm", "kernel": "k_query", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": QUERY_DRAM_BYTES_PER_FACE * avg_faces,
+            "launches": ph["calls"], "avg_launch_ms": ph["ms"] / max(ph["calls"], 1),
+            "bytes_per_launch_avg": total_bytes / max(len(round_faces), 1),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs") else "fallback"}
 
 
 def count_intersections(ctx, V, F, dev):
@@ -405,7 +434,8 @@ def product_arm(args):
             "cpu_baseline": cpu,
             "intersections": intersections,
             "phases_ms": {k: round(v["ms"], 3) for k, v in phases.items()},
-            "roofline": roofline_edge_cost(phases, round_faces, peaks),
+            "roofline": roofline_query(phases, round_faces, peaks),
+            "roofline_edge_cost": roofline_edge_cost(phases, round_faces, peaks),
             "round_faces": round_faces if args.dump_rounds else None,
         }
         print(json.dumps(line))
