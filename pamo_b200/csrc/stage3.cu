@@ -578,64 +578,6 @@ __device__ void hinge_blocks(F3 x0, F3 x1, F3 x2, F3 x3, float rest_angle, float
     }
 }
 
-// Eigenvalue clamp of the symmetric part of the 9x9 matrix of hinge vertices 0-2
-// (cyclic Jacobi, `sweeps` sweeps), then vertex 3's rows and columns from
-// translation invariance.
-__device__ void spd_project(float B[16][9], int sweeps)
-{
-    float A[9][9], V[9][9];
-    for (int bi = 0; bi < 3; ++bi)
-        for (int bj = 0; bj < 3; ++bj)
-            for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 3; ++c) A[bi * 3 + r][bj * 3 + c] = B[bi * 4 + bj][r * 3 + c];
-    for (int i = 0; i < 9; ++i)
-        for (int j = i + 1; j < 9; ++j) {
-            float s = 0.5f * (A[i][j] + A[j][i]);
-            A[i][j] = A[j][i] = s;
-        }
-    for (int i = 0; i < 9; ++i)
-        for (int j = 0; j < 9; ++j) V[i][j] = i == j ? 1.f : 0.f;
-    for (int sw = 0; sw < sweeps; ++sw)
-        for (int p = 0; p < 8; ++p)
-            for (int qq = p + 1; qq < 9; ++qq) {
-                float apq = A[p][qq];
-                if (!(fabsf(apq) > 1e-30f)) continue;
-                float theta = (A[qq][qq] - A[p][p]) / (2.f * apq);
-                float sg = theta >= 0.f ? 1.f : -1.f;
-                float t = sg / (fabsf(theta) + sqrtf(theta * theta + 1.f));
-                float c = 1.f / sqrtf(t * t + 1.f), s = t * c;
-                for (int k = 0; k < 9; ++k) {  // A <- A J
-                    float akp = A[k][p], akq = A[k][qq];
-                    A[k][p] = c * akp - s * akq;
-                    A[k][qq] = s * akp + c * akq;
-                }
-                for (int k = 0; k < 9; ++k) {  // A <- J^T A
-                    float apk = A[p][k], aqk = A[qq][k];
-                    A[p][k] = c * apk - s * aqk;
-                    A[qq][k] = s * apk + c * aqk;
-                }
-                for (int k = 0; k < 9; ++k) {  // V <- V J
-                    float vkp = V[k][p], vkq = V[k][qq];
-                    V[k][p] = c * vkp - s * vkq;
-                    V[k][qq] = s * vkp + c * vkq;
-                }
-            }
-    float lam[9];
-    for (int i = 0; i < 9; ++i) lam[i] = fmaxf(A[i][i], 0.f);
-    for (int i = 0; i < 9; ++i)
-        for (int j = 0; j < 9; ++j) {
-            float s = 0.f;
-            for (int k = 0; k < 9; ++k) s += V[i][k] * lam[k] * V[j][k];
-            B[(i / 3) * 4 + (j / 3)][(i % 3) * 3 + (j % 3)] = s;
-        }
-    for (int j = 0; j < 3; ++j)
-        for (int e = 0; e < 9; ++e) B[12 + j][e] = -(B[0 + j][e] + B[4 + j][e] + B[8 + j][e]);
-    for (int j = 0; j < 3; ++j)
-        for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c) B[j * 4 + 3][r * 3 + c] = B[12 + j][c * 3 + r];
-    for (int e = 0; e < 9; ++e) B[15][e] = -(B[3][e] + B[7][e] + B[11][e]);
-}
-
 struct DArgs {
     const float4 *q;
     int nt, nh;
@@ -649,6 +591,7 @@ struct DArgs {
     int spd_iters;
     float4 *kval;
     const int *tri_slot, *hinge_slot;
+    float *hblk;  // the unprojected hinge blocks, for k_hinge_spd
     const int4 *bidx;
     const int *bkind, *bsub;
     const float *bd;
@@ -765,9 +708,10 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
                 // diagonal of the unprojected block, as the reference adds it before projecting
                 atomic_add3(A.diag, idx[a], mk(B[a * 5][0], B[a * 5][4], B[a * 5][8]));
             }
-            spd_project(B, A.spd_iters);
-            const int *slot = A.hinge_slot + 16 * (size_t)h;
-            for (int b = 0; b < 16; ++b) add_block(A.kval, slot[b], B[b]);
+            float *dst = A.hblk + (size_t)h * 81;  // vertices 0-2: projected and assembled by k_hinge_spd
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int e = 0; e < 9; ++e) dst[(a * 3 + b) * 9 + e] = B[a * 4 + b][e];
         } else {
             int b = (int)(k - A.nt - A.nh);
             float d = A.bd[b];
@@ -795,6 +739,122 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
             A.bact[grp.shfl(base, 0) + (int)grp.thread_rank()] = b;
         }
     }
+}
+
+// The SPD projection of the hinge blocks (block_spd_project_kernel,
+// kernels/utils_kernels.py:20-39: the fork-only wp.spd_project_blocks(3, B, 3),
+// read as an eigenvalue clamp): `sweeps` cyclic Jacobi sweeps
+// on the symmetric part of the 9 x 9 matrix of hinge vertices 0-2, negative
+// eigenvalues set to zero, then vertex 3's rows and columns refilled by
+// translation invariance.  One thread per hinge with every rotation unrolled,
+// so A and V live in registers (a rolled loop indexes them at run time, which
+// puts them in local memory).  The projected blocks are added into the
+// assembled Hessian.
+__global__ void __launch_bounds__(64) k_hinge_spd(const float *hblk, int nh, int sweeps, const int *hinge_slot,
+                                                  float4 *kval)
+{
+    const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    const float *src = hblk + (size_t)h * 81;  // blocks (a, b), a, b < 3, row-major
+    float A[9][9], V[9][9];
+#pragma unroll
+    for (int bi = 0; bi < 3; ++bi)
+#pragma unroll
+        for (int bj = 0; bj < 3; ++bj)
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) A[bi * 3 + r][bj * 3 + c] = src[(bi * 3 + bj) * 9 + r * 3 + c];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+#pragma unroll
+        for (int j = i + 1; j < 9; ++j) {
+            float s = 0.5f * (A[i][j] + A[j][i]);
+            A[i][j] = A[j][i] = s;
+        }
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+#pragma unroll
+        for (int j = 0; j < 9; ++j) V[i][j] = i == j ? 1.f : 0.f;
+    for (int sw = 0; sw < sweeps; ++sw) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+#pragma unroll
+            for (int qq = p + 1; qq < 9; ++qq) {
+                float apq = A[p][qq];
+                if (fabsf(apq) > 1e-30f) {
+                    float theta = (A[qq][qq] - A[p][p]) / (2.f * apq);
+                    float sg = theta >= 0.f ? 1.f : -1.f;
+                    float t = sg / (fabsf(theta) + sqrtf(theta * theta + 1.f));
+                    float c = 1.f / sqrtf(t * t + 1.f), s = t * c;
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) {  // A <- A J
+                        float akp = A[k][p], akq = A[k][qq];
+                        A[k][p] = c * akp - s * akq;
+                        A[k][qq] = s * akp + c * akq;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) {  // A <- J^T A
+                        float apk = A[p][k], aqk = A[qq][k];
+                        A[p][k] = c * apk - s * aqk;
+                        A[qq][k] = s * apk + c * aqk;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) {  // V <- V J
+                        float vkp = V[k][p], vkq = V[k][qq];
+                        V[k][p] = c * vkp - s * vkq;
+                        V[k][qq] = s * vkp + c * vkq;
+                    }
+                }
+            }
+    }
+    float lam[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) lam[i] = fmaxf(A[i][i], 0.f);
+    // S = V diag(lam) V^T, into A
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) s += V[i][k] * lam[k] * V[j][k];
+            A[i][j] = s;
+        }
+    const int *sl = hinge_slot + 16 * (size_t)h;
+    float blk[9], b3[3][9];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) blk[r * 3 + c] = A[a * 3 + r][b * 3 + c];
+            add_block(kval, sl[a * 4 + b], blk);
+        }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)  // block (3, j) = -(blocks (0, j) + (1, j) + (2, j))
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                b3[j][r * 3 + c] = -(A[0 + r][j * 3 + c] + A[3 + r][j * 3 + c] + A[6 + r][j * 3 + c]);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        add_block(kval, sl[12 + j], b3[j]);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)  // block (j, 3) = block (3, j)^T
+#pragma unroll
+            for (int c = 0; c < 3; ++c) blk[r * 3 + c] = b3[j][c * 3 + r];
+        add_block(kval, sl[j * 4 + 3], blk);
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {  // block (3, 3) = -(blocks (0, 3) + (1, 3) + (2, 3)), block (j, 3) = (3, j)^T
+        const int r = e / 3, c = e % 3;
+        blk[e] = -(b3[0][c * 3 + r] + b3[1][c * 3 + r] + b3[2][c * 3 + r]);
+    }
+    add_block(kval, sl[15], blk);
 }
 
 // ---------------------------------------------------------------- A * dx
@@ -863,10 +923,10 @@ __device__ __forceinline__ void op_rows(const OpArgs &A, long long warp0, long l
 // The contact terms c (g . dx) g of blocks [first, ...), added into out with
 // atomics; returns this thread's share of dx . (their sum).
 template <class LDX>
-__device__ __forceinline__ double op_contacts(const OpArgs &A, long long first, long long stride, LDX ldx, float4 *out)
+__device__ __forceinline__ double op_contacts(const OpArgs &A, long long first, long long stride, LDX ldx, float4 *out,
+                                              long long nb)
 {
     double dxh = 0.0;
-    const long long nb = min((long long)A.iscal[I_NACT], A.cap_b);
     for (long long k = first; k < nb; k += stride) {
         const int b = A.bact[k];
         const float c = A.bb2[b];
@@ -896,7 +956,7 @@ __global__ void __launch_bounds__(kThreads) k_op_rows(OpArgs A, const float4 *dx
 __global__ void __launch_bounds__(kThreads) k_op_contacts(OpArgs A, const float4 *dx, float4 *out)
 {
     op_contacts(A, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)blockDim.x * gridDim.x,
-                [&](int j) { return ld(dx, j); }, out);
+                [&](int j) { return ld(dx, j); }, out, min((long long)A.iscal[I_NACT], A.cap_b));
 }
 
 // ------------------------------------------------------- the block pattern
@@ -1133,15 +1193,22 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const f
 //       K v go to Av, the contact terms are added into Avc (zeroed by the owner
 //       in the previous pass), and v . A v is gathered;
 //   (D) p += alpha v, r -= alpha (Av + Avc), z = r / diag, Avc = 0, and z . r.
-// A sum ends in a grid barrier whose last arriving block adds the per-block
-// partials in block order and publishes the total, so the sums do not depend
-// on scheduling.  The total itself is the release: sum k goes to slot k % 2,
-// which holds an all-ones bit pattern until then (a negative NaN that no sum
-// produces: sums and products give the positive canonical NaN), so a waiting
-// block reads the value in the load that sees the release.  The last block of
-// sum k resets slot (k - 1) % 2, which every block read before arriving.  The
-// wait spins with a limit; on timeout it records the error and the kernel
-// returns.
+// The time of an iteration is the length of its chains of dependent memory
+// accesses, so what stays fixed during the solve is read once: each lane keeps
+// the columns of its first row slots in registers, and the contact count is
+// read at the start.
+//
+// A sum: every block writes its partial with a release store into its own slot
+// of the sum's parity (slots hold an all-ones pattern until written: a negative
+// NaN that no sum produces, since sums and products give the positive canonical
+// NaN); block 0 waits for all slots with acquire loads, adds them in block order
+// and publishes the total the same way, and the other blocks wait for that.
+// The sums therefore do not depend on scheduling, and a block's writes before
+// its partial are visible to every block after the total.  Block 0 resets a
+// partial slot once it has read it (it is written again two sums later, after
+// block 0's next release), and the other total slot before publishing (every
+// block read it before writing this sum's partial).  Waits spin with a limit;
+// on timeout the error is recorded and the kernel returns.
 constexpr int kCgThreads = 512;
 constexpr unsigned long long kSumPending = ~0ull;
 
@@ -1149,54 +1216,82 @@ struct CGArgs {
     OpArgs op;
     const float4 *grad, *diag;
     float4 *p, *r, *z, *v0, *v1, *Av, *Avc;
-    double *partials;         // one per block
-    unsigned long long *red;  // two slots for the published totals (all ones before the solve)
+    unsigned long long *slots;  // 2 x gridDim partial slots, then 2 total slots (all ones before the solve)
     int *iscal;
     int np, n_iters;
 };
 
+__device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// waits until *p holds a value; false after the spin limit (error recorded)
+__device__ __forceinline__ bool wait_value(const unsigned long long *p, unsigned long long &v, int *iscal)
+{
+    v = ld_acquire(p);
+    for (long long spins = 0; v == kSumPending; ++spins) {
+        if (spins > (1LL << 24)) {  // ~ seconds: a block never arrived
+            atomicExch(iscal + I_BAR_ERR, 1);
+            return false;
+        }
+        __nanosleep(32);
+        v = ld_acquire(p);
+    }
+    return true;
+}
+
 // Block sum of `acc`, then the grid-wide total (see above).  Returns false on
-// a barrier timeout.
+// a wait timeout.
 __device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, int k, double &total)
 {
-    __shared__ int s_last, s_ok;
+    __shared__ int s_ok;
     __shared__ double s_val;
+    __shared__ double s_part[kCgThreads];  // block 0: every block's partial, in block order
+    const int G = (int)gridDim.x;
+    unsigned long long *part = A.slots + (size_t)(k & 1) * G;
+    unsigned long long *tot = A.slots + 2 * (size_t)G + (k & 1), *tot_next = A.slots + 2 * (size_t)G + ((k + 1) & 1);
     const double bs = block_sum<kCgThreads>(acc);
     if (threadIdx.x == 0) {
-        A.partials[blockIdx.x] = bs;
         s_ok = 1;
-        __threadfence();
-        s_last = atomicAdd(A.iscal + I_BAR_COUNT, 1) == (int)gridDim.x - 1;
+        st_release(part + blockIdx.x, (unsigned long long)__double_as_longlong(bs));
     }
-    __syncthreads();
-    if (s_last) {
+    if (blockIdx.x == 0) {
+        // thread i waits for block i's partial (all in parallel), then warp 0
+        // adds them in block order
+        int ok = 1;
+        if ((int)threadIdx.x < G) {
+            unsigned long long bits = 0;
+            if (wait_value(part + threadIdx.x, bits, A.iscal)) {
+                s_part[threadIdx.x] = __longlong_as_double((long long)bits);
+                part[threadIdx.x] = kSumPending;  // rewritten two sums later, after block 0's next release
+            } else {
+                ok = 0;
+            }
+        }
+        ok = __syncthreads_and(ok);
         if (threadIdx.x < 32) {
-            __threadfence();
             double v = 0.0;
-            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) v += __ldcg(&A.partials[i]);
+            for (int i = threadIdx.x; i < G; i += 32) v += s_part[i];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
             if (threadIdx.x == 0) {
+                *tot_next = kSumPending;
+                if (ok) st_release(tot, (unsigned long long)__double_as_longlong(v));
                 s_val = v;
-                A.iscal[I_BAR_COUNT] = 0;
-                A.red[(k + 1) & 1] = kSumPending;
-                __threadfence();
-                *(volatile unsigned long long *)(A.red + (k & 1)) = (unsigned long long)__double_as_longlong(v);
+                s_ok = ok;
             }
         }
     } else if (threadIdx.x == 0) {
-        volatile unsigned long long *slot = A.red + (k & 1);
-        unsigned long long bits = *slot;
-        for (long long spins = 0; bits == kSumPending; ++spins) {
-            if (spins > (1LL << 24)) {  // ~ seconds: a block never arrived
-                atomicExch(A.iscal + I_BAR_ERR, 1);
-                s_ok = 0;
-                break;
-            }
-            __nanosleep(32);
-            bits = *slot;
-        }
-        __threadfence();
-        s_val = __longlong_as_double((long long)bits);
+        unsigned long long bits = 0;
+        if (wait_value(tot, bits, A.iscal)) s_val = __longlong_as_double((long long)bits);
+        else s_ok = 0;
     }
     __syncthreads();
     total = s_val;
@@ -1207,6 +1302,21 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
 {
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long gs = (long long)blockDim.x * gridDim.x;
+    const int lane = threadIdx.x & 31, sub = lane & 3;
+    const long long warp0 = t0 >> 5, nwarps = gs >> 5;
+    const OpArgs &O = A.op;
+    const long long nb = min((long long)A.iscal[I_NACT], O.cap_b);
+    // this lane's first row (eight rows per warp, four lanes per row) and the
+    // columns of its first four slots, kept for the whole solve
+    constexpr int kRowBatch = 4;
+    const long long i0 = warp0 * 8 + (lane >> 2);
+    int s0 = 0, e0 = 0, c0[kRowBatch];
+    if (i0 < A.np) {
+        s0 = O.row_ptr[i0] + sub;
+        e0 = O.row_ptr[i0 + 1];
+    }
+#pragma unroll
+    for (int k = 0; k < kRowBatch; ++k) c0[k] = s0 + 4 * k < e0 ? O.col[s0 + 4 * k] : -1;
     // r = g, z = g / (diag + 1e-6), p = 0, Avc = 0
     double acc = 0.0;
     for (long long i = t0; i < A.np; i += gs) {
@@ -1232,13 +1342,56 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
             return ld(z, j) + beta * ld(vo, j);
         };
         acc = 0.0;
-        op_rows(A.op, t0 >> 5, gs >> 5, dir, [&](int i, F3 kv) {
-            const F3 vv = dir(i);
-            st(vn, i, vv);
-            st(A.Av, i, kv);
-            acc += (double)dot(vv, kv);
-        });
-        acc += op_contacts(A.op, t0, gs, dir, A.Avc);
+        // rows of K v: every load of a lane's row slots, and the row owner's own
+        // direction, issued before any use
+        for (long long base = warp0 * 8, g = 0; base < A.np; base += nwarps * 8, ++g) {
+            const long long i = base + (lane >> 2);
+            int s = s0, e = e0, cidx[kRowBatch];
+            if (g == 0) {
+#pragma unroll
+                for (int k = 0; k < kRowBatch; ++k) cidx[k] = c0[k];
+            } else {
+                s = 0;
+                e = 0;
+                if (i < A.np) {
+                    s = O.row_ptr[i] + sub;
+                    e = O.row_ptr[i + 1];
+                }
+#pragma unroll
+                for (int k = 0; k < kRowBatch; ++k) cidx[k] = s + 4 * k < e ? O.col[s + 4 * k] : -1;
+            }
+            F3 x[kRowBatch];
+#pragma unroll
+            for (int k = 0; k < kRowBatch; ++k) x[k] = cidx[k] >= 0 ? dir(cidx[k]) : mk(0.f, 0.f, 0.f);
+            const F3 own = (i < A.np && sub == 0) ? dir((int)i) : mk(0.f, 0.f, 0.f);
+            F3 kv = mk(0.f, 0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < kRowBatch; ++k) {
+                if (cidx[k] < 0) continue;
+                const size_t b = 3 * (size_t)(s + 4 * k);
+                const float4 k0 = O.kval[b], k1 = O.kval[b + 1], k2 = O.kval[b + 2];
+                kv = kv + mk(k0.x * x[k].x + k0.y * x[k].y + k0.z * x[k].z, k1.x * x[k].x + k1.y * x[k].y + k1.z * x[k].z,
+                             k2.x * x[k].x + k2.y * x[k].y + k2.z * x[k].z);
+            }
+            for (int ss = s + 4 * kRowBatch; ss < e; ss += 4) {  // rows longer than 4 x kRowBatch
+                const F3 xx = dir(O.col[ss]);
+                const float4 k0 = O.kval[3 * (size_t)ss], k1 = O.kval[3 * (size_t)ss + 1], k2 = O.kval[3 * (size_t)ss + 2];
+                kv = kv + mk(k0.x * xx.x + k0.y * xx.y + k0.z * xx.z, k1.x * xx.x + k1.y * xx.y + k1.z * xx.z,
+                             k2.x * xx.x + k2.y * xx.y + k2.z * xx.z);
+            }
+#pragma unroll
+            for (int o = 1; o < 4; o <<= 1) {
+                kv.x += __shfl_xor_sync(0xffffffffu, kv.x, o);
+                kv.y += __shfl_xor_sync(0xffffffffu, kv.y, o);
+                kv.z += __shfl_xor_sync(0xffffffffu, kv.z, o);
+            }
+            if (i < A.np && sub == 0) {
+                st(vn, (int)i, own);
+                st(A.Av, (int)i, kv);
+                acc += (double)dot(own, kv);
+            }
+        }
+        acc += op_contacts(O, t0, gs, dir, A.Avc, nb);
         if (!grid_sum(acc, A, nsum++, vav)) return;
         zr_last = zr;
         const bool upd = vav > 1e-16;
@@ -1368,7 +1521,7 @@ __global__ void k_f4_to_aos(const float4 *in, float *out, int n)
 void Stage3::release()
 {
     void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, v2, Av, Avc, q_gather, wk, tris, area, inv_dm,
-                    edges4, hinges, rest_angle, rest_elen, row_ptr, col, kval, tri_slot, hinge_slot, diag_slot, pat_cnt,
+                    edges4, hinges, rest_angle, rest_elen, row_ptr, col, kval, tri_slot, hinge_slot, diag_slot, hblk, pat_cnt,
                     pat_cur, pat_off, pat_cand, pat_scan, bidx, bkind, bsub, bd, bb2, bg, bact, gt_pts, gt_tris, dscal, fscal,
                     iscal, partials};
     drop_graph();
@@ -1387,6 +1540,7 @@ void Stage3::release()
     if (h_dscal) cudaFreeHost(h_dscal);
     q = q_prev = q_det = p = grad = diag = target = r = z = v = v2 = Av = Avc = q_gather = nullptr;
     row_ptr = col = tri_slot = hinge_slot = diag_slot = nullptr;
+    hblk = nullptr;
     pat_cnt = pat_cur = pat_off = pat_cand = pat_scan = nullptr;
     kval = nullptr;
     nnz = cap_nnz = cap_cand = 0;
@@ -1424,7 +1578,7 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
     A3(wk, cp * 4);
     A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16); A3(tri_slot, ct * 36);
     A3(edges4, ce * 16);
-    A3(hinges, ch * 16); A3(rest_angle, ch * 4); A3(rest_elen, ch * 4); A3(hinge_slot, ch * 64);
+    A3(hinges, ch * 16); A3(rest_angle, ch * 4); A3(rest_elen, ch * 4); A3(hinge_slot, ch * 64); A3(hblk, ch * 81 * 4);
     A3(row_ptr, (cp + 1) * 4); A3(diag_slot, cp * 4); A3(pat_cnt, (cp + 1) * 4); A3(pat_cur, cp * 4);
     A3(pat_off, (cp + 1) * 4); A3(pat_scan, scan_scratch_ints(cp + 1) * 4);
     A3(gt_pts, cgp * 16); A3(gt_tris, cgt * 16);
@@ -1695,13 +1849,16 @@ int Stage3::newton_body(cudaStream_t s)
     DArgs d{q, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
             cfg.elas_young_modulus * cfg.elas_poisson_ratio /
                 ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
-            hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, kval, tri_slot, hinge_slot, bidx,
+            hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, kval, tri_slot, hinge_slot, hblk, bidx,
             bkind, bsub, bd, bg, bb2, iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag, bact};
     // the Hessian's values: zero, the vertex term, then the elements (k_diff_elements)
     S3_TRY(cudaMemsetAsync(kval, 0, (size_t)nnz * 48, s));
     launch(k_diag_term, grid_for(np), kThreads, 0, s, (const float *)wk, (const int *)diag_slot, np, kval);
     S3_TRY(cudaMemsetAsync(iscal + I_NACT, 0, sizeof(int), s));
     launch(k_diff_elements, grid_for((long long)nt + nh + cap_b, 128), 128, 0, s, d);
+    if (nh > 0)
+        launch(k_hinge_spd, (int)((nh + 63) / 64), 64, 0, s, (const float *)hblk, nh, cfg.spd_max_iters,
+               (const int *)hinge_slot, kval);
     // Jacobi-preconditioned CG (cg_solver.py:96-158)
     if (prof) prof->begin(PH_S3_CG, s);
     if (cg_persistent < 0) {  // first use: can all blocks of the solve be resident at once?
@@ -1716,12 +1873,11 @@ int Stage3::newton_body(cudaStream_t s)
     }
     const OpArgs op{np, row_ptr, col, kval, bidx, bg, bb2, bact, iscal, cap_b};
     if (cg_persistent == 1) {
-        // partials: 2 x kRedBlocks doubles; the solve uses the first cg_blocks, and
-        // the two published-total slots sit at kRedBlocks
-        unsigned long long *slots = reinterpret_cast<unsigned long long *>(partials + kRedBlocks);
-        CGArgs ca{op, grad, diag, p, r, z, v, v2, Av, Avc, partials, slots, iscal, np, cfg.n_cg_iters};
-        S3_TRY(cudaMemsetAsync(iscal + I_BAR_COUNT, 0, sizeof(int), s));
-        S3_TRY(cudaMemsetAsync(slots, 0xFF, 2 * sizeof(unsigned long long), s));  // kSumPending
+        // partials (2 x kRedBlocks doubles) hold the solve's 2 x cg_blocks partial
+        // slots and its two total slots, all set to kSumPending
+        unsigned long long *slots = reinterpret_cast<unsigned long long *>(partials);
+        CGArgs ca{op, grad, diag, p, r, z, v, v2, Av, Avc, slots, iscal, np, cfg.n_cg_iters};
+        S3_TRY(cudaMemsetAsync(slots, 0xFF, (2 * (size_t)cg_blocks + 2) * sizeof(unsigned long long), s));
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(cg_blocks);
         lc.blockDim = dim3(kCgThreads);

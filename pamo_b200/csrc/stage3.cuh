@@ -46,6 +46,7 @@ struct Stage3 {
     int *tri_slot = nullptr;    // [9 nt]: block (a, b) of triangle t at 9 t + 3 a + b
     int *hinge_slot = nullptr;  // [16 nh]: block (a, b) of hinge h at 16 h + 4 a + b
     int *diag_slot = nullptr;   // [np]
+    float *hblk = nullptr;      // [81 nh]: the unprojected hinge blocks of vertices 0-2 (current Newton iteration)
     int *pat_cnt = nullptr, *pat_cur = nullptr, *pat_off = nullptr, *pat_cand = nullptr, *pat_scan = nullptr;
     long long nnz = 0, cap_nnz = 0, cap_cand = 0;
     float4 *Avc = nullptr;      // contact terms of A v (the persistent solve)
