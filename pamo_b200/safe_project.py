@@ -96,7 +96,8 @@ def edges_unique(F):
     x = np.concatenate([F[:, 0], F[:, 1], F[:, 2]])
     y = np.concatenate([F[:, 1], F[:, 2], F[:, 0]])
     n = int(F.max()) + 1
-    k = np.unique(np.minimum(x, y) * n + np.maximum(x, y))
+    k = np.sort(np.minimum(x, y) * n + np.maximum(x, y))  # np.unique's result, without its slower path
+    k = k[np.concatenate([[True], k[1:] != k[:-1]])]
     return np.stack([k // n, k % n], axis=1)
 
 
@@ -104,18 +105,23 @@ def hinges(F):
     """(x0, x1, x2, x3) per interior edge: the face with directed edge x1->x2
     (x1 < x2) and the face with x2->x1; x0 / x3 their opposite vertices."""
     F = np.asarray(F, np.int64)
-    D = np.concatenate([np.stack([F[:, k], F[:, (k + 1) % 3], F[:, (k + 2) % 3]], 1) for k in range(3)])
+    # directed edges a -> b of every face (corner k to k + 1), c the third vertex
+    a = np.concatenate([F[:, 0], F[:, 1], F[:, 2]])
+    b = np.concatenate([F[:, 1], F[:, 2], F[:, 0]])
+    c = np.concatenate([F[:, 2], F[:, 0], F[:, 1]])
     n = int(F.max()) + 1 if len(F) else 1
-    fwd = D[D[:, 0] < D[:, 1]]
-    bwd = D[D[:, 0] > D[:, 1]]
-    kf = fwd[:, 0] * n + fwd[:, 1]
-    kb = bwd[:, 1] * n + bwd[:, 0]
+    mf, mb = a < b, a > b
+    af, bf, cf = a[mf], b[mf], c[mf]
+    kf = af * n + bf
+    kb = b[mb] * n + a[mb]
+    cb = c[mb]
     ob = np.argsort(kb, kind="stable")
     kbs = kb[ob]
     pos = np.searchsorted(kbs, kf)
     ok = (pos < len(kbs)) & (kbs[np.minimum(pos, max(len(kbs) - 1, 0))] == kf) if len(kbs) else np.zeros(len(kf), bool)
-    H = np.stack([fwd[ok, 2], fwd[ok, 0], fwd[ok, 1], bwd[ob][pos[ok], 2]], 1)
-    return H[np.lexsort((H[:, 2], H[:, 1]))]
+    H = np.stack([cf[ok], af[ok], bf[ok], cb[ob][pos[ok]]], 1)
+    # ordered by (x1, x2): the key x1 * n + x2 orders the same way (stable, as lexsort)
+    return H[np.argsort(kf[ok], kind="stable")]
 
 
 def voronoi_areas(V, F):
@@ -162,6 +168,23 @@ def merge_vertices(V, F, digits=8):
     after merging."""
     V = np.asarray(V, np.float64)
     key = np.round(V, digits)
+    # no two rows equal (the usual case): nothing merges, nothing moves.  Equal
+    # rows have equal x, so only runs of equal x need a full comparison.
+    if len(key) < 2:
+        return V, np.asarray(F)
+    ox = np.argsort(key[:, 0], kind="stable")
+    kx = key[ox]
+    same_x = kx[1:, 0] == kx[:-1, 0]
+    if not same_x.any():
+        return V, np.asarray(F)
+    # the rows in runs of equal x, sorted by (x, y, z): equal rows are adjacent
+    in_run = np.zeros(len(kx), bool)
+    in_run[1:] |= same_x
+    in_run[:-1] |= same_x
+    sub_rows = kx[in_run]
+    k3 = sub_rows[np.lexsort((sub_rows[:, 2], sub_rows[:, 1], sub_rows[:, 0]))]
+    if not ((k3[1:] == k3[:-1]).all(axis=1)).any():
+        return V, np.asarray(F)
     _, first, inv = np.unique(key, axis=0, return_index=True, return_inverse=True)
     order = np.argsort(first)
     rank = np.empty_like(order)
