@@ -365,6 +365,10 @@ cudaError_t Lbvh::ensure(long long n)
     ALLOC(vals2, c * 4);
     ALLOC(hist, (long long)256 * sort_tiles * 4 + 64);
     ALLOC(hist_scratch, scan_scratch_ints((long long)256 * sort_tiles) * 4);
+    if ((e = scan_scratch_init(hist_scratch, scan_scratch_ints((long long)256 * sort_tiles))) != cudaSuccess) {
+        release();
+        return e;
+    }
     ALLOC(nodes, c * sizeof(BvhNode));
     ALLOC(parent, 2 * c * 4);
     ALLOC(flags, c * 4);

@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include "lbvh.cuh"
+#include "scan.cuh"
 #include "stage2.cuh"
 
 namespace pamo {
@@ -27,7 +28,7 @@ constexpr size_t kOffVals = kOffKeys2 + align256(4 * (size_t)kMaxFaces);
 constexpr size_t kOffVals2 = kOffVals + align256(4 * (size_t)kMaxFaces);
 constexpr size_t kOffHist = kOffVals2 + align256(4 * (size_t)kMaxFaces);
 constexpr size_t kOffHistScratch = kOffHist + align256(4 * (256 * (size_t)kTiles + 64));
-constexpr size_t kOffNodes = kOffHistScratch + align256(4 * ((256 * (size_t)kTiles + 2047) / 2048 + 64));
+constexpr size_t kOffNodes = kOffHistScratch + align256(4 * (size_t)scan_scratch_ints(256LL * kTiles));
 constexpr size_t kOffParent = kOffNodes + align256(sizeof(BvhNode) * kMaxFaces);
 constexpr size_t kOffFlags = kOffParent + align256(4 * 2 * (size_t)kMaxFaces);
 constexpr size_t kOffLeafOfFace = kOffFlags + align256(4 * (size_t)kMaxFaces);

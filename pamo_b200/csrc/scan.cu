@@ -97,9 +97,124 @@ __global__ void __launch_bounds__(kSingleThreads) k_scan_single(const int *in, i
     if (threadIdx.x == 0 && d_total) *d_total = tot;
 }
 
-cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *d_n, int *scratch, int *d_total,
-                           cudaStream_t s)
+// Single pass with decoupled look-back (see scan.cuh).  Header: [0] next tile,
+// [1] finished blocks, [2] fault.  Status word of a tile: high half the call's
+// epoch (30 bits) and a flag (1: the tile's own sum, 2: its inclusive prefix),
+// low half the value; a word from an earlier call (another epoch) reads as not
+// yet published.
+constexpr unsigned kFlagSum = 1, kFlagPrefix = 2;
+
+__device__ __forceinline__ unsigned long long status_word(unsigned epoch, unsigned flag, int value)
 {
+    return ((unsigned long long)((epoch << 2) | flag) << 32) | (unsigned)value;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const int *in, int *out, long long n_max,
+                                                                const int *d_n, int *scratch, int *d_total,
+                                                                int *fault, unsigned epoch)
+{
+    __shared__ int tile[kScanTile];
+    __shared__ long long s_t;
+    __shared__ int s_prefix;
+    volatile unsigned long long *status = reinterpret_cast<volatile unsigned long long *>(scratch + kScanHeader);
+    const long long n = d_n ? (long long)*d_n : n_max;
+    const long long n_tiles = (n + kScanTile - 1) / kScanTile;
+    if (threadIdx.x == 0) s_t = atomicAdd(&scratch[0], 1);
+    __syncthreads();
+    const long long t = s_t;
+    if (t < n_tiles) {
+        const long long base = t * kScanTile;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            long long i = base + (long long)k * kScanThreads + threadIdx.x;
+            tile[k * kScanThreads + threadIdx.x] = i < n ? in[i] : 0;
+        }
+        __syncthreads();
+        int local[kScanItems];
+        int sum = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            local[k] = sum;
+            sum += tile[threadIdx.x * kScanItems + k];
+        }
+        int agg;
+        const int ex = block_excl_scan<kScanThreads>(sum, agg);
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            if (lane == 0) status[t] = status_word(epoch, t == 0 ? kFlagPrefix : kFlagSum, agg);
+            int prefix = 0;
+            bool timed_out = false;
+            for (long long top = t - 1; top >= 0 && !timed_out;) {
+                // lane l looks at tile top - l (lane 0 the nearest)
+                const long long j = top - lane;
+                unsigned flag = kFlagPrefix;
+                int val = 0;
+                if (j >= 0) {
+                    unsigned long long w = status[j];
+                    for (long long spins = 0;; ++spins) {
+                        const unsigned hi = (unsigned)(w >> 32);
+                        if ((hi >> 2) == (epoch & 0x3FFFFFFFu) && (hi & 3u) != 0) {
+                            flag = hi & 3u;
+                            val = (int)(unsigned)w;
+                            break;
+                        }
+                        if (spins > (1LL << 22)) {  // a tile that started earlier never published
+                            timed_out = true;
+                            break;
+                        }
+                        __nanosleep(20);
+                        w = status[j];
+                    }
+                }
+                timed_out = __any_sync(0xffffffffu, timed_out);
+                // the nearest tile with its prefix ends the look-back (a lane past
+                // tile 0 counts as one, with value 0); before it, the tiles' sums
+                const unsigned stops = __ballot_sync(0xffffffffu, flag == kFlagPrefix);
+                const int stop = stops ? __ffs(stops) - 1 : 31;
+                int v = lane <= stop ? val : 0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                prefix += v;
+                if (stops) break;
+                top -= 32;
+            }
+            if (lane == 0) {
+                if (timed_out) {
+                    atomicExch(&scratch[2], 1);
+                    if (fault) atomicExch(fault, 1);
+                }
+                status[t] = status_word(epoch, kFlagPrefix, prefix + agg);
+                s_prefix = prefix;
+                if (t == n_tiles - 1 && d_total) *d_total = prefix + agg;
+            }
+        }
+        __syncthreads();
+        const int off = s_prefix + ex;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) tile[threadIdx.x * kScanItems + k] = local[k] + off;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            long long i = base + (long long)k * kScanThreads + threadIdx.x;
+            if (i < n) out[i] = tile[k * kScanThreads + threadIdx.x];
+        }
+    } else if (n_tiles == 0 && t == 0 && threadIdx.x == 0 && d_total) {
+        *d_total = 0;
+    }
+    // the last block to finish leaves the header at zero for the next scan
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&scratch[1], 1) == (int)gridDim.x - 1) {
+            scratch[0] = 0;
+            scratch[1] = 0;
+        }
+    }
+}
+
+cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *d_n, int *scratch, int *d_total,
+                           cudaStream_t s, int *fault)
+{
+    static std::atomic<unsigned> epochs{0};
     if (n_max <= 0) {
         if (d_total) return cudaMemsetAsync(d_total, 0, sizeof(int), s);
         return cudaSuccess;
@@ -108,10 +223,9 @@ cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *
         launch(k_scan_single, 1, kSingleThreads, 0, s, in, out, n_max, d_n, d_total);
         return cudaGetLastError();
     }
-    long long tiles = (n_max + kScanTile - 1) / kScanTile;
-    launch(k_scan_reduce, (unsigned)tiles, kScanThreads, 0, s, in, n_max, d_n, scratch);
-    launch(k_scan_tile_sums, 1, 1024, 0, s, scratch, tiles, n_max, d_n, d_total);
-    launch(k_scan_down, (unsigned)tiles, kScanThreads, 0, s, in, out, n_max, d_n, scratch);
+    const long long tiles = (n_max + kScanTile - 1) / kScanTile;
+    const unsigned epoch = (epochs.fetch_add(1, std::memory_order_relaxed) + 1) & 0x3FFFFFFFu;
+    launch(k_scan_lookback, (unsigned)tiles, kScanThreads, 0, s, in, out, n_max, d_n, scratch, d_total, fault, epoch);
     return cudaGetLastError();
 }
 

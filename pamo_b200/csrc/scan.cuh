@@ -1,9 +1,16 @@
 // Device-wide exclusive prefix sums and block-level scan helpers.
 //
-// Reduce-then-scan in three launches (tile reduce, scan of tile sums, tile scan
-// with offsets).  No inter-block waiting, so there is nothing to bound; results
-// are deterministic.  The item count may live in device memory (d_n), in which
-// case n_max only sizes the grid.
+// One launch per scan: tiles of 2048 items take their index from a counter in
+// the order their blocks start, and each adds the totals of the tiles before it
+// as they publish them (decoupled look-back: a tile publishes its own sum at
+// once and its inclusive prefix when it has it, so a tile waits only on tiles
+// that started earlier).  The waits spin with a limit and record a fault when
+// it runs out.  Results are deterministic.  The item count may live in device
+// memory (d_n), in which case n_max only sizes the grid.
+//
+// The scratch (scan_scratch_ints(n_max) ints) must be all zero before its first
+// scan (scan_scratch_init); every scan leaves its counters zero again.  Scans
+// on one scratch must not overlap.
 #pragma once
 
 #include "common.cuh"
@@ -72,12 +79,22 @@ __global__ void k_scan_reduce(const int *__restrict__ in, long long n_max, const
 __global__ void k_scan_tile_sums(int *tile_sums, long long n_tiles_max, long long n_max, const int *d_n, int *d_total);
 __global__ void k_scan_down(const int *in, int *out, long long n_max, const int *d_n, const int *__restrict__ tile_sums);
 
-// Scratch needed by exclusive_scan for up to n_max items (ints).
-inline long long scan_scratch_ints(long long n_max) { return (n_max + kScanTile - 1) / kScanTile + 32; }
+// Scratch needed by exclusive_scan for up to n_max items (ints): a header of
+// kScanHeader ints, then one 64-bit status word per tile.
+constexpr int kScanHeader = 8;
+constexpr long long scan_scratch_ints(long long n_max) { return kScanHeader + 2 * ((n_max + kScanTile - 1) / kScanTile) + 2; }
+
+// Zeroes a freshly allocated scratch of `ints` ints.
+inline cudaError_t scan_scratch_init(int *scratch, long long ints, cudaStream_t s = 0)
+{
+    return cudaMemsetAsync(scratch, 0, (size_t)ints * sizeof(int), s);
+}
 
 // out[i] = sum_{j<i} in[i] for i < n, with n = d_n ? *d_n : n_max.  in may equal
-// out.  If d_total is non-null the grand total is written there.
+// out.  If d_total is non-null the grand total is written there.  If fault is
+// non-null, 1 is written there when a wait ran out (the scratch header keeps a
+// copy in any case).
 cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *d_n, int *scratch, int *d_total,
-                           cudaStream_t s);
+                           cudaStream_t s, int *fault = nullptr);
 
 }  // namespace pamo

@@ -1231,6 +1231,7 @@ int Stage2::ensure(long long n, long long m)
         release();
         return PAMO_ERR_OOM;
     }
+    scan_scratch_init(scan_scratch, scan_scratch_len);
     // state the reference reads stale starts at zero
     cudaMemset(edge_cost, 0, (ce + 1) * 4);
     cudaMemset(pts_map, 0, (cp + 1) * 4);
@@ -1311,7 +1312,7 @@ static cudaError_t undo_check(Stage2 &S, cudaStream_t s)
     launch(k_undo_flags, grid_for(NC), kThreads, 0, s, S.collapsed, S.dcnt, S.edges, S.first_near, S.near_tris, S.isect,
                                                    S.uflag);
     // positions of the flagged entries (in collapsed-list order)
-    cudaError_t e = exclusive_scan(S.uflag, S.eflag, NC, &S.dcnt->n_considered, S.scan_scratch, &S.dcnt->n_undo, s);
+    cudaError_t e = exclusive_scan(S.uflag, S.eflag, NC, &S.dcnt->n_considered, S.scan_scratch, &S.dcnt->n_undo, s, &S.dcnt->scan_fault);
     if (e != cudaSuccess) return e;
     launch(k_undo_scatter, grid_for(NC), kThreads, 0, s, S.uflag, S.eflag, S.dcnt, S.collapsed, S.edges, S.undo_edges,
                                                      S.tmp_undo);
@@ -1348,8 +1349,8 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
                                                                        cursor, vmin, n, m);
     launch(k_face_a, grid_for(m), kThreads, 0, s, pts, tris, m, first_near, first_edge, plane, elen4);
     if (m > 0) S2_TRY(cudaMemsetAsync(first_edge + m, 0, 4, s));
-    S2_TRY(exclusive_scan(first_near, first_near, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
-    S2_TRY(exclusive_scan(first_edge, first_edge, (long long)m + 1, nullptr, scan_scratch, &dcnt->n_edges, s));
+    S2_TRY(exclusive_scan(first_near, first_near, (long long)n + 1, nullptr, scan_scratch, nullptr, s, &dcnt->scan_fault));
+    S2_TRY(exclusive_scan(first_edge, first_edge, (long long)m + 1, nullptr, scan_scratch, &dcnt->n_edges, s, &dcnt->scan_fault));
     const int *d_n_edges = &dcnt->n_edges;
     launch(k_face_b, grid_for(m), kThreads, 0, s, tris, m, first_near, cursor, near_tris, first_edge, edges);
     launch(k_vertex_quadric, grid_for(n), kThreads, 0, s, first_near, near_tris, plane, tris, quad, nxt, n);
@@ -1375,7 +1376,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
                     collapse_t, nullptr, nullptr, nullptr};
     prof.begin(PH_COLLAPSE, s);
     launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
-    S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
+    S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s, &dcnt->scan_fault));
     launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
     prof.begin(PH_CLEANUP, s);
     launch(k_remove_invalid_faces, grid_for(m), kThreads, 0, s, tris, m);
@@ -1403,6 +1404,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
         if (hcnt->pair_overflow > 0) return PAMO_ERR_CAPACITY;
     }
     if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
+    if (hcnt->scan_fault) return PAMO_ERR_DEVICE;
     last_stats[0] = hcnt->n_edges;
     last_stats[1] = hcnt->n_main;
     last_stats[2] = hcnt->n_total;
@@ -1436,6 +1438,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
             if (hcnt->pair_overflow > 0) return PAMO_ERR_CAPACITY;
         }
         if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
+    if (hcnt->scan_fault) return PAMO_ERR_DEVICE;
         cnt_undo = hcnt->n_undo;
         nvu += 2 * cnt_undo;
         if (nvu > cap_undo) return PAMO_ERR_CAPACITY;
@@ -1445,7 +1448,7 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     last_stats[4] = nvu;
     // pts_map = exclusive scan of occ[0..n]
     prof.begin(PH_COMPACT, s);
-    S2_TRY(exclusive_scan(occ, pts_map, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
+    S2_TRY(exclusive_scan(occ, pts_map, (long long)n + 1, nullptr, scan_scratch, nullptr, s, &dcnt->scan_fault));
     prof.end(s);
     *n_undo_out = nvu;
     return PAMO_OK;
@@ -1485,6 +1488,7 @@ int Stage2::self_intersect_all(int n, int m, cudaStream_t s)
         if (hcnt->pair_overflow > 0) return PAMO_ERR_CAPACITY;
     }
     if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
+    if (hcnt->scan_fault) return PAMO_ERR_DEVICE;
     return PAMO_OK;
 }
 
@@ -1492,7 +1496,7 @@ int Stage2::compact(int n, int m, cudaStream_t s)
 {
     prof.begin(PH_COMPACT, s);
     launch(k_face_live_flags, grid_for(m), kThreads, 0, s, tris, m, fflag);
-    S2_TRY(exclusive_scan(fflag, uflag, m, nullptr, scan_scratch, nullptr, s));
+    S2_TRY(exclusive_scan(fflag, uflag, m, nullptr, scan_scratch, nullptr, s, &dcnt->scan_fault));
     launch(k_compact, grid_for(n > m ? n : m), kThreads, 0, s, pts, occ, pts_map, n, tris, fflag, uflag, m, opts, otris,
                                                            dcnt);
     if (bvh_leaves > 0 && bvh_leaves >= m) {
@@ -1504,6 +1508,7 @@ int Stage2::compact(int n, int m, cudaStream_t s)
     S2_TRY(cudaMemcpyAsync(hcnt, dcnt, sizeof(RoundCounters), cudaMemcpyDeviceToHost, s));
     S2_TRY(cudaStreamSynchronize(s));
     prof.collect();
+    if (hcnt->scan_fault) return PAMO_ERR_DEVICE;
     return PAMO_OK;
 }
 
@@ -1546,7 +1551,7 @@ static cudaError_t undo_check_batch(Stage2 &S, int K, cudaStream_t s)
     const long long NC = S.cap_edges;
     launch(k_undo_flags, grid_for(NC), kThreads, 0, s, S.cand, S.dcnt, S.edges, S.first_near, S.near_tris, S.isect,
            S.uflag);
-    cudaError_t e = exclusive_scan(S.uflag, S.eflag, NC, &S.dcnt->n_considered, S.scan_scratch, &S.dcnt->n_undo, s);
+    cudaError_t e = exclusive_scan(S.uflag, S.eflag, NC, &S.dcnt->n_considered, S.scan_scratch, &S.dcnt->n_undo, s, &S.dcnt->scan_fault);
     if (e != cudaSuccess) return e;
     launch(k_b_undo_counts, grid_for(K), kThreads, 0, s, S.eflag, S.dcnt, S.scnt, K);
     launch(k_b_undo_scatter, grid_for(NC), kThreads, 0, s, S.uflag, S.eflag, S.dcnt, S.cand, S.edges, S.vslot,
@@ -1592,8 +1597,8 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
            cursor, vmin, n, m);
     launch(k_face_a, grid_for(m), kThreads, 0, s, pts, tris, m, first_near, first_edge, plane, elen4);
     S2_TRY(cudaMemsetAsync(first_edge + m, 0, 4, s));
-    S2_TRY(exclusive_scan(first_near, first_near, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
-    S2_TRY(exclusive_scan(first_edge, first_edge, (long long)m + 1, nullptr, scan_scratch, &dcnt->n_edges, s));
+    S2_TRY(exclusive_scan(first_near, first_near, (long long)n + 1, nullptr, scan_scratch, nullptr, s, &dcnt->scan_fault));
+    S2_TRY(exclusive_scan(first_edge, first_edge, (long long)m + 1, nullptr, scan_scratch, &dcnt->n_edges, s, &dcnt->scan_fault));
     const int *d_n_edges = &dcnt->n_edges;
     launch(k_face_b, grid_for(m), kThreads, 0, s, tris, m, first_near, cursor, near_tris, first_edge, edges);
     launch(k_vertex_quadric, grid_for(n), kThreads, 0, s, first_near, near_tris, plane, tris, quad, nxt, n);
@@ -1612,7 +1617,7 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
                     0u, slots, scnt, vslot};
     prof.begin(PH_COLLAPSE, s);
     launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
-    S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s));
+    S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s, &dcnt->scan_fault));
     launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
     launch(k_b_main, grid_for(K), kThreads, 0, s, (const int *)uflag, (const RoundCounters *)dcnt, scnt, K);
     prof.begin(PH_CLEANUP, s);
@@ -1646,6 +1651,7 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
             if (hcnt->pair_overflow > 0) return PAMO_ERR_CAPACITY;
         }
         if (hcnt->stack_overflow > 0) return PAMO_ERR_CAPACITY;
+    if (hcnt->scan_fault) return PAMO_ERR_DEVICE;
         return PAMO_OK;
     };
     int rc = pass(false);
@@ -1692,7 +1698,7 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
     last_stats[3] = it;
     // the packed vertex map, each mesh's own map and undo-list copy
     prof.begin(PH_COMPACT, s);
-    S2_TRY(exclusive_scan(occ, gmap, (long long)n + 1, nullptr, scan_scratch, nullptr, s));
+    S2_TRY(exclusive_scan(occ, gmap, (long long)n + 1, nullptr, scan_scratch, nullptr, s, &dcnt->scan_fault));
     long long max_nvu = 0;
     for (int r = 0; r < K; ++r) {
         hslots[r].nvu = nvu[r];
@@ -1711,7 +1717,7 @@ int Stage2::compact_batch(int n, int m, int K, cudaStream_t s)
     prof.begin(PH_COMPACT, s);
     launch(k_face_live_flags, grid_for(m), kThreads, 0, s, tris, m, fflag);
     S2_TRY(cudaMemsetAsync(fflag + m, 0, 4, s));
-    S2_TRY(exclusive_scan(fflag, uflag, (long long)m + 1, nullptr, scan_scratch, nullptr, s));
+    S2_TRY(exclusive_scan(fflag, uflag, (long long)m + 1, nullptr, scan_scratch, nullptr, s, &dcnt->scan_fault));
     launch(k_compact, grid_for(n > m ? n : m), kThreads, 0, s, pts, occ, gmap, n, tris, fflag, uflag, m, opts, otris,
            dcnt);
     launch(k_b_next, grid_for(K), kThreads, 0, s, (const SlotInfo *)slots, (const int *)gmap, (const int *)uflag, scnt,

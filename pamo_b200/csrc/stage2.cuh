@@ -22,7 +22,8 @@ struct RoundCounters {
     int n_tris_next;
     int n_edges;
     int n_query;         // faces in this pass's query list
-    int pad[4];
+    int scan_fault;      // a prefix scan's wait ran out (see scan.cuh)
+    int pad[3];
 };
 
 // ---------------------------------------------------------------------------

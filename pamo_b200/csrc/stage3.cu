@@ -1581,6 +1581,10 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
     A3(hinges, ch * 16); A3(rest_angle, ch * 4); A3(rest_elen, ch * 4); A3(hinge_slot, ch * 64); A3(hblk, ch * 81 * 4);
     A3(row_ptr, (cp + 1) * 4); A3(diag_slot, cp * 4); A3(pat_cnt, (cp + 1) * 4); A3(pat_cur, cp * 4);
     A3(pat_off, (cp + 1) * 4); A3(pat_scan, scan_scratch_ints(cp + 1) * 4);
+    if (scan_scratch_init(pat_scan, scan_scratch_ints(cp + 1)) != cudaSuccess) {
+        release();
+        return PAMO_ERR_OOM;
+    }
     A3(gt_pts, cgp * 16); A3(gt_tris, cgt * 16);
     A3(dscal, 64); A3(fscal, 64); A3(iscal, 64);
     A3(partials, 2 * kRedBlocks * 8);  // two buffers for the persistent solve
