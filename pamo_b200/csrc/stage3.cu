@@ -419,6 +419,9 @@ struct EArgs {
     // (energy below the start's), as the reference's loop stops there
     int n_halves;
     const double *dscal;
+    // line search (n_halves >= 0): the largest step length of a vertex, which
+    // bounds how far a block's distance can have moved from the start's bd
+    const float *step_bound;
 };
 
 __device__ __forceinline__ void elastic_F(const float4 *q, int4 f, float4 im, F3 &b1, F3 &b2, float F[4])
@@ -465,13 +468,23 @@ __global__ void __launch_bounds__(kThreads) k_energy(EArgs A)
             acc += (double)(0.5f * A.hinge_k * dt * dt * A.rest_elen[h]);
         } else {
             int b = (int)(k - A.np - A.nt - A.nh);
+            if (A.n_halves >= 0) {
+                // A trial point: every vertex moved at most step_bound from the
+                // start, where the block's distance was bd, and a pair distance
+                // changes by at most the sum of its two primitives' largest
+                // moves.  A block that stays beyond d_hat adds nothing (the
+                // margin covers the fp32 evaluation of the distances).
+                if (A.bd[b] - 2.f * *A.step_bound > A.d_hat + 1e-5f) continue;
+            }
             int4 i = A.bidx[b];
             int kind = A.bkind[b];
             F3 x[4] = {ld(A.q, i.x), ld(A.q, i.y), ld(A.q, i.z), ld(A.q, i.w)};
             int ty = classify(kind, x, A.ee_thres);
             float d = classified_distance(kind, ty, x);
-            A.bsub[b] = ty;
-            A.bd[b] = d;
+            if (A.n_halves < 0) {  // the start of a Newton iteration: kept for the differentials
+                A.bsub[b] = ty;
+                A.bd[b] = d;
+            }
             if (d < A.d_hat) acc += barrier((double)d, (double)A.d_hat) * (double)A.kappa;
         }
     }
@@ -1415,6 +1428,15 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
 }
 
 // ---------------------------------------------------------- clamp, CCD, line search
+// largest |p_i| (float bits of a non-negative value order like ints; out zeroed before)
+__global__ void k_max_norm(const float4 *p, int np, float *out)
+{
+    float m = 0.f;
+    PAMO_GRID_STRIDE(i, np) m = fmaxf(m, len(ld(p, (int)i)));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(reinterpret_cast<int *>(out), __float_as_int(m));
+}
+
 __global__ void k_clamp(float4 *p, const float4 *q_prev, const float4 *q_det, int np, float radius)
 {
     PAMO_GRID_STRIDE(i, np)
@@ -1780,7 +1802,7 @@ static int energy_pass(Stage3 &S, cudaStream_t s, int n_halves = -1)
             S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
                 ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
             S.hinges, S.rest_angle, S.rest_elen, S.cfg.hinge_stiffness, S.bidx, S.bkind, S.bsub, S.bd, S.iscal, S.cap_b,
-            S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials, n_halves, S.dscal};
+            S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials, n_halves, S.dscal, S.fscal + 1};
     launch(k_energy, kRedBlocks, kThreads, 0, s, e);
     launch(k_finish_sum, 1, 32, 0, s, S.partials, kRedBlocks, S.dscal + D_ENERGY);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
@@ -1909,6 +1931,8 @@ int Stage3::newton_body(cudaStream_t s)
     if (prof) prof->begin(PH_S3_CCD, s);
     launch(k_clamp, grid_for(np), kThreads, 0, s, p, q_prev, q_det, np, cfg.contact_detection_radius);
     launch(k_set_float, 1, 1, 0, s, fscal, 1.0f);
+    launch(k_set_float, 1, 1, 0, s, fscal + 1, 0.0f);
+    launch(k_max_norm, grid_for(np), kThreads, 0, s, (const float4 *)p, np, fscal + 1);
     launch(k_accd, grid_for(cap_b, 128), 128, 0, s, q, p, bidx, bkind, iscal, cap_b, cfg.ccd_slackness, cfg.ccd_thickness,
                                                 cfg.ccd_max_iters, cfg.ee_classify_thres, fscal);
     // line search (system.py:393-409)
