@@ -1,6 +1,7 @@
 // Stage-3 safe projection on the device (sm_100a): barrier-energy Newton
-// iterations with a matrix-free Jacobi-PCG, contact detection on LBVHs, additive
-// CCD and a halving line search (simp_cuda/safe_project/src/pamo_safe_project:
+// iterations with a Jacobi-PCG on the assembled block-sparse Hessian (contact
+// terms matrix-free), contact detection on LBVHs, additive CCD and a halving
+// line search (simp_cuda/safe_project/src/pamo_safe_project:
 // system.py:411-470, cg_solver.py:46-158, energy.py, kernels/*).
 //
 // Precision: positions, distances, gradients and the CG vectors are FP32; the
