@@ -986,6 +986,11 @@ struct pamo_batch {
     std::vector<int> nvu;
     long long rounds_run = 0;
     std::vector<long long> done_ids;  // jobs that finished or failed in the last step
+    // The jobs' device memory (inputs, per-mesh regions, results) comes from the
+    // engine's own stream-ordered pool, which keeps what it has mapped until the
+    // engine is destroyed: a device pool that hands memory back at each
+    // synchronisation stalled single rounds for up to 0.7 s remapping it.
+    cudaMemPool_t pool = nullptr;
 };
 
 namespace pamo {
@@ -1004,7 +1009,7 @@ int batch_admit(pamo_batch *b, BatchJob *j)
     Stage2 &S = b->S;
     long long cu = 0;
     j->region_bytes = region_bytes_for(j->n0, j->m0, &cu);
-    CU_RET(cudaMallocAsync((void **)&j->region, (size_t)j->region_bytes, s));
+    CU_RET(cudaMallocFromPoolAsync((void **)&j->region, (size_t)j->region_bytes, b->pool, s));
     CU_RET(cudaMemsetAsync(j->region, 0, (size_t)j->region_bytes, s));
     auto al = [](long long x) { return (x + 255) / 256 * 256; };
     unsigned char *p = j->region;
@@ -1063,8 +1068,8 @@ int batch_admit(pamo_batch *b, BatchJob *j)
 int batch_finish(pamo_batch *b, BatchJob *j)
 {
     cudaStream_t s = b->s;
-    CU_RET(cudaMallocAsync((void **)&j->out_p, (size_t)(j->n > 0 ? j->n : 1) * 12, s));
-    CU_RET(cudaMallocAsync((void **)&j->out_t, (size_t)(j->m > 0 ? j->m : 1) * 12, s));
+    CU_RET(cudaMallocFromPoolAsync((void **)&j->out_p, (size_t)(j->n > 0 ? j->n : 1) * 12, b->pool, s));
+    CU_RET(cudaMallocFromPoolAsync((void **)&j->out_t, (size_t)(j->m > 0 ? j->m : 1) * 12, b->pool, s));
     launch(k_b_extract, grid_for(j->n > j->m ? j->n : j->m), kThreads, 0, s, (const float4 *)b->S.opts,
            (const int4 *)b->S.otris, j->vert_off, j->n, j->face_off, j->m, (const JobHeader *)j->hdr, j->out_p,
            j->out_t);
@@ -1105,9 +1110,21 @@ int pamo_batch_create(int device, long long max_verts, long long max_faces, int 
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return PAMO_ERR_NO_DEVICE;
     if (device < 0 || device >= count) return PAMO_ERR_INVALID_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return PAMO_ERR_DEVICE;
-    if (retain_pool_memory() != cudaSuccess) return PAMO_ERR_DEVICE;
     pamo_batch *b = new (std::nothrow) pamo_batch();
     if (!b) return PAMO_ERR_OOM;
+    {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        unsigned long long keep = ~0ull;
+        if (cudaMemPoolCreate(&b->pool, &props) != cudaSuccess ||
+            cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+            if (b->pool) cudaMemPoolDestroy(b->pool);
+            delete b;
+            return PAMO_ERR_DEVICE;
+        }
+    }
     b->device = device;
     b->s = (cudaStream_t)stream;
     b->cap_v = max_verts;
@@ -1153,6 +1170,7 @@ int pamo_batch_destroy(pamo_batch *b)
     if (b->S.hscnt) cudaFreeHost(b->S.hscnt);
     if (b->d_moves) cudaFree(b->d_moves);
     if (b->h_moves) cudaFreeHost(b->h_moves);
+    if (b->pool) cudaMemPoolDestroy(b->pool);
     delete b;
     return PAMO_OK;
 }
@@ -1179,8 +1197,8 @@ int pamo_batch_submit(pamo_batch *b, const float *points, const int *tris, int n
     float ct = (0.0f > threshold) ? 0.0f : threshold;
     ct = (ct < 10.0f) ? ct : 10.0f;
     j->collapse_t = (uint32_t)(unsigned long long)(ct / 10.0f * 4294967296.0f);
-    if (cudaMallocAsync((void **)&j->raw_p, (size_t)n_pts * 12, s) != cudaSuccess ||
-        cudaMallocAsync((void **)&j->raw_t, (size_t)n_tris * 12, s) != cudaSuccess) {
+    if (cudaMallocFromPoolAsync((void **)&j->raw_p, (size_t)n_pts * 12, b->pool, s) != cudaSuccess ||
+        cudaMallocFromPoolAsync((void **)&j->raw_t, (size_t)n_tris * 12, b->pool, s) != cudaSuccess) {
         batch_fail(b, j, PAMO_ERR_OOM);
         delete j;
         return PAMO_ERR_OOM;
