@@ -193,6 +193,18 @@ int pamo_point_stats(const float *d_pts, int n, double *h_out6, void *stream);
 int pamo_voronoi_areas(const double *d_v, const int *d_f, int nv, int nf, float *d_out, double *h_min_angle_deg,
                        void *stream);
 
+/* The unique edges and the hinges of a closed 2-manifold triangle mesh, on the
+   host (replaces the O(NT^2) face scan of hinge_preprocess_slow_kernel,
+   energy_kernels/hinge_energy.py:21-57, and trimesh's edges_unique):
+   h_edges [n_edges,2] (a < b, ascending by a * n_pts + b), h_hinges
+   [n_edges,4] (x0, x1, x2, x3) in the same order, where x1 < x2 is the edge,
+   x0 the third vertex of the face with directed edge x1 -> x2 and x3 that of
+   the face with x2 -> x1.  Both output buffers hold 3 * n_tris / 2 rows.
+   Returns PAMO_ERR_INVALID_ARG for an index outside [0, n_pts) and
+   PAMO_ERR_CAPACITY when an edge is not shared by exactly two faces, once
+   each way (the caller then uses a general method). */
+int pamo_mesh_hinges(const int *h_tris, int n_tris, int n_pts, int *h_edges, int *h_hinges, int *out_n_edges);
+
 /* Stage-3 input normalisation on the device (processing.py:57-59 applies it
    to the ground truth on the host): out[i] = float((in[i] * scale + t) * post)
    per coordinate of n points [n,3], each step in double with one rounding, so

@@ -29,6 +29,7 @@ SIGNATURES = {
     "pamo_version": (_i, []),
     "pamo_launch_count": (_ll, []),
     "pamo_voronoi_areas": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(ctypes.c_double), _vp]),
+    "pamo_mesh_hinges": (_i, [_vp, _i, _i, _vp, _vp, ctypes.POINTER(ctypes.c_int)]),
     "pamo_point_stats": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_double), _vp]),
     "pamo_affine_points": (_i, [_vp, _i, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                 ctypes.c_double, _vp, _vp]),

@@ -774,6 +774,72 @@ int pamo_point_stats(const float *d_pts, int n, double *h_out6, void *stream)
     return PAMO_OK;
 }
 
+int pamo_mesh_hinges(const int *h_tris, int n_tris, int n_pts, int *h_edges, int *h_hinges, int *out_n_edges)
+{
+    if (!h_tris || n_tris < 0 || n_pts < 0 || !out_n_edges || (n_tris && (!h_edges || !h_hinges)))
+        return PAMO_ERR_INVALID_ARG;
+    *out_n_edges = 0;
+    if (n_tris == 0) return PAMO_OK;
+    const long long nd = 3LL * n_tris;  // directed edges: corner k -> k + 1 of every face, k-major
+    for (long long i = 0; i < nd; ++i)
+        if (h_tris[i] < 0 || h_tris[i] >= n_pts) return PAMO_ERR_INVALID_ARG;
+    if (nd % 2) return PAMO_ERR_CAPACITY;
+    std::vector<int> from((size_t)nd), to((size_t)nd), opp((size_t)nd);
+    for (int k = 0; k < 3; ++k)
+        for (int f = 0; f < n_tris; ++f) {
+            const size_t e = (size_t)k * n_tris + f;
+            from[e] = h_tris[3 * (size_t)f + k];
+            to[e] = h_tris[3 * (size_t)f + (k + 1) % 3];
+            opp[e] = h_tris[3 * (size_t)f + (k + 2) % 3];
+        }
+    // bucket by the smaller vertex (counting sort, stable), then order each
+    // bucket by the larger vertex: keys ascend as lo * n + hi
+    std::vector<int> start((size_t)n_pts + 1, 0), order((size_t)nd), hi((size_t)nd);
+    for (size_t e = 0; e < (size_t)nd; ++e) {
+        start[(size_t)std::min(from[e], to[e]) + 1]++;
+        hi[e] = std::max(from[e], to[e]);
+    }
+    for (int v = 0; v < n_pts; ++v) start[(size_t)v + 1] += start[(size_t)v];
+    {
+        std::vector<int> cur(start.begin(), start.end() - 1);
+        for (size_t e = 0; e < (size_t)nd; ++e) order[(size_t)cur[(size_t)std::min(from[e], to[e])]++] = (int)e;
+    }
+    for (int v = 0; v < n_pts; ++v) {
+        const int a = start[(size_t)v], b = start[(size_t)v + 1];
+        for (int i = a + 1; i < b; ++i) {  // insertion sort by the larger vertex (stable)
+            const int x = order[(size_t)i], kx = hi[(size_t)x];
+            int j = i - 1;
+            while (j >= a && hi[(size_t)order[(size_t)j]] > kx) {
+                order[(size_t)j + 1] = order[(size_t)j];
+                --j;
+            }
+            order[(size_t)j + 1] = x;
+        }
+    }
+    // every key exactly twice, once each way
+    long long ne = 0;
+    for (long long i = 0; i < nd; i += 2) {
+        const size_t e0 = (size_t)order[(size_t)i], e1 = (size_t)order[(size_t)i + 1];
+        const int lo = std::min(from[e0], to[e0]), h = hi[e0];
+        if (lo == h || std::min(from[e1], to[e1]) != lo || hi[e1] != h || (from[e0] < to[e0]) == (from[e1] < to[e1]))
+            return PAMO_ERR_CAPACITY;
+        if (i + 2 < nd) {  // the next key must differ
+            const size_t e2 = (size_t)order[(size_t)i + 2];
+            if (std::min(from[e2], to[e2]) == lo && hi[e2] == h) return PAMO_ERR_CAPACITY;
+        }
+        const size_t ef = from[e0] < to[e0] ? e0 : e1, eb = from[e0] < to[e0] ? e1 : e0;
+        h_edges[2 * ne] = lo;
+        h_edges[2 * ne + 1] = h;
+        h_hinges[4 * ne] = opp[ef];
+        h_hinges[4 * ne + 1] = lo;
+        h_hinges[4 * ne + 2] = h;
+        h_hinges[4 * ne + 3] = opp[eb];
+        ++ne;
+    }
+    *out_n_edges = (int)ne;
+    return PAMO_OK;
+}
+
 int pamo_affine_points(const float *d_in, int n, double scale, double tx, double ty, double tz, double post,
                        float *d_out, void *stream)
 {

@@ -115,6 +115,14 @@ def hinges(F):
     kf = af * n + bf
     kb = b[mb] * n + a[mb]
     cb = c[mb]
+    # closed 2-manifold (the usual case): every edge once each way, so the two
+    # sorted key lists pair up element by element
+    if len(kf) == len(kb):
+        of = np.argsort(kf, kind="stable")
+        ob = np.argsort(kb, kind="stable")
+        kfs = kf[of]
+        if np.array_equal(kfs, kb[ob]) and (len(kfs) < 2 or bool((kfs[1:] != kfs[:-1]).all())):
+            return np.stack([cf[of], af[of], bf[of], cb[ob]], 1)
     ob = np.argsort(kb, kind="stable")
     kbs = kb[ob]
     pos = np.searchsorted(kbs, kf)
@@ -122,6 +130,46 @@ def hinges(F):
     H = np.stack([cf[ok], af[ok], bf[ok], cb[ob][pos[ok]]], 1)
     # ordered by (x1, x2): the key x1 * n + x2 orders the same way (stable, as lexsort)
     return H[np.argsort(kf[ok], kind="stable")]
+
+
+def edges_and_hinges(F):
+    """(edges_unique(F), hinges(F)).  A closed 2-manifold (every edge in
+    exactly two faces, once each way) takes the library's linear-time host
+    builder (pamo_mesh_hinges); otherwise one sort of the 3 m directed face
+    edges by undirected key pairs them up, and meshes where that fails take the
+    two separate functions.  The builder's arrays are int32, the others int64."""
+    if len(F) == 0:
+        return edges_unique(F), hinges(F)
+    F32 = np.ascontiguousarray(F, np.int32)
+    n_pts = int(F32.max()) + 1
+    cap = (3 * len(F)) // 2 + 1
+    E32, H32 = np.empty((cap, 2), np.int32), np.empty((cap, 4), np.int32)
+    ne = ctypes.c_int(0)
+    rc = _lib.lib().pamo_mesh_hinges(F32.ctypes.data, len(F32), n_pts, E32.ctypes.data, H32.ctypes.data,
+                                     ctypes.byref(ne))
+    if rc == 0:
+        return E32[:ne.value], H32[:ne.value]
+    F = np.asarray(F, np.int64)
+    a = np.concatenate([F[:, 0], F[:, 1], F[:, 2]])
+    b = np.concatenate([F[:, 1], F[:, 2], F[:, 0]])
+    c = np.concatenate([F[:, 2], F[:, 0], F[:, 1]])
+    n = int(F.max()) + 1
+    lo, hi = np.minimum(a, b), np.maximum(a, b)
+    key = lo * n + hi
+    o = np.argsort(key, kind="stable")
+    ks = key[o]
+    if len(ks) % 2 == 0:
+        k0, k1 = ks[0::2], ks[1::2]
+        o0, o1 = o[0::2], o[1::2]
+        fwd0 = a[o0] < b[o0]
+        if (np.array_equal(k0, k1) and (len(k0) < 2 or bool((k0[1:] != k0[:-1]).all()))
+                and bool((fwd0 != (a[o1] < b[o1])).all())):
+            of = np.where(fwd0, o0, o1)
+            ob = np.where(fwd0, o1, o0)
+            E = np.stack([k0 // n, k0 % n], axis=1)
+            H = np.stack([c[of], a[of], b[of], c[ob]], 1)
+            return E, H
+    return edges_unique(F), hinges(F)
 
 
 def voronoi_areas(V, F):
@@ -218,8 +266,7 @@ class Stage3System:
         dev = torch.device("cuda", self.device)
         V64 = np.asarray(V, np.float64) * c.system_scale
         F = np.asarray(F, np.int64)
-        E = edges_unique(F)
-        H = hinges(F)
+        E, H = edges_and_hinges(F)
         if len(H) != len(E):
             raise ValueError(f"number of hinges {len(H)} != number of edges {len(E)} (mesh not closed 2-manifold)")
         t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)

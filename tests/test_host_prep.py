@@ -1,8 +1,9 @@
-"""Stage-3 host preparation (pamo_b200/safe_project.py): the unique edges, the
-hinges and trimesh-style vertex merging give exactly what the plain numpy forms
-(np.unique with axis / return_index / return_inverse, lexsort) give, on closed
-meshes, on meshes with duplicated and near-duplicated vertices, and on grids
-with many equal coordinates."""
+"""Stage-3 host preparation (pamo_b200/safe_project.py and the library's
+pamo_mesh_hinges): the unique edges, the hinges and trimesh-style vertex
+merging give exactly what the plain numpy forms (np.unique with axis /
+return_index / return_inverse, lexsort) give, on closed meshes, on meshes with
+duplicated and near-duplicated vertices, on grids with many equal coordinates
+and on an open patch (where the builder declines and numpy takes over)."""
 import numpy as np
 import pytest
 
@@ -57,14 +58,33 @@ def _cases():
     V4[30] = V4[31]
     V4[40] = V4[41] + 1e-10  # equal after rounding to 8 digits
     out.append((V4, F))
+    Vo, Fo = mg.icosphere(2)
+    out.append((Vo, Fo[:60]))  # an open patch: boundary edges have one face
     return out
 
 
-@pytest.mark.parametrize("case", range(7))
+def test_mesh_hinges_rejects_bad_input():
+    import ctypes
+
+    from pamo_b200 import _lib
+
+    F = np.ascontiguousarray(mg.icosphere(1)[1], np.int32)
+    E, H, ne = np.empty((100, 2), np.int32), np.empty((100, 4), np.int32), ctypes.c_int()
+    L = _lib.lib()
+    assert L.pamo_mesh_hinges(F.ctypes.data, len(F), int(F.max()), E.ctypes.data, H.ctypes.data, ctypes.byref(ne)) \
+        == 1  # PAMO_ERR_INVALID_ARG: an index equal to n_pts
+    assert L.pamo_mesh_hinges(F.ctypes.data, 10, int(F.max()) + 1, E.ctypes.data, H.ctypes.data, ctypes.byref(ne)) \
+        == 6  # PAMO_ERR_CAPACITY: open, edges with one face
+
+
+@pytest.mark.parametrize("case", range(8))
 def test_host_prep_matches_numpy_forms(case):
     V, F = _cases()[case]
     assert np.array_equal(sp.edges_unique(F), _edges_ref(F))
     assert np.array_equal(sp.hinges(F), _hinges_ref(F))
+    E, H = sp.edges_and_hinges(F)  # the library's host builder on closed meshes
+    assert np.array_equal(E, _edges_ref(F))
+    assert np.array_equal(H, _hinges_ref(F))
     a, b = sp.merge_vertices(V, F), _merge_ref(V, F)
     assert np.array_equal(a[0], b[0])
     assert np.array_equal(np.asarray(a[1]), np.asarray(b[1]))
