@@ -157,6 +157,10 @@ typedef struct pamo_s3_config {
     float hinge_stiffness;     /* 1e-2 */
     float mesh2gt_dist_stiffness; /* 1e3 */
     long long max_blocks;      /* 2^25: contact blocks before the radius is halved */
+    /* 0.  1: the ground truth (pointers, sizes and contents) is the one of the
+       context's previous call, so its device copy and hierarchy are kept
+       (no reference counterpart: the reference registers it every time) */
+    int reuse_gt;
 } pamo_s3_config;
 
 void pamo_s3_default_config(pamo_s3_config *cfg);

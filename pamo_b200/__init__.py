@@ -198,6 +198,7 @@ class PaMO:
                     self._gt_f_pinned = torch.from_numpy(self.gt_mesh[1].astype(np.int32)).pin_memory()
                 gt_v = self._gt_f32_pinned
             gt_f = self._gt_f_pinned if self._gt_f32 is not None else self.gt_mesh[1]
-            verts, faces = process(gt_v, gt_f, v2, f2, 5, system=self.system, config=self.config)
+            # the ground truth is this object's own copy, the same on every run
+            verts, faces = process(gt_v, gt_f, v2, f2, 5, system=self.system, config=self.config, gt_static=True)
             self.timings["stage3"] = time.time() - t0
         return verts, faces

@@ -673,6 +673,7 @@ void pamo_s3_default_config(pamo_s3_config *c)
     c->hinge_stiffness = 1e-2f;
     c->mesh2gt_dist_stiffness = 1e3f;
     c->max_blocks = 1LL << 25;
+    c->reuse_gt = 0;
 }
 
 int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int n_gt_v, int n_gt_f,

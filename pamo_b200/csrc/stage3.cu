@@ -1542,6 +1542,7 @@ __global__ void k_f4_to_aos(const float4 *in, float *out, int n)
 
 void Stage3::release()
 {
+    gt_ready = false;
     void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, v2, Av, Avc, q_gather, wk, tris, area, inv_dm,
                     edges4, hinges, rest_angle, rest_elen, row_ptr, col, kval, tri_slot, hinge_slot, diag_slot, hblk, pat_cnt,
                     pat_cur, pat_off, pat_cand, pat_scan, bidx, bkind, bsub, bd, bb2, bg, bact, gt_pts, gt_tris, dscal, fscal,
@@ -1658,8 +1659,11 @@ int Stage3::register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, in
                           const int *d_f, int n_v, int n_f, const int *d_e, int n_e, const int *d_h, int n_h,
                           const float *d_vor, cudaStream_t s)
 {
-    int rc = ensure(n_v, n_f, n_e, n_h, n_gt_v, n_gt_f);
+    const int prev_gp = ngp, prev_gt = ngt;
+    int rc = ensure(n_v, n_f, n_e, n_h, n_gt_v, n_gt_f);  // a reallocation clears gt_ready
     if (rc) return rc;
+    const bool keep_gt = cfg.reuse_gt && gt_ready && d_gt_v == gt_src_v && d_gt_f == gt_src_f && n_gt_v == prev_gp &&
+                         n_gt_f == prev_gt;
     drop_graph();  // sizes and configuration are baked into the captured iteration
     gathered = false;  // new geometry: contact candidates are gathered again
     np = n_v; nt = n_f; ne = n_e; nh = n_h; ngp = n_gt_v; ngt = n_gt_f;
@@ -1668,15 +1672,23 @@ int Stage3::register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, in
     launch(k_aos_to_i4, grid_for(nt), kThreads, 0, s, d_f, tris, nt, 3, 0);
     launch(k_aos_to_i4, grid_for(ne), kThreads, 0, s, d_e, edges4, ne, 2, 1);
     launch(k_aos_to_i4, grid_for(nh), kThreads, 0, s, d_h, hinges, nh, 4, 0);
-    launch(k_aos_to_f4, grid_for(ngp), kThreads, 0, s, d_gt_v, gt_pts, nullptr, ngp);
-    launch(k_aos_to_i4, grid_for(ngt), kThreads, 0, s, d_gt_f, gt_tris, ngt, 3, 0);
+    if (!keep_gt) {
+        launch(k_aos_to_f4, grid_for(ngp), kThreads, 0, s, d_gt_v, gt_pts, nullptr, ngp);
+        launch(k_aos_to_i4, grid_for(ngt), kThreads, 0, s, d_gt_f, gt_tris, ngt, 3, 0);
+    }
     // Voronoi areas x GT-distance stiffness
     S3_TRY(cudaMemcpyAsync(wk, d_vor, (size_t)np * 4, cudaMemcpyDeviceToDevice, s));
     launch(k_scale, grid_for(np), kThreads, 0, s, wk, np, cfg.mesh2gt_dist_stiffness);
     launch(k_elastic_pre, grid_for(nt), kThreads, 0, s, q, tris, nt, area, inv_dm);
     launch(k_hinge_pre, grid_for(nh), kThreads, 0, s, q, hinges, nh, rest_angle, rest_elen);
-    S3_TRY(lbvh_build(gt_bvh, gt_pts, gt_tris, ngt, s));
-    S3_TRY(lbvh_refit(gt_bvh, gt_pts, gt_tris, ngt, s));
+    if (!keep_gt) {
+        gt_ready = false;
+        S3_TRY(lbvh_build(gt_bvh, gt_pts, gt_tris, ngt, s));
+        S3_TRY(lbvh_refit(gt_bvh, gt_pts, gt_tris, ngt, s));
+        gt_src_v = d_gt_v;
+        gt_src_f = d_gt_f;
+        gt_ready = true;
+    }
     S3_TRY(lbvh_build(tri_bvh, q, tris, nt, s));
     S3_TRY(lbvh_build(edge_bvh, q, edges4, ne, s));
     S3_TRY(cudaMemsetAsync(iscal, 0, 64, s));

@@ -66,6 +66,10 @@ struct Stage3 {
     Lbvh tri_bvh, edge_bvh, gt_bvh;
     float4 *gt_pts = nullptr;
     int4 *gt_tris = nullptr;
+    // the ground truth of the last registration (kept when cfg.reuse_gt says so)
+    const float *gt_src_v = nullptr;
+    const int *gt_src_f = nullptr;
+    bool gt_ready = false;
     // scalars and reduction partials
     double *dscal = nullptr;  // [0] energy [1] energy_prev [2] zr [3] zr_last [4] vAv
     float *fscal = nullptr;   // [0] ccd step

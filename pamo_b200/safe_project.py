@@ -28,7 +28,8 @@ class pamo_s3_config(ctypes.Structure):
                 ("ee_classify_thres", ctypes.c_float), ("ccd_slackness", ctypes.c_float),
                 ("ccd_thickness", ctypes.c_float), ("elas_young_modulus", ctypes.c_float),
                 ("elas_poisson_ratio", ctypes.c_float), ("hinge_stiffness", ctypes.c_float),
-                ("mesh2gt_dist_stiffness", ctypes.c_float), ("max_blocks", ctypes.c_longlong)]
+                ("mesh2gt_dist_stiffness", ctypes.c_float), ("max_blocks", ctypes.c_longlong),
+                ("reuse_gt", ctypes.c_int)]
 
 
 class Stage3Config:
@@ -40,6 +41,7 @@ class Stage3Config:
         self.seed = 0
         self.max_particles = 1 << 20
         self.max_blocks = 1 << 25
+        self.reuse_gt = 0  # set per call by Stage3System.project
         self.max_gt_particles = 1 << 24
         self.max_gt_samples = 1 << 14
         self.n_newton_iters = 10
@@ -251,15 +253,21 @@ class Stage3System:
         self.device = device
         self.ctx = Context(device)
         self.last_stats = None
+        # a ground truth that stays the same from call to call (PaMO.run's):
+        # its device copies, normalisation and the library's hierarchy are kept
+        self._gt_raw = None   # ((gt_V, gt_F), raw device points, scale, t)
+        self._gt_norm = None  # ((raw points, gt_F, scale, t, system_scale), normalised points, faces)
 
     def clear(self):
         self.last_stats = None
 
-    def project(self, gt_V, gt_F, V, F, n_steps, gt_affine=None):
+    def project(self, gt_V, gt_F, V, F, n_steps, gt_affine=None, gt_static=False):
         """Normalised-frame arrays in, projected vertices (float32) out.  With
         gt_affine = (scale, t), gt_V holds the raw ground-truth points and the
         normalisation gt_V * scale + t is applied on the device (float64, then
-        rounded to float32 as the host path does)."""
+        rounded to float32 as the host path does).  gt_static: the caller
+        promises that gt_V / gt_F are the same objects with the same contents
+        as in its earlier calls, so their device forms are kept."""
         import torch
 
         c = self.config
@@ -279,7 +287,16 @@ class Stage3System:
         check("pamo_voronoi_areas", _lib.lib().pamo_voronoi_areas(
             d_v64.data_ptr(), d_f.data_ptr(), len(V64), len(F), d_w.data_ptr(), ctypes.byref(min_ang), stream))
         do_nothing = min_ang.value <= c.min_angle_thres
-        if gt_affine is None:
+        reuse = 0
+        key = None
+        if gt_static and gt_affine is not None:
+            key = (gt_V, gt_F, float(gt_affine[0]), tuple(float(x) for x in gt_affine[1]), float(c.system_scale))
+            old = self._gt_norm
+            if old is not None and old[0][0] is key[0] and old[0][1] is key[1] and old[0][2:] == key[2:]:
+                reuse = 1
+        if reuse:
+            _, d_gv, d_gf = self._gt_norm
+        elif gt_affine is None:
             d_gv = t(np.asarray(gt_V, np.float64) * c.system_scale, np.float32)
         else:
             raw = gt_V if isinstance(gt_V, torch.Tensor) else t(gt_V, np.float32)
@@ -289,11 +306,14 @@ class Stage3System:
             check("pamo_affine_points", _lib.lib().pamo_affine_points(
                 raw.data_ptr(), int(raw.shape[0]), float(sc), float(tr[0]), float(tr[1]), float(tr[2]),
                 float(c.system_scale), d_gv.data_ptr(), stream))
-        d_gf = gt_F.to(dev, torch.int32).contiguous() if isinstance(gt_F, torch.Tensor) else t(gt_F, np.int32)
+        if not reuse:
+            d_gf = gt_F.to(dev, torch.int32).contiguous() if isinstance(gt_F, torch.Tensor) else t(gt_F, np.int32)
+            self._gt_norm = (key, d_gv, d_gf) if key is not None else None
         d_v = d_v64.to(torch.float32)
         d_e, d_h = t(E, np.int32), t(H, np.int32)
         out = torch.empty((len(V64), 3), dtype=torch.float32, device=dev)
         cfg = c.to_c()
+        cfg.reuse_gt = reuse
         check("pamo_safe_project", _lib.lib().pamo_safe_project(
             self.ctx.handle, d_gv.data_ptr(), d_gf.data_ptr(), len(d_gv), len(d_gf), d_v.data_ptr(), d_f.data_ptr(),
             len(V64), len(F), d_e.data_ptr(), len(E), d_h.data_ptr(), len(H), d_w.data_ptr(), int(n_steps),
@@ -306,7 +326,7 @@ class Stage3System:
 
 
 def process(gt_V, gt_F, stage2_V, stage2_F, n_iters, system: Stage3System | None = None,
-            config: Stage3Config | None = None, eval=False, return_curve=False):
+            config: Stage3Config | None = None, eval=False, return_curve=False, gt_static=False):
     """processing.py:23-108: normalise by the ground truth, project, undo the
     normalisation.  Faces are returned unchanged."""
     if system is None:
@@ -321,20 +341,26 @@ def process(gt_V, gt_F, stage2_V, stage2_F, n_iters, system: Stage3System | None
         # cast to float32 all run on the device (the mean is a fixed-order
         # double sum, which rounds differently from numpy's by ~1e-16)
         dev = torch.device("cuda", system.device)
-        d_gt = gt_V if isinstance(gt_V, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(gt_V))
-        d_gt = d_gt.to(dev, torch.float32, non_blocking=True).contiguous()
-        st = (ctypes.c_double * 6)()
-        check("pamo_point_stats", _lib.lib().pamo_point_stats(
-            d_gt.data_ptr(), int(d_gt.shape[0]), st, ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
-        center = np.array(st[0:3])
-        scale = 1.0 / max(st[3], st[4], st[5])
-        t = -center * scale
+        old = system._gt_raw if gt_static else None
+        if old is not None and old[0][0] is gt_V and old[0][1] is gt_F:
+            _, d_gt, scale, t = old
+        else:
+            d_gt = gt_V if isinstance(gt_V, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(gt_V))
+            d_gt = d_gt.to(dev, torch.float32, non_blocking=True).contiguous()
+            st = (ctypes.c_double * 6)()
+            check("pamo_point_stats", _lib.lib().pamo_point_stats(
+                d_gt.data_ptr(), int(d_gt.shape[0]), st, ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+            center = np.array(st[0:3])
+            scale = 1.0 / max(st[3], st[4], st[5])
+            t = -center * scale
+            system._gt_raw = ((gt_V, gt_F), d_gt, scale, t) if gt_static else None
         gt_in = d_gt
     else:  # float64 ground truth: normalised on the host, as processing.py does
         scale, t = normalization(gt_V)
         gt_in = np.asarray(gt_V, np.float64) * scale + t
     sV = np.asarray(stage2_V, np.float64) * scale + t
-    q = system.project(gt_in, gt_F, sV, stage2_F, n_iters, gt_affine=(scale, t) if on_device else None)
+    q = system.project(gt_in, gt_F, sV, stage2_F, n_iters, gt_affine=(scale, t) if on_device else None,
+                       gt_static=gt_static and on_device)
     return (q.astype(np.float64) - t) / scale, np.asarray(stage2_F)
 
 

@@ -105,3 +105,25 @@ def test_pamo_run_all_stages_but_remesh(torch_cuda):
     v, f = pm.run(torch_cuda.from_numpy(V).cuda(), torch_cuda.from_numpy(F).cuda(), 0.1, min_verts=0)
     assert v.shape[1] == 3 and f.shape[1] == 3 and len(f) <= int(0.1 * len(F))
     assert np.isfinite(v).all()
+
+
+def test_pamo_run_keeps_ground_truth_between_runs(torch_cuda):
+    """A PaMO object keeps its ground truth on the device after the first run
+    (its normalisation, copies and hierarchy); later runs give what a fresh
+    object gives, within the CG's summation-order noise."""
+    import pamo_b200
+    from pamo_b200 import meshgen as mg
+
+    V, F = mg.displaced_icosphere(4, 2)
+    V = V.astype(np.float32)
+    args = (torch_cuda.from_numpy(V).cuda(), torch_cuda.from_numpy(F).cuda(), 0.1)
+    pm = pamo_b200.PaMO((V, F), use_stage1=False, use_stage3=True, verbose=False)
+    v1, f1 = pm.run(*args, min_verts=0)
+    assert pm.system._gt_norm is not None
+    v2, f2 = pm.run(*args, min_verts=0)  # the kept ground truth
+    fresh = pamo_b200.PaMO((V, F), use_stage1=False, use_stage3=True, verbose=False)
+    v3, f3 = fresh.run(*args, min_verts=0)
+    diag = float(np.linalg.norm(V.max(0) - V.min(0)))
+    assert np.array_equal(f1, f2) and np.array_equal(f1, f3)
+    assert np.abs(v2 - v3).max() / diag < 1e-6
+    assert np.abs(v1 - v2).max() / diag < 1e-6
