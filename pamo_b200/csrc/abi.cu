@@ -704,6 +704,11 @@ int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int
     if (!S.work) CU_RET(cudaStreamCreateWithFlags(&S.work, cudaStreamNonBlocking));
     if (!S.ev_in) CU_RET(cudaEventCreateWithFlags(&S.ev_in, cudaEventDisableTiming));
     if (!S.ev_out) CU_RET(cudaEventCreateWithFlags(&S.ev_out, cudaEventDisableTiming));
+    for (int b = 0; b < 2; ++b) {
+        if (!S.side[b]) CU_RET(cudaStreamCreateWithFlags(&S.side[b], cudaStreamNonBlocking));
+        if (!S.ev_join[b]) CU_RET(cudaEventCreateWithFlags(&S.ev_join[b], cudaEventDisableTiming));
+    }
+    if (!S.ev_fork) CU_RET(cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming));
     CU_RET(cudaEventRecord(S.ev_in, s));
     CU_RET(cudaStreamWaitEvent(S.work, S.ev_in, 0));
     cudaStream_t caller = s;

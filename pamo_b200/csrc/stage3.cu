@@ -32,7 +32,7 @@ constexpr int kStack = 96;
 
 enum { D_ENERGY = 0, D_ENERGY_PREV, D_ZR, D_ZR_LAST, D_VAV };
 enum { I_NB = 0, I_OVERFLOW, I_STACK, I_NACT, I_NCAND_PT, I_NCAND_EE, I_TICKET, I_DISP, I_BAR_ERR, I_BAR_COUNT,
-       I_BAR_GEN };
+       I_BAR_GEN, I_ETICKET };
 
 __device__ __forceinline__ F3 ld(const float4 *a, int i) { return f3(a[i]); }
 __device__ __forceinline__ void st(float4 *a, int i, F3 v) { a[i] = make_float4(v.x, v.y, v.z, 0.f); }
@@ -72,13 +72,31 @@ __device__ __forceinline__ double block_sum(double v)
     return r;
 }
 
-// sums partials[0..n) in a fixed order into dst (one warp)
-__global__ void k_finish_sum(const double *partials, int n, double *dst)
+// Each reduction kernel writes one partial per block; the last block to finish
+// (a ticket counter, no waiting) adds the partials in a fixed order (32 lanes
+// strided over the blocks, then a shuffle tree), so the sums are deterministic
+// and a separate finishing launch is not needed.  Returns true in the last block (all its threads).
+__device__ __forceinline__ bool last_block_sum(double block_total, double *partials, int *ticket, double *dst)
 {
-    double v = 0.0;
-    for (int i = threadIdx.x; i < n; i += 32) v += partials[i];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) *dst = v;
+    __shared__ bool s_last;
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = block_total;
+        __threadfence();
+        s_last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) v += __ldcg(&partials[i]);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) {
+            *dst = v;
+            *ticket = 0;
+        }
+    }
+    return true;
 }
 
 // ------------------------------------------------------------ preprocessing
@@ -411,14 +429,14 @@ struct EArgs {
     const int *bkind;
     int *bsub;
     float *bd;
-    const int *iscal;
+    int *iscal;  // block count; I_ETICKET: the energy sum's ticket
     long long cap_b;
     float d_hat, kappa, ee_thres;
     double *partials;
     // line search: halving n_halves > 0 is skipped once a trial was accepted
     // (energy below the start's), as the reference's loop stops there
     int n_halves;
-    const double *dscal;
+    double *dscal;  // D_ENERGY: written by the last block
     // line search (n_halves >= 0): the largest step length of a vertex, which
     // bounds how far a block's distance can have moved from the start's bd
     const float *step_bound;
@@ -438,7 +456,7 @@ __device__ __forceinline__ void elastic_F(const float4 *q, int4 f, float4 im, F3
 
 __global__ void __launch_bounds__(kThreads) k_energy(EArgs A)
 {
-    // the partials then still hold the accepted trial's energy
+    // D_ENERGY then still holds the accepted trial's energy
     if (A.n_halves > 0 && A.dscal[D_ENERGY] < A.dscal[D_ENERGY_PREV]) return;
     const long long nb = min((long long)A.iscal[I_NB], A.cap_b);
     const long long total = (long long)A.np + A.nt + A.nh + nb;
@@ -488,8 +506,7 @@ __global__ void __launch_bounds__(kThreads) k_energy(EArgs A)
             if (d < A.d_hat) acc += barrier((double)d, (double)A.d_hat) * (double)A.kappa;
         }
     }
-    double r = block_sum<kThreads>(acc);
-    if (threadIdx.x == 0) A.partials[blockIdx.x] = r;
+    last_block_sum(block_sum<kThreads>(acc), A.partials, A.iscal + I_ETICKET, A.dscal + D_ENERGY);
 }
 
 // --------------------------------------------------------------------- diff
@@ -648,13 +665,19 @@ __device__ __forceinline__ void membrane_apply(F3 b1, F3 b2, const float F[4], f
     f2 = H01 * b1 + H11 * b2;
 }
 
-__global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
+// One kind of element per launch (PART 0 membranes, 1 hinges, 2 contact
+// blocks), so the three run as concurrent branches of the iteration and each
+// is compiled for its own register count.
+template <int PART>
+__global__ void __launch_bounds__(128) k_diff_part(DArgs A)
 {
     const long long nb = min((long long)A.iscal[I_NB], A.cap_b);
-    const long long total = (long long)A.nt + A.nh + nb;
-    PAMO_GRID_STRIDE(k, total)
+    const long long first = PART == 0 ? 0 : PART == 1 ? (long long)A.nt : (long long)A.nt + A.nh;
+    const long long count = PART == 0 ? (long long)A.nt : PART == 1 ? (long long)A.nh : nb;
+    PAMO_GRID_STRIDE(j, count)
     {
-        if (k < A.nt) {
+        const long long k = first + j;
+        if (PART == 0) {
             int t = (int)k;
             int4 f = A.tris[t];
             F3 b1, b2;
@@ -707,7 +730,7 @@ __global__ void __launch_bounds__(128) k_diff_elements(DArgs A)
                         }
                     add_block(A.kval, slot[3 * a + b], blk);
                 }
-        } else if (k < (long long)A.nt + A.nh) {
+        } else if (PART == 1) {
             int h = (int)(k - A.nt);
             int4 i = A.hinges[h];
             int idx[4] = {i.x, i.y, i.z, i.w};
@@ -873,7 +896,7 @@ __global__ void __launch_bounds__(64) k_hinge_spd(const float *hblk, int nh, int
 // ---------------------------------------------------------------- A * dx
 // The operator of the CG: rows of the assembled block matrix (vertex term,
 // membrane, hinges) plus the rank-one Gauss-Newton terms of the contact blocks
-// with d < d_hat (listed by k_diff_elements).
+// with d < d_hat (listed by k_diff_part<2>).
 struct OpArgs {
     int np;
     const int *row_ptr, *col;
@@ -1106,32 +1129,6 @@ __global__ void k_diag_term(const float *wk, const int *diag_slot, int np, float
 }
 
 // -------------------------------------------------------------------- CG
-// Each reduction kernel writes one partial per block; the last block to finish
-// (a ticket counter, no waiting) adds the partials in a fixed order -- the order
-// k_finish_sum uses -- so the sums are deterministic and a separate finishing
-// launch is not needed.  Returns true in the last block (all its threads).
-__device__ __forceinline__ bool last_block_sum(double block_total, double *partials, int *ticket, double *dst)
-{
-    __shared__ bool s_last;
-    if (threadIdx.x == 0) {
-        partials[blockIdx.x] = block_total;
-        __threadfence();
-        s_last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!s_last) return false;
-    __threadfence();
-    if (threadIdx.x < 32) {
-        double v = 0.0;
-        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) v += __ldcg(&partials[i]);
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) {
-            *dst = v;
-            *ticket = 0;
-        }
-    }
-    return true;
-}
 
 __global__ void __launch_bounds__(kThreads) k_cg_init(const float4 *grad, const float4 *diag, int np, float4 *p,
                                                       float4 *r, float4 *z, float4 *v, double *partials, int *ticket,
@@ -1212,24 +1209,28 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const f
 // read at the start.
 //
 // A sum: every block writes its partial with a release store into its own slot
-// of the sum's parity (slots hold an all-ones pattern until written: a negative
-// NaN that no sum produces, since sums and products give the positive canonical
-// NaN); block 0 waits for all slots with acquire loads, adds them in block order
-// and publishes the total the same way, and the other blocks wait for that.
-// The sums therefore do not depend on scheduling, and a block's writes before
-// its partial are visible to every block after the total.  Block 0 resets a
-// partial slot once it has read it (it is written again two sums later, after
-// block 0's next release), and the other total slot before publishing (every
-// block read it before writing this sum's partial).  Waits spin with a limit;
-// on timeout the error is recorded and the kernel returns.
+// of the sum's set (three sets, used in turn; slots hold an all-ones pattern
+// until written: a negative NaN that no sum produces, since sums and products
+// give the positive canonical NaN), then waits for all slots of the set with
+// acquire loads, one thread per slot, and adds them in block order -- the same
+// order in every block, so every block gets the same total, independent of
+// scheduling, with one hop between the blocks.  A block's writes before its
+// partial are visible to every block after the sum.  Once a block has seen all
+// partials of sum k, every block has finished reading sum k - 1, so it resets
+// its own slot of that set, which sum k + 2 reuses (the reset precedes its
+// release of sum k + 1, which every reader of sum k + 2 has acquired).  Slots
+// sit one 128-byte line apart.  Waits spin with a limit; on timeout the error
+// is recorded and the kernel returns.
 constexpr int kCgThreads = 512;
 constexpr unsigned long long kSumPending = ~0ull;
+constexpr int kSlotStride = 16;  // u64 words per slot
+constexpr int kSlotSets = 3;
 
 struct CGArgs {
     OpArgs op;
     const float4 *grad, *diag;
     float4 *p, *r, *z, *v0, *v1, *Av, *Avc;
-    unsigned long long *slots;  // 2 x gridDim partial slots, then 2 total slots (all ones before the solve)
+    unsigned long long *slots;  // kSlotSets x gridDim slots, kSlotStride apart (all ones before the solve)
     int *iscal;
     int np, n_iters;
 };
@@ -1237,6 +1238,11 @@ struct CGArgs {
 __device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v)
 {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_relaxed(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p)
@@ -1265,50 +1271,36 @@ __device__ __forceinline__ bool wait_value(const unsigned long long *p, unsigned
 // a wait timeout.
 __device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, int k, double &total)
 {
-    __shared__ int s_ok;
     __shared__ double s_val;
-    __shared__ double s_part[kCgThreads];  // block 0: every block's partial, in block order
+    __shared__ double s_part[kCgThreads];  // every block's partial, in block order
     const int G = (int)gridDim.x;
-    unsigned long long *part = A.slots + (size_t)(k & 1) * G;
-    unsigned long long *tot = A.slots + 2 * (size_t)G + (k & 1), *tot_next = A.slots + 2 * (size_t)G + ((k + 1) & 1);
+    const size_t set_words = (size_t)G * kSlotStride;
+    unsigned long long *set = A.slots + (size_t)(k % kSlotSets) * set_words;
+    unsigned long long *prev = A.slots + (size_t)((k + kSlotSets - 1) % kSlotSets) * set_words;
     const double bs = block_sum<kCgThreads>(acc);
-    if (threadIdx.x == 0) {
-        s_ok = 1;
-        st_release(part + blockIdx.x, (unsigned long long)__double_as_longlong(bs));
-    }
-    if (blockIdx.x == 0) {
-        // thread i waits for block i's partial (all in parallel), then warp 0
-        // adds them in block order
-        int ok = 1;
-        if ((int)threadIdx.x < G) {
-            unsigned long long bits = 0;
-            if (wait_value(part + threadIdx.x, bits, A.iscal)) {
-                s_part[threadIdx.x] = __longlong_as_double((long long)bits);
-                part[threadIdx.x] = kSumPending;  // rewritten two sums later, after block 0's next release
-            } else {
-                ok = 0;
-            }
-        }
-        ok = __syncthreads_and(ok);
-        if (threadIdx.x < 32) {
-            double v = 0.0;
-            for (int i = threadIdx.x; i < G; i += 32) v += s_part[i];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (threadIdx.x == 0) {
-                *tot_next = kSumPending;
-                if (ok) st_release(tot, (unsigned long long)__double_as_longlong(v));
-                s_val = v;
-                s_ok = ok;
-            }
-        }
-    } else if (threadIdx.x == 0) {
+    if (threadIdx.x == 0)
+        st_release(set + (size_t)blockIdx.x * kSlotStride, (unsigned long long)__double_as_longlong(bs));
+    int ok = 1;
+    if ((int)threadIdx.x < G) {
         unsigned long long bits = 0;
-        if (wait_value(tot, bits, A.iscal)) s_val = __longlong_as_double((long long)bits);
-        else s_ok = 0;
+        if (wait_value(set + (size_t)threadIdx.x * kSlotStride, bits, A.iscal))
+            s_part[threadIdx.x] = __longlong_as_double((long long)bits);
+        else
+            ok = 0;
+    }
+    ok = __syncthreads_and(ok);
+    if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (int i = threadIdx.x; i < G; i += 32) v += s_part[i];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) {
+            s_val = v;
+            if (ok) st_relaxed(prev + (size_t)blockIdx.x * kSlotStride, kSumPending);
+        }
     }
     __syncthreads();
     total = s_val;
-    return s_ok != 0;
+    return ok != 0;
 }
 
 __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
@@ -1557,6 +1549,14 @@ void Stage3::release()
     if (ev_out) cudaEventDestroy(ev_out);
     work = nullptr;
     ev_in = ev_out = nullptr;
+    for (int b = 0; b < 2; ++b) {
+        if (side[b]) cudaStreamDestroy(side[b]);
+        if (ev_join[b]) cudaEventDestroy(ev_join[b]);
+        side[b] = nullptr;
+        ev_join[b] = nullptr;
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    ev_fork = nullptr;
     for (void *x : ptrs)
         if (x) cudaFree(x);
     if (h_iscal) cudaFreeHost(h_iscal);
@@ -1610,7 +1610,7 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
     }
     A3(gt_pts, cgp * 16); A3(gt_tris, cgt * 16);
     A3(dscal, 64); A3(fscal, 64); A3(iscal, 64);
-    A3(partials, 2 * kRedBlocks * 8);  // two buffers for the persistent solve
+    A3(partials, (size_t)kSlotSets * kRedBlocks * kSlotStride * 8);  // reduction partials; the persistent solve's slots
 #undef A3
     if (cudaMallocHost((void **)&h_iscal, 64) != cudaSuccess || cudaMallocHost((void **)&h_dscal, 64) != cudaSuccess) {
         release();
@@ -1816,7 +1816,6 @@ static int energy_pass(Stage3 &S, cudaStream_t s, int n_halves = -1)
             S.hinges, S.rest_angle, S.rest_elen, S.cfg.hinge_stiffness, S.bidx, S.bkind, S.bsub, S.bd, S.iscal, S.cap_b,
             S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials, n_halves, S.dscal, S.fscal + 1};
     launch(k_energy, kRedBlocks, kThreads, 0, s, e);
-    launch(k_finish_sum, 1, 32, 0, s, S.partials, kRedBlocks, S.dscal + D_ENERGY);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
@@ -1881,7 +1880,6 @@ int Stage3::newton_body(cudaStream_t s)
     int rc;
     if (prof) prof->begin(PH_S3_DIFF, s);
     S3_TRY(cudaMemcpyAsync(q_det, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
-    if ((rc = energy_pass(*this, s))) return rc;
     // gradient (coefficient -1) and diagonal
     launch(k_diff_vertex, grid_for(np), kThreads, 0, s, q, target, wk, np, grad, diag);
     DArgs d{q, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
@@ -1889,14 +1887,28 @@ int Stage3::newton_body(cudaStream_t s)
                 ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
             hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, kval, tri_slot, hinge_slot, hblk, bidx,
             bkind, bsub, bd, bg, bb2, iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag, bact};
-    // the Hessian's values: zero, the vertex term, then the elements (k_diff_elements)
+    // the Hessian's values: zero and the vertex term, then the elements
     S3_TRY(cudaMemsetAsync(kval, 0, (size_t)nnz * 48, s));
     launch(k_diag_term, grid_for(np), kThreads, 0, s, (const float *)wk, (const int *)diag_slot, np, kval);
     S3_TRY(cudaMemsetAsync(iscal + I_NACT, 0, sizeof(int), s));
-    launch(k_diff_elements, grid_for((long long)nt + nh + cap_b, 128), 128, 0, s, d);
-    if (nh > 0)
-        launch(k_hinge_spd, (int)((nh + 63) / 64), 64, 0, s, (const float *)hblk, nh, cfg.spd_max_iters,
+    // Three independent branches, all adding into grad, diag and the Hessian's
+    // values by atomics: [energy at the iterate (the blocks' distances and
+    // classes) -> contact terms] and [hinge terms -> their SPD projection] on
+    // the side streams, the membranes here; they meet before the solve.
+    S3_TRY(cudaEventRecord(ev_fork, s));
+    for (int b = 0; b < 2; ++b) S3_TRY(cudaStreamWaitEvent(side[b], ev_fork, 0));
+    if ((rc = energy_pass(*this, side[0]))) return rc;
+    launch(k_diff_part<2>, grid_for(cap_b, 128), 128, 0, side[0], d);
+    if (nh > 0) {
+        launch(k_diff_part<1>, grid_for(nh, 128), 128, 0, side[1], d);
+        launch(k_hinge_spd, (int)((nh + 63) / 64), 64, 0, side[1], (const float *)hblk, nh, cfg.spd_max_iters,
                (const int *)hinge_slot, kval);
+    }
+    launch(k_diff_part<0>, grid_for(nt, 128), 128, 0, s, d);
+    for (int b = 0; b < 2; ++b) {
+        S3_TRY(cudaEventRecord(ev_join[b], side[b]));
+        S3_TRY(cudaStreamWaitEvent(s, ev_join[b], 0));
+    }
     // Jacobi-preconditioned CG (cg_solver.py:96-158)
     if (prof) prof->begin(PH_S3_CG, s);
     if (cg_persistent < 0) {  // first use: can all blocks of the solve be resident at once?
@@ -1911,11 +1923,10 @@ int Stage3::newton_body(cudaStream_t s)
     }
     const OpArgs op{np, row_ptr, col, kval, bidx, bg, bb2, bact, iscal, cap_b};
     if (cg_persistent == 1) {
-        // partials (2 x kRedBlocks doubles) hold the solve's 2 x cg_blocks partial
-        // slots and its two total slots, all set to kSumPending
+        // partials hold the solve's kSlotSets x cg_blocks slots, all set to kSumPending
         unsigned long long *slots = reinterpret_cast<unsigned long long *>(partials);
         CGArgs ca{op, grad, diag, p, r, z, v, v2, Av, Avc, slots, iscal, np, cfg.n_cg_iters};
-        S3_TRY(cudaMemsetAsync(slots, 0xFF, (2 * (size_t)cg_blocks + 2) * sizeof(unsigned long long), s));
+        S3_TRY(cudaMemsetAsync(slots, 0xFF, (size_t)kSlotSets * cg_blocks * kSlotStride * sizeof(unsigned long long), s));
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(cg_blocks);
         lc.blockDim = dim3(kCgThreads);

@@ -85,6 +85,9 @@ struct Stage3 {
     int cg_persistent = -1;  // 1: one cooperative launch per solve; 0: one launch per phase; -1: not decided
     cudaStream_t work = nullptr;  // the solve's own stream (graphs cannot be captured on the legacy stream)
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    // the differentials' two side branches (created with the solve's stream)
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
 
     int ensure(long long np_, long long nt_, long long ne_, long long nh_, long long ngp_, long long ngt_);
     int ensure_blocks(long long nb);
