@@ -823,18 +823,19 @@ __global__ void __launch_bounds__(64) k_hinge_spd(const float *hblk, int nh, int
                     float sg = theta >= 0.f ? 1.f : -1.f;
                     float t = sg / (fabsf(theta) + sqrtf(theta * theta + 1.f));
                     float c = 1.f / sqrtf(t * t + 1.f), s = t * c;
+                    // A <- J^T A J in the symmetric form: rows and columns p and q
+                    // (a_pq becomes 0, a_pp and a_qq move by -/+ t a_pq)
 #pragma unroll
-                    for (int k = 0; k < 9; ++k) {  // A <- A J
-                        float akp = A[k][p], akq = A[k][qq];
-                        A[k][p] = c * akp - s * akq;
-                        A[k][qq] = s * akp + c * akq;
+                    for (int k = 0; k < 9; ++k) {
+                        if (k == p || k == qq) continue;
+                        const float akp = A[k][p], akq = A[k][qq];
+                        const float nkp = c * akp - s * akq, nkq = s * akp + c * akq;
+                        A[k][p] = A[p][k] = nkp;
+                        A[k][qq] = A[qq][k] = nkq;
                     }
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) {  // A <- J^T A
-                        float apk = A[p][k], aqk = A[qq][k];
-                        A[p][k] = c * apk - s * aqk;
-                        A[qq][k] = s * apk + c * aqk;
-                    }
+                    A[p][p] -= t * apq;
+                    A[qq][qq] += t * apq;
+                    A[p][qq] = A[qq][p] = 0.f;
 #pragma unroll
                     for (int k = 0; k < 9; ++k) {  // V <- V J
                         float vkp = V[k][p], vkq = V[k][qq];
@@ -1322,6 +1323,18 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
     }
 #pragma unroll
     for (int k = 0; k < kRowBatch; ++k) c0[k] = s0 + 4 * k < e0 ? O.col[s0 + 4 * k] : -1;
+    // contact blocks are taken from the top of the grid down, by threads that
+    // hold no rows when there are few of them; a thread's first block (index,
+    // curvature, vertices) is kept for the whole solve
+    const long long tc = gs - 1 - t0;
+    int cb0 = -1;
+    float cc0 = 0.f;
+    int4 ci0 = make_int4(0, 0, 0, 0);
+    if (tc < nb) {
+        cb0 = O.bact[tc];
+        cc0 = O.bb2[cb0];
+        ci0 = O.bidx[cb0];
+    }
     // r = g, z = g / (diag + 1e-6), p = 0, Avc = 0
     double acc = 0.0;
     for (long long i = t0; i < A.np; i += gs) {
@@ -1396,7 +1409,28 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
                 acc += (double)dot(own, kv);
             }
         }
-        acc += op_contacts(O, t0, gs, dir, A.Avc, nb);
+        for (long long k = tc; k < nb; k += gs) {
+            int b = cb0;
+            float c = cc0;
+            int4 i4 = ci0;
+            if (k != tc) {
+                b = O.bact[k];
+                c = O.bb2[b];
+                i4 = O.bidx[b];
+            }
+            if (c == 0.f) continue;
+            const int idx[4] = {i4.x, i4.y, i4.z, i4.w};
+            F3 g[4];
+            float sdx = 0.f;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                g[a] = f3(O.bg[4 * (size_t)b + a]);
+                sdx += dot(g[a], dir(idx[a]));
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a) atomic_add3(A.Avc, idx[a], (c * sdx) * g[a]);
+            acc += (double)(c * sdx) * (double)sdx;
+        }
         if (!grid_sum(acc, A, nsum++, vav)) return;
         zr_last = zr;
         const bool upd = vav > 1e-16;
