@@ -209,6 +209,32 @@ int pamo_voronoi_areas(const double *d_v, const int *d_f, int nv, int nf, float 
    each way (the caller then uses a general method). */
 int pamo_mesh_hinges(const int *h_tris, int n_tris, int n_pts, int *h_edges, int *h_hinges, int *out_n_edges);
 
+/* Wavefront OBJ text (host memory, `len` bytes) to vertices [n,3] and
+   triangles [m,3] int, on the host, over `n_threads` threads (<= 0: all).
+   Replaces trimesh.load(path, force='mesh', process=False) in the reference's
+   example.py:24 (float64 vertices, into `verts_f64`) and the `.float()` /
+   `.int()` of example.py:31-32 (into `verts`); either vertex buffer may be
+   null.  `v` lines give the vertices (read as double; `verts` gets them
+   rounded to float), `f` lines their first
+   index of each corner (1-based; negative counts back from the vertices read
+   so far), polygons split into fans (c0, c_k, c_k+1); other statements are
+   skipped.  Always writes the counts to out_n_verts / out_n_tris; returns
+   PAMO_ERR_CAPACITY (nothing written) when they exceed the capacities, so a
+   first call with zero capacities sizes the buffers.  A malformed `v` or `f`
+   line or an index outside the vertices returns PAMO_ERR_INVALID_ARG with the
+   line's byte offset in *out_err_offset (if given). */
+int pamo_obj_parse(const char *text, long long len, float *verts, double *verts_f64, long long cap_verts, int *tris,
+                   long long cap_tris, int n_threads, long long *out_n_verts, long long *out_n_tris,
+                   long long *out_err_offset);
+
+/* Vertices and triangles to OBJ text (`v x y z` with the shortest decimal form
+   that reads back as the same float, then `f a b c`, 1-based), as the
+   reference's example.py:39-43 export does with trimesh.  Writes the length to
+   *out_len; PAMO_ERR_CAPACITY (nothing written) when it exceeds `cap`;
+   PAMO_ERR_INVALID_ARG for an index outside [0, n_verts). */
+int pamo_obj_format(const float *verts, long long n_verts, const int *tris, long long n_tris, char *out,
+                    long long cap, int n_threads, long long *out_len);
+
 /* Stage-3 input normalisation on the device (processing.py:57-59 applies it
    to the ground truth on the host): out[i] = float((in[i] * scale + t) * post)
    per coordinate of n points [n,3], each step in double with one rounding, so

@@ -30,6 +30,9 @@ SIGNATURES = {
     "pamo_launch_count": (_ll, []),
     "pamo_voronoi_areas": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(ctypes.c_double), _vp]),
     "pamo_mesh_hinges": (_i, [_vp, _i, _i, _vp, _vp, ctypes.POINTER(ctypes.c_int)]),
+    "pamo_obj_parse": (_i, [_vp, _ll, _vp, _vp, _ll, _vp, _ll, _i, ctypes.POINTER(_ll), ctypes.POINTER(_ll),
+                            ctypes.POINTER(_ll)]),
+    "pamo_obj_format": (_i, [_vp, _ll, _vp, _ll, _vp, _ll, _i, ctypes.POINTER(_ll)]),
     "pamo_point_stats": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_double), _vp]),
     "pamo_affine_points": (_i, [_vp, _i, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                 ctypes.c_double, _vp, _vp]),

@@ -21,6 +21,7 @@ ROOT = os.path.dirname(HERE)
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpamo_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CXX = os.environ.get("CXX", "g++")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -30,7 +31,7 @@ NO_FMA = {"stage2.cu", "lbvh.cu", "scan.cu", "abi.cu", "shuffle.cu", "noalloc.cu
 
 
 def sources():
-    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+    return sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
 def _deps_mtime():
@@ -40,14 +41,17 @@ def _deps_mtime():
 
 
 def _compile(src: str, force: bool) -> str:
-    obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+    obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
     path = os.path.join(CSRC, src)
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(path), _deps_mtime()):
         return obj
-    flags = list(COMMON)
-    if src in NO_FMA:
-        flags.append("--fmad=false")
-    cmd = [NVCC, *ARCH, *flags, "-c", path, "-o", obj]
+    if src.endswith(".cpp"):  # host-only code
+        cmd = [CXX, "-O3", "-std=c++17", "-fPIC", "-pthread", "-I", os.path.join(ROOT, "include"), "-c", path, "-o", obj]
+    else:
+        flags = list(COMMON)
+        if src in NO_FMA:
+            flags.append("--fmad=false")
+        cmd = [NVCC, *ARCH, *flags, "-c", path, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")

@@ -1,0 +1,134 @@
+"""OBJ ingest / egress (pamo_obj_parse / pamo_obj_format through
+pamo_b200.meshio) on the host, against a plain-Python reading of the same
+statements (the OBJ specification: `v` vertices, `f` polygons as fans, 1-based
+and negative indices, `i/t/n` corners)."""
+import numpy as np
+import pytest
+
+from pamo_b200 import meshgen as mg
+from pamo_b200 import meshio
+
+
+def _plain_obj(text: str):
+    """The OBJ statements this reader takes, one line at a time in Python."""
+    V, F = [], []
+    for line in text.splitlines():
+        t = line.split("#", 1)[0].split()
+        if not t:
+            continue
+        if t[0] == "v":
+            V.append([float(x) for x in t[1:4]])
+        elif t[0] == "f":
+            idx = []
+            for c in t[1:]:
+                i = int(c.split("/")[0])
+                idx.append(i - 1 if i > 0 else len(V) + i)
+            for k in range(1, len(idx) - 1):
+                F.append([idx[0], idx[k], idx[k + 1]])
+    return np.array(V, np.float64).reshape(-1, 3), np.array(F, np.int64).reshape(-1, 3)
+
+
+SAMPLE = """# a comment
+mtllib house.mtl
+o roof
+v 0 0 0
+v 1.0 0.0 0.0   # trailing comment
+v 1 1 0 1.0
+v\t0\t1\t0
+vt 0.5 0.5
+vn 0 0 1
+usemtl tin
+s off
+f 1 2 3
+f 1/1/1 3/1/1 4/1/1
+g walls
+v -1e-3 2.5E+2 +3.25
+v 0.1 0.2 0.3\r
+f -2 -1 1 2\r
+f 2//1 3//1 5//1 6//1 4//1
+l 1 2
+"""
+
+
+def test_statements_fans_and_index_forms():
+    got = meshio.parse_obj(SAMPLE.encode())
+    V, F = _plain_obj(SAMPLE)
+    assert got.vertices.dtype == np.float64 and got.faces.dtype == np.int32
+    np.testing.assert_array_equal(got.vertices, V)
+    np.testing.assert_array_equal(got.faces, F)
+    assert got.faces.tolist() == [[0, 1, 2], [0, 2, 3], [4, 5, 0], [4, 0, 1], [1, 2, 4], [1, 4, 5], [1, 5, 3]]
+    f32 = meshio.parse_obj(SAMPLE.encode(), dtype=np.float32)
+    np.testing.assert_array_equal(f32.vertices, V.astype(np.float32))  # double, then rounded once
+
+
+def test_round_trip_is_exact_and_thread_count_free():
+    V, F = mg.displaced_icosphere(4, 3)
+    rng = np.random.default_rng(0)
+    V = (V * rng.uniform(0.1, 1e4, size=(1, 3))).astype(np.float32)
+    V[:7] = [[0, -0.0, 1e-38], [3.4e38, -1.5e-45, 1], [0.1, 0.2, 0.3], [1 / 3, 2 / 3, -7], [1e-7, 1e7, 123456.7],
+             [np.float32(np.pi), -np.float32(np.e), 2 ** -20], [65504, -65504, 1e-30]]
+    text = meshio.format_obj(V, F)
+    for threads in (1, 3, 0):
+        assert meshio.format_obj(V, F, n_threads=threads) == text
+        back = meshio.parse_obj(text, n_threads=threads, dtype=np.float32)
+        np.testing.assert_array_equal(back.vertices.view(np.uint32), V.view(np.uint32))
+        np.testing.assert_array_equal(back.faces, F.astype(np.int32))
+    pv, pf = _plain_obj(text.decode())
+    np.testing.assert_array_equal(pv.astype(np.float32), V)
+    np.testing.assert_array_equal(pf, F)
+
+
+def test_large_text_splits_across_threads():
+    """A text long enough for many chunks, with negative indices that refer
+    back across chunk boundaries."""
+    rng = np.random.default_rng(1)
+    n = 60_000
+    lines = []
+    for k in range(n):
+        lines.append("v %.9g %.9g %.9g" % tuple(rng.standard_normal(3)))
+        if k >= 3:
+            lines.append("f -1 -3 -4" if k % 2 else "f %d %d %d" % (k + 1, k, k - 2))
+    text = ("\n".join(lines) + "\n").encode()
+    assert len(text) > 3 << 20
+    V, F = _plain_obj(text.decode())
+    for threads in (1, 2, 8):
+        got = meshio.parse_obj(text, n_threads=threads)
+        np.testing.assert_array_equal(got.vertices, V)
+        np.testing.assert_array_equal(got.faces, F)
+
+
+@pytest.mark.parametrize("bad, line", [
+    ("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 4\n", 4),      # index past the vertices
+    ("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 0 1 2\n", 4),      # index 0
+    ("v 0 0 0\nv 1 0 0\nf -3 1 2\n", 3),              # relative index before the first vertex
+    ("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2\n", 4),        # two corners
+    ("v 0 0 0\nv 1 x 0\n", 2),                        # malformed coordinate
+    ("v 0 0\n", 1),                                   # missing coordinate
+    ("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3q\n", 4),     # malformed index
+])
+def test_malformed_statements_raise_with_their_line(bad, line):
+    with pytest.raises(ValueError, match=f"OBJ line {line}:"):
+        meshio.parse_obj(bad.encode())
+
+
+def test_empty_and_statement_free_texts():
+    for text in (b"", b"# nothing\n\nvn 0 0 1\n"):
+        m = meshio.parse_obj(text)
+        assert m.vertices.shape == (0, 3) and m.faces.shape == (0, 3)
+    assert meshio.format_obj(np.zeros((0, 3)), np.zeros((0, 3))) == b""
+
+
+def test_format_rejects_bad_indices():
+    from pamo_b200._lib import PamoError
+
+    with pytest.raises(PamoError):
+        meshio.format_obj(np.zeros((3, 3)), np.array([[0, 1, 3]]))
+
+
+def test_files(tmp_path):
+    V, F = mg.displaced_icosphere(2, 1)
+    p = str(tmp_path / "m.obj")
+    meshio.save_obj(p, V, F)
+    m = meshio.load_obj(p)  # float64: the decimals written, which round back to the float32 values
+    np.testing.assert_array_equal(m.vertices.astype(np.float32), V.astype(np.float32))
+    np.testing.assert_array_equal(m.faces, F)
