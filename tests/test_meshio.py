@@ -132,3 +132,12 @@ def test_files(tmp_path):
     m = meshio.load_obj(p)  # float64: the decimals written, which round back to the float32 values
     np.testing.assert_array_equal(m.vertices.astype(np.float32), V.astype(np.float32))
     np.testing.assert_array_equal(m.faces, F)
+
+
+def test_cli_needs_stage1_disabled(tmp_path, capsys):
+    """The command line mirrors example.py's options; stage 1 is not built, so
+    it stops before loading anything unless --disable_stage1 is given."""
+    from pamo_b200 import cli
+
+    rc = cli.main(["-i", str(tmp_path / "missing.obj"), "-o", str(tmp_path / "o.obj"), "-r", "0.1"])
+    assert rc == 2 and "--disable_stage1" in capsys.readouterr().err
