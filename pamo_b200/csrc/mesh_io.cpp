@@ -9,7 +9,8 @@
 // the vertex index is used; 1-based, negative = relative to the vertices read
 // so far), split into the fan (c0, c_k, c_k+1); every other statement is
 // skipped.  Coordinates are read as doubles and rounded to float, as loading
-// into float64 and then calling `.float()` does.
+// into float64 and then calling `.float()` does.  Line continuations (a
+// trailing backslash) are not supported: such a `v` line reports an error.
 #include <algorithm>
 #include <charconv>
 #include <cstring>
