@@ -235,6 +235,22 @@ int pamo_obj_parse(const char *text, long long len, float *verts, double *verts_
 int pamo_obj_format(const float *verts, long long n_verts, const int *tris, long long n_tris, char *out,
                     long long cap, int n_threads, long long *out_len);
 
+/* Stanford PLY (ASCII, binary little- or big-endian; host memory) to vertices
+   and triangles, with the conventions of pamo_obj_parse: an element `vertex`
+   with properties x, y, z (read as double; `verts` rounds them to float), the
+   list property `vertex_indices` or `vertex_index` of an element `face` split
+   into fans, every other element and property skipped.  A malformed header, a
+   truncated body or an index outside the vertices returns
+   PAMO_ERR_INVALID_ARG.  Replaces trimesh.load for .ply inputs. */
+int pamo_ply_parse(const char *data, long long len, float *verts, double *verts_f64, long long cap_verts, int *tris,
+                   long long cap_tris, long long *out_n_verts, long long *out_n_tris);
+
+/* Vertices and triangles as binary little-endian PLY (float x, y, z; list
+   uchar int vertex_indices).  Writes the length to *out_len;
+   PAMO_ERR_CAPACITY (nothing written) when it exceeds `cap`. */
+int pamo_ply_format(const float *verts, long long n_verts, const int *tris, long long n_tris, char *out, long long cap,
+                    long long *out_len);
+
 /* Stage-3 input normalisation on the device (processing.py:57-59 applies it
    to the ground truth on the host): out[i] = float((in[i] * scale + t) * post)
    per coordinate of n points [n,3], each step in double with one rounding, so

@@ -33,6 +33,8 @@ SIGNATURES = {
     "pamo_obj_parse": (_i, [_vp, _ll, _vp, _vp, _ll, _vp, _ll, _i, ctypes.POINTER(_ll), ctypes.POINTER(_ll),
                             ctypes.POINTER(_ll)]),
     "pamo_obj_format": (_i, [_vp, _ll, _vp, _ll, _vp, _ll, _i, ctypes.POINTER(_ll)]),
+    "pamo_ply_parse": (_i, [_vp, _ll, _vp, _vp, _ll, _vp, _ll, ctypes.POINTER(_ll), ctypes.POINTER(_ll)]),
+    "pamo_ply_format": (_i, [_vp, _ll, _vp, _ll, _vp, _ll, ctypes.POINTER(_ll)]),
     "pamo_point_stats": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_double), _vp]),
     "pamo_affine_points": (_i, [_vp, _i, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                 ctypes.c_double, _vp, _vp]),

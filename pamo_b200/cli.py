@@ -1,4 +1,4 @@
-"""Command-line simplification of an OBJ mesh, with the options of the
+"""Command-line simplification of an OBJ or PLY mesh, with the options of the
 reference's example.py:13-21:
 
     python -m pamo_b200.cli -i in.obj -o out.obj -r 0.1 [-mv 0] [--disable_stage1] [--disable_stage3]
@@ -28,9 +28,9 @@ def main(argv=None) -> int:
     import torch
 
     from . import PaMO
-    from .meshio import load_obj, save_obj
+    from .meshio import load_mesh, save_mesh
 
-    mesh = load_obj(args.input)
+    mesh = load_mesh(args.input)
     print(f"# of input verts : {len(mesh.vertices)}")
     print(f"# of input faces : {len(mesh.faces)}")
     pamo = PaMO(mesh, use_stage1=False, use_stage3=not args.disable_stage3)
@@ -40,7 +40,7 @@ def main(argv=None) -> int:
     print("Total time: ", time.time() - start)
     print(f"# of output verts : {len(verts)}")
     print(f"# of output faces : {len(faces)}")
-    save_obj(args.output, verts, faces)
+    save_mesh(args.output, verts, faces)
     return 0
 
 

@@ -1,9 +1,10 @@
-"""Wavefront OBJ in and out, on the host, through libpamo_b200.so
-(``pamo_obj_parse`` / ``pamo_obj_format``): the mesh loading and saving that
-the reference's example.py:24-43 does with trimesh.
+"""Wavefront OBJ and Stanford PLY in and out, on the host, through
+libpamo_b200.so (``pamo_obj_parse`` / ``pamo_obj_format``, ``pamo_ply_parse`` /
+``pamo_ply_format``): the mesh loading and saving that the reference's
+example.py:24-43 does with trimesh.
 
-    mesh = load_obj("in.obj")            # Mesh(vertices float64 [n,3], faces int32 [m,3])
-    save_obj("out.obj", verts, faces)
+    mesh = load_mesh("in.obj")           # Mesh(vertices float64 [n,3], faces int32 [m,3]); .obj or .ply
+    save_mesh("out.ply", verts, faces)
 
 ``Mesh`` has ``.vertices`` and ``.faces``, so it can be passed to ``PaMO`` as
 the input mesh.
@@ -81,5 +82,71 @@ def format_obj(vertices, faces, n_threads: int = 0) -> bytes:
 
 def save_obj(path: str, vertices, faces, n_threads: int = 0) -> None:
     data = format_obj(vertices, faces, n_threads)
+    with open(path, "wb") as fh:
+        fh.write(data)
+
+
+def _sized_parse(fn, data: bytes, dtype, extra=()):
+    dtype = np.dtype(dtype)
+    if dtype not in (np.float32, np.float64):
+        raise ValueError("dtype must be float32 or float64")
+    buf = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(0, np.uint8)
+    L = _lib.lib()
+    nv, nt = ctypes.c_longlong(), ctypes.c_longlong()
+    rc = getattr(L, fn)(_ptr(buf), len(buf), None, None, 0, None, 0, *extra, ctypes.byref(nv), ctypes.byref(nt))
+    if rc == 6:
+        V = np.empty((nv.value, 3), dtype)
+        F = np.empty((nt.value, 3), np.int32)
+        v32, v64 = (_ptr(V), None) if dtype == np.float32 else (None, _ptr(V))
+        rc = getattr(L, fn)(_ptr(buf), len(buf), v32, v64, nv.value, _ptr(F), nt.value, *extra, ctypes.byref(nv),
+                            ctypes.byref(nt))
+    else:
+        V = np.zeros((0, 3), dtype)
+        F = np.zeros((0, 3), np.int32)
+    if rc == 1:
+        raise ValueError(f"{fn}: malformed or truncated mesh data, or a face index outside the vertices")
+    _lib.check(fn, rc)
+    return Mesh(V, F)
+
+
+def parse_ply(data: bytes, dtype=np.float64) -> Mesh:
+    """PLY (ASCII or binary) to (vertices [n,3] of `dtype`, faces int32 [m,3]);
+    polygons are split into fans, other elements and properties skipped."""
+    return _sized_parse("pamo_ply_parse", data, dtype)
+
+
+def format_ply(vertices, faces) -> bytes:
+    """Vertices and triangles as binary little-endian PLY."""
+    V = np.ascontiguousarray(np.asarray(vertices, dtype=np.float32).reshape(-1, 3))
+    F = np.ascontiguousarray(np.asarray(faces, dtype=np.int32).reshape(-1, 3))
+    L = _lib.lib()
+    n = ctypes.c_longlong()
+    rc = L.pamo_ply_format(_ptr(V), len(V), _ptr(F), len(F), None, 0, ctypes.byref(n))
+    if rc != 6:
+        _lib.check("pamo_ply_format", rc)
+    out = np.empty(n.value, np.uint8)
+    _lib.check("pamo_ply_format", L.pamo_ply_format(_ptr(V), len(V), _ptr(F), len(F), _ptr(out), n.value,
+                                                    ctypes.byref(n)))
+    return out.tobytes()
+
+
+def load_mesh(path: str, dtype=np.float64) -> Mesh:
+    """A .obj or .ply file (by its extension)."""
+    with open(path, "rb") as fh:
+        data = fh.read()
+    if path.lower().endswith(".ply"):
+        return parse_ply(data, dtype)
+    if path.lower().endswith(".obj"):
+        return parse_obj(data, 0, dtype)
+    raise ValueError(f"{path}: only .obj and .ply are read")
+
+
+def save_mesh(path: str, vertices, faces) -> None:
+    if path.lower().endswith(".ply"):
+        data = format_ply(vertices, faces)
+    elif path.lower().endswith(".obj"):
+        data = format_obj(vertices, faces)
+    else:
+        raise ValueError(f"{path}: only .obj and .ply are written")
     with open(path, "wb") as fh:
         fh.write(data)

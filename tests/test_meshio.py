@@ -141,3 +141,58 @@ def test_cli_needs_stage1_disabled(tmp_path, capsys):
 
     rc = cli.main(["-i", str(tmp_path / "missing.obj"), "-o", str(tmp_path / "o.obj"), "-r", "0.1"])
     assert rc == 2 and "--disable_stage1" in capsys.readouterr().err
+
+
+def _ply_bytes(V, polys, fmt):
+    """A PLY file with extra vertex properties (normal, colour), a face
+    property before the index list, and an extra element after the faces."""
+    import struct
+
+    head = [
+        "ply", f"format {fmt} 1.0", "comment made by the test", f"element vertex {len(V)}",
+        "property double x", "property float nx", "property double y", "property double z", "property uchar red",
+        f"element face {len(polys)}", "property int flags", "property list uchar uint vertex_indices",
+        "element edge 1", "property list int int vertex_index", "end_header",
+    ]
+    out = ("\n".join(head) + "\n").encode()
+    if fmt == "ascii":
+        rows = [f"{float(x)!r} 0.5 {float(y)!r} {float(z)!r} 200" for x, y, z in V]
+        rows += [" ".join(["7", str(len(p))] + [str(i) for i in p]) for p in polys]
+        rows += ["2 0 1"]
+        return out + ("\n".join(rows) + "\n").encode()
+    e = "<" if fmt == "binary_little_endian" else ">"
+    body = b"".join(struct.pack(e + "dfddB", x, 0.5, y, z, 200) for x, y, z in V)
+    body += b"".join(struct.pack(e + "iB%dI" % len(p), 7, len(p), *p) for p in polys)
+    body += struct.pack(e + "iii", 2, 0, 1)
+    return out + body
+
+
+@pytest.mark.parametrize("fmt", ["ascii", "binary_little_endian", "binary_big_endian"])
+def test_ply_formats_properties_and_fans(fmt):
+    rng = np.random.default_rng(2)
+    V = rng.standard_normal((9, 3))
+    polys = [[0, 1, 2], [2, 3, 4, 5], [5, 6, 7, 8, 0]]
+    m = meshio.parse_ply(_ply_bytes(V, polys, fmt))
+    np.testing.assert_array_equal(m.vertices, V)  # doubles as stored
+    assert m.faces.tolist() == [[0, 1, 2], [2, 3, 4], [2, 4, 5], [5, 6, 7], [5, 7, 8], [5, 8, 0]]
+    m32 = meshio.parse_ply(_ply_bytes(V, polys, fmt), dtype=np.float32)
+    np.testing.assert_array_equal(m32.vertices, V.astype(np.float32))
+
+
+def test_ply_round_trip_and_errors(tmp_path):
+    V, F = mg.displaced_icosphere(3, 2)
+    V = V.astype(np.float32)
+    p = str(tmp_path / "m.ply")
+    meshio.save_mesh(p, V, F)
+    m = meshio.load_mesh(p, dtype=np.float32)
+    np.testing.assert_array_equal(m.vertices.view(np.uint32), V.view(np.uint32))
+    np.testing.assert_array_equal(m.faces, F)
+    data = meshio.format_ply(V, F)
+    with pytest.raises(ValueError):
+        meshio.parse_ply(data[:-5])  # truncated
+    with pytest.raises(ValueError):
+        meshio.parse_ply(_ply_bytes(np.zeros((3, 3)), [[0, 1, 3]], "ascii"))  # index past the vertices
+    with pytest.raises(ValueError):
+        meshio.parse_ply(b"ply\nformat ascii 1.0\nelement vertex 1\nproperty float x\nend_header\n1\n")  # no y, z
+    with pytest.raises(ValueError):
+        meshio.parse_ply(b"solid stl\n")
