@@ -69,15 +69,11 @@ def format_obj(vertices, faces, n_threads: int = 0) -> bytes:
     F = np.ascontiguousarray(np.asarray(faces, dtype=np.int32).reshape(-1, 3))
     L = _lib.lib()
     n = ctypes.c_longlong()
-    rc = L.pamo_obj_format(_ptr(V), len(V), _ptr(F), len(F), None, 0, n_threads, ctypes.byref(n))
-    if rc == 0:
-        return b""
-    if rc != 6:
-        _lib.check("pamo_obj_format", rc)
-    out = np.empty(n.value, np.uint8)
-    _lib.check("pamo_obj_format", L.pamo_obj_format(_ptr(V), len(V), _ptr(F), len(F), _ptr(out), n.value, n_threads,
+    # longest lines: "v" + 3 x (" " + 15 characters of a float) + "\n", "f" + 3 x (" " + 10 digits) + "\n"
+    out = np.empty(len(V) * 50 + len(F) * 35 + 1, np.uint8)
+    _lib.check("pamo_obj_format", L.pamo_obj_format(_ptr(V), len(V), _ptr(F), len(F), _ptr(out), out.size, n_threads,
                                                     ctypes.byref(n)))
-    return out.tobytes()
+    return out[:n.value].tobytes()
 
 
 def save_obj(path: str, vertices, faces, n_threads: int = 0) -> None:
