@@ -273,11 +273,16 @@ int pamo_safe_project_stats(pamo_ctx *ctx, double *h_out3);
  * the device and stall its other streams.  Same inputs and output as
  * pamo_self_intersect, with no context.  All scratch lives in one ~11 MB
  * file-scope device array that every GPU loading the library holds until the
- * process exits.  Limits: n_tris <= 32768, n_pts <= 65536 and at most 24
- * candidate pairs per face; larger inputs return PAMO_ERR_CAPACITY.  The first
- * call on each device looks up the array's device address (do that first call
- * before any stream capture).  Every call shares the array: calls that overlap
- * on the GPU, on any stream, race and must be serialised by the caller.
+ * process exits.  Limits: n_tris <= 32768, n_pts <= 65536 and at most 786,432
+ * candidate pairs (box-overlapping face pairs) in total; larger inputs return
+ * PAMO_ERR_CAPACITY.  An empty mesh (n_tris == 0) returns at once with
+ * *out_n_pairs = 0.  Each call looks up the array's device address on the
+ * current device; the first call on a device also loads the library's device
+ * code there, so make that first call before any stream capture.  Each call
+ * waits for its stream twice (index validation, then the counters are read
+ * back to the host).  Every call shares the array: calls that overlap on the
+ * GPU, on any stream or host thread, race and must be serialised by the
+ * caller.
  */
 int pamo_self_intersect_noalloc(const float *d_points, const int *d_tris, int n_pts, int n_tris,
                                 unsigned char *d_out_flags, long long *out_n_pairs, void *stream);

@@ -15,6 +15,10 @@ if [ ! -f "$REF/simp_cuda/src/cusimp_free.cu" ]; then
   echo "reference sources not found under $REF; keeping existing $OUT" >&2
   exit 0
 fi
+if [ -f "$OUT/libref_harness.so" ] && [ -f "$OUT/libpamo_ref_cabi.so" ] \
+   && [ "$OUT/libref_harness.so" -nt "$HERE/ref_harness.cu" ] && [ "$OUT/libref_harness.so" -nt "$0" ]; then
+  exit 0  # up to date
+fi
 NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
 FLAGS="-O3 --extended-lambda --expt-relaxed-constexpr --fmad=false -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -shared -w"
 "$NVCC" $FLAGS -I"$REF/simp_cuda/src" "$HERE/ref_harness.cu" -o "$OUT/libref_harness.so"

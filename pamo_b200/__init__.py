@@ -156,7 +156,8 @@ class PaMO:
         self.last_rounds = 0
         self.timings = {}
         if use_stage1:
-            from . import remesh  # noqa: F401  (raises if stage 1 is unavailable)
+            raise NotImplementedError("stage 1 (SDF + dual marching cubes remesh) is not built; "
+                                      "use PaMO(..., use_stage1=False)")
         if use_stage3:
             from .safe_project import Stage3Config, Stage3System
 

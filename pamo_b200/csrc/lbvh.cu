@@ -5,9 +5,9 @@ namespace pamo {
 
 namespace {
 
-constexpr int kSortThreads = 256;
-constexpr int kSortItems = 8;
-constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kSortThreads = kLbvhSortThreads;
+constexpr int kSortItems = kLbvhSortItems;
+constexpr int kSortTile = kLbvhSortTile;
 
 __device__ __forceinline__ uint32_t expand10(uint32_t v)
 {

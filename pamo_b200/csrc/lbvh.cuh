@@ -21,6 +21,11 @@
 namespace pamo {
 
 constexpr int kRefitTile = 256;  // leaves per refit block
+// radix-sort tile of lbvh_build (threads x items per thread); Lbvh::hist holds
+// 256 counts per tile
+constexpr int kLbvhSortThreads = 256;
+constexpr int kLbvhSortItems = 8;
+constexpr int kLbvhSortTile = kLbvhSortThreads * kLbvhSortItems;
 constexpr int kRefitTileShift = 8;
 static_assert(kRefitTile == 1 << kRefitTileShift, "refit tile");
 

@@ -208,6 +208,9 @@ bool body_pass(const char *data, long long len, long long body, Format fmt, cons
             if (is_f && pr.count_type != T_NONE && (pr.name == "vertex_indices" || pr.name == "vertex_index")) il = k;
         }
         if (is_v && (ix < 0 || iy < 0 || iz < 0)) return false;
+        // an element without properties occupies no bytes: nothing to walk (and
+        // a huge count must not spin the loop below)
+        if (el.props.empty()) continue;
         long long t = 0;
         for (long long i = 0; i < el.count; ++i) {
             double xyz[3] = {0, 0, 0};

@@ -12,9 +12,8 @@ namespace {
 
 constexpr int kMaxFaces = 32768;   // limit of this entry point
 constexpr int kMaxVerts = 65536;
-constexpr int kPairsPerFace = 24;  // candidate pairs kept per face before PAMO_ERR_CAPACITY
-constexpr int kSortTile = 2048;    // lbvh.cu radix-sort tile
-constexpr int kTiles = (kMaxFaces + kSortTile - 1) / kSortTile;
+constexpr int kPairsPerFace = 24;  // sizes the pair buffer: 24 * kMaxFaces candidate pairs in total
+constexpr int kTiles = (kMaxFaces + kLbvhSortTile - 1) / kLbvhSortTile;  // lbvh_build's sort tiles
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -37,12 +36,11 @@ constexpr size_t kOffPairs = kOffScene + align256(64);
 constexpr size_t kOffCounters = kOffPairs + align256(sizeof(uint2) * kPairsPerFace * (size_t)kMaxFaces);
 constexpr size_t kOffBad = kOffCounters + align256(sizeof(RoundCounters));
 constexpr size_t kScratchBytes = kOffBad + 256;  // about 11 MB
+static_assert(kOffHistScratch - kOffHist >= 4 * (256 * (size_t)kTiles), "radix histogram area");
+static_assert(kOffPairs - kOffScene >= 64, "scene area");
 
 // Held by every GPU that loads the library, until the process exits.
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
-
-constexpr int kMaxDevices = 64;
-unsigned char *g_scratch_addr[kMaxDevices] = {};  // device address of g_scratch per device
 
 __global__ void k_na_validate(const int *tris, int m, int n, int *bad)
 {
@@ -75,19 +73,19 @@ using namespace pamo;
 extern "C" int pamo_self_intersect_noalloc(const float *d_points, const int *d_tris, int n_pts, int n_tris,
                                            unsigned char *d_out_flags, long long *out_n_pairs, void *stream)
 {
-    if (n_pts <= 0 || n_tris < 0 || !d_points || (n_tris && (!d_tris || !d_out_flags))) return PAMO_ERR_INVALID_ARG;
+    if (n_pts < 0 || n_tris < 0 || (n_tris && (n_pts == 0 || !d_points || !d_tris || !d_out_flags)))
+        return PAMO_ERR_INVALID_ARG;
     if (n_tris > kMaxFaces || n_pts > kMaxVerts) return PAMO_ERR_CAPACITY;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return PAMO_ERR_NO_DEVICE;
-    if (dev < 0 || dev >= kMaxDevices) return PAMO_ERR_DEVICE;
-    // set-up, once per device, with that device current: the array's name is a
-    // host-side stand-in, the kernels need its device address
-    if (!g_scratch_addr[dev]) {
-        void *addr = nullptr;
-        if (cudaGetSymbolAddress(&addr, g_scratch) != cudaSuccess || !addr) return PAMO_ERR_DEVICE;
-        g_scratch_addr[dev] = static_cast<unsigned char *>(addr);
-    }
-    unsigned char *base = g_scratch_addr[dev];
+    // The array's name is a host-side stand-in; the kernels need its device
+    // address on the current device.  It is looked up on every call (a table
+    // lookup in the runtime once the module is loaded), so no cached address
+    // can outlive a device reset or belong to another thread's device.  The
+    // first call on a device loads the module.
+    void *addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_scratch) != cudaSuccess || !addr) return PAMO_ERR_DEVICE;
+    unsigned char *base = static_cast<unsigned char *>(addr);
     cudaStream_t s = (cudaStream_t)stream;
     if (n_tris == 0) {
         if (out_n_pairs) *out_n_pairs = 0;

@@ -2,7 +2,7 @@
 stage-2 build (oracle/_ref/, compiled from the reference sources by
 oracle/build_ref.sh) on a CUDA device.
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out <directory>
 
 Cases (each in a fresh process, so the reference's persistent state starts
 empty as it does for a new CUDSP_Free object):
@@ -185,7 +185,7 @@ def run_ref_timing(out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="directory for the generated fixtures")
     ap.add_argument("--case", default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)

@@ -196,3 +196,18 @@ def test_ply_round_trip_and_errors(tmp_path):
         meshio.parse_ply(b"ply\nformat ascii 1.0\nelement vertex 1\nproperty float x\nend_header\n1\n")  # no y, z
     with pytest.raises(ValueError):
         meshio.parse_ply(b"solid stl\n")
+
+
+def test_ply_element_without_properties_is_skipped_at_once():
+    """A header element with a huge count and no properties occupies no body
+    bytes; the reader must not walk its count."""
+    import time
+
+    hdr = (b"ply\nformat binary_little_endian 1.0\nelement empty 9000000000000000000\n"
+           b"element vertex 3\nproperty float x\nproperty float y\nproperty float z\n"
+           b"element face 1\nproperty list uchar int vertex_indices\nend_header\n")
+    body = np.eye(3, dtype=np.float32).tobytes() + bytes([3]) + np.array([0, 1, 2], np.int32).tobytes()
+    t0 = time.time()
+    m = meshio.parse_ply(hdr + body)
+    assert time.time() - t0 < 5.0
+    np.testing.assert_array_equal(m.faces, [[0, 1, 2]])

@@ -44,6 +44,11 @@ def _meshes():
     cases = [(g[f"{k}_V"], g[f"{k}_F"]) for k in ("two_spheres", "crumpled", "folded_grids", "soup")]
     cases.append(mg.displaced_icosphere(5, 0))
     cases.append(mg.thin_shell_pair(20000, 2e-3, 1))
+    # removed faces (-1, -1, -1) spread through an intersecting mesh
+    V, F = cases[1]
+    F = np.array(F, np.int32)
+    F[::7] = -1
+    cases.append((V, F))
     return cases
 
 
@@ -60,6 +65,20 @@ def test_noalloc_matches_allocating_entry_point(torch_cuda):
             assert rc == 0, f"status {rc}"
             assert np.array_equal(got, want), f"call {call}: {np.sum(got != want)} flags differ"
             assert pairs == want_pairs
+
+
+def test_noalloc_empty_mesh(torch_cuda):
+    """No faces: status OK and no candidate pairs, with or without points."""
+    from pamo_b200 import _lib
+
+    n = ctypes.c_longlong(-1)
+    stream = ctypes.c_void_p(torch_cuda.cuda.current_stream().cuda_stream)
+    assert _lib.lib().pamo_self_intersect_noalloc(None, None, 0, 0, None, ctypes.byref(n), stream) == 0
+    assert n.value == 0
+    pv = torch_cuda.zeros((4, 3), dtype=torch_cuda.float32, device="cuda")
+    n.value = -1
+    assert _lib.lib().pamo_self_intersect_noalloc(pv.data_ptr(), None, 4, 0, None, ctypes.byref(n), stream) == 0
+    assert n.value == 0
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit(torch_cuda):
