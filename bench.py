@@ -288,16 +288,21 @@ def roofline_query(phases, round_faces, peaks):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs") else "fallback"}
 
 
-def count_intersections(ctx, V, F, dev):
-    """Faces of a result that the reference's pair predicate flags as
-    intersecting (pamo_self_intersect over the whole mesh)."""
-    import torch
+def acceptance(V_in, F_in, v, f, dev):
+    """The acceptance checks of a result (pamo_b200.metrics, on the device):
+    intersecting face pairs under exact predicates, watertight / manifold,
+    and the two-sided Hausdorff distance to the input by dense sampling, as a
+    fraction of the input's bounding-box diagonal."""
+    from pamo_b200 import metrics
 
-    import pamo_b200
-
-    flags, _ = pamo_b200.self_intersect(ctx, torch.from_numpy(np.ascontiguousarray(V, np.float32)).to(dev),
-                                        torch.from_numpy(np.ascontiguousarray(F, np.int32)).to(dev))
-    return int(flags.sum().item())
+    chk = metrics.check_mesh(v, f, device=dev.index or 0)
+    hd = metrics.hausdorff(V_in, F_in, v, f, 1, 16, device=dev.index or 0)
+    Vd = np.asarray(V_in, np.float64)
+    diag = float(np.linalg.norm(Vd.max(0) - Vd.min(0)))
+    return {"intersecting_pairs_exact": chk["intersecting_pairs"], "watertight_manifold": chk["watertight_manifold"],
+            "degenerate_faces": chk["degenerate_faces"], "hausdorff_of_diag": hd["hausdorff"] / diag,
+            "hausdorff_upper_of_diag": hd["upper"] / diag,
+            "checker": "pamo_check_mesh (exact orient3d) + pamo_mesh_distance (input sampled at k=1, output at k=16)"}
 
 
 def product_arm(args):
@@ -387,7 +392,8 @@ def product_arm(args):
         L.pamo_profile_enable(h, 1)
     v_out, f_out = run_resident()
     torch.cuda.synchronize()
-    intersections = count_intersections(pamo_b200.Context(local), v_out, f_out, dev)
+    accept = acceptance(V, F, v_out, f_out, dev)
+    intersections = accept["intersecting_pairs_exact"]
     phases = {}
     for h in handles:
         ph_ms = (ctypes.c_double * 16)()
@@ -433,6 +439,7 @@ def product_arm(args):
             "clocks": clocks,
             "cpu_baseline": cpu,
             "intersections": intersections,
+            "acceptance": accept,
             "phases_ms": {k: round(v["ms"], 3) for k, v in phases.items()},
             "roofline": roofline_query(phases, round_faces, peaks),
             "roofline_edge_cost": roofline_edge_cost(phases, round_faces, peaks),
@@ -554,11 +561,12 @@ def batched_arm(args):
     rounds_run = eng.stats()["rounds_run"]
     import pamo_b200 as _pb
 
-    chk = _pb.Context(local)
     intersections = 0
+    not_manifold = 0
     for info in res:
-        fl, _ = _pb.self_intersect(chk, *info.pop("out"))
-        intersections += int(fl.sum().item())
+        r = _pb.metrics.check_mesh(*info.pop("out"), device=local)
+        intersections += r["intersecting_pairs"]
+        not_manifold += 0 if r["watertight_manifold"] else 1
     # the plain per-mesh drop-in on the same meshes (same device, fresh context)
     import pamo_b200
 
@@ -586,7 +594,7 @@ def batched_arm(args):
             "e2e": {"value": total_faces / 1e6 / e2e_dt, "unit": "Mfaces/s", "h2d_bytes_per_step": int(bi),
                     "d2h_bytes_per_step": int(bo)},
             "gpu_launches": int(launches), "clocks": clocks, "phases_ms": batch_phases,
-            "intersections": intersections,
+            "intersections": intersections, "meshes_not_watertight_manifold": not_manifold,
             "rounds_per_step": rounds_run // (args.warmup + args.steps + 2),
         }
         print(json.dumps(line))

@@ -266,6 +266,30 @@ int pamo_affine_points(const float *d_in, int n, double scale, double tx, double
 int pamo_safe_project_stats(pamo_ctx *ctx, double *h_out3);
 
 /*
+ * Per-Newton-iteration record of the last pamo_safe_project call (no
+ * reference counterpart; the quantities are those of Stage3System.step,
+ * system.py:354-470): six doubles per iteration = {energy at the iterate after
+ * contact detection, energy after the line search, CCD step (accd_kernel,
+ * ccd_kernels.py:8-110), index of the last line-search halving tried, contact
+ * blocks, blocks closer than d_hat}.  Copies up to cap_rows rows to h_out and
+ * writes the number of iterations recorded to *out_rows.
+ */
+int pamo_safe_project_trace(pamo_ctx *ctx, double *h_out, int cap_rows, int *out_rows);
+
+/*
+ * The stage-3 Jacobi-preconditioned CG (cg_solver.py:96-158, the solve each
+ * Newton iteration runs) on a caller's symmetric matrix of 3x3 blocks over n
+ * vertices in block-CSR form: d_row_ptr [n+1], d_col [n_blocks] (ascending per
+ * row), d_blocks [n_blocks*9] row-major, preconditioner d_diag [n*3] (the
+ * matrix's diagonal), right-hand side d_rhs [n*3]; `iters` CG iterations from
+ * x = 0, solution in d_out [n*3].  For tests of the solver against known
+ * answers (the reference's tests/test_dummy_energy.py).  Replaces the stage-3
+ * state held by the context.
+ */
+int pamo_bsr_pcg(pamo_ctx *ctx, int n, const int *d_row_ptr, const int *d_col, const float *d_blocks,
+                 long long n_blocks, const float *d_diag, const float *d_rhs, int iters, float *d_out, void *stream);
+
+/*
  * pamo_self_intersect without any allocation (no counterpart in the reference).
  * For callers that may not allocate device memory themselves or have the
  * library do it: a host application that owns all device memory through its own
@@ -286,6 +310,46 @@ int pamo_safe_project_stats(pamo_ctx *ctx, double *h_out3);
  */
 int pamo_self_intersect_noalloc(const float *d_points, const int *d_tris, int n_pts, int n_tris,
                                 unsigned char *d_out_flags, long long *out_n_pairs, void *stream);
+
+/*
+ * Acceptance checker of a triangle mesh, on the device.  It takes the role of
+ * the reference's exact self-intersection script
+ * (simp_cuda/safe_project/scripts/cgal_intersect/main.cpp:19-111,
+ * CGAL PMP::self_intersections) as a library call.  Every pair of live faces
+ * whose closed bounding boxes overlap is decided with exact-sign orientation
+ * predicates (a double filter with an exact expansion fallback): faces with
+ * no common vertex intersect when the closed triangles share any point, faces
+ * sharing one vertex when they share another point, faces sharing an edge when
+ * they are coplanar and fold onto each other, and a repeated face always.
+ * Degenerate faces (a repeated index or collinear corners) are counted and
+ * left out of the pair tests.  Faces (-1,-1,-1) are ignored.
+ *   d_out_flags [n_tris] (optional): 1 for each face of an intersecting pair.
+ *   h_out[11] (host) = {intersecting pairs, faces in them, degenerate faces,
+ *     boundary half-edges (no reverse half-edge), non-manifold half-edges (an
+ *     edge in more than two faces or twice in one direction), vertices whose
+ *     faces do not form one closed fan, unreferenced vertices, candidate pairs
+ *     (box overlaps), dead faces, traversal errors, out-of-range indices}.
+ * The mesh is watertight and manifold when h_out[2..5] are all zero.
+ * Returns PAMO_ERR_INVALID_ARG for an index outside [0, n_pts).
+ */
+int pamo_check_mesh(const float *d_points, const int *d_tris, int n_pts, int n_tris, unsigned char *d_out_flags,
+                    long long *h_out, void *stream);
+
+/*
+ * One-sided surface distance from mesh A to mesh B (device arrays), by dense
+ * sampling: every live face of A is sampled on the barycentric grid
+ * (i/subdiv, j/subdiv), i + j <= subdiv, and each sample's distance to the
+ * closest point of B is found through B's LBVH.  Replaces the Hausdorff and
+ * Chamfer terms of the reference's metrics.py:31-51 (igl.hausdorff,
+ * igl.point_mesh_squared_distance).
+ *   h_out4 = {largest sample distance (a lower bound of the one-sided
+ *     Hausdorff distance), an upper bound of it (plus each face's longest
+ *     edge / subdiv / sqrt 3: every point of a face lies that close to a
+ *     sample), mean squared sample distance, number of samples}.
+ * The two-sided Hausdorff distance is the larger of the A->B and B->A values.
+ */
+int pamo_mesh_distance(const float *d_pa, const int *d_fa, int na, int nfa, const float *d_pb, const int *d_fb,
+                       int nb, int nfb, int subdiv, double *h_out4, void *stream);
 
 /*
  * Host-pointer simplifier.  Same signature and meaning as the reference's

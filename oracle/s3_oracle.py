@@ -465,6 +465,10 @@ class Stage3Oracle:
         self.radius = c.contact_detection_radius
         self.blocks = np.zeros((0, 4), np.int64)
         self.kinds = np.zeros(0, np.int64)
+        # per Newton iteration: energy at the iterate, energy after the line
+        # search, CCD step, last halving tried, contact blocks, blocks within d_hat
+        self.trace = []
+        self.nact = 0
 
     @staticmethod
     def _frame(x01, x02):
@@ -615,10 +619,12 @@ class Stage3Oracle:
         self.hinge_blocks = spd_project(Hb, c.spd_max_iters)
         # collision (Gauss-Newton)
         self.coll = None
+        self.nact = 0
         if len(self.blocks):
             X, ty = self._classify_blocks(q)
             d, G = pair_distance_grad(X, self.kinds, ty)
             act = d < c.d_hat
+            self.nact = int(act.sum())
             with np.errstate(divide="ignore", invalid="ignore"):
                 b1c = self.barrier_d1(d, c.d_hat) * c.coll_stiffness
                 b2c = self.barrier_d2(d, c.d_hat) * c.coll_stiffness
@@ -836,11 +842,14 @@ class Stage3Oracle:
         p = self.clamp(p, q_prev, q_det)
         step = self.accd(p)
         e = e0
+        last = -1
         for nh in range(c.n_line_search_iters):
             if nh > 0 and e < e0:
                 break
             self.q = q_prev + step * (0.5 ** nh) * p
             e = self.energy(self.q)
+            last = nh
+        self.trace.append((e0, e, step, last, len(self.blocks), self.nact))
         return e
 
     def step(self):
@@ -885,9 +894,10 @@ def spd_project(B, sweeps):
     return out
 
 
-def process(gt_V, gt_F, V, F, n_iters=5, config=None, dtype=np.float64):
+def process(gt_V, gt_F, V, F, n_iters=5, config=None, dtype=np.float64, trace=None):
     """processing.py:23-108 in FP64: normalise by the GT, run n_iters steps,
-    undo the normalisation.  Faces are unchanged."""
+    undo the normalisation.  Faces are unchanged.  A list given as `trace`
+    receives the Newton trace (Stage3Oracle.trace)."""
     scale, t = normalization(np.asarray(gt_V, np.float64))
     gV = np.asarray(gt_V, np.float64) * scale + t
     sV = np.asarray(V, np.float64) * scale + t
@@ -895,4 +905,6 @@ def process(gt_V, gt_F, V, F, n_iters=5, config=None, dtype=np.float64):
     o.register(gV, gt_F, sV, F)
     for _ in range(n_iters):
         o.step()
+    if trace is not None:
+        trace.extend(o.trace)
     return (o.q - t) / scale, np.asarray(F)

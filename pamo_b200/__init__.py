@@ -19,6 +19,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import Context, PamoError, check
+from . import metrics  # noqa: F401  (acceptance checks: check_mesh, hausdorff)
 
 __all__ = ["PaMO", "CUDSP_Free", "Context", "PamoError", "stage2_run", "self_intersect"]
 __version__ = "0.1.0"

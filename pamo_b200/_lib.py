@@ -65,7 +65,11 @@ SIGNATURES = {
     "pamo_safe_project": (_i, [_vp, _vp, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _i, _vp, _i, _vp, _i, _i, _vp, _vp,
                                _vp]),
     "pamo_safe_project_stats": (_i, [_vp, _vp]),
+    "pamo_safe_project_trace": (_i, [_vp, _vp, _i, _ip]),
+    "pamo_bsr_pcg": (_i, [_vp, _i, _vp, _vp, _vp, _ll, _vp, _vp, _i, _vp, _vp]),
     "pamo_self_intersect_noalloc": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(_ll), _vp]),
+    "pamo_check_mesh": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(_ll), _vp]),
+    "pamo_mesh_distance": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _i, _i, ctypes.POINTER(ctypes.c_double), _vp]),
     "pamo_simplify": (None, [_vp, _vp, _vp, _vp, _vp, _f]),
     "pamo_simplify_ctx": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f]),
 }

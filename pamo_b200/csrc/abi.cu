@@ -693,6 +693,7 @@ int pamo_safe_project(pamo_ctx *ctx, const float *d_gt_v, const int *d_gt_f, int
         S.cfg.spd_max_iters < 0 || !(S.cfg.d_hat > 0.f) || S.cfg.max_blocks <= 0)
         return PAMO_ERR_INVALID_ARG;
     RET_IF(S.ensure(n_v, n_f, n_e, n_h, n_gt_v, n_gt_f));
+    RET_IF(S.ensure_trace((long long)n_steps * S.cfg.n_newton_iters));
     int *bad = S.iscal + 8;
     RET_IF(s3_validate(d_f, 3LL * n_f, n_v, bad, S.h_iscal, s));
     RET_IF(s3_validate(d_e, 2LL * n_e, n_v, bad, S.h_iscal, s));
@@ -862,6 +863,37 @@ int pamo_safe_project_stats(pamo_ctx *ctx, double *h_out3)
     if (!ctx || !h_out3) return PAMO_ERR_INVALID_ARG;
     for (int k = 0; k < 3; ++k) h_out3[k] = ctx->s3_stats[k];
     return PAMO_OK;
+}
+
+int pamo_safe_project_trace(pamo_ctx *ctx, double *h_out, int cap_rows, int *out_rows)
+{
+    if (!ctx || cap_rows < 0 || (cap_rows && !h_out) || !out_rows) return PAMO_ERR_INVALID_ARG;
+    pamo::s3::Stage3 &S = ctx->s3;
+    *out_rows = 0;
+    if (!S.trace || !S.iscal) return PAMO_OK;
+    RET_IF(set_device(ctx));
+    int rows = 0;
+    CU_RET(cudaMemcpy(&rows, S.iscal + 13, sizeof(int), cudaMemcpyDeviceToHost));  // the trace's row counter
+    if (rows > S.cap_trace) rows = (int)S.cap_trace;
+    const int n = rows < cap_rows ? rows : cap_rows;
+    if (n > 0) CU_RET(cudaMemcpy(h_out, S.trace, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost));
+    *out_rows = rows;
+    return PAMO_OK;
+}
+
+int pamo_bsr_pcg(pamo_ctx *ctx, int n, const int *d_row_ptr, const int *d_col, const float *d_blocks,
+                 long long n_blocks, const float *d_diag, const float *d_rhs, int iters, float *d_out, void *stream)
+{
+    if (!ctx || n <= 0 || n_blocks <= 0 || iters < 0 || !d_row_ptr || !d_col || !d_blocks || !d_diag || !d_rhs ||
+        !d_out)
+        return PAMO_ERR_INVALID_ARG;
+    RET_IF(set_device(ctx));
+    cudaStream_t s = (cudaStream_t)stream;
+    pamo::s3::Stage3 &S = ctx->s3;
+    RET_IF(S.ensure(n, 1, 1, 1, 1, 1));
+    int *bad = S.iscal + 8;
+    RET_IF(s3_validate(d_col, n_blocks, n, bad, S.h_iscal, s));
+    return S.solve_bsr(n, d_row_ptr, d_col, d_blocks, n_blocks, d_diag, d_rhs, iters, d_out, s);
 }
 
 int pamo_simplify_ctx(pamo_ctx *ctx, const float *h_in_verts, const int *h_in_tris, float *h_out_verts,

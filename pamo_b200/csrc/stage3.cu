@@ -32,7 +32,7 @@ constexpr int kStack = 96;
 
 enum { D_ENERGY = 0, D_ENERGY_PREV, D_ZR, D_ZR_LAST, D_VAV };
 enum { I_NB = 0, I_OVERFLOW, I_STACK, I_NACT, I_NCAND_PT, I_NCAND_EE, I_TICKET, I_DISP, I_BAR_ERR, I_BAR_COUNT,
-       I_BAR_GEN, I_ETICKET };
+       I_BAR_GEN, I_ETICKET, I_LS, I_TRACE };
 
 __device__ __forceinline__ F3 ld(const float4 *a, int i) { return f3(a[i]); }
 __device__ __forceinline__ void st(float4 *a, int i, F3 v) { a[i] = make_float4(v.x, v.y, v.z, 0.f); }
@@ -1523,14 +1523,45 @@ __global__ void __launch_bounds__(128) k_accd(const float4 *q, const float4 *pv,
 }
 
 __global__ void k_line_search(const float4 *q_prev, const float4 *p, const float *ccd_step, int n_halves,
-                              const double *dscal, int np, float4 *q)
+                              const double *dscal, int np, float4 *q, int *iscal)
 {
     if (n_halves > 0 && dscal[D_ENERGY] < dscal[D_ENERGY_PREV]) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) iscal[I_LS] = n_halves;  // the last trial taken
     const float a = ccd_step[0] * ldexpf(1.f, -n_halves);
     PAMO_GRID_STRIDE(i, np) st(q, (int)i, ld(q_prev, (int)i) + a * ld(p, (int)i));
 }
 
 __global__ void k_copy_energy_prev(double *dscal) { dscal[D_ENERGY_PREV] = dscal[D_ENERGY]; }
+
+// One row of the Newton trace per iteration: energy at the iterate, energy
+// after the line search, CCD step, index of the last halving tried, contact
+// blocks, blocks within d_hat.
+__global__ void k_trace(const double *dscal, const float *fscal, int *iscal, double *trace, long long cap)
+{
+    const int i = iscal[I_TRACE];
+    if (i < cap) {
+        double *r = trace + 6LL * i;
+        r[0] = dscal[D_ENERGY_PREV];
+        r[1] = dscal[D_ENERGY];
+        r[2] = fscal[0];
+        r[3] = iscal[I_LS];
+        r[4] = iscal[I_NB];
+        r[5] = iscal[I_NACT];
+    }
+    iscal[I_TRACE] = i + 1;
+}
+
+// 3x3 blocks given as 9 row-major floats -> the solve's three float4 rows
+__global__ void k_blocks9_to_rows(const float *b9, long long nb, float4 *kval)
+{
+    PAMO_GRID_STRIDE(k, nb)
+    {
+        const float *b = b9 + 9 * k;
+        kval[3 * k] = make_float4(b[0], b[1], b[2], 0.f);
+        kval[3 * k + 1] = make_float4(b[3], b[4], b[5], 0.f);
+        kval[3 * k + 2] = make_float4(b[6], b[7], b[8], 0.f);
+    }
+}
 
 __global__ void k_set_float(float *f, float v) { *f = v; }
 
@@ -1572,7 +1603,7 @@ void Stage3::release()
     void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, v2, Av, Avc, q_gather, wk, tris, area, inv_dm,
                     edges4, hinges, rest_angle, rest_elen, row_ptr, col, kval, tri_slot, hinge_slot, diag_slot, hblk, pat_cnt,
                     pat_cur, pat_off, pat_cand, pat_scan, bidx, bkind, bsub, bd, bb2, bg, bact, gt_pts, gt_tris, dscal, fscal,
-                    iscal, partials};
+                    iscal, partials, trace};
     drop_graph();
     if (cand_pt) cudaFree(cand_pt);
     if (cand_ee) cudaFree(cand_ee);
@@ -1606,6 +1637,8 @@ void Stage3::release()
     rest_angle = rest_elen = nullptr; bidx = nullptr; bkind = bsub = nullptr; bd = bb2 = nullptr;
     bg = nullptr; bact = nullptr; gt_pts = nullptr; gt_tris = nullptr; dscal = nullptr; fscal = nullptr; iscal = nullptr;
     partials = nullptr; h_iscal = nullptr; h_dscal = nullptr;
+    trace = nullptr;
+    cap_trace = 0;
     tri_bvh.release();
     edge_bvh.release();
     gt_bvh.release();
@@ -1945,6 +1978,31 @@ int Stage3::newton_body(cudaStream_t s)
     }
     // Jacobi-preconditioned CG (cg_solver.py:96-158)
     if (prof) prof->begin(PH_S3_CG, s);
+    if ((rc = cg_solve(s))) return rc;
+    if (prof) prof->begin(PH_S3_CCD, s);
+    launch(k_clamp, grid_for(np), kThreads, 0, s, p, q_prev, q_det, np, cfg.contact_detection_radius);
+    launch(k_set_float, 1, 1, 0, s, fscal, 1.0f);
+    launch(k_set_float, 1, 1, 0, s, fscal + 1, 0.0f);
+    launch(k_max_norm, grid_for(np), kThreads, 0, s, (const float4 *)p, np, fscal + 1);
+    launch(k_accd, grid_for(cap_b, 128), 128, 0, s, q, p, bidx, bkind, iscal, cap_b, cfg.ccd_slackness, cfg.ccd_thickness,
+                                                cfg.ccd_max_iters, cfg.ee_classify_thres, fscal);
+    // line search (system.py:393-409)
+    if (prof) prof->begin(PH_S3_LINE, s);
+    launch(k_copy_energy_prev, 1, 1, 0, s, dscal);
+    for (int nh_ = 0; nh_ < cfg.n_line_search_iters; ++nh_) {
+        launch(k_line_search, grid_for(np), kThreads, 0, s, q_prev, p, fscal, nh_, dscal, np, q, iscal);
+        if ((rc = energy_pass(*this, s, nh_))) return rc;
+    }
+    if (trace) launch(k_trace, 1, 1, 0, s, (const double *)dscal, (const float *)fscal, iscal, trace, cap_trace);
+    if (prof) prof->end(s);
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+// The Jacobi-preconditioned CG of one Newton iteration (cg_solver.py:96-158):
+// solves K p = grad (grad holds -dE/dx) with the assembled blocks plus the
+// active contact terms, diag as the preconditioner, cfg.n_cg_iters iterations.
+int Stage3::cg_solve(cudaStream_t s)
+{
     if (cg_persistent < 0) {  // first use: can all blocks of the solve be resident at once?
         int dev = 0, coop = 0, per_sm = 0, sms = 0;
         cudaGetDevice(&dev);
@@ -1974,32 +2032,19 @@ int Stage3::newton_body(cudaStream_t s)
         g_launches.fetch_add(1, std::memory_order_relaxed);
         S3_TRY(cudaLaunchKernelEx(&lc, k_cg_solve, ca));
     } else {
-    int *ticket = iscal + I_TICKET;
-    launch(k_cg_init, kRedBlocks, kThreads, 0, s, grad, diag, np, p, r, z, v, partials, ticket, dscal);
-    for (int it = 0; it < cfg.n_cg_iters; ++it) {
-        launch(k_cg_pre, grid_for(np), kThreads, 0, s, (const float4 *)z, (const double *)dscal, np, it == 0 ? 1 : 0, v);
-        launch(k_op_rows, grid_for(4LL * np), kThreads, 0, s, op, (const float4 *)v, Av);
-        launch(k_op_contacts, grid_for(cap_b), kThreads, 0, s, op, (const float4 *)v, Av);
-        launch(k_cg_dot, kRedBlocks, kThreads, 0, s, (const float4 *)v, (const float4 *)Av, np, partials, ticket, dscal);
-        launch(k_cg_update, kRedBlocks, kThreads, 0, s, (const float4 *)v, (const float4 *)Av, (const float4 *)diag, dscal,
-               np, p, r, z, partials, ticket);
+        int *ticket = iscal + I_TICKET;
+        launch(k_cg_init, kRedBlocks, kThreads, 0, s, grad, diag, np, p, r, z, v, partials, ticket, dscal);
+        for (int it = 0; it < cfg.n_cg_iters; ++it) {
+            launch(k_cg_pre, grid_for(np), kThreads, 0, s, (const float4 *)z, (const double *)dscal, np, it == 0 ? 1 : 0,
+                   v);
+            launch(k_op_rows, grid_for(4LL * np), kThreads, 0, s, op, (const float4 *)v, Av);
+            launch(k_op_contacts, grid_for(cap_b), kThreads, 0, s, op, (const float4 *)v, Av);
+            launch(k_cg_dot, kRedBlocks, kThreads, 0, s, (const float4 *)v, (const float4 *)Av, np, partials, ticket,
+                   dscal);
+            launch(k_cg_update, kRedBlocks, kThreads, 0, s, (const float4 *)v, (const float4 *)Av, (const float4 *)diag,
+                   dscal, np, p, r, z, partials, ticket);
+        }
     }
-    }
-    if (prof) prof->begin(PH_S3_CCD, s);
-    launch(k_clamp, grid_for(np), kThreads, 0, s, p, q_prev, q_det, np, cfg.contact_detection_radius);
-    launch(k_set_float, 1, 1, 0, s, fscal, 1.0f);
-    launch(k_set_float, 1, 1, 0, s, fscal + 1, 0.0f);
-    launch(k_max_norm, grid_for(np), kThreads, 0, s, (const float4 *)p, np, fscal + 1);
-    launch(k_accd, grid_for(cap_b, 128), 128, 0, s, q, p, bidx, bkind, iscal, cap_b, cfg.ccd_slackness, cfg.ccd_thickness,
-                                                cfg.ccd_max_iters, cfg.ee_classify_thres, fscal);
-    // line search (system.py:393-409)
-    if (prof) prof->begin(PH_S3_LINE, s);
-    launch(k_copy_energy_prev, 1, 1, 0, s, dscal);
-    for (int nh_ = 0; nh_ < cfg.n_line_search_iters; ++nh_) {
-        launch(k_line_search, grid_for(np), kThreads, 0, s, q_prev, p, fscal, nh_, dscal, np, q);
-        if ((rc = energy_pass(*this, s, nh_))) return rc;
-    }
-    if (prof) prof->end(s);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
 
@@ -2015,6 +2060,55 @@ int Stage3::step(cudaStream_t s)
         if (rc) return rc;
     }
     return PAMO_OK;
+}
+
+int Stage3::ensure_trace(long long rows)
+{
+    if (rows <= cap_trace && trace) return PAMO_OK;
+    if (trace) cudaFree(trace);
+    trace = nullptr;
+    cap_trace = 0;
+    if (rows <= 0) return PAMO_OK;
+    if (cudaMalloc((void **)&trace, (size_t)rows * 6 * sizeof(double)) != cudaSuccess) return PAMO_ERR_OOM;
+    cap_trace = rows;
+    drop_graph();  // the captured iteration holds the trace pointer
+    return PAMO_OK;
+}
+
+int Stage3::solve_bsr(int n, const int *d_row_ptr, const int *d_col, const float *d_blocks, long long n_blocks,
+                      const float *d_diag, const float *d_rhs, int iters, float *d_out, cudaStream_t s)
+{
+    int rc = ensure(n, 1, 1, 1, 1, 1);
+    if (rc) return rc;
+    if (n_blocks > cap_nnz || !kval) {
+        if (col) cudaFree(col);
+        if (kval) cudaFree(kval);
+        col = nullptr;
+        kval = nullptr;
+        cap_nnz = 0;
+        if (cudaMalloc((void **)&col, (size_t)n_blocks * 4) != cudaSuccess ||
+            cudaMalloc((void **)&kval, (size_t)n_blocks * 48) != cudaSuccess)
+            return PAMO_ERR_OOM;
+        cap_nnz = n_blocks;
+    }
+    drop_graph();
+    gathered = false;
+    gt_ready = false;  // the stage-3 state of this context is replaced
+    np = n;
+    nnz = n_blocks;
+    cfg.n_cg_iters = iters;
+    S3_TRY(cudaMemcpyAsync(row_ptr, d_row_ptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToDevice, s));
+    S3_TRY(cudaMemcpyAsync(col, d_col, (size_t)n_blocks * 4, cudaMemcpyDeviceToDevice, s));
+    launch(k_blocks9_to_rows, grid_for(n_blocks), kThreads, 0, s, d_blocks, n_blocks, kval);
+    launch(k_aos_to_f4, grid_for(np), kThreads, 0, s, d_diag, diag, nullptr, np);
+    launch(k_aos_to_f4, grid_for(np), kThreads, 0, s, d_rhs, grad, nullptr, np);
+    S3_TRY(cudaMemsetAsync(iscal, 0, 64, s));  // no contact blocks
+    S3_TRY(cudaMemsetAsync(dscal, 0, 64, s));
+    if ((rc = cg_solve(s))) return rc;
+    launch(k_f4_to_aos, grid_for(np), kThreads, 0, s, (const float4 *)p, d_out, np);
+    S3_TRY(cudaMemcpyAsync(h_iscal, iscal, 12 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    S3_TRY(cudaStreamSynchronize(s));
+    return h_iscal[I_BAR_ERR] ? PAMO_ERR_DEVICE : PAMO_OK;
 }
 
 int Stage3::energy_now(double *out, cudaStream_t s)

@@ -77,6 +77,8 @@ struct Stage3 {
     double *partials = nullptr;
     int *h_iscal = nullptr;   // pinned
     double *h_dscal = nullptr;
+    double *trace = nullptr;  // [cap_trace][6] per Newton iteration (k_trace); null: not recorded
+    long long cap_trace = 0;
     Profiler *prof = nullptr;  // the context's phase timer (optional)
     cudaGraphExec_t graph = nullptr;  // one Newton iteration after detection
     long long graph_cap_b = -1, graph_kernels = 0;
@@ -103,6 +105,12 @@ struct Stage3 {
     int newton(cudaStream_t s);
     int newton_body(cudaStream_t s);
     int detect(cudaStream_t s);
+    int cg_solve(cudaStream_t s);
+    int ensure_trace(long long rows);
+    // K x = rhs by cg_solve for a caller's matrix of 3x3 blocks (BSR over n
+    // vertices); replaces the context's stage-3 state
+    int solve_bsr(int n, const int *d_row_ptr, const int *d_col, const float *d_blocks, long long n_blocks,
+                  const float *d_diag, const float *d_rhs, int iters, float *d_out, cudaStream_t s);
     void drop_graph();
     // diagnostics
     int energy_now(double *out, cudaStream_t s);

@@ -253,6 +253,7 @@ class Stage3System:
         self.device = device
         self.ctx = Context(device)
         self.last_stats = None
+        self.last_trace = None
         # a ground truth that stays the same from call to call (PaMO.run's):
         # its device copies, normalisation and the library's hierarchy are kept
         self._gt_raw = None   # ((gt_V, gt_F), raw device points, scale, t)
@@ -322,6 +323,14 @@ class Stage3System:
         _lib.lib().pamo_safe_project_stats(self.ctx.handle, st)
         self.last_stats = {"energy": st[0], "contacts": int(st[1]), "newton_iters": int(st[2]),
                            "do_nothing": bool(do_nothing)}
+        rows = ctypes.c_int(0)
+        cap = max(1, int(n_steps) * c.n_newton_iters)
+        tr = np.zeros((cap, 6), np.float64)
+        check("pamo_safe_project_trace", _lib.lib().pamo_safe_project_trace(
+            self.ctx.handle, tr.ctypes.data, cap, ctypes.byref(rows)))
+        # per Newton iteration: energy at the iterate, energy after the line
+        # search, CCD step, last halving tried, contact blocks, blocks within d_hat
+        self.last_trace = tr[:min(rows.value, cap)]
         return out.cpu().numpy() / c.system_scale
 
 

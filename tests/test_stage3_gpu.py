@@ -1,15 +1,28 @@
 """Stage 3 (safe projection) on the GPU: FP32 Newton-PCG with FP64 barrier /
 CCD terms against the FP64 oracle of the same algorithm (oracle/s3_oracle.py),
-and the invariants the reference relies on (energy decreases, no
-self-intersection, faces unchanged)."""
+whose runs are committed as fixtures (tests/golden/make_s3_oracle.py): the
+final vertices, and per Newton iteration the energies, the CCD step, the
+line-search halving taken and the contact-block counts -- with contacts active
+(thin-shell pairs) and without (config 1) -- plus the invariants the reference
+relies on (energy decreases, no self-intersection, faces unchanged) and the
+CG's known answer (the reference's tests/test_dummy_energy.py)."""
+import ctypes
+import importlib.util
+import os
+
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-# FP32 solve vs FP64 solve of the same steps: max vertex deviation allowed, as a
-# fraction of the ground truth's bounding-box diagonal
-TOL_DIAG = 1e-3
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+# FP32 solve vs FP64 solve of the same steps: largest vertex deviation allowed,
+# as a fraction of the ground truth's bounding-box diagonal (measured on a
+# B200: config 1 4.4e-8, the contact cases below)
+TOL_DIAG_C1 = 1e-6
+TOL_DIAG_CONTACT = 1e-4
+TOL_ENERGY = 1e-4  # relative, per Newton iteration
 
 
 @pytest.fixture(scope="module")
@@ -20,14 +33,18 @@ def torch_cuda():
     return torch
 
 
+def _golden_case(name):
+    spec = importlib.util.spec_from_file_location("make_s3_oracle", os.path.join(GOLDEN, "make_s3_oracle.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    V, F, ratio, steps = m.case_input(name)
+    return V, F, ratio, steps, np.load(os.path.join(GOLDEN, f"s3_{name}.npz"))
+
+
 @pytest.fixture(scope="module")
 def c1_stage2():
-    from oracle import oracle as O
-    from pamo_b200 import meshgen as mg
-
-    V, F = mg.displaced_icosphere(5, 0)
-    v, f, _ = O.pamo_run_stage2(V, F, 0.05, min_verts=0)
-    return V, F, v, f
+    V, F, _, _, fx = _golden_case("c1")
+    return V, F, fx["v"], fx["f"]
 
 
 def _diag(V):
@@ -35,20 +52,152 @@ def _diag(V):
     return float(np.linalg.norm(V.max(0) - V.min(0)))
 
 
-def test_stage3_c1_matches_fp64_oracle(torch_cuda, c1_stage2):
-    from oracle import s3_oracle as S
+def _compare_case(torch_cuda, name, tol_diag):
+    """GPU stage 2 must equal the fixture's (oracle) stage 2 bit for bit; then
+    stage 3 on it against the FP64 oracle run."""
+    import pamo_b200
     from pamo_b200 import safe_project as SP
 
-    V, F, v, f = c1_stage2
-    want, _ = S.process(V, F, v.astype(np.float64), f, n_iters=5)
+    V, F, ratio, steps, fx = _golden_case(name)
+    ctx = pamo_b200.Context(0)
+    v2, f2, _ = pamo_b200.stage2_run(ctx, torch_cuda.from_numpy(V).cuda(), torch_cuda.from_numpy(F).cuda(),
+                                     int(ratio * len(F)))
+    assert np.array_equal(f2.cpu().numpy(), fx["f"])
+    assert np.array_equal(v2.cpu().numpy().view(np.uint32), fx["v"].view(np.uint32))
     sysm = SP.Stage3System()
-    got, gf = SP.process(V, F, v, f, 5, system=sysm)
-    assert np.array_equal(gf, f)
-    err = np.abs(got - want).max() / _diag(V)
-    moved = np.abs(want - v).max() / _diag(V)
-    print(f"stage3 C1: max |fp32 - fp64| = {err:.3e} of bbox diag (moved {moved:.3e}), {sysm.last_stats}")
+    got, gf = SP.process(V, F, fx["v"], fx["f"], int(fx["steps"]), system=sysm)
+    assert np.array_equal(gf, fx["f"])
+    want, tr_w = fx["q"], fx["trace"]
+    tr_g = sysm.last_trace
+    diag = _diag(V)
+    err = np.abs(got - want).max() / diag
+    moved = np.abs(want - fx["v"]).max() / diag
+    e_rel = np.abs(tr_g[:, :2] - tr_w[:, :2]).max() / np.abs(tr_w[:, :2]).max()
+    print(f"stage3 {name}: max |fp32 - fp64| = {err:.3e} of bbox diag (moved {moved:.3e}); energies rel "
+          f"{e_rel:.3e}; CCD steps max diff {np.abs(tr_g[:, 2] - tr_w[:, 2]).max():.3e}; "
+          f"halvings equal {np.array_equal(tr_g[:, 3], tr_w[:, 3])}; blocks {int(tr_g[:, 4].max())} vs "
+          f"{int(tr_w[:, 4].max())}, within d_hat {int(tr_g[:, 5].max())} vs {int(tr_w[:, 5].max())}; "
+          f"{sysm.last_stats}")
+    assert len(tr_g) == len(tr_w)
     assert moved > 10 * err  # the projection does move the mesh
-    assert err < TOL_DIAG
+    assert err < tol_diag
+    assert e_rel < TOL_ENERGY
+    assert np.array_equal(tr_g[:, 3], tr_w[:, 3])  # the same line-search trial is taken
+    assert np.abs(tr_g[:, 2] - tr_w[:, 2]).max() < 1e-3  # CCD step
+    # contact-block counts: the FP32 and FP64 distance tests differ only at the thresholds
+    assert np.all(np.abs(tr_g[:, 4] - tr_w[:, 4]) <= 1e-3 * np.maximum(tr_w[:, 4], 1000))
+    assert np.all(np.abs(tr_g[:, 5] - tr_w[:, 5]) <= 1e-3 * np.maximum(tr_w[:, 5], 1000))
+    return sysm, got, tr_g
+
+
+def test_stage3_c1_matches_fp64_oracle(torch_cuda):
+    _compare_case(torch_cuda, "c1", TOL_DIAG_C1)
+
+
+def test_stage3_thin_shell_contacts_match_fp64_oracle(torch_cuda):
+    """Thin-shell pair with ~30,000 contact blocks within d_hat and CCD-limited
+    steps: the contact barrier, its Gauss-Newton terms in the CG, the CCD and
+    the line search against the FP64 oracle."""
+    sysm, got, tr = _compare_case(torch_cuda, "shell8k", TOL_DIAG_CONTACT)
+    assert tr[:, 5].min() > 10000 and (tr[:, 2] < 1.0).any()
+
+
+def test_stage3_config3_thin_shell_pair_at_size(torch_cuda):
+    """Config 3's pair of 250k-face shells (gap 2e-3), ratio 0.05, 5 steps."""
+    if not os.path.exists(os.path.join(GOLDEN, "s3_shell500k.npz")):
+        pytest.skip("fixture not generated")
+    _compare_case(torch_cuda, "shell500k", TOL_DIAG_CONTACT)
+
+
+def test_cg_known_answer(torch_cuda):
+    """The reference's only stage-3 test (tests/test_dummy_energy.py:30-39):
+    Newton steps with the CG on E = 0.5 x^T A x + b^T x (A = R^T R, two
+    particles) reach solve(A, -b) within 1e-6.  The CG is the library's own
+    (pamo_bsr_pcg: the solve of every Newton iteration)."""
+    import pamo_b200
+    from pamo_b200 import _lib
+
+    rng = np.random.RandomState(998244353)
+    n = 2
+    R = rng.randn(3 * n, 3 * n)
+    A = R.T @ R
+    b = rng.randn(3 * n)
+    x = rng.randn(n, 3).astype(np.float64).reshape(-1)
+    ctx = pamo_b200.Context(0)
+    dev = torch_cuda.device("cuda", 0)
+    row_ptr = torch_cuda.tensor([0, 2, 4], dtype=torch_cuda.int32, device=dev)
+    col = torch_cuda.tensor([0, 1, 0, 1], dtype=torch_cuda.int32, device=dev)
+    blocks = np.stack([A[3 * i:3 * i + 3, 3 * j:3 * j + 3] for i in range(n) for j in range(n)]).astype(np.float32)
+    d_blocks = torch_cuda.from_numpy(np.ascontiguousarray(blocks.reshape(-1))).to(dev)
+    d_diag = torch_cuda.from_numpy(np.diag(A).astype(np.float32)).to(dev)
+    out = torch_cuda.empty(3 * n, dtype=torch_cuda.float32, device=dev)
+    stream = ctypes.c_void_p(torch_cuda.cuda.current_stream(dev).cuda_stream)
+    for _ in range(10):  # the Newton iterations of one step
+        rhs = torch_cuda.from_numpy((-(A @ x + b)).astype(np.float32)).to(dev)
+        rc = _lib.lib().pamo_bsr_pcg(ctx.handle, n, row_ptr.data_ptr(), col.data_ptr(), d_blocks.data_ptr(), 4,
+                                     d_diag.data_ptr(), rhs.data_ptr(), 40, out.data_ptr(), stream)
+        assert rc == 0
+        x = x + out.cpu().numpy().astype(np.float64)
+    x_gt = np.linalg.solve(A, -b)
+    assert np.allclose(x, x_gt, atol=1e-6), np.abs(x - x_gt).max()
+
+
+def test_cg_matches_fp64_iteration(torch_cuda):
+    """40 iterations of the library's CG on a larger sparse SPD block system
+    (a 3-D chain Laplacian plus a diagonal shift, 500 vertices) against the same
+    iteration in FP64 (cg_solver.py:96-158 as the oracle restates it)."""
+    import pamo_b200
+    from pamo_b200 import _lib
+
+    rng = np.random.default_rng(5)
+    n = 500
+    rows, cols, blks = [], [], []
+    K = np.zeros((3 * n, 3 * n))
+    for i in range(n):
+        for j in (i - 1, i, i + 1):
+            if 0 <= j < n:
+                if i == j:
+                    B = np.eye(3) * (2.5 + rng.random()) + 0.1 * np.ones((3, 3))
+                else:
+                    B = -np.eye(3) * 0.9
+                rows.append(i)
+                cols.append(j)
+                blks.append(B)
+                K[3 * i:3 * i + 3, 3 * j:3 * j + 3] = B
+    K = 0.5 * (K + K.T)
+    blks = [K[3 * i:3 * i + 3, 3 * j:3 * j + 3] for i, j in zip(rows, cols)]
+    row_ptr = np.searchsorted(np.array(rows), np.arange(n + 1)).astype(np.int32)
+    g = rng.standard_normal(3 * n)
+    dg = np.diag(K).copy()
+    # the oracle's iteration (Stage3Oracle.cg) with this operator
+    p = np.zeros_like(g)
+    r = g.copy()
+    z = r / (dg + 1e-6)
+    v = z.copy()
+    zr = z @ r
+    for _ in range(40):
+        Av = K @ v
+        vAv = v @ Av
+        zr_last = zr
+        if vAv > 1e-16:
+            alpha = zr_last / vAv
+            p = p + alpha * v
+            r = r - alpha * Av
+        z = r / dg
+        zr = z @ r
+        v = z + (zr / zr_last) * v
+    ctx = pamo_b200.Context(0)
+    dev = torch_cuda.device("cuda", 0)
+    t = lambda a, dt: torch_cuda.from_numpy(np.ascontiguousarray(a, dt)).to(dev)
+    out = torch_cuda.empty(3 * n, dtype=torch_cuda.float32, device=dev)
+    stream = ctypes.c_void_p(torch_cuda.cuda.current_stream(dev).cuda_stream)
+    keep = [t(row_ptr, np.int32), t(cols, np.int32), t(np.array(blks).reshape(-1), np.float32), t(dg, np.float32),
+            t(g, np.float32)]  # alive until the call returns
+    rc = _lib.lib().pamo_bsr_pcg(ctx.handle, n, keep[0].data_ptr(), keep[1].data_ptr(), keep[2].data_ptr(), len(cols),
+                                 keep[3].data_ptr(), keep[4].data_ptr(), 40, out.data_ptr(), stream)
+    assert rc == 0
+    got = out.cpu().numpy()
+    assert np.abs(got - p).max() <= 1e-4 * np.abs(p).max()
 
 
 def test_stage3_reduces_distance_to_gt(torch_cuda, c1_stage2):
@@ -68,26 +217,6 @@ def test_stage3_output_has_no_self_intersections(torch_cuda, c1_stage2):
 
     V, F, v, f = c1_stage2
     got, _ = SP.process(V, F, v, f, 5)
-    ctx = pamo_b200.Context(0)
-    flags, _ = pamo_b200.self_intersect(ctx, torch_cuda.from_numpy(got.astype(np.float32)).cuda(),
-                                        torch_cuda.from_numpy(f.astype(np.int32)).cuda())
-    assert int(flags.sum()) == 0
-
-
-def test_stage3_thin_shell_contacts(torch_cuda):
-    """Two concentric shells 2e-3 apart, simplified, then projected: the contact
-    barrier is active and the result stays intersection-free."""
-    import pamo_b200
-    from oracle import oracle as O
-    from pamo_b200 import meshgen as mg
-    from pamo_b200 import safe_project as SP
-
-    V, F = mg.thin_shell_pair(8000, 2e-3, 3)
-    v, f, _ = O.pamo_run_stage2(V, F, 0.2, min_verts=0)
-    sysm = SP.Stage3System()
-    got, _ = SP.process(V, F, v, f, 2, system=sysm)
-    assert sysm.last_stats["contacts"] > 0
-    assert np.isfinite(got).all()
     ctx = pamo_b200.Context(0)
     flags, _ = pamo_b200.self_intersect(ctx, torch_cuda.from_numpy(got.astype(np.float32)).cuda(),
                                         torch_cuda.from_numpy(f.astype(np.int32)).cuda())
