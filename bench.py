@@ -144,7 +144,8 @@ def cpu_sample(args, V, F, ratio):
     extrapolated by the face-rounds of the whole run; stage 3 = one Newton
     iteration of the FP64 numpy restatement on a stand-in of the stage-2 output,
     extrapolated to PaMO.run's 5 steps x 10 Newton iterations (plus its setup).
-    Returns (seconds for the whole workload, sample description, threads)."""
+    Returns (measured seconds of the sample, estimated seconds for the whole
+    workload, sample description, threads)."""
     from oracle import oracle as O
 
     target = int(ratio * len(F))
@@ -156,6 +157,7 @@ def cpu_sample(args, V, F, ratio):
     t0 = time.perf_counter()
     o.run(Vc, Fs, target, 4, 1e-3, args.sample_rounds if frac else 1000000)
     t2 = time.perf_counter() - t0
+    measured = t2
     if frac:
         total = t2 / frac
         desc = (f"stage 2: first {args.sample_rounds} rounds ({frac * 100:.1f}% of the run's face-rounds, "
@@ -180,34 +182,90 @@ def cpu_sample(args, V, F, ratio):
         t0 = time.perf_counter()
         s3.newton()
         t_newton = time.perf_counter() - t0
+        measured += t_reg + t_tgt + t_newton
         n_newton = 5 * s3.c.n_newton_iters
         total += t_reg + 5 * t_tgt + n_newton * t_newton
         desc += (f"; stage 3: one Newton iteration on a {len(f):,}-face stand-in of the stage-2 output "
                  f"({t_newton:.1f} s, {len(s3.blocks):,} contact blocks) x {n_newton} + setup")
-    return total, desc, O.lib().s2o_num_threads()
+    return measured, total, desc, O.lib().s2o_num_threads()
+
+
+def reference_gpu_stage2(V, F, ratio, reps=3):
+    """The reference's own stage-2 CUDA build (oracle/_ref/, compiled from the
+    reference sources by oracle/build_ref.sh), driven like PaMO.run's stage-2
+    loop (simp_cuda/pamo/__init__.py:148-189) with its torch compaction, on the
+    same inputs: wall time per run (device-resident inputs, host result, as
+    PaMO.run returns it).  None when the build or a device is missing."""
+    from oracle import ref as R
+
+    if not R.available():
+        return {"unavailable": "oracle/_ref not built (the reference sources were absent at build time)"}
+    import torch
+
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    P = torch.from_numpy(np.ascontiguousarray(V, np.float32)).cuda()
+    T = torch.from_numpy(np.ascontiguousarray(F, np.int32)).cuda()
+    times, st = [], {}
+    v = f = None
+    for _ in range(reps + 1):  # the first run warms up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        v, f = R.pamo_run_stage2_torch(P, T, ratio, min_verts=0, stats=st)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times[1:]))
+    return {"value": len(F) / 1e6 / t, "unit": "Mfaces/s", "ms": t * 1e3, "runs": reps, "faces_out": int(len(f)),
+            "rounds": st.get("rounds"),
+            "what": "the reference's CUSimp_Free::forward (its own CUDA sources, sm_100a, --fmad=false) in "
+                    "PaMO.run's stage-2 loop; wall clock per run, median"}
 
 
 def reference_arm(args):
     """The reference's algorithm on the host cores: the CPU restatement under
     oracle/ (the reference has no CPU path for stage 2, and its stage-3 CPU
-    device, Warp, is absent), bounded samples of the same workload."""
+    device, Warp, is absent), one bounded sample of the workload per step.
+
+    `ms_per_step` is the measured time of one sample.  `value` is the input
+    Mfaces/s of the whole workload estimated from the sample (stage 2 by the
+    face-rounds the sample covers, stage 3 by Newton iterations); the line
+    says so under `extrapolated`.  The reference's own stage-2 GPU build is
+    timed beside it on the full workload (`reference_gpu_stage2`)."""
     ws, rank, _ = dist_init(args)
     if rank != 0:
         return 0
     V, F, ratio, desc = workload(args.workload)
-    secs = []
+    measured, totals = [], []
+    sample = cores = None
     for _ in range(args.warmup + args.steps):
-        total, sample, cores = cpu_sample(args, V, F, ratio)
-        secs.append(total)
-    total_s = float(np.median(secs[args.warmup:]))
+        t_meas, total, sample, cores = cpu_sample(args, V, F, ratio)
+        measured.append(t_meas)
+        totals.append(total)
+    t_step = float(np.median(measured[args.warmup:]))
+    total_s = float(np.median(totals[args.warmup:]))
     value = len(F) / 1e6 / total_s
+    gpu = None
+    if args.workload in ("c1", "c2") and not args.no_reference_gpu:
+        try:
+            gpu = reference_gpu_stage2(V, F, ratio)
+        except Exception as e:  # the reference build failed on this device
+            gpu = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     line = {"metric": "input Mfaces/s", "value": value, "unit": "Mfaces/s", "impl": "reference", "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "stages": STAGES[args.stages]},
+            "config": {"workload": desc, "stages": STAGES[args.stages], "sample": sample},
+            "extrapolated": {"measured_s_per_step": t_step, "estimated_s_whole_workload": total_s,
+                             "basis": "each step times a bounded sample (ms_per_step); value = input faces / the "
+                                      "whole workload's time estimated from that sample"},
             "cpu_baseline": {"value": value, "unit": "Mfaces/s", "cores": cores, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": "Mfaces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+            "e2e": {"value": value, "unit": "Mfaces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu_stage2": gpu}
+    print(json.dumps(line), flush=True)
+    if gpu and "ms" in gpu:
+        # the reference build keeps device vectors in a static object whose
+        # destructor would run after the CUDA runtime has unloaded
+        sys.stdout.flush()
+        os._exit(0)
     return 0
 
 
@@ -414,8 +472,9 @@ def product_arm(args):
         ms_max, e2e_ms = replicas.max_over_ranks([dev_ms, e2e_ms], device=dev)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        total, sample, cores = cpu_sample(args, V, F, ratio)
-        cpu = {"value": nF / 1e6 / total, "unit": "Mfaces/s", "cores": cores, "kind": "port", "sample": sample}
+        _, total, sample, cores = cpu_sample(args, V, F, ratio)
+        cpu = {"value": nF / 1e6 / total, "unit": "Mfaces/s", "cores": cores, "kind": "port", "sample": sample,
+               "extrapolated": True}
     if rank == 0:
         value = ws * nF / 1e6 / (ms_max / 1e3)
         e2e = ws * nF / 1e6 / (e2e_ms / 1e3)
@@ -715,6 +774,8 @@ def main():
     ap.add_argument("--serve-max-faces", type=int, default=16_000_000)
     ap.add_argument("--sample-rounds", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="--impl reference: skip timing the reference's own stage-2 GPU build")
     ap.add_argument("--dump-rounds", action="store_true")
     ap.add_argument("--iters", type=int, default=1000000,
                     help="PaMO.run's iter: the most collapse rounds per simplification")

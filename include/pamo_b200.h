@@ -286,6 +286,19 @@ int pamo_safe_project_trace(pamo_ctx *ctx, double *h_out, int cap_rows, int *out
  * answers (the reference's tests/test_dummy_energy.py).  Replaces the stage-3
  * state held by the context.
  */
+/*
+ * Test of the library's bounded device waits (no counterpart in the
+ * reference).  which = 0: a prefix scan (the single-pass look-back of every
+ * stage-2 round) in which one tile never publishes; which = 1: the persistent
+ * CG solve of stage 3 in which one block never publishes its partial sums.
+ * The waiting blocks give up after `spin_limit` polls (at most 2^24), record
+ * the fault and return; the call then reports what a real run reports for
+ * such a fault, PAMO_ERR_DEVICE, and the context stays usable.  Returns
+ * PAMO_OK if nothing waited (PAMO_ERR_INVALID_ARG when the device cannot run
+ * the persistent solve, so there is no wait to test).
+ */
+int pamo_debug_wait_timeout(pamo_ctx *ctx, int which, long long spin_limit, void *stream);
+
 int pamo_bsr_pcg(pamo_ctx *ctx, int n, const int *d_row_ptr, const int *d_col, const float *d_blocks,
                  long long n_blocks, const float *d_diag, const float *d_rhs, int iters, float *d_out, void *stream);
 

@@ -66,6 +66,7 @@ SIGNATURES = {
                                _vp]),
     "pamo_safe_project_stats": (_i, [_vp, _vp]),
     "pamo_safe_project_trace": (_i, [_vp, _vp, _i, _ip]),
+    "pamo_debug_wait_timeout": (_i, [_vp, _i, _ll, _vp]),
     "pamo_bsr_pcg": (_i, [_vp, _i, _vp, _vp, _vp, _ll, _vp, _vp, _i, _vp, _vp]),
     "pamo_self_intersect_noalloc": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(_ll), _vp]),
     "pamo_check_mesh": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(_ll), _vp]),

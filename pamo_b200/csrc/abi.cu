@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "scan.cuh"
 #include "stage2.cuh"
@@ -879,6 +880,69 @@ int pamo_safe_project_trace(pamo_ctx *ctx, double *h_out, int cap_rows, int *out
     if (n > 0) CU_RET(cudaMemcpy(h_out, S.trace, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost));
     *out_rows = rows;
     return PAMO_OK;
+}
+
+int pamo_debug_wait_timeout(pamo_ctx *ctx, int which, long long spin_limit, void *stream)
+{
+    if (!ctx || (which != 0 && which != 1) || spin_limit < 0 || spin_limit > (1LL << 24)) return PAMO_ERR_INVALID_ARG;
+    RET_IF(set_device(ctx));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (which == 0) {
+        // a 32-tile scan whose tile 3 never publishes: the tiles after it wait
+        // on it, give up after spin_limit polls and record the fault
+        const long long n = 32LL * pamo::kScanTile;
+        const long long sc = pamo::scan_scratch_ints(n);
+        int *buf = nullptr;
+        CU_RET(cudaMalloc((void **)&buf, (size_t)(2 * n + sc + 1) * 4));
+        int *in = buf, *out = buf + n, *scratch = buf + 2 * n, *fault = scratch + sc;
+        int h_fault = 0;
+        cudaError_t e = cudaMemsetAsync(buf, 0, (size_t)(2 * n + sc + 1) * 4, s);
+        if (e == cudaSuccess) e = pamo::exclusive_scan_waits(in, out, n, nullptr, scratch, nullptr, s, fault, spin_limit, 3);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h_fault, fault, 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFree(buf);
+        if (e != cudaSuccess) return map_cuda_error(e);
+        return h_fault ? PAMO_ERR_DEVICE : PAMO_OK;
+    }
+    // the persistent CG with block 1 never publishing its partial sums: every
+    // block's wait on that slot gives up, the solve returns with the error
+    // recorded and the call reports PAMO_ERR_DEVICE
+    const int n = 4096;
+    std::vector<int> rp(n + 1), cl(n);
+    std::vector<float> blk(9 * (size_t)n, 0.f), dg(3 * (size_t)n, 2.f), rhs(3 * (size_t)n, 1.f);
+    for (int i = 0; i < n; ++i) {
+        rp[i] = i;
+        cl[i] = i;
+        blk[9 * (size_t)i] = blk[9 * (size_t)i + 4] = blk[9 * (size_t)i + 8] = 2.f;
+    }
+    rp[n] = n;
+    int *d_i = nullptr;
+    float *d_f = nullptr;
+    CU_RET(cudaMalloc((void **)&d_i, (size_t)(2 * n + 1) * 4));
+    if (cudaMalloc((void **)&d_f, (size_t)(9 + 3 + 3 + 3) * n * 4) != cudaSuccess) {
+        cudaFree(d_i);
+        return PAMO_ERR_OOM;
+    }
+    float *d_blk = d_f, *d_dg = d_f + 9 * (size_t)n, *d_rhs = d_dg + 3 * (size_t)n, *d_out = d_rhs + 3 * (size_t)n;
+    cudaError_t e = cudaMemcpy(d_i, rp.data(), (size_t)(n + 1) * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_i + n + 1, cl.data(), (size_t)n * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_blk, blk.data(), blk.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_dg, dg.data(), dg.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_rhs, rhs.data(), rhs.size() * 4, cudaMemcpyHostToDevice);
+    int rc = e == cudaSuccess ? PAMO_OK : map_cuda_error(e);
+    pamo::s3::Stage3 &S = ctx->s3;
+    if (rc == PAMO_OK) {
+        const long long keep_limit = S.cg_spin_limit;
+        S.cg_spin_limit = spin_limit;
+        S.cg_absent_block = 1;
+        rc = S.solve_bsr(n, d_i, d_i + n + 1, d_blk, n, d_dg, d_rhs, 4, d_out, s);
+        S.cg_spin_limit = keep_limit;
+        S.cg_absent_block = -1;
+        if (rc == PAMO_OK && S.cg_persistent != 1) rc = PAMO_ERR_INVALID_ARG;  // no waits to test here
+    }
+    cudaFree(d_i);
+    cudaFree(d_f);
+    return rc;
 }
 
 int pamo_bsr_pcg(pamo_ctx *ctx, int n, const int *d_row_ptr, const int *d_col, const float *d_blocks,

@@ -109,9 +109,12 @@ __device__ __forceinline__ unsigned long long status_word(unsigned epoch, unsign
     return ((unsigned long long)((epoch << 2) | flag) << 32) | (unsigned)value;
 }
 
+// spin_limit bounds each wait (polls); absent_tile >= 0 makes that tile never
+// publish (only the wait-timeout test passes one: its waiters must give up).
 __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const int *in, int *out, long long n_max,
                                                                 const int *d_n, int *scratch, int *d_total,
-                                                                int *fault, unsigned epoch)
+                                                                int *fault, unsigned epoch, long long spin_limit,
+                                                                long long absent_tile)
 {
     __shared__ int tile[kScanTile];
     __shared__ long long s_t;
@@ -141,7 +144,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const int *in, i
         const int ex = block_excl_scan<kScanThreads>(sum, agg);
         if (threadIdx.x < 32) {
             const int lane = threadIdx.x;
-            if (lane == 0) status[t] = status_word(epoch, t == 0 ? kFlagPrefix : kFlagSum, agg);
+            if (lane == 0 && t != absent_tile) status[t] = status_word(epoch, t == 0 ? kFlagPrefix : kFlagSum, agg);
             int prefix = 0;
             bool timed_out = false;
             for (long long top = t - 1; top >= 0 && !timed_out;) {
@@ -158,7 +161,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const int *in, i
                             val = (int)(unsigned)w;
                             break;
                         }
-                        if (spins > (1LL << 22)) {  // a tile that started earlier never published
+                        if (spins > spin_limit) {  // a tile that started earlier never published
                             timed_out = true;
                             break;
                         }
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const int *in, i
                     atomicExch(&scratch[2], 1);
                     if (fault) atomicExch(fault, 1);
                 }
-                status[t] = status_word(epoch, kFlagPrefix, prefix + agg);
+                if (t != absent_tile) status[t] = status_word(epoch, kFlagPrefix, prefix + agg);
                 s_prefix = prefix;
                 if (t == n_tiles - 1 && d_total) *d_total = prefix + agg;
             }
@@ -211,8 +214,16 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const int *in, i
     }
 }
 
+constexpr long long kScanSpinLimit = 1LL << 22;  // ~0.1 s of polls: far beyond any real wait
+
 cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *d_n, int *scratch, int *d_total,
                            cudaStream_t s, int *fault)
+{
+    return exclusive_scan_waits(in, out, n_max, d_n, scratch, d_total, s, fault, kScanSpinLimit, -1);
+}
+
+cudaError_t exclusive_scan_waits(const int *in, int *out, long long n_max, const int *d_n, int *scratch, int *d_total,
+                                 cudaStream_t s, int *fault, long long spin_limit, long long absent_tile)
 {
     static std::atomic<unsigned> epochs{0};
     if (n_max <= 0) {
@@ -225,7 +236,8 @@ cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *
     }
     const long long tiles = (n_max + kScanTile - 1) / kScanTile;
     const unsigned epoch = (epochs.fetch_add(1, std::memory_order_relaxed) + 1) & 0x3FFFFFFFu;
-    launch(k_scan_lookback, (unsigned)tiles, kScanThreads, 0, s, in, out, n_max, d_n, scratch, d_total, fault, epoch);
+    launch(k_scan_lookback, (unsigned)tiles, kScanThreads, 0, s, in, out, n_max, d_n, scratch, d_total, fault, epoch,
+           spin_limit, absent_tile);
     return cudaGetLastError();
 }
 

@@ -97,4 +97,10 @@ inline cudaError_t scan_scratch_init(int *scratch, long long ints, cudaStream_t 
 cudaError_t exclusive_scan(const int *in, int *out, long long n_max, const int *d_n, int *scratch, int *d_total,
                            cudaStream_t s, int *fault = nullptr);
 
+// exclusive_scan with each look-back wait bounded by `spin_limit` polls, and
+// tile `absent_tile` (>= 0) never publishing -- for the test that makes the
+// waits run out (pamo_debug_wait_timeout); -1 for a normal scan.
+cudaError_t exclusive_scan_waits(const int *in, int *out, long long n_max, const int *d_n, int *scratch, int *d_total,
+                                 cudaStream_t s, int *fault, long long spin_limit, long long absent_tile);
+
 }  // namespace pamo

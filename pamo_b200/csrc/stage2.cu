@@ -248,46 +248,57 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, boo
     if (is_stuck) return false;
     const int ua = A.first_near[u], ub = A.first_near[u + 1];
     const int va = A.first_near[v], vb = A.first_near[v + 1];
+    // link condition: common next-vertices of the two one-rings (the count is
+    // what matters; > 2 stops early).  v's list is held in registers when short,
+    // so each of u's entries is compared without reloading it.
+    constexpr int kRing = 12;
     int dup = 0;
-    for (int a = ua; a < ub; ++a) {
-        int iu = A.nxt[a];
-        for (int b = va; b < vb; ++b) {
-            int iv = A.nxt[b];
-            if (iu == iv) dup++;
+    if (vb - va <= kRing) {
+        int vn[kRing];
+#pragma unroll
+        for (int k = 0; k < kRing; ++k) vn[k] = va + k < vb ? A.nxt[va + k] : -3;  // -3 matches no entry
+        for (int a = ua; a < ub; ++a) {
+            const int iu = A.nxt[a];
+#pragma unroll
+            for (int k = 0; k < kRing; ++k) dup += (vn[k] == iu);
             if (dup > 2) {
                 out = 0xFFFFFFFFu;
                 return true;
             }
         }
+    } else {
+        for (int a = ua; a < ub; ++a) {
+            int iu = A.nxt[a];
+            for (int b = va; b < vb; ++b) {
+                int iv = A.nxt[b];
+                if (iu == iv) dup++;
+                if (dup > 2) {
+                    out = 0xFFFFFFFFu;
+                    return true;
+                }
+            }
+        }
     }
     if (dup != 2) return false;
 
-    float elen = 0.0f;
-    int nedge = 0;
+    // One walk over both one-rings (u's faces, then v's) feeds the two sums in
+    // the reference's order: the mean incident edge length (descending-pair
+    // edges of every face) and the skinny penalties of the faces that do not
+    // hold both endpoints, after their normal-flip test.
+    const V3 v0 = v3(A.pts[u]), v1 = v3(A.pts[v]);
+    const V3 mid = vmid(v0, v1);
+    float elen = 0.0f, Qa = 0.0f;
+    int nedge = 0, ntri = 0;
     for (int pass = 0; pass < 2; ++pass) {
-        int lo = pass ? va : ua, hi = pass ? vb : ub;
+        const int w = pass ? v : u, other = pass ? u : v;
+        const int lo = pass ? va : ua, hi = pass ? vb : ub;
         for (int a = lo; a < hi; ++a) {
             const int f = A.near_tris[a];
-            int4 t = A.tris[f];
-            float4 l = A.elen[f];
+            const int4 t = A.tris[f];
+            const float4 l = A.elen[f];
             if (t.x > t.y) { elen += l.x; nedge++; }
             if (t.y > t.z) { elen += l.y; nedge++; }
             if (t.z > t.x) { elen += l.z; nedge++; }
-        }
-    }
-    V3 v0 = v3(A.pts[u]), v1 = v3(A.pts[v]);
-    elen = elen / (float)nedge / edge_s * tres;
-    elen = elen + vnorm(vsub(v0, v1)) / edge_s * tres;
-    V3 mid = vmid(v0, v1);
-
-    float Qa = 0.0f;
-    int ntri = 0;
-    for (int pass = 0; pass < 2; ++pass) {
-        int w = pass ? v : u, other = pass ? u : v;
-        int lo = pass ? va : ua, hi = pass ? vb : ub;
-        for (int a = lo; a < hi; ++a) {
-            const int f = A.near_tris[a];
-            int4 t = A.tris[f];
             if (face_has(t, other)) continue;
             V3 o0 = v3(A.pts[t.x]), o1 = v3(A.pts[t.y]), o2 = v3(A.pts[t.z]);
             V3 n0 = t.x == w ? mid : o0;
@@ -304,6 +315,8 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, boo
             ntri++;
         }
     }
+    elen = elen / (float)nedge / edge_s * tres;
+    elen = elen + vnorm(vsub(v0, v1)) / edge_s * tres;
     Qa = 5.0f * Qa;
     float4 a0 = A.quad[3 * u], a1 = A.quad[3 * u + 1], a2 = A.quad[3 * u + 2];
     float4 b0 = A.quad[3 * v], b1 = A.quad[3 * v + 1], b2 = A.quad[3 * v + 2];
@@ -644,69 +657,133 @@ __global__ void k_active_list(const int *__restrict__ vals, const int *scene, co
     }
 }
 
-// For each active live face, enumerate overlapping leaves and append candidate
-// pairs.  A pair of two active faces is emitted once (by the lower index);
-// pairs sharing two or more vertex indices are never reported by the reference
-// and are dropped here.
-__global__ void __launch_bounds__(kThreads) k_query(const BvhNode *__restrict__ nodes, const int *__restrict__ vals,
-                                                    const int *scene, const float4 *__restrict__ pts,
-                                                    const int4 *__restrict__ tris, const uint8_t *__restrict__ active,
-                                                    int m, uint2 *pairs, long long cap_pairs, RoundCounters *cnt,
-                                                    const int *roots, const int *vslot, const int *qlist)
+// For each active live face, enumerate the overlapping leaves and append
+// candidate pairs.  A pair of two active faces is emitted once (by the lower
+// index); pairs sharing two or more vertex indices are never reported by the
+// reference and are dropped here.
+//
+// One traversal per warp: the warp's 32 queries (neighbouring
+// active faces in leaf order, so their boxes are close) walk the hierarchy
+// together.  A node is fetched once for the warp (one broadcast load instead of
+// up to 32 scattered ones), each lane tests its own box against both child
+// boxes, and a child goes on the warp's stack in shared memory when any lane
+// overlaps it.  Leaves are handled by the lanes that overlap them.  Each lane
+// emits exactly the pairs its own walk would (their order in the list depends
+// on scheduling, which nothing reads).  In a batch, a warp whose queries start in different mesh subtrees
+// walks each lane's own subtree with the per-lane stack instead.
+constexpr int kWarpStack = 96;
+constexpr int kQueryWarps = kThreads / 32;
+
+__device__ __forceinline__ void query_leaf(int leaf, int f, int4 t, const int *__restrict__ vals,
+                                           const uint8_t *__restrict__ active, const int4 *__restrict__ tris,
+                                           uint2 *pairs, long long cap_pairs, RoundCounters *cnt)
 {
+    const int g = vals[leaf];
+    if (g < 0 || g == f) return;  // empty leaves have empty boxes; guard anyway
+    if (active[g] && g < f) return;
+    const int4 tg = tris[g];
+    if (shared_indices(t, tg) >= 2) return;
+    cg::coalesced_group grp = cg::coalesced_threads();
+    int base = 0;
+    if (grp.thread_rank() == 0) base = atomicAdd(&cnt->n_pairs, (int)grp.size());
+    const int pos = grp.shfl(base, 0) + (int)grp.thread_rank();
+    if (pos < cap_pairs) pairs[pos] = make_uint2((unsigned)f, (unsigned)g);
+    else atomicAdd(&cnt->pair_overflow, 1);
+}
+
+__global__ void __launch_bounds__(kThreads) k_query_warp(const BvhNode *__restrict__ nodes,
+                                                         const int *__restrict__ vals, const int *scene,
+                                                         const float4 *__restrict__ pts,
+                                                         const int4 *__restrict__ tris,
+                                                         const uint8_t *__restrict__ active, int m, uint2 *pairs,
+                                                         long long cap_pairs, RoundCounters *cnt, const int *roots,
+                                                         const int *vslot, const int *qlist)
+{
+    __shared__ int stk[kQueryWarps][kWarpStack];
     const int L = scene[7];
-    int stack[kStack];
-    // queries from the list of active faces (k_active_list), or every leaf in
-    // leaf order with the inactive ones skipped
     const int N = qlist ? cnt->n_query : L;
-    PAMO_GRID_STRIDE(pp, N)
-    {
-        const int f = qlist ? qlist[pp] : vals[pp];
-        if (f < 0 || !active[f] || L < 2) continue;
-        int4 t = tris[f];
-        if (t.x == -1) continue;
-        float4 a = pts[t.x], b = pts[t.y], c = pts[t.z];
-        float3 qlo = make_float3(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)));
-        float3 qhi = make_float3(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)));
-        // a batch starts at the face's own mesh subtree (a leaf: a one-face mesh)
-        const int start = roots ? roots[vslot[t.x]] : 0;
-        if (start < 0) continue;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long warps = (long long)gridDim.x * kQueryWarps;
+    if (L < 2) return;
+    for (long long base = ((long long)blockIdx.x * kQueryWarps + w) * 32; base < N; base += warps * 32) {
+        const long long pp = base + lane;
+        int f = -1;
+        int4 t = make_int4(-1, -1, -1, 0);
+        if (pp < N) {
+            f = qlist ? qlist[pp] : vals[pp];
+            if (f >= 0 && active[f]) t = tris[f];
+            else f = -1;
+            if (t.x == -1) f = -1;
+        }
+        const bool valid = f >= 0;
+        const unsigned vball = __ballot_sync(0xffffffffu, valid);
+        if (!vball) continue;
+        float3 qlo = make_float3(INFINITY, INFINITY, INFINITY), qhi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+        int start = 0;
+        if (valid) {
+            const float4 a = pts[t.x], b = pts[t.y], c = pts[t.z];
+            qlo = make_float3(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)));
+            qhi = make_float3(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)));
+            if (roots) start = roots[vslot[t.x]];
+        }
+        // a batch: the warp walks together only if all its queries start at one subtree
+        const int first = __shfl_sync(0xffffffffu, start, __ffs(vball) - 1);
+        const bool uniform = __all_sync(0xffffffffu, !valid || start == first);
+        if (!uniform) {
+            if (!valid || start < 0) continue;
+            int stack[kStack];
+            int sp = 0;
+            stack[sp++] = start;
+            int budget = 2 * L + 16;
+            while (sp > 0) {
+                if (--budget < 0) {
+                    atomicAdd(&cnt->stack_overflow, 1);
+                    break;
+                }
+                const BvhNode nd = nodes[stack[--sp]];
+#pragma unroll
+                for (int side = 0; side < 2; ++side) {
+                    const float4 lo = side ? nd.rlo : nd.llo, hi = side ? nd.rhi : nd.lhi;
+                    if (!box_overlap(lo, hi, qlo, qhi)) continue;
+                    const int child = __float_as_int(lo.w);
+                    if (child < 0) query_leaf(~child, f, t, vals, active, tris, pairs, cap_pairs, cnt);
+                    else if (sp < kStack) stack[sp++] = child;
+                    else atomicAdd(&cnt->stack_overflow, 1);
+                }
+            }
+            continue;
+        }
+        if (first < 0) continue;  // a one-face mesh: its subtree is a single leaf
         int sp = 0;
-        stack[sp++] = start;
-        // a tree visits each of its L-1 inner nodes at most once per query; the
-        // bound only guards against a corrupted hierarchy
+        if (lane == 0) stk[w][0] = first;
+        sp = 1;
+        __syncwarp();
         int budget = 2 * L + 16;
         while (sp > 0) {
             if (--budget < 0) {
-                atomicAdd(&cnt->stack_overflow, 1);
+                if (lane == 0) atomicAdd(&cnt->stack_overflow, 1);
                 break;
             }
-            const BvhNode nd = nodes[stack[--sp]];
+            const int node = stk[w][--sp];
+            __syncwarp();
+            const BvhNode nd = nodes[node];
+            // the right child goes on the stack first, so the left is walked first
 #pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                float4 lo = side ? nd.rlo : nd.llo;
-                float4 hi = side ? nd.rhi : nd.lhi;
-                if (!box_overlap(lo, hi, qlo, qhi)) continue;
-                int child = __float_as_int(lo.w);
+            for (int side = 1; side >= 0; --side) {
+                const float4 lo = side ? nd.rlo : nd.llo, hi = side ? nd.rhi : nd.lhi;
+                const bool ov = valid && box_overlap(lo, hi, qlo, qhi);
+                if (!__any_sync(0xffffffffu, ov)) continue;
+                const int child = __float_as_int(lo.w);
                 if (child < 0) {
-                    int g = vals[~child];
-                    if (g < 0 || g == f) continue;  // empty leaves have empty boxes; guard anyway
-                    if (active[g] && g < f) continue;
-                    int4 tg = tris[g];
-                    if (shared_indices(t, tg) >= 2) continue;
-                    // one atomic per group of lanes appending together
-                    cg::coalesced_group grp = cg::coalesced_threads();
-                    int base = 0;
-                    if (grp.thread_rank() == 0) base = atomicAdd(&cnt->n_pairs, (int)grp.size());
-                    int pos = grp.shfl(base, 0) + (int)grp.thread_rank();
-                    if (pos < cap_pairs) pairs[pos] = make_uint2((unsigned)f, (unsigned)g);
-                    else atomicAdd(&cnt->pair_overflow, 1);
-                } else if (sp < kStack) {
-                    stack[sp++] = child;
-                } else {
+                    if (ov) query_leaf(~child, f, t, vals, active, tris, pairs, cap_pairs, cnt);
+                } else if (sp < kWarpStack) {
+                    if (lane == 0) stk[w][sp] = child;
+                    ++sp;
+                } else if (lane == 0) {
                     atomicAdd(&cnt->stack_overflow, 1);
                 }
             }
+            __syncwarp();
         }
     }
 }
@@ -1296,9 +1373,10 @@ static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s, const int *dirty
     launch(k_active_list, grid_for(m), kThreads, 0, s, (const int *)S.bvh.vals, (const int *)S.bvh.scene,
            (const uint8_t *)S.active, (const int4 *)S.tris, S.fflag, S.dcnt,
            batch ? (const SlotInfo *)S.slots : nullptr, batch ? (const int *)S.vslot : nullptr);
-    launch(k_query, grid_for(m), kThreads, 0, s, S.bvh.nodes, S.bvh.vals, S.bvh.scene, S.pts, S.tris, S.active, m,
-                                             S.pairs, S.cap_pairs, S.dcnt, batch ? (const int *)S.roots : nullptr,
-                                             batch ? (const int *)S.vslot : nullptr, (const int *)S.fflag);
+    launch(k_query_warp, grid_for(m), kThreads, 0, s, (const BvhNode *)S.bvh.nodes, (const int *)S.bvh.vals,
+           (const int *)S.bvh.scene, (const float4 *)S.pts, (const int4 *)S.tris, (const uint8_t *)S.active, m,
+           S.pairs, S.cap_pairs, S.dcnt, batch ? (const int *)S.roots : nullptr,
+           batch ? (const int *)S.vslot : nullptr, (const int *)S.fflag);
     S.prof.begin(PH_PAIRS, s);
     launch(k_pairs, grid_for(S.cap_pairs), kThreads, 0, s, S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris, S.isect, 1e-3f);
     S.prof.end(s);
@@ -1458,7 +1536,7 @@ cudaError_t query_and_test_pairs(const BvhNode *nodes, const int *vals, const in
                                  const int4 *tris, const uint8_t *active, int m, uint2 *pairs, long long cap_pairs,
                                  RoundCounters *cnt, uint8_t *isect, cudaStream_t s)
 {
-    launch(k_query, grid_for(m), kThreads, 0, s, nodes, vals, scene, pts, tris, active, m, pairs, cap_pairs, cnt,
+    launch(k_query_warp, grid_for(m), kThreads, 0, s, nodes, vals, scene, pts, tris, active, m, pairs, cap_pairs, cnt,
            (const int *)nullptr, (const int *)nullptr, (const int *)nullptr);
     launch(k_pairs, grid_for(cap_pairs), kThreads, 0, s, pairs, cnt, cap_pairs, pts, tris, isect, 1e-3f);
     return cudaGetLastError();

@@ -1234,6 +1234,8 @@ struct CGArgs {
     unsigned long long *slots;  // kSlotSets x gridDim slots, kSlotStride apart (all ones before the solve)
     int *iscal;
     int np, n_iters;
+    long long spin_limit;  // polls per wait before it gives up
+    int absent_block;      // >= 0: that block never publishes its partials (the wait-timeout test); else -1
 };
 
 __device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v)
@@ -1254,11 +1256,12 @@ __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long lon
 }
 
 // waits until *p holds a value; false after the spin limit (error recorded)
-__device__ __forceinline__ bool wait_value(const unsigned long long *p, unsigned long long &v, int *iscal)
+__device__ __forceinline__ bool wait_value(const unsigned long long *p, unsigned long long &v, int *iscal,
+                                           long long spin_limit)
 {
     v = ld_acquire(p);
     for (long long spins = 0; v == kSumPending; ++spins) {
-        if (spins > (1LL << 24)) {  // ~ seconds: a block never arrived
+        if (spins > spin_limit) {  // a block never arrived
             atomicExch(iscal + I_BAR_ERR, 1);
             return false;
         }
@@ -1279,12 +1282,12 @@ __device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, int k, dou
     unsigned long long *set = A.slots + (size_t)(k % kSlotSets) * set_words;
     unsigned long long *prev = A.slots + (size_t)((k + kSlotSets - 1) % kSlotSets) * set_words;
     const double bs = block_sum<kCgThreads>(acc);
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0 && (int)blockIdx.x != A.absent_block)
         st_release(set + (size_t)blockIdx.x * kSlotStride, (unsigned long long)__double_as_longlong(bs));
     int ok = 1;
     if ((int)threadIdx.x < G) {
         unsigned long long bits = 0;
-        if (wait_value(set + (size_t)threadIdx.x * kSlotStride, bits, A.iscal))
+        if (wait_value(set + (size_t)threadIdx.x * kSlotStride, bits, A.iscal, A.spin_limit))
             s_part[threadIdx.x] = __longlong_as_double((long long)bits);
         else
             ok = 0;
@@ -2017,7 +2020,8 @@ int Stage3::cg_solve(cudaStream_t s)
     if (cg_persistent == 1) {
         // partials hold the solve's kSlotSets x cg_blocks slots, all set to kSumPending
         unsigned long long *slots = reinterpret_cast<unsigned long long *>(partials);
-        CGArgs ca{op, grad, diag, p, r, z, v, v2, Av, Avc, slots, iscal, np, cfg.n_cg_iters};
+        CGArgs ca{op, grad, diag, p, r, z, v, v2, Av, Avc, slots, iscal, np, cfg.n_cg_iters, cg_spin_limit,
+                  cg_absent_block};
         S3_TRY(cudaMemsetAsync(slots, 0xFF, (size_t)kSlotSets * cg_blocks * kSlotStride * sizeof(unsigned long long), s));
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(cg_blocks);

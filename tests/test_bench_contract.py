@@ -25,3 +25,9 @@ def test_reference_arm_prints_one_contract_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"] and cb["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # one step's time is the measured sample; the whole-workload estimate is labelled
+    ex = d["extrapolated"]
+    assert abs(ex["measured_s_per_step"] * 1e3 - d["ms_per_step"]) < 1e-6 * d["ms_per_step"]
+    assert ex["estimated_s_whole_workload"] > 0 and "basis" in ex
+    # no GPU here: the reference's own GPU build is reported as unavailable
+    assert d["reference_gpu_stage2"] is None or "unavailable" in d["reference_gpu_stage2"]
