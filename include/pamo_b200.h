@@ -89,6 +89,37 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
                     int *out_n_tris, int *out_rounds);
 
 /*
+ * pamo_stage2_run on points that are already centred -- stage 1's output,
+ * which the reference's PaMO.run passes to stage 2 without centring again
+ * (simp_cuda/pamo/__init__.py:130-144) -- with h_offset3 (host float[3], the
+ * input's tris_mean) added back by pamo_stage2_fetch.
+ */
+int pamo_stage2_run_centred(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
+                            const float *h_offset3, long long target_faces, int tolerance, float threshold, int iters,
+                            void *stream, int *out_n_pts, int *out_n_tris, int *out_rounds);
+
+/*
+ * Stage 1 of PaMO.run, remeshing (replaces PaMO.preprocess_mesh + remesh,
+ * simp_cuda/pamo/__init__.py:60-120,130-142, which call torchcumesh2sdf and
+ * pdmc): the triangles normalised into the unit cube as preprocess_mesh does,
+ * a narrow-band signed distance field on a resolution^3 grid (band 3 /
+ * resolution; sign by flood fill from the grid boundary; shifted by
+ * -0.9 / resolution), dual marching cubes (one vertex per surface patch of a
+ * cell), and each quad split into the triangle pair with the larger smallest
+ * angle.  PaMO.run uses resolution 256, 128 when the target is at most 1000
+ * faces, 64 at most 50.  The result is in the frame centred on the input's
+ * tris_mean; *out_n_verts / *out_n_tris give its size and pamo_remesh_fetch
+ * copies it.
+ */
+int pamo_remesh(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris, int resolution,
+                void *stream, int *out_n_verts, int *out_n_tris);
+
+/* Copies the last pamo_remesh result to device buffers (vertices [n,3] in the
+   centred frame, faces [m,3]) and the input's tris_mean to h_offset3
+   (optional, host float[3]). */
+int pamo_remesh_fetch(pamo_ctx *ctx, float *d_out_verts, int *d_out_tris, float *h_offset3, void *stream);
+
+/*
  * Copies the result of the last pamo_stage2_run: vertices with the centring
  * offset added back (float32, as PaMO.run's "verts + tris_mean"), and faces.
  * `to_host` != 0 means out_points/out_tris are host pointers.

@@ -220,38 +220,43 @@ def dual_mc(d):
             V[base + p] = s / k
     # quads: crossed grid edges, axis by axis, lower sample in x-fastest order
     quads = []
-    # (axis offset, the other two axes' unit offsets in cyclic order)
-    axes = [((1, 0, 0), (0, 1, 0), (0, 0, 1)), ((0, 1, 0), (0, 0, 1), (1, 0, 0)), ((0, 0, 1), (1, 0, 0), (0, 1, 0))]
-    edge_base = [0, 4, 8]  # cube edges along x, y, z
-    for ax, (e_a, e_b, e_c) in enumerate(axes):
-        for z in range(R):
-            for y in range(R):
-                for x in range(R):
-                    x2, y2, z2 = x + e_a[0], y + e_a[1], z + e_a[2]
-                    if x2 >= R or y2 >= R or z2 >= R:
-                        continue
-                    i0, i1 = inside[z, y, x], inside[z2, y2, x2]
-                    if i0 == i1:
-                        continue
-                    vs = []
-                    ok = True
-                    for ob, oc in ((0, 0), (-1, 0), (-1, -1), (0, -1)):
-                        cx_ = x + ob * e_b[0] + oc * e_c[0]
-                        cy_ = y + ob * e_b[1] + oc * e_c[1]
-                        cz_ = z + ob * e_b[2] + oc * e_c[2]
-                        if not (0 <= cx_ < C and 0 <= cy_ < C and 0 <= cz_ < C):
-                            ok = False
-                            break
-                        # the grid edge's corner pair inside this cell
-                        lx, ly, lz = x - cx_, y - cy_, z - cz_
-                        ca = lx + 2 * ly + 4 * lz
-                        cb = ca + (1 if ax == 0 else (2 if ax == 1 else 4))
-                        e = _edge_of(ca, cb)
-                        p = table[case[cz_, cy_, cx_], e]
-                        vs.append(int(first[(cz_ * C + cy_) * C + cx_] + p))
-                    if not ok:
-                        continue
-                    quads.append(vs if i0 else vs[::-1])
+    # (the edge's axis, the other two axes in cyclic order)
+    axes = [(0, 1, 2), (1, 2, 0), (2, 0, 1)]
+    edge_index = np.zeros((3, 8), np.int64)  # cube edge from (axis, lower corner)
+    for e, (a, b) in enumerate(EDGE_CORNERS):
+        ax = {1: 0, 2: 1, 4: 2}[b - a]
+        edge_index[ax, a] = e
+    for ax, bax, cax in axes:
+        sl_lo = [slice(None)] * 3
+        sl_hi = [slice(None)] * 3
+        # arrays are [z, y, x]: axis k of (x, y, z) is array dimension 2 - k
+        sl_lo[2 - ax] = slice(0, R - 1)
+        sl_hi[2 - ax] = slice(1, R)
+        cross = np.zeros((R, R, R), bool)
+        cross[tuple(sl_lo)] = inside[tuple(sl_lo)] != inside[tuple(sl_hi)]
+        # all four cells must exist: the other coordinates in [1, R - 2]
+        for k in (bax, cax):
+            sl = [slice(None)] * 3
+            sl[2 - k] = 0
+            cross[tuple(sl)] = False
+            sl[2 - k] = R - 1
+            cross[tuple(sl)] = False
+        z, y, x = np.nonzero(cross)  # row-major: x fastest
+        P = np.stack([x, y, z], 1)
+        vs = []
+        for ob, oc in ((0, 0), (-1, 0), (-1, -1), (0, -1)):
+            cc = P.copy()
+            cc[:, bax] += ob
+            cc[:, cax] += oc
+            lo_corner = (P[:, 0] - cc[:, 0]) + 2 * (P[:, 1] - cc[:, 1]) + 4 * (P[:, 2] - cc[:, 2])
+            e = edge_index[ax, lo_corner]
+            cs = case[cc[:, 2], cc[:, 1], cc[:, 0]]
+            vs.append(first[(cc[:, 2] * C + cc[:, 1]) * C + cc[:, 0]] + table[cs, e])
+        vs = np.stack(vs, 1)
+        lower_inside = inside[z, y, x]
+        vs = np.where(lower_inside[:, None], vs, vs[:, ::-1])
+        quads.append(vs)
+    quads = np.concatenate(quads) if quads else np.zeros((0, 4), np.int64)
     return V, np.array(quads, np.int64).reshape(-1, 4)
 
 

@@ -21,7 +21,7 @@ from . import _lib
 from ._lib import Context, PamoError, check
 from . import metrics  # noqa: F401  (acceptance checks: check_mesh, hausdorff)
 
-__all__ = ["PaMO", "CUDSP_Free", "Context", "PamoError", "stage2_run", "self_intersect"]
+__all__ = ["PaMO", "CUDSP_Free", "Context", "PamoError", "stage2_run", "self_intersect", "remesh", "metrics"]
 __version__ = "0.1.0"
 
 
@@ -92,10 +92,12 @@ class CUDSP_Free:
         return ov, ot, oo, om, undo
 
 
-def stage2_run(ctx: Context, points, triangles, target_faces: int, tolerance=4, threshold=1e-3, iters=1000000):
+def stage2_run(ctx: Context, points, triangles, target_faces: int, tolerance=4, threshold=1e-3, iters=1000000,
+               offset=None):
     """Device-resident stage-2 loop of PaMO.run.  Returns (verts, faces) CUDA
     tensors (verts already shifted back by the centring offset) and the number of
-    rounds."""
+    rounds.  With `offset` (3 floats) the points are already centred -- stage
+    1's output -- and `offset` is added back instead of centring here."""
     import ctypes
 
     torch = _torch()
@@ -104,14 +106,53 @@ def stage2_run(ctx: Context, points, triangles, target_faces: int, tolerance=4, 
     dev = points.device
     stream = _stream_ptr(dev)
     on, om, rounds = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-    check("pamo_stage2_run", _lib.lib().pamo_stage2_run(
-        ctx.handle, points.data_ptr(), triangles.data_ptr(), int(points.shape[0]), int(triangles.shape[0]),
-        int(min(int(target_faces), 2**62)), int(tolerance), float(threshold), int(min(iters, 2**31 - 1)), stream,
-        ctypes.byref(on), ctypes.byref(om), ctypes.byref(rounds)))
+    args = (int(min(int(target_faces), 2**62)), int(tolerance), float(threshold), int(min(iters, 2**31 - 1)), stream,
+            ctypes.byref(on), ctypes.byref(om), ctypes.byref(rounds))
+    if offset is None:
+        check("pamo_stage2_run", _lib.lib().pamo_stage2_run(
+            ctx.handle, points.data_ptr(), triangles.data_ptr(), int(points.shape[0]), int(triangles.shape[0]), *args))
+    else:
+        off = (ctypes.c_float * 3)(*[float(x) for x in offset])
+        check("pamo_stage2_run_centred", _lib.lib().pamo_stage2_run_centred(
+            ctx.handle, points.data_ptr(), triangles.data_ptr(), int(points.shape[0]), int(triangles.shape[0]), off,
+            *args))
     v = torch.empty((on.value, 3), dtype=torch.float32, device=dev)
     f = torch.empty((om.value, 3), dtype=torch.int32, device=dev)
     check("pamo_stage2_fetch", _lib.lib().pamo_stage2_fetch(ctx.handle, v.data_ptr(), f.data_ptr(), 0, stream))
     return v, f, rounds.value
+
+
+def remesh(ctx: Context, points, triangles, resolution=256):
+    """Stage 1 of PaMO.run on the device (pamo_remesh): returns (verts, faces)
+    CUDA tensors in the frame centred on the input's tris_mean, and tris_mean
+    (numpy float32 [3]), as the reference's preprocess_mesh + remesh give them
+    (simp_cuda/pamo/__init__.py:60-142)."""
+    import ctypes
+
+    torch = _torch()
+    points = points.contiguous()
+    triangles = triangles.contiguous()
+    dev = points.device
+    stream = _stream_ptr(dev)
+    nv, nt = ctypes.c_int(), ctypes.c_int()
+    check("pamo_remesh", _lib.lib().pamo_remesh(ctx.handle, points.data_ptr(), triangles.data_ptr(),
+                                                int(points.shape[0]), int(triangles.shape[0]), int(resolution), stream,
+                                                ctypes.byref(nv), ctypes.byref(nt)))
+    v = torch.empty((nv.value, 3), dtype=torch.float32, device=dev)
+    f = torch.empty((nt.value, 3), dtype=torch.int32, device=dev)
+    off = (ctypes.c_float * 3)()
+    check("pamo_remesh_fetch", _lib.lib().pamo_remesh_fetch(ctx.handle, v.data_ptr(), f.data_ptr(), off, stream))
+    return v, f, np.array(off[:], np.float32)
+
+
+def stage1_resolution(target_faces):
+    """PaMO.run's grid resolution for stage 1 (pamo/__init__.py:134-137)."""
+    R = 256
+    if target_faces <= 1000:
+        R = 128
+    if target_faces <= 50:
+        R = 64
+    return R
 
 
 def self_intersect(ctx: Context, points, triangles):
@@ -156,9 +197,6 @@ class PaMO:
         self.target_faces = None
         self.last_rounds = 0
         self.timings = {}
-        if use_stage1:
-            raise NotImplementedError("stage 1 (SDF + dual marching cubes remesh) is not built; "
-                                      "use PaMO(..., use_stage1=False)")
         if use_stage3:
             from .safe_project import Stage3Config, Stage3System
 
@@ -170,16 +208,17 @@ class PaMO:
         self.target_faces = max(int(ratio * len(triangles)), min_verts)
         if self.verbose:
             print("Target faces : {}".format(self.target_faces))
+        offset = None
         if self.use_stage1:
-            from .remesh import remesh_tensors
-
             t0 = time.time()
-            points, triangles = remesh_tensors(points, triangles, self.target_faces)
+            points, triangles, offset = remesh(self.ctx, points, triangles, stage1_resolution(self.target_faces))
             self.timings["stage1"] = time.time() - t0
+            self.stage1_faces = int(triangles.shape[0])
             if self.verbose:
                 print(f"Time for Remeshing: {self.timings['stage1']} sec")
         t0 = time.time()
-        v, f, rounds = stage2_run(self.ctx, points, triangles, self.target_faces, tolerance, threshold, iter)
+        v, f, rounds = stage2_run(self.ctx, points, triangles, self.target_faces, tolerance, threshold, iter,
+                                  offset=offset)
         self.last_rounds = rounds
         verts = v.cpu().numpy()
         faces = f.cpu().numpy()

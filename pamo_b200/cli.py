@@ -2,8 +2,6 @@
 reference's example.py:13-21:
 
     python -m pamo_b200.cli -i in.obj -o out.obj -r 0.1 [-mv 0] [--disable_stage1] [--disable_stage3]
-
-Stage 1 (remeshing) is not built here, so the run needs --disable_stage1.
 """
 from __future__ import annotations
 
@@ -21,9 +19,6 @@ def main(argv=None) -> int:
     ap.add_argument("--disable_stage1", action="store_true", help="Disable remeshing")
     ap.add_argument("--disable_stage3", action="store_true", help="Disable safe projection")
     args = ap.parse_args(argv)
-    if not args.disable_stage1:
-        print("stage 1 (remeshing) is not available in pamo_b200: pass --disable_stage1", file=sys.stderr)
-        return 2
 
     import torch
 
@@ -33,7 +28,7 @@ def main(argv=None) -> int:
     mesh = load_mesh(args.input)
     print(f"# of input verts : {len(mesh.vertices)}")
     print(f"# of input faces : {len(mesh.faces)}")
-    pamo = PaMO(mesh, use_stage1=False, use_stage3=not args.disable_stage3)
+    pamo = PaMO(mesh, use_stage1=not args.disable_stage1, use_stage3=not args.disable_stage3)
     start = time.time()
     verts, faces = pamo.run(torch.from_numpy(mesh.vertices).float().cuda(), torch.from_numpy(mesh.faces).int().cuda(),
                             min_verts=args.min_vertex, ratio=args.ratio)

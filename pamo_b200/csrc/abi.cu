@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "scan.cuh"
+#include "stage1.cuh"
 #include "stage2.cuh"
 #include "stage3.cuh"
 
@@ -19,6 +20,7 @@ struct pamo_ctx {
     int device = 0;
     pamo::Stage2 s2;
     pamo::s3::Stage3 s3;
+    pamo::s1::Stage1 s1;
     double s3_stats[3] = {0, 0, 0};
     int *undo_prev = nullptr;  // copy of the previous round's undo list (PaMO.run passes a clone)
     long long undo_prev_cap = 0;
@@ -410,6 +412,19 @@ using namespace pamo;
         if (_e != cudaSuccess) return map_cuda_error(_e); \
     } while (0)
 
+// tris_mean of PaMO.run: each face's corner mean, then the rows added one by
+// one in float32 (numpy's order); scratch holds 3 m floats
+static int centring_mean(const float *d_points, const int *d_tris, int m, float *scratch, float *mean_dev,
+                         cudaStream_t s)
+{
+    launch(k_face_means, grid_for(m), kThreads, 0, s, d_points, d_tris, m, scratch, scratch + m, scratch + 2LL * m);
+    const int smem = 2 * 3 * kMeanChunk * (int)sizeof(float);
+    CU_RET(cudaFuncSetAttribute(k_sequential_mean, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    launch(k_sequential_mean, 1, 1024, smem, s, scratch, scratch + m, scratch + 2LL * m, m, mean_dev);
+    CU_RET(cudaGetLastError());
+    return PAMO_OK;
+}
+
 extern "C" {
 
 int pamo_version(void) { return 100; }
@@ -455,6 +470,7 @@ int pamo_ctx_destroy(pamo_ctx *ctx)
         cudaDeviceSynchronize();
         ctx->s2.release();
         ctx->s3.release();
+        ctx->s1.release();
         if (ctx->undo_prev) cudaFree(ctx->undo_prev);
         if (ctx->stage) cudaFree(ctx->stage);
         if (ctx->istage) cudaFree(ctx->istage);
@@ -502,9 +518,13 @@ int pamo_free_copy_undo(pamo_ctx *ctx, int *d_out, int n, void *stream)
     return PAMO_OK;
 }
 
-int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
-                    long long target_faces, int tolerance, float threshold, int iters, void *stream, int *out_n_pts,
-                    int *out_n_tris, int *out_rounds)
+// The stage-2 loop of PaMO.run.  offset3 == nullptr: the points are centred
+// here (tris_mean in numpy's float32 order) as PaMO.run does without stage 1;
+// otherwise they are already centred (stage 1's output) and offset3 is the
+// tris_mean added back at the end.
+static int stage2_loop(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
+                       const float *offset3, long long target_faces, int tolerance, float threshold, int iters,
+                       void *stream, int *out_n_pts, int *out_n_tris, int *out_rounds)
 {
     if (!ctx || n_pts <= 0 || n_tris <= 0 || !d_points || !d_tris || !out_n_pts || !out_n_tris || !out_rounds)
         return PAMO_ERR_INVALID_ARG;
@@ -519,12 +539,10 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
     float *mean_dev = reinterpret_cast<float *>(S.dev_misc);
     int *bounds = S.dev_misc + 8;
     float *bounds_f = reinterpret_cast<float *>(S.dev_misc + 16);
-    launch(k_face_means, grid_for(n_tris), kThreads, 0, s, d_points, d_tris, n_tris, mxyz, mxyz + n_tris,
-                                                       mxyz + 2LL * n_tris);
-    {
-        const int smem = 2 * 3 * kMeanChunk * (int)sizeof(float);
-        CU_RET(cudaFuncSetAttribute(k_sequential_mean, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        launch(k_sequential_mean, 1, 1024, smem, s, mxyz, mxyz + n_tris, mxyz + 2LL * n_tris, n_tris, mean_dev);
+    if (offset3) {
+        CU_RET(cudaMemsetAsync(mean_dev, 0, 3 * sizeof(float), s));  // already centred
+    } else {
+        RET_IF(centring_mean(d_points, d_tris, n_tris, mxyz, mean_dev, s));
     }
     launch(k_bounds_init, 1, 32, 0, s, bounds);
     launch(k_centre, grid_for(n_pts), kThreads, 0, s, d_points, n_pts, mean_dev, S.opts, bounds);
@@ -534,7 +552,7 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
     CU_RET(cudaMemcpyAsync(S.h_scalars, mean_dev, 3 * 4, cudaMemcpyDeviceToHost, s));
     CU_RET(cudaMemcpyAsync(S.h_scalars + 4, bounds_f, 6 * 4, cudaMemcpyDeviceToHost, s));
     CU_RET(cudaStreamSynchronize(s));
-    for (int k = 0; k < 3; ++k) S.offset[k] = S.h_scalars[k];
+    for (int k = 0; k < 3; ++k) S.offset[k] = offset3 ? offset3[k] : S.h_scalars[k];
     const float *bf = S.h_scalars + 4;
     float sx = bf[3] - bf[0], sy = bf[4] - bf[1], sz = bf[5] - bf[2];
     float scale = sy > sx ? sy : sx;  // Python max() keeps the first maximal argument
@@ -571,6 +589,60 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
     *out_n_pts = n;
     *out_n_tris = m;
     *out_rounds = rounds;
+    return PAMO_OK;
+}
+
+int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
+                    long long target_faces, int tolerance, float threshold, int iters, void *stream, int *out_n_pts,
+                    int *out_n_tris, int *out_rounds)
+{
+    return stage2_loop(ctx, d_points, d_tris, n_pts, n_tris, nullptr, target_faces, tolerance, threshold, iters, stream,
+                       out_n_pts, out_n_tris, out_rounds);
+}
+
+int pamo_stage2_run_centred(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
+                            const float *h_offset3, long long target_faces, int tolerance, float threshold, int iters,
+                            void *stream, int *out_n_pts, int *out_n_tris, int *out_rounds)
+{
+    if (!h_offset3) return PAMO_ERR_INVALID_ARG;
+    return stage2_loop(ctx, d_points, d_tris, n_pts, n_tris, h_offset3, target_faces, tolerance, threshold, iters,
+                       stream, out_n_pts, out_n_tris, out_rounds);
+}
+
+int pamo_remesh(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris, int resolution,
+                void *stream, int *out_n_verts, int *out_n_tris)
+{
+    if (!ctx || n_pts <= 0 || n_tris <= 0 || !d_points || !d_tris || !out_n_verts || !out_n_tris || resolution < 4 ||
+        resolution > 1024)
+        return PAMO_ERR_INVALID_ARG;
+    RET_IF(set_device(ctx));
+    cudaStream_t s = (cudaStream_t)stream;
+    pamo::s1::Stage1 &S = ctx->s1;
+    RET_IF(S.ensure(n_tris, resolution));
+    int h_bad = 0;
+    RET_IF(s3_validate(d_tris, 3LL * n_tris, n_pts, S.dev + 15, &h_bad, s));
+    // tris_mean of the input (the scratch: the normalised-triangle buffer, 9 m floats)
+    RET_IF(centring_mean(d_points, d_tris, n_tris, S.tris, S.mean_dev, s));
+    CU_RET(cudaMemcpyAsync(S.offset, S.mean_dev, 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    RET_IF(pamo::s1::remesh(S, d_points, d_tris, n_pts, n_tris, S.mean_dev, resolution, s));
+    CU_RET(cudaStreamSynchronize(s));
+    *out_n_verts = S.n_verts;
+    *out_n_tris = S.n_tris;
+    return PAMO_OK;
+}
+
+int pamo_remesh_fetch(pamo_ctx *ctx, float *d_out_verts, int *d_out_tris, float *h_offset3, void *stream)
+{
+    if (!ctx || !d_out_verts || !d_out_tris) return PAMO_ERR_INVALID_ARG;
+    RET_IF(set_device(ctx));
+    cudaStream_t s = (cudaStream_t)stream;
+    pamo::s1::Stage1 &S = ctx->s1;
+    if (S.n_tris <= 0) return PAMO_ERR_INVALID_ARG;
+    CU_RET(cudaMemcpyAsync(d_out_verts, S.verts, (size_t)S.n_verts * 12, cudaMemcpyDeviceToDevice, s));
+    CU_RET(cudaMemcpyAsync(d_out_tris, S.faces, (size_t)S.n_tris * 12, cudaMemcpyDeviceToDevice, s));
+    if (h_offset3)
+        for (int k = 0; k < 3; ++k) h_offset3[k] = S.offset[k];
+    CU_RET(cudaStreamSynchronize(s));
     return PAMO_OK;
 }
 

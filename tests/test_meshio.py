@@ -134,13 +134,38 @@ def test_files(tmp_path):
     np.testing.assert_array_equal(m.faces, F)
 
 
-def test_cli_needs_stage1_disabled(tmp_path, capsys):
-    """The command line mirrors example.py's options; stage 1 is not built, so
-    it stops before loading anything unless --disable_stage1 is given."""
+def test_cli_passes_the_stage_switches(tmp_path, monkeypatch):
+    """The command line mirrors example.py's options: --disable_stage1 /
+    --disable_stage3 reach PaMO, the mesh is loaded and the result saved."""
+    import sys
+    import types
+
+    import pamo_b200
     from pamo_b200 import cli
 
-    rc = cli.main(["-i", str(tmp_path / "missing.obj"), "-o", str(tmp_path / "o.obj"), "-r", "0.1"])
-    assert rc == 2 and "--disable_stage1" in capsys.readouterr().err
+    seen = {}
+
+    class FakePaMO:
+        def __init__(self, mesh, use_stage1=True, use_stage3=True):
+            seen["stages"] = (use_stage1, use_stage3)
+            self.mesh = mesh
+
+        def run(self, points, triangles, ratio, min_verts):
+            seen["ratio"], seen["min_verts"] = ratio, min_verts
+            return self.mesh.vertices.astype(np.float32), self.mesh.faces
+
+    fake_torch = types.SimpleNamespace(from_numpy=lambda a: types.SimpleNamespace(
+        float=lambda: types.SimpleNamespace(cuda=lambda: a), int=lambda: types.SimpleNamespace(cuda=lambda: a)))
+    monkeypatch.setitem(sys.modules, "torch", fake_torch)
+    monkeypatch.setattr(pamo_b200, "PaMO", FakePaMO)
+    V, F = mg.displaced_icosphere(1, 0)
+    src, dst = str(tmp_path / "in.obj"), str(tmp_path / "out.obj")
+    meshio.save_obj(src, V, F)
+    assert cli.main(["-i", src, "-o", dst, "-r", "0.2", "--disable_stage1"]) == 0
+    assert seen == {"stages": (False, True), "ratio": 0.2, "min_verts": 0}
+    assert cli.main(["-i", src, "-o", dst, "--disable_stage3", "-mv", "5"]) == 0
+    assert seen["stages"] == (True, False) and seen["min_verts"] == 5
+    np.testing.assert_array_equal(meshio.load_mesh(dst).faces, F)
 
 
 def _ply_bytes(V, polys, fmt):
