@@ -1,15 +1,18 @@
 """Benchmark: PaMO on one B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
-                    [--workload c2|c1|c4|c5] [--stages 23|2] [--no-cpu-baseline]
+                    [--workload c2|c1|c4|c5] [--stages 123|23|2] [--no-cpu-baseline] [--no-c4]
 
 Default workload "c2" (config 2): a 1024x1024 noisy torus (1,048,576 verts /
-2,097,152 faces, fp32/int32, seeded) through PaMO(mesh, use_stage1=False,
-use_stage3=True).run(points, triangles, 0.01, min_verts=0): the stage-2
-simplification loop (centring, init permutation, collapse rounds with the
-self-intersection undo, compaction) to ~20,971 faces, then stage 3 (safe
-projection against the input, 5 steps of 10 Newton iterations).  Stage 1 is
-not built.  "c1" is config 1 (level-5 displaced icosphere, ratio 0.05).
+2,097,152 faces, fp32/int32, seeded) through PaMO(mesh, use_stage1=True,
+use_stage3=True).run(points, triangles, 0.01, min_verts=0): stage 1 (the
+remesh through a 256^3 narrow-band distance field and dual marching cubes),
+the stage-2 simplification loop (init permutation, collapse rounds with the
+self-intersection undo, compaction) to <= 20,971 faces, then stage 3 (safe
+projection against the input, 5 steps of 10 Newton iterations).  --stages 23
+leaves stage 1 out.  "c1" is config 1 (level-5 displaced icosphere, ratio
+0.05).  At one GPU the line also carries config 4's batched-vs-plain
+comparison (256 meshes, one pass each; --no-c4 skips it).
 
 One step = one whole PaMO.run.  `value` = input Mfaces/s with the inputs
 resident in device memory (CUDA events around the steps; PaMO.run returns host
@@ -165,7 +168,7 @@ def cpu_sample(args, V, F, ratio):
     else:  # no recorded round sizes for this workload: the whole loop
         total = t2
         desc = f"stage 2: the whole loop ({t2:.1f} s)"
-    if args.stages == "23":
+    if "3" in args.stages:
         from oracle import s3_oracle as S3  # numpy FP64 restatement
 
         v, f = stage3_stand_in(args.workload)
@@ -187,6 +190,9 @@ def cpu_sample(args, V, F, ratio):
         total += t_reg + 5 * t_tgt + n_newton * t_newton
         desc += (f"; stage 3: one Newton iteration on a {len(f):,}-face stand-in of the stage-2 output "
                  f"({t_newton:.1f} s, {len(s3.blocks):,} contact blocks) x {n_newton} + setup")
+    if "1" in args.stages:
+        desc += ("; stage 1 is not in the sample (the reference runs it through GPU libraries only; its "
+                 "restatement under oracle/ is a numpy test oracle)")
     return measured, total, desc, O.lib().s2o_num_threads()
 
 
@@ -269,7 +275,8 @@ def reference_arm(args):
     return 0
 
 
-STAGES = {"23": "stages 2 + 3 of PaMO.run (stage 1 is not built)", "2": "stage 2 of PaMO.run"}
+STAGES = {"123": "stages 1 + 2 + 3 of PaMO.run", "23": "stages 2 + 3 of PaMO.run (stage 1 off)",
+          "2": "stage 2 of PaMO.run"}
 
 
 def _sample_fraction(args, sample_rounds):
@@ -382,7 +389,8 @@ def product_arm(args):
     Fd = torch.from_numpy(F).to(dev)
     Ph = torch.from_numpy(V).pin_memory()
     Fh = torch.from_numpy(F).pin_memory()
-    pm = pamo_b200.PaMO((V, F), use_stage1=False, use_stage3=args.stages == "23", device=local, verbose=False)
+    pm = pamo_b200.PaMO((V, F), use_stage1="1" in args.stages, use_stage3="3" in args.stages, device=local,
+                        verbose=False)
 
     def run_resident():
         """One PaMO.run from device-resident inputs to its host (verts, faces)."""
@@ -416,7 +424,7 @@ def product_arm(args):
     for k in range(args.steps):
         run_resident()
         evs[k + 1].record(s)
-        stage_ms.append([round(1e3 * pm.timings.get(key, 0.0), 1) for key in ("stage2", "stage3")])
+        stage_ms.append([round(1e3 * pm.timings.get(key, 0.0), 1) for key in ("stage1", "stage2", "stage3")])
     torch.cuda.synchronize()
     launches = L.pamo_launch_count() - launches0
     dev_ms = evs[0].elapsed_time(evs[-1]) / args.steps
@@ -445,7 +453,7 @@ def product_arm(args):
     s2_ms = ev0.elapsed_time(ev1) / n_s2
     clocks = clk.stop()
     # one more run with per-phase CUDA events on both stages (outside the timed region)
-    handles = [pm.ctx.handle] + ([pm.system.ctx.handle] if args.stages == "23" else [])
+    handles = [pm.ctx.handle] + ([pm.system.ctx.handle] if "3" in args.stages else [])
     for h in handles:
         L.pamo_profile_enable(h, 1)
     v_out, f_out = run_resident()
@@ -470,6 +478,9 @@ def product_arm(args):
         from pamo_b200 import replicas
 
         ms_max, e2e_ms = replicas.max_over_ranks([dev_ms, e2e_ms], device=dev)
+    c4 = None
+    if ws == 1 and args.workload == "c2" and not args.no_c4:
+        c4 = c4_compare(local)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         _, total, sample, cores = cpu_sample(args, V, F, ratio)
@@ -485,16 +496,20 @@ def product_arm(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "stages": STAGES[args.stages], "faces_out": om.value, "verts_out": on.value,
                        "rounds": rounds, "iters": args.iters, "l2": "inputs/working set > L2, no flush",
-                       "parallelism": f"replicas x{ws}", "api": "PaMO(mesh, use_stage1=False, use_stage3).run"},
+                       "parallelism": f"replicas x{ws}",
+                       "api": f"PaMO(mesh, use_stage1={'1' in args.stages}, use_stage3={'3' in args.stages}).run",
+                       "stage1_faces": getattr(pm, "stage1_faces", None)},
             "gpu_launches": int(launches),
             "step_ms": step_ms,
             "step_stage_ms": stage_ms,
+            "step_stage_keys": ["stage1", "stage2", "stage3"],
             "latency_ms": {"p50": float(np.percentile(lat, 50)) * 1e3, "p99": float(np.percentile(lat, 99)) * 1e3},
             "e2e": {"value": e2e, "unit": "Mfaces/s", "h2d_bytes_per_step": int(nF * 12 + len(V) * 12),
                     "d2h_bytes_per_step": int(d2h)},
             "stage_ms": {k: round(v * 1e3, 3) for k, v in timings.items()},
             "stage2_device": {"value": nF / 1e6 / (s2_ms / 1e3), "unit": "Mfaces/s", "ms": s2_ms,
-                              "what": "pamo_stage2_run alone, device-resident in and out"},
+                              "what": "pamo_stage2_run alone on the unremeshed input, device-resident in and out"},
+            "batched_vs_plain": c4,
             "clocks": clocks,
             "cpu_baseline": cpu,
             "intersections": intersections,
@@ -510,6 +525,64 @@ def product_arm(args):
 
         replicas.finalize()
     return 0
+
+
+def c4_compare(local, n_meshes=256, seed=0):
+    """Config 4 on the side of the default line: 256 meshes of uneven sizes
+    (log-uniform 5k..500k faces; spheres, tori, thin-shell pairs; ratios
+    0.001 / 0.01 / 0.05), stage 2 with min_verts 0, once through the batch
+    engine and once through the plain per-mesh loop, on device-resident
+    inputs, after one warm-up pass of each.  Latency = each mesh's completion
+    time from the common start."""
+    import torch
+
+    import pamo_b200
+    from pamo_b200 import _lib
+    from pamo_b200 import meshgen as mg
+    from pamo_b200.batch import BatchEngine, target_faces
+
+    dev = torch.device("cuda", local)
+    t_gen = time.perf_counter()
+    mix = mg.mixed_batch(n_meshes, seed=seed)
+    t_gen = time.perf_counter() - t_gen
+    total_faces = sum(len(F) for _, _, F, _ in mix)
+    targets = [target_faces(len(F), r, 0) for _, _, F, r in mix]
+    dmeshes = [(torch.from_numpy(V).to(dev), torch.from_numpy(F).to(dev), t) for (_, V, F, _), t in zip(mix, targets)]
+    eng = BatchEngine(device=local, max_verts=sum(len(V) for _, V, _, _ in mix), max_faces=total_faces,
+                      max_meshes=len(mix))
+    L = _lib.lib()
+    ctx = pamo_b200.Context(local)
+    sp = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+    def batched():
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        jobs = [eng.submit(P, F, target=t) for P, F, t in dmeshes]
+        finish = {}
+        while True:
+            r, p = eng.step()
+            now = time.perf_counter() - t0
+            for j in eng.finished():
+                finish[j] = now
+            if r == 0 and p == 0:
+                break
+        for j in jobs:
+            eng.release(j)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, [finish[j] for j in jobs]
+
+    batched()
+    dt_b, lat_b = batched()
+    _plain_runs(ctx, L, dmeshes[:16], dev, sp, torch)  # warm-up
+    lat_p = _plain_runs(ctx, L, dmeshes, dev, sp, torch)
+    dt_p = lat_p[-1]
+    eng.close()
+    side = lambda dt, lat: {"value": total_faces / 1e6 / dt, "unit": "Mfaces/s", "ms": dt * 1e3,
+                            "latency_ms": {"p50": float(np.percentile(lat, 50)) * 1e3,
+                                           "p99": float(np.percentile(lat, 99)) * 1e3}}
+    return {"workload": f"config 4: {len(mix)} meshes, {total_faces:,} faces, stage 2, device-resident inputs",
+            "batched": side(dt_b, lat_b), "plain": side(dt_p, lat_p), "batched_over_plain": dt_p / dt_b,
+            "mesh_generation_s": round(t_gen, 1)}
 
 
 def _plain_runs(ctx, L, meshes, dev, sp, torch):
@@ -764,8 +837,9 @@ def main():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4", "c5"],
                     help="c1/c2: one mesh (plain loop); c4: 256-mesh batch; c5: Poisson serving")
-    ap.add_argument("--stages", default="23", choices=["23", "2"],
-                    help="c1/c2: PaMO.run with stage 3 (default) or stage 2 alone")
+    ap.add_argument("--no-c4", action="store_true", help="c2 at one GPU: skip the config-4 batched-vs-plain keys")
+    ap.add_argument("--stages", default="123", choices=["123", "23", "2"],
+                    help="c1/c2: PaMO.run with all three stages (default), stages 2 + 3, or stage 2 alone")
     ap.add_argument("--n-meshes", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--pool", type=int, default=24, help="c5: distinct request meshes")

@@ -89,6 +89,23 @@ int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int
                     int *out_n_tris, int *out_rounds);
 
 /*
+ * Quality mode of the stage-2 rounds of this context (no reference
+ * counterpart; off by default, which is the reference's algorithm bit for
+ * bit).  On: each vertex's quadric is accumulated in FP64 from FP64 face
+ * planes; an edge collapses to the minimiser of the summed quadric (the 3x3
+ * system solved in FP64; the midpoint when it is close to singular or the
+ * minimiser lies farther than the edge's length from the midpoint), whose FP64
+ * quadric error is the cost's QEM term; the candidate pairs of the
+ * self-intersection undo include faces sharing an edge, and every pair is
+ * decided by the exact-predicate test of pamo_check_mesh (a degenerate face
+ * counts as intersecting).  Affects pamo_stage2_run(_centred),
+ * pamo_free_forward and pamo_simplify_ctx on this context.  The reference
+ * keeps fp32 quadrics and the midpoint (simp_cuda/src/cusimp_free.cu:337-366,
+ * 491) and an inexact pair test (simp_cuda/src/bvh/tri_tri_3d.cuh:131-276).
+ */
+int pamo_set_quality(pamo_ctx *ctx, int on);
+
+/*
  * pamo_stage2_run on points that are already centred -- stage 1's output,
  * which the reference's PaMO.run passes to stage 2 without centring again
  * (simp_cuda/pamo/__init__.py:130-144) -- with h_offset3 (host float[3], the

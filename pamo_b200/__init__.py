@@ -175,10 +175,13 @@ class PaMO:
     """Drop-in for the reference's ``PaMO`` (simp_cuda/pamo/__init__.py:18-205).
 
     ``input_mesh`` is any object with ``vertices``/``faces`` (e.g. a trimesh) or a
-    ``(V, F)`` pair; it is kept as the ground truth for stage 3.
+    ``(V, F)`` pair; it is kept as the ground truth for stage 3.  ``quality=True``
+    switches stage 2 to its quality mode (see pamo_set_quality); the default is
+    the reference's algorithm.
     """
 
-    def __init__(self, input_mesh, use_stage1=True, use_stage3=True, device: int = 0, verbose: bool = True):
+    def __init__(self, input_mesh, use_stage1=True, use_stage3=True, device: int = 0, verbose: bool = True,
+                 quality: bool = False):
         self.use_stage1 = use_stage1
         self.use_stage3 = use_stage3
         self.verbose = verbose
@@ -193,6 +196,11 @@ class PaMO:
         self._gt_f32 = np.array(V_in, dtype=np.float32) if getattr(V_in, "dtype", None) == np.float32 else None
         self._gt_f32_pinned = None
         self.ctx = Context(device)
+        # quality mode (no reference counterpart): FP64 quadrics, the quadric's
+        # minimiser as collapse position, exact-predicate undo (pamo_set_quality)
+        self.quality = bool(quality)
+        if self.quality:
+            check("pamo_set_quality", _lib.lib().pamo_set_quality(self.ctx.handle, 1))
         self.device = device
         self.target_faces = None
         self.last_rounds = 0

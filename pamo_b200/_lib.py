@@ -55,6 +55,7 @@ SIGNATURES = {
     "pamo_free_copy_undo": (_i, [_vp, _vp, _i, _vp]),
     "pamo_stage2_run": (_i, [_vp, _vp, _vp, _i, _i, _ll, _i, _f, _i, _vp, _ip, _ip, _ip]),
     "pamo_stage2_fetch": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "pamo_set_quality": (_i, [_vp, _i]),
     "pamo_stage2_run_centred": (_i, [_vp, _vp, _vp, _i, _i, _vp, _ll, _i, _f, _i, _vp, _ip, _ip, _ip]),
     "pamo_remesh": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _ip, _ip]),
     "pamo_remesh_fetch": (_i, [_vp, _vp, _vp, _vp, _vp]),

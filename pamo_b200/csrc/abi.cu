@@ -592,6 +592,13 @@ static int stage2_loop(pamo_ctx *ctx, const float *d_points, const int *d_tris, 
     return PAMO_OK;
 }
 
+int pamo_set_quality(pamo_ctx *ctx, int on)
+{
+    if (!ctx) return PAMO_ERR_INVALID_ARG;
+    ctx->s2.quality = on != 0;
+    return PAMO_OK;
+}
+
 int pamo_stage2_run(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_pts, int n_tris,
                     long long target_faces, int tolerance, float threshold, int iters, void *stream, int *out_n_pts,
                     int *out_n_tris, int *out_rounds)

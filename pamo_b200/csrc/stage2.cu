@@ -29,6 +29,7 @@
 #include <cstring>
 
 #include "scan.cuh"
+#include "exact.cuh"
 #include "stage2.cuh"
 #include "tritri.cuh"
 
@@ -148,6 +149,63 @@ __global__ void k_vertex_quadric(const int *__restrict__ first_near, int *near_t
     }
 }
 
+// Quality mode: each vertex's quadric in FP64, the planes recomputed from the
+// positions in FP64 (unit normal n, d = -n . a), summed over the vertex's faces
+// in its (sorted) list order, so the result is deterministic.
+__global__ void k_vertex_quadric64(const int *__restrict__ first_near, const int *__restrict__ near_tris,
+                                   const float4 *__restrict__ pts, const int4 *__restrict__ tris, double *q64, int n)
+{
+    PAMO_GRID_STRIDE(v, n)
+    {
+        double q[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int s = first_near[v]; s < first_near[v + 1]; ++s) {
+            const int4 t = tris[near_tris[s]];
+            const float4 fa = pts[t.x], fb = pts[t.y], fc = pts[t.z];
+            const double ax = fa.x, ay = fa.y, az = fa.z;
+            const double ux = fb.x - ax, uy = fb.y - ay, uz = fb.z - az;
+            const double wx = fc.x - ax, wy = fc.y - ay, wz = fc.z - az;
+            double nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
+            const double len = sqrt(nx * nx + ny * ny + nz * nz);
+            if (!(len > 0.0)) continue;  // a degenerate face has no plane
+            nx /= len;
+            ny /= len;
+            nz /= len;
+            const double d = -(nx * ax + ny * ay + nz * az);
+            q[0] += nx * nx; q[1] += nx * ny; q[2] += nx * nz; q[3] += nx * d;
+            q[4] += ny * ny; q[5] += ny * nz; q[6] += ny * d;
+            q[7] += nz * nz; q[8] += nz * d; q[9] += d * d;
+        }
+        for (int k = 0; k < 10; ++k) q64[10 * (size_t)v + k] = q[k];
+    }
+}
+
+// Quality mode: the point minimising v^T (Qu + Qv) v, from the 3 x 3 system
+// A x = -b of the summed quadric (Cramer's rule in FP64).  The midpoint is kept
+// when the system is close to singular (|det| below 1e-12 of the product of
+// A's row norms) or the minimiser lies more than the edge's length from the
+// midpoint (a nearly flat, ill-conditioned quadric).
+__device__ V3 qem_position(const double *qu, const double *qv, V3 p0, V3 p1)
+{
+    double q[10];
+    for (int k = 0; k < 10; ++k) q[k] = qu[k] + qv[k];
+    const double a00 = q[0], a01 = q[1], a02 = q[2], a11 = q[4], a12 = q[5], a22 = q[7];
+    const double b0 = -q[3], b1 = -q[6], b2 = -q[8];
+    const double c00 = a11 * a22 - a12 * a12, c01 = a02 * a12 - a01 * a22, c02 = a01 * a12 - a02 * a11;
+    const double det = a00 * c00 + a01 * c01 + a02 * c02;
+    const double r0 = sqrt(a00 * a00 + a01 * a01 + a02 * a02), r1 = sqrt(a01 * a01 + a11 * a11 + a12 * a12);
+    const double r2 = sqrt(a02 * a02 + a12 * a12 + a22 * a22);
+    const V3 mid = vmid(p0, p1);
+    if (!(fabs(det) > 1e-12 * r0 * r1 * r2)) return mid;
+    const double c11 = a00 * a22 - a02 * a02, c12 = a01 * a02 - a00 * a12, c22 = a00 * a11 - a01 * a01;
+    const double x = (c00 * b0 + c01 * b1 + c02 * b2) / det;
+    const double y = (c01 * b0 + c11 * b1 + c12 * b2) / det;
+    const double z = (c02 * b0 + c12 * b1 + c22 * b2) / det;
+    const double ex = (double)p1.x - p0.x, ey = (double)p1.y - p0.y, ez = (double)p1.z - p0.z;
+    const double dx = x - mid.x, dy = y - mid.y, dz = z - mid.z;
+    if (!(dx * dx + dy * dy + dz * dz <= ex * ex + ey * ey + ez * ez)) return mid;
+    return {(float)x, (float)y, (float)z};
+}
+
 __device__ __forceinline__ int next_after(int4 t, int v)
 {
     if (t.x == v) return t.y;
@@ -235,12 +293,19 @@ struct CostArgs {
     const SlotInfo *slots;
     const SlotCounters *scnt;
     const int *vslot;
+    // quality mode (null otherwise): FP64 quadrics in, collapse positions out
+    const double *quad64;
+    float4 *epos;
 };
 
 // Returns true when the reference writes a new cost for the edge.
 __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, bool inv_v, float tres, float edge_s,
-                                int is_stuck, uint32_t &out)
+                                int is_stuck, uint32_t &out, int e = -1)
 {
+    if (A.epos) {  // quality mode: an edge whose cost is not rewritten collapses to its midpoint
+        const V3 m0 = vmid(v3(A.pts[u]), v3(A.pts[v]));
+        A.epos[e] = make_float4(m0.x, m0.y, m0.z, 0.f);
+    }
     if (inv_u && inv_v) {
         out = 0xFFFFFFFFu;
         return true;
@@ -248,57 +313,49 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, boo
     if (is_stuck) return false;
     const int ua = A.first_near[u], ub = A.first_near[u + 1];
     const int va = A.first_near[v], vb = A.first_near[v + 1];
-    // link condition: common next-vertices of the two one-rings (the count is
-    // what matters; > 2 stops early).  v's list is held in registers when short,
-    // so each of u's entries is compared without reloading it.
-    constexpr int kRing = 12;
     int dup = 0;
-    if (vb - va <= kRing) {
-        int vn[kRing];
-#pragma unroll
-        for (int k = 0; k < kRing; ++k) vn[k] = va + k < vb ? A.nxt[va + k] : -3;  // -3 matches no entry
-        for (int a = ua; a < ub; ++a) {
-            const int iu = A.nxt[a];
-#pragma unroll
-            for (int k = 0; k < kRing; ++k) dup += (vn[k] == iu);
+    for (int a = ua; a < ub; ++a) {
+        int iu = A.nxt[a];
+        for (int b = va; b < vb; ++b) {
+            int iv = A.nxt[b];
+            if (iu == iv) dup++;
             if (dup > 2) {
                 out = 0xFFFFFFFFu;
                 return true;
             }
         }
-    } else {
-        for (int a = ua; a < ub; ++a) {
-            int iu = A.nxt[a];
-            for (int b = va; b < vb; ++b) {
-                int iv = A.nxt[b];
-                if (iu == iv) dup++;
-                if (dup > 2) {
-                    out = 0xFFFFFFFFu;
-                    return true;
-                }
-            }
-        }
     }
     if (dup != 2) return false;
 
-    // One walk over both one-rings (u's faces, then v's) feeds the two sums in
-    // the reference's order: the mean incident edge length (descending-pair
-    // edges of every face) and the skinny penalties of the faces that do not
-    // hold both endpoints, after their normal-flip test.
-    const V3 v0 = v3(A.pts[u]), v1 = v3(A.pts[v]);
-    const V3 mid = vmid(v0, v1);
-    float elen = 0.0f, Qa = 0.0f;
-    int nedge = 0, ntri = 0;
+    float elen = 0.0f;
+    int nedge = 0;
     for (int pass = 0; pass < 2; ++pass) {
-        const int w = pass ? v : u, other = pass ? u : v;
-        const int lo = pass ? va : ua, hi = pass ? vb : ub;
+        int lo = pass ? va : ua, hi = pass ? vb : ub;
         for (int a = lo; a < hi; ++a) {
             const int f = A.near_tris[a];
-            const int4 t = A.tris[f];
-            const float4 l = A.elen[f];
+            int4 t = A.tris[f];
+            float4 l = A.elen[f];
             if (t.x > t.y) { elen += l.x; nedge++; }
             if (t.y > t.z) { elen += l.y; nedge++; }
             if (t.z > t.x) { elen += l.z; nedge++; }
+        }
+    }
+    V3 v0 = v3(A.pts[u]), v1 = v3(A.pts[v]);
+    elen = elen / (float)nedge / edge_s * tres;
+    elen = elen + vnorm(vsub(v0, v1)) / edge_s * tres;
+    // the collapse position: the midpoint (the reference), or in quality mode
+    // the FP64 quadric's minimiser
+    const V3 mid = A.quad64 ? qem_position(A.quad64 + 10 * (size_t)u, A.quad64 + 10 * (size_t)v, v0, v1) : vmid(v0, v1);
+    if (A.epos) A.epos[e] = make_float4(mid.x, mid.y, mid.z, 0.f);
+
+    float Qa = 0.0f;
+    int ntri = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        int w = pass ? v : u, other = pass ? u : v;
+        int lo = pass ? va : ua, hi = pass ? vb : ub;
+        for (int a = lo; a < hi; ++a) {
+            const int f = A.near_tris[a];
+            int4 t = A.tris[f];
             if (face_has(t, other)) continue;
             V3 o0 = v3(A.pts[t.x]), o1 = v3(A.pts[t.y]), o2 = v3(A.pts[t.z]);
             V3 n0 = t.x == w ? mid : o0;
@@ -315,9 +372,18 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, boo
             ntri++;
         }
     }
-    elen = elen / (float)nedge / edge_s * tres;
-    elen = elen + vnorm(vsub(v0, v1)) / edge_s * tres;
     Qa = 5.0f * Qa;
+    if (A.quad64) {  // quality mode: the quadric error in FP64 at the chosen position
+        const double *qu = A.quad64 + 10 * (size_t)u, *qv = A.quad64 + 10 * (size_t)v;
+        double q[10];
+        for (int k = 0; k < 10; ++k) q[k] = qu[k] + qv[k];
+        const double x = mid.x, y = mid.y, z = mid.z;
+        const double qe = x * (q[0] * x + q[1] * y + q[2] * z + q[3]) + y * (q[1] * x + q[4] * y + q[5] * z + q[6]) +
+                          z * (q[2] * x + q[5] * y + q[7] * z + q[8]) + (q[3] * x + q[6] * y + q[8] * z + q[9]);
+        const float cost = (float)(qe / ((double)edge_s * (double)edge_s));
+        out = quantise_cost(cost + elen + Qa / (float)ntri * tres);
+        return true;
+    }
     float4 a0 = A.quad[3 * u], a1 = A.quad[3 * u + 1], a2 = A.quad[3 * u + 2];
     float4 b0 = A.quad[3 * v], b1 = A.quad[3 * v + 1], b2 = A.quad[3 * v + 2];
     float m00 = a0.x + b0.x, m01 = a0.y + b0.y, m02 = a0.z + b0.z, m03 = a0.w + b0.w;
@@ -368,7 +434,8 @@ __global__ void __launch_bounds__(kThreads) k_edge_cost(CostArgs A, const int *o
             int2 ed = A.edges[e];
             uint32_t c;
             if (!A.slots) {
-                if (edge_cost_value(A, ed.x, ed.y, A.invalid[ed.x], A.invalid[ed.y], A.tres, A.edge_s, A.is_stuck, c))
+                if (edge_cost_value(A, ed.x, ed.y, A.invalid[ed.x], A.invalid[ed.y], A.tres, A.edge_s, A.is_stuck, c,
+                                    e))
                     A.edge_cost[e] = c;
                 else
                     c = A.edge_cost[e];  // the reference keeps the previous round's value
@@ -418,6 +485,7 @@ struct CollapseArgs {
     const SlotInfo *slots;  // batch mode (null otherwise)
     const SlotCounters *scnt;
     const int *vslot;
+    const float4 *epos;  // quality mode: the position the edge cost chose (null: the midpoint)
 };
 
 __device__ __forceinline__ bool faces_min_ok(const CollapseArgs &A, int lo, int hi, unsigned long long key)
@@ -456,7 +524,7 @@ __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
             if (A.vmin[u] == key && A.vmin[v] == key && faces_min_ok(A, ua, ub, key) && faces_min_ok(A, va, vb, key)) {
                 win = 1;
                 V3 p0 = v3(A.opts[u]), p1 = v3(A.opts[v]);
-                V3 mid = vmid(p0, p1);
+                V3 mid = A.epos ? v3(A.epos[e]) : vmid(p0, p1);
                 A.pts[u] = make_float4(mid.x, mid.y, mid.z, 0.f);
                 A.pts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
                 A.occ[v] = 0;
@@ -657,133 +725,71 @@ __global__ void k_active_list(const int *__restrict__ vals, const int *scene, co
     }
 }
 
-// For each active live face, enumerate the overlapping leaves and append
-// candidate pairs.  A pair of two active faces is emitted once (by the lower
-// index); pairs sharing two or more vertex indices are never reported by the
-// reference and are dropped here.
-//
-// One traversal per warp: the warp's 32 queries (neighbouring
-// active faces in leaf order, so their boxes are close) walk the hierarchy
-// together.  A node is fetched once for the warp (one broadcast load instead of
-// up to 32 scattered ones), each lane tests its own box against both child
-// boxes, and a child goes on the warp's stack in shared memory when any lane
-// overlaps it.  Leaves are handled by the lanes that overlap them.  Each lane
-// emits exactly the pairs its own walk would (their order in the list depends
-// on scheduling, which nothing reads).  In a batch, a warp whose queries start in different mesh subtrees
-// walks each lane's own subtree with the per-lane stack instead.
-constexpr int kWarpStack = 96;
-constexpr int kQueryWarps = kThreads / 32;
-
-__device__ __forceinline__ void query_leaf(int leaf, int f, int4 t, const int *__restrict__ vals,
-                                           const uint8_t *__restrict__ active, const int4 *__restrict__ tris,
-                                           uint2 *pairs, long long cap_pairs, RoundCounters *cnt)
+// For each active live face, enumerate overlapping leaves and append candidate
+// pairs.  A pair of two active faces is emitted once (by the lower index);
+// pairs sharing `skip_shared` or more vertex indices are dropped: 2 for the
+// reference's test, which never reports pairs sharing an edge; 4 (none) for
+// the exact test of quality mode.
+__global__ void __launch_bounds__(kThreads) k_query(const BvhNode *__restrict__ nodes, const int *__restrict__ vals,
+                                                    const int *scene, const float4 *__restrict__ pts,
+                                                    const int4 *__restrict__ tris, const uint8_t *__restrict__ active,
+                                                    int m, uint2 *pairs, long long cap_pairs, RoundCounters *cnt,
+                                                    const int *roots, const int *vslot, const int *qlist,
+                                                    int skip_shared)
 {
-    const int g = vals[leaf];
-    if (g < 0 || g == f) return;  // empty leaves have empty boxes; guard anyway
-    if (active[g] && g < f) return;
-    const int4 tg = tris[g];
-    if (shared_indices(t, tg) >= 2) return;
-    cg::coalesced_group grp = cg::coalesced_threads();
-    int base = 0;
-    if (grp.thread_rank() == 0) base = atomicAdd(&cnt->n_pairs, (int)grp.size());
-    const int pos = grp.shfl(base, 0) + (int)grp.thread_rank();
-    if (pos < cap_pairs) pairs[pos] = make_uint2((unsigned)f, (unsigned)g);
-    else atomicAdd(&cnt->pair_overflow, 1);
-}
-
-__global__ void __launch_bounds__(kThreads) k_query_warp(const BvhNode *__restrict__ nodes,
-                                                         const int *__restrict__ vals, const int *scene,
-                                                         const float4 *__restrict__ pts,
-                                                         const int4 *__restrict__ tris,
-                                                         const uint8_t *__restrict__ active, int m, uint2 *pairs,
-                                                         long long cap_pairs, RoundCounters *cnt, const int *roots,
-                                                         const int *vslot, const int *qlist)
-{
-    __shared__ int stk[kQueryWarps][kWarpStack];
     const int L = scene[7];
+    int stack[kStack];
+    // queries from the list of active faces (k_active_list), or every leaf in
+    // leaf order with the inactive ones skipped
     const int N = qlist ? cnt->n_query : L;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const long long warps = (long long)gridDim.x * kQueryWarps;
-    if (L < 2) return;
-    for (long long base = ((long long)blockIdx.x * kQueryWarps + w) * 32; base < N; base += warps * 32) {
-        const long long pp = base + lane;
-        int f = -1;
-        int4 t = make_int4(-1, -1, -1, 0);
-        if (pp < N) {
-            f = qlist ? qlist[pp] : vals[pp];
-            if (f >= 0 && active[f]) t = tris[f];
-            else f = -1;
-            if (t.x == -1) f = -1;
-        }
-        const bool valid = f >= 0;
-        const unsigned vball = __ballot_sync(0xffffffffu, valid);
-        if (!vball) continue;
-        float3 qlo = make_float3(INFINITY, INFINITY, INFINITY), qhi = make_float3(-INFINITY, -INFINITY, -INFINITY);
-        int start = 0;
-        if (valid) {
-            const float4 a = pts[t.x], b = pts[t.y], c = pts[t.z];
-            qlo = make_float3(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)));
-            qhi = make_float3(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)));
-            if (roots) start = roots[vslot[t.x]];
-        }
-        // a batch: the warp walks together only if all its queries start at one subtree
-        const int first = __shfl_sync(0xffffffffu, start, __ffs(vball) - 1);
-        const bool uniform = __all_sync(0xffffffffu, !valid || start == first);
-        if (!uniform) {
-            if (!valid || start < 0) continue;
-            int stack[kStack];
-            int sp = 0;
-            stack[sp++] = start;
-            int budget = 2 * L + 16;
-            while (sp > 0) {
-                if (--budget < 0) {
-                    atomicAdd(&cnt->stack_overflow, 1);
-                    break;
-                }
-                const BvhNode nd = nodes[stack[--sp]];
-#pragma unroll
-                for (int side = 0; side < 2; ++side) {
-                    const float4 lo = side ? nd.rlo : nd.llo, hi = side ? nd.rhi : nd.lhi;
-                    if (!box_overlap(lo, hi, qlo, qhi)) continue;
-                    const int child = __float_as_int(lo.w);
-                    if (child < 0) query_leaf(~child, f, t, vals, active, tris, pairs, cap_pairs, cnt);
-                    else if (sp < kStack) stack[sp++] = child;
-                    else atomicAdd(&cnt->stack_overflow, 1);
-                }
-            }
-            continue;
-        }
-        if (first < 0) continue;  // a one-face mesh: its subtree is a single leaf
+    PAMO_GRID_STRIDE(pp, N)
+    {
+        const int f = qlist ? qlist[pp] : vals[pp];
+        if (f < 0 || !active[f] || L < 2) continue;
+        int4 t = tris[f];
+        if (t.x == -1) continue;
+        float4 a = pts[t.x], b = pts[t.y], c = pts[t.z];
+        float3 qlo = make_float3(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)));
+        float3 qhi = make_float3(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)));
+        // a batch starts at the face's own mesh subtree (a leaf: a one-face mesh)
+        const int start = roots ? roots[vslot[t.x]] : 0;
+        if (start < 0) continue;
         int sp = 0;
-        if (lane == 0) stk[w][0] = first;
-        sp = 1;
-        __syncwarp();
+        stack[sp++] = start;
+        // a tree visits each of its L-1 inner nodes at most once per query; the
+        // bound only guards against a corrupted hierarchy
         int budget = 2 * L + 16;
         while (sp > 0) {
             if (--budget < 0) {
-                if (lane == 0) atomicAdd(&cnt->stack_overflow, 1);
+                atomicAdd(&cnt->stack_overflow, 1);
                 break;
             }
-            const int node = stk[w][--sp];
-            __syncwarp();
-            const BvhNode nd = nodes[node];
-            // the right child goes on the stack first, so the left is walked first
+            const BvhNode nd = nodes[stack[--sp]];
 #pragma unroll
-            for (int side = 1; side >= 0; --side) {
-                const float4 lo = side ? nd.rlo : nd.llo, hi = side ? nd.rhi : nd.lhi;
-                const bool ov = valid && box_overlap(lo, hi, qlo, qhi);
-                if (!__any_sync(0xffffffffu, ov)) continue;
-                const int child = __float_as_int(lo.w);
+            for (int side = 0; side < 2; ++side) {
+                float4 lo = side ? nd.rlo : nd.llo;
+                float4 hi = side ? nd.rhi : nd.lhi;
+                if (!box_overlap(lo, hi, qlo, qhi)) continue;
+                int child = __float_as_int(lo.w);
                 if (child < 0) {
-                    if (ov) query_leaf(~child, f, t, vals, active, tris, pairs, cap_pairs, cnt);
-                } else if (sp < kWarpStack) {
-                    if (lane == 0) stk[w][sp] = child;
-                    ++sp;
-                } else if (lane == 0) {
+                    int g = vals[~child];
+                    if (g < 0 || g == f) continue;  // empty leaves have empty boxes; guard anyway
+                    if (active[g] && g < f) continue;
+                    int4 tg = tris[g];
+                    if (shared_indices(t, tg) >= skip_shared) continue;
+                    // one atomic per group of lanes appending together
+                    cg::coalesced_group grp = cg::coalesced_threads();
+                    int base = 0;
+                    if (grp.thread_rank() == 0) base = atomicAdd(&cnt->n_pairs, (int)grp.size());
+                    int pos = grp.shfl(base, 0) + (int)grp.thread_rank();
+                    if (pos < cap_pairs) pairs[pos] = make_uint2((unsigned)f, (unsigned)g);
+                    else atomicAdd(&cnt->pair_overflow, 1);
+                } else if (sp < kStack) {
+                    stack[sp++] = child;
+                } else {
                     atomicAdd(&cnt->stack_overflow, 1);
                 }
             }
-            __syncwarp();
         }
     }
 }
@@ -800,12 +806,33 @@ __device__ __forceinline__ void load_face(const float4 *pts, int4 t, float out[3
 
 __global__ void __launch_bounds__(kThreads) k_pairs(const uint2 *pairs, const RoundCounters *cnt,
                                                     long long cap_pairs, const float4 *__restrict__ pts,
-                                                    const int4 *__restrict__ tris, uint8_t *isect, float eps)
+                                                    const int4 *__restrict__ tris, uint8_t *isect, float eps,
+                                                    int exact_pred)
 {
     long long N = cnt->n_pairs < cap_pairs ? cnt->n_pairs : cap_pairs;
     PAMO_GRID_STRIDE(k, N)
     {
         uint2 pr = pairs[k];
+        if (exact_pred) {
+            // quality mode: the acceptance checker's exact predicate (exact.cuh);
+            // a degenerate face counts as intersecting
+            exact::P3 P[3], Q[3];
+            const int4 ta = tris[pr.x], tb = tris[pr.y];
+            const int ia[3] = {ta.x, ta.y, ta.z}, ib[3] = {tb.x, tb.y, tb.z};
+            for (int c = 0; c < 3; ++c) {
+                const float4 a = pts[ia[c]], b = pts[ib[c]];
+                P[c] = {a.x, a.y, a.z};
+                Q[c] = {b.x, b.y, b.z};
+            }
+            const bool da = exact::tri_degenerate(P, ia), db = exact::tri_degenerate(Q, ib);
+            if (da) isect[pr.x] = 1;
+            if (db) isect[pr.y] = 1;
+            if (!da && !db && exact::faces_intersect(P, ia, Q, ib)) {
+                isect[pr.x] = 1;
+                isect[pr.y] = 1;
+            }
+            continue;
+        }
         float A[3][3], B[3][3];
         int ia[3], ib[3];
         load_face(pts, tris[pr.x], A, ia);
@@ -1230,9 +1257,12 @@ void Stage2::release()
 {
     void *p[] = {edge_cost, pts_map, undo_list, tmp_undo, invalid_table, opts, pts, otris, tris, occ,
                  first_near, cursor, near_tris, first_edge, edges, plane, elen4, nxt, quad, vmin, eflag, collapsed,
-                 active, isect, uflag, undo_edges, fflag, pairs, scan_scratch, dev_misc, dcnt};
+                 active, isect, uflag, undo_edges, fflag, pairs, scan_scratch, dev_misc, dcnt, quad64, epos};
     for (void *q : p)
         if (q) cudaFree(q);
+    quad64 = nullptr;
+    epos = nullptr;
+    cap_q64 = cap_epos = 0;
     if (hcnt) cudaFreeHost(hcnt);
     if (h_scalars) cudaFreeHost(h_scalars);
     prof.release();
@@ -1373,12 +1403,13 @@ static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s, const int *dirty
     launch(k_active_list, grid_for(m), kThreads, 0, s, (const int *)S.bvh.vals, (const int *)S.bvh.scene,
            (const uint8_t *)S.active, (const int4 *)S.tris, S.fflag, S.dcnt,
            batch ? (const SlotInfo *)S.slots : nullptr, batch ? (const int *)S.vslot : nullptr);
-    launch(k_query_warp, grid_for(m), kThreads, 0, s, (const BvhNode *)S.bvh.nodes, (const int *)S.bvh.vals,
+    launch(k_query, grid_for(m), kThreads, 0, s, (const BvhNode *)S.bvh.nodes, (const int *)S.bvh.vals,
            (const int *)S.bvh.scene, (const float4 *)S.pts, (const int4 *)S.tris, (const uint8_t *)S.active, m,
            S.pairs, S.cap_pairs, S.dcnt, batch ? (const int *)S.roots : nullptr,
-           batch ? (const int *)S.vslot : nullptr, (const int *)S.fflag);
+           batch ? (const int *)S.vslot : nullptr, (const int *)S.fflag, S.quality ? 4 : 2);
     S.prof.begin(PH_PAIRS, s);
-    launch(k_pairs, grid_for(S.cap_pairs), kThreads, 0, s, S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris, S.isect, 1e-3f);
+    launch(k_pairs, grid_for(S.cap_pairs), kThreads, 0, s, S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris, S.isect, 1e-3f,
+           S.quality ? 1 : 0);
     S.prof.end(s);
     return cudaGetLastError();
 }
@@ -1432,6 +1463,12 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     const int *d_n_edges = &dcnt->n_edges;
     launch(k_face_b, grid_for(m), kThreads, 0, s, tris, m, first_near, cursor, near_tris, first_edge, edges);
     launch(k_vertex_quadric, grid_for(n), kThreads, 0, s, first_near, near_tris, plane, tris, quad, nxt, n);
+    if (quality) {
+        int rc = ensure_quality(n, 3LL * m);
+        if (rc) return rc;
+        launch(k_vertex_quadric64, grid_for(n), kThreads, 0, s, (const int *)first_near, (const int *)near_tris,
+               (const float4 *)pts, (const int4 *)tris, quad64, n);
+    }
     // The hierarchy only needs the round input's faces as leaves: build it, or
     // keep the previous round's (leaves renumbered by compact(), removed faces
     // as empty leaves) while at least kRebuildFraction of its leaves are faces.
@@ -1448,10 +1485,11 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     const long long EMAX = 3LL * m;
     prof.begin(PH_EDGE_COST, s);
     CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, nxt, plane, elen4, quad, invalid_table,
-                edge_cost, vmin, tres, edge_s, is_stuck ? 1 : 0, nullptr, nullptr, nullptr};
+                edge_cost, vmin, tres, edge_s, is_stuck ? 1 : 0, nullptr, nullptr, nullptr,
+                quality ? (const double *)quad64 : nullptr, quality ? epos : nullptr};
     launch(k_edge_cost, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
     CollapseArgs cl{edges, d_n_edges, edge_cost, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
-                    collapse_t, nullptr, nullptr, nullptr};
+                    collapse_t, nullptr, nullptr, nullptr, quality ? (const float4 *)epos : nullptr};
     prof.begin(PH_COLLAPSE, s);
     launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s, &dcnt->scan_fault));
@@ -1536,10 +1574,31 @@ cudaError_t query_and_test_pairs(const BvhNode *nodes, const int *vals, const in
                                  const int4 *tris, const uint8_t *active, int m, uint2 *pairs, long long cap_pairs,
                                  RoundCounters *cnt, uint8_t *isect, cudaStream_t s)
 {
-    launch(k_query_warp, grid_for(m), kThreads, 0, s, nodes, vals, scene, pts, tris, active, m, pairs, cap_pairs, cnt,
-           (const int *)nullptr, (const int *)nullptr, (const int *)nullptr);
-    launch(k_pairs, grid_for(cap_pairs), kThreads, 0, s, pairs, cnt, cap_pairs, pts, tris, isect, 1e-3f);
+    launch(k_query, grid_for(m), kThreads, 0, s, nodes, vals, scene, pts, tris, active, m, pairs, cap_pairs, cnt,
+           (const int *)nullptr, (const int *)nullptr, (const int *)nullptr, 2);
+    launch(k_pairs, grid_for(cap_pairs), kThreads, 0, s, pairs, cnt, cap_pairs, pts, tris, isect, 1e-3f, 0);
     return cudaGetLastError();
+}
+
+int Stage2::ensure_quality(long long n_pts, long long n_edges)
+{
+    if (n_pts > cap_q64 || !quad64) {
+        if (quad64) cudaFree(quad64);
+        quad64 = nullptr;
+        cap_q64 = 0;
+        const long long c = n_pts > cap_pts ? n_pts : cap_pts;
+        if (cudaMalloc((void **)&quad64, (size_t)(c + 1) * 10 * sizeof(double)) != cudaSuccess) return PAMO_ERR_OOM;
+        cap_q64 = c;
+    }
+    if (n_edges > cap_epos || !epos) {
+        if (epos) cudaFree(epos);
+        epos = nullptr;
+        cap_epos = 0;
+        const long long c = n_edges > cap_edges ? n_edges : cap_edges;
+        if (cudaMalloc((void **)&epos, (size_t)(c + 1) * sizeof(float4)) != cudaSuccess) return PAMO_ERR_OOM;
+        cap_epos = c;
+    }
+    return PAMO_OK;
 }
 
 int Stage2::self_intersect_all(int n, int m, cudaStream_t s)
@@ -1689,10 +1748,10 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
     const long long EMAX = 3LL * m;
     prof.begin(PH_EDGE_COST, s);
     CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, nxt, plane, elen4, quad, nullptr,
-                nullptr, vmin, 0.f, 1.f, 0, slots, scnt, vslot};
+                nullptr, vmin, 0.f, 1.f, 0, slots, scnt, vslot, nullptr, nullptr};
     launch(k_edge_cost, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
     CollapseArgs cl{edges, d_n_edges, nullptr, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
-                    0u, slots, scnt, vslot};
+                    0u, slots, scnt, vslot, nullptr};
     prof.begin(PH_COLLAPSE, s);
     launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s, &dcnt->scan_fault));

@@ -172,6 +172,15 @@ struct Stage2 {
     int *cand = nullptr;             // device [cap_edges + 1]: per-mesh undo-candidate windows
     int *gmap = nullptr;             // device [cap_pts + 1]: packed vertex map
 
+    // Quality mode (no reference counterpart; off by default): FP64 quadrics,
+    // the collapse position from the quadric's minimiser instead of the
+    // midpoint, and the self-intersection undo decided with exact predicates.
+    bool quality = false;
+    double *quad64 = nullptr;  // [10 per vertex] FP64 quadrics
+    float4 *epos = nullptr;    // [per edge] the collapse position chosen by the edge cost
+    long long cap_q64 = 0, cap_epos = 0;
+    int ensure_quality(long long n_pts, long long n_edges);
+
     // input staging for the per-round ABI ([n,3] layouts)
     // results of the device loop
     int res_n_pts = 0, res_n_tris = 0, res_rounds = 0;
