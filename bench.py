@@ -462,9 +462,9 @@ def product_arm(args):
     intersections = accept["intersecting_pairs_exact"]
     phases = {}
     for h in handles:
-        ph_ms = (ctypes.c_double * 16)()
-        ph_calls = (ctypes.c_longlong * 16)()
-        nph = L.pamo_profile_read(h, ph_ms, ph_calls, 16)
+        ph_ms = (ctypes.c_double * 32)()
+        ph_calls = (ctypes.c_longlong * 32)()
+        nph = L.pamo_profile_read(h, ph_ms, ph_calls, 32)
         L.pamo_profile_enable(h, 0)
         for i in range(min(nph, len(_lib.PHASES))):
             if ph_calls[i]:

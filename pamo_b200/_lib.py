@@ -109,7 +109,8 @@ def check(fn: str, code: int):
 
 
 PHASES = ["setup", "lbvh_build", "edge_cost", "collapse", "cleanup", "refit", "query", "pair_tests", "undo",
-          "compact", "s3_closest", "s3_detect", "s3_diff", "s3_cg", "s3_ccd", "s3_line"]
+          "compact", "s3_closest", "s3_detect", "s3_diff", "s3_cg", "s3_ccd", "s3_line", "s1_prep", "s1_dist",
+          "s1_flood", "s1_dmc"]
 
 
 class Context:

@@ -453,7 +453,8 @@ int pamo_ctx_create(int device, pamo_ctx **out)
     if (!c) return PAMO_ERR_OOM;
     c->device = device;
     c->s2.device = device;
-    c->s3.prof = &c->s2.prof;  // one phase timer for both stages
+    c->s3.prof = &c->s2.prof;  // one phase timer for all stages
+    c->s1.prof = &c->s2.prof;
     int rc = set_device(c);
     if (rc) {
         delete c;
@@ -633,6 +634,7 @@ int pamo_remesh(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_p
     CU_RET(cudaMemcpyAsync(S.offset, S.mean_dev, 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
     RET_IF(pamo::s1::remesh(S, d_points, d_tris, n_pts, n_tris, S.mean_dev, resolution, s));
     CU_RET(cudaStreamSynchronize(s));
+    if (S.prof) S.prof->collect();
     *out_n_verts = S.n_verts;
     *out_n_tris = S.n_tris;
     return PAMO_OK;

@@ -639,12 +639,14 @@ int remesh(Stage1 &S, const float *d_points, const int *d_tris, int n_pts, int m
     const double band = 3.0 / R, margin = band * 2 + 1;
     const long long n3 = (long long)R * R * R, c3 = (long long)(R - 1) * (R - 1) * (R - 1);
     // 1. normalise
+    if (S.prof) S.prof->begin(PH_S1_PREP, s);
     launch(k_s1_dev_init, 1, 32, 0, s, S.dev);
     launch(k_s1_min, grid_for(m), kThreads, 0, s, d_points, d_tris, m, mean_dev, S.dev);
     launch(k_s1_max, grid_for(m), kThreads, 0, s, d_points, d_tris, m, mean_dev, S.dev);
     launch(k_s1_normalise, grid_for(m), kThreads, 0, s, d_points, d_tris, m, mean_dev, (const int *)S.dev,
            (float)band, (float)margin, S.tris);
     // 2. unsigned distance: squared distances start at band^2 (bits of a double)
+    if (S.prof) S.prof->begin(PH_S1_DIST, s);
     {
         const double b2 = band * band;
         unsigned long long bits;
@@ -655,6 +657,7 @@ int remesh(Stage1 &S, const float *d_points, const int *d_tris, int n_pts, int m
     launch(k_s1_udist, grid_for(32LL * m), 256, 0, s, (const float *)S.tris, m, R, band, S.field);
     launch(k_s1_state, grid_for(n3), kThreads, 0, s, S.field, n3, R, band, S.state);
     // 3. flood fill from the boundary, until nothing changes
+    if (S.prof) S.prof->begin(PH_S1_FLOOD, s);
     const int tpr = (R + kTile - 1) / kTile;
     const int tiles = tpr * tpr * tpr;
     bool settled = false;
@@ -663,11 +666,13 @@ int remesh(Stage1 &S, const float *d_points, const int *d_tris, int n_pts, int m
         for (int k = 0; k < 8; ++k) launch(k_s1_flood, tiles, kTile * kTile * kTile, 0, s, S.state, R, S.dev);
         S1_TRY(cudaMemcpyAsync(S.h_dev, S.dev, 64, cudaMemcpyDeviceToHost, s));
         S1_TRY(cudaStreamSynchronize(s));
+        if (S.prof) S.prof->collect();
         settled = S.h_dev[4] == 0;
     }
     if (!settled) return PAMO_ERR_DEVICE;  // cannot happen within 4 R sweeps of tiles
     launch(k_s1_field, grid_for(n3), kThreads, 0, s, S.field, (const uint8_t *)S.state, n3, R);
     // 4. dual marching cubes: patch vertices
+    if (S.prof) S.prof->begin(PH_S1_DMC, s);
     launch(k_s1_cells, grid_for(c3), kThreads, 0, s, (const unsigned long long *)S.field, R, S.cell_cnt);
     S1_TRY(cudaMemsetAsync(S.cell_cnt + c3, 0, 4, s));
     S1_TRY(exclusive_scan(S.cell_cnt, S.cell_cnt, c3 + 1, nullptr, S.scan_cells, nullptr, s, S.dev + 6));
@@ -703,6 +708,7 @@ int remesh(Stage1 &S, const float *d_points, const int *d_tris, int n_pts, int m
     const int n1 = S.h_dev[10];
     launch(k_s1_faces, grid_for(nq), kThreads, 0, s, (const int4 *)S.quads, (const int *)S.q_first, (const int *)qpos,
            (int)nq, n1, S.faces);
+    if (S.prof) S.prof->end(s);
     S1_TRY(cudaGetLastError());
     S.n_verts = (int)nv;
     S.n_tris = (int)(2 * nq);

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "stage2.cuh"  // Profiler
 
 namespace pamo {
 namespace s1 {
@@ -28,6 +29,7 @@ struct Stage1 {
     float *mean_dev = nullptr;          // [4] the centring mean (tris_mean)
     int n_verts = 0, n_tris = 0;
     float offset[3] = {0, 0, 0};        // tris_mean of the input (added back after stage 2)
+    Profiler *prof = nullptr;           // the context's phase timer (optional)
 
     int ensure(long long m, int R_);
     int ensure_out(long long nv, long long nq);

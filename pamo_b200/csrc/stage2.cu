@@ -298,11 +298,14 @@ struct CostArgs {
     float4 *epos;
 };
 
-// Returns true when the reference writes a new cost for the edge.
+// Returns true when the reference writes a new cost for the edge.  QUALITY:
+// quality mode (FP64 quadric terms and the chosen collapse position in epos);
+// compiled separately so the reference's path carries none of it.
+template <bool QUALITY>
 __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, bool inv_v, float tres, float edge_s,
                                 int is_stuck, uint32_t &out, int e = -1)
 {
-    if (A.epos) {  // quality mode: an edge whose cost is not rewritten collapses to its midpoint
+    if constexpr (QUALITY) {  // an edge whose cost is not rewritten collapses to its midpoint
         const V3 m0 = vmid(v3(A.pts[u]), v3(A.pts[v]));
         A.epos[e] = make_float4(m0.x, m0.y, m0.z, 0.f);
     }
@@ -345,8 +348,13 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, boo
     elen = elen + vnorm(vsub(v0, v1)) / edge_s * tres;
     // the collapse position: the midpoint (the reference), or in quality mode
     // the FP64 quadric's minimiser
-    const V3 mid = A.quad64 ? qem_position(A.quad64 + 10 * (size_t)u, A.quad64 + 10 * (size_t)v, v0, v1) : vmid(v0, v1);
-    if (A.epos) A.epos[e] = make_float4(mid.x, mid.y, mid.z, 0.f);
+    V3 mid;
+    if constexpr (QUALITY) {
+        mid = qem_position(A.quad64 + 10 * (size_t)u, A.quad64 + 10 * (size_t)v, v0, v1);
+        A.epos[e] = make_float4(mid.x, mid.y, mid.z, 0.f);
+    } else {
+        mid = vmid(v0, v1);
+    }
 
     float Qa = 0.0f;
     int ntri = 0;
@@ -373,7 +381,7 @@ __device__ bool edge_cost_value(const CostArgs &A, int u, int v, bool inv_u, boo
         }
     }
     Qa = 5.0f * Qa;
-    if (A.quad64) {  // quality mode: the quadric error in FP64 at the chosen position
+    if constexpr (QUALITY) {  // the quadric error in FP64 at the chosen position
         const double *qu = A.quad64 + 10 * (size_t)u, *qv = A.quad64 + 10 * (size_t)v;
         double q[10];
         for (int k = 0; k < 10; ++k) q[k] = qu[k] + qv[k];
@@ -422,6 +430,7 @@ __device__ __forceinline__ int chunk_edges(const int *order, const int *first_ed
     return total;
 }
 
+template <bool QUALITY>
 __global__ void __launch_bounds__(kThreads) k_edge_cost(CostArgs A, const int *order, const int *scene,
                                                         const int *first_edge)
 {
@@ -434,8 +443,8 @@ __global__ void __launch_bounds__(kThreads) k_edge_cost(CostArgs A, const int *o
             int2 ed = A.edges[e];
             uint32_t c;
             if (!A.slots) {
-                if (edge_cost_value(A, ed.x, ed.y, A.invalid[ed.x], A.invalid[ed.y], A.tres, A.edge_s, A.is_stuck, c,
-                                    e))
+                if (edge_cost_value<QUALITY>(A, ed.x, ed.y, A.invalid[ed.x], A.invalid[ed.y], A.tres, A.edge_s,
+                                             A.is_stuck, c, e))
                     A.edge_cost[e] = c;
                 else
                     c = A.edge_cost[e];  // the reference keeps the previous round's value
@@ -443,8 +452,8 @@ __global__ void __launch_bounds__(kThreads) k_edge_cost(CostArgs A, const int *o
                 const int r = A.vslot[ed.x];
                 const SlotInfo &S = A.slots[r];
                 const int el = e - A.scnt[r].edge_off;
-                if (edge_cost_value(A, ed.x, ed.y, S.invalid[ed.x - S.vert_off], S.invalid[ed.y - S.vert_off], S.tres,
-                                    *S.scale, S.is_stuck, c))
+                if (edge_cost_value<QUALITY>(A, ed.x, ed.y, S.invalid[ed.x - S.vert_off], S.invalid[ed.y - S.vert_off],
+                                             S.tres, *S.scale, S.is_stuck, c))
                     S.edge_cost[el] = c;
                 else
                     c = S.edge_cost[el];
@@ -499,6 +508,7 @@ __device__ __forceinline__ bool faces_min_ok(const CollapseArgs &A, int lo, int 
 
 // One thread per edge: most edges fail the threshold or the key test at once,
 // and a winner's collapse is long, so no block-wide step waits on it.
+template <bool QUALITY>
 __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
 {
     const int E = *A.n_edges;
@@ -524,7 +534,9 @@ __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
             if (A.vmin[u] == key && A.vmin[v] == key && faces_min_ok(A, ua, ub, key) && faces_min_ok(A, va, vb, key)) {
                 win = 1;
                 V3 p0 = v3(A.opts[u]), p1 = v3(A.opts[v]);
-                V3 mid = A.epos ? v3(A.epos[e]) : vmid(p0, p1);
+                V3 mid;
+                if constexpr (QUALITY) mid = v3(A.epos[e]);  // the position the edge cost chose
+                else mid = vmid(p0, p1);
                 A.pts[u] = make_float4(mid.x, mid.y, mid.z, 0.f);
                 A.pts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
                 A.occ[v] = 0;
@@ -804,16 +816,16 @@ __device__ __forceinline__ void load_face(const float4 *pts, int4 t, float out[3
     }
 }
 
+template <bool EXACT>
 __global__ void __launch_bounds__(kThreads) k_pairs(const uint2 *pairs, const RoundCounters *cnt,
                                                     long long cap_pairs, const float4 *__restrict__ pts,
-                                                    const int4 *__restrict__ tris, uint8_t *isect, float eps,
-                                                    int exact_pred)
+                                                    const int4 *__restrict__ tris, uint8_t *isect, float eps)
 {
     long long N = cnt->n_pairs < cap_pairs ? cnt->n_pairs : cap_pairs;
     PAMO_GRID_STRIDE(k, N)
     {
         uint2 pr = pairs[k];
-        if (exact_pred) {
+        if constexpr (EXACT) {
             // quality mode: the acceptance checker's exact predicate (exact.cuh);
             // a degenerate face counts as intersecting
             exact::P3 P[3], Q[3];
@@ -1408,8 +1420,12 @@ static cudaError_t isect_pass(Stage2 &S, int m, cudaStream_t s, const int *dirty
            S.pairs, S.cap_pairs, S.dcnt, batch ? (const int *)S.roots : nullptr,
            batch ? (const int *)S.vslot : nullptr, (const int *)S.fflag, S.quality ? 4 : 2);
     S.prof.begin(PH_PAIRS, s);
-    launch(k_pairs, grid_for(S.cap_pairs), kThreads, 0, s, S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris, S.isect, 1e-3f,
-           S.quality ? 1 : 0);
+    if (S.quality)
+        launch(k_pairs<true>, grid_for(S.cap_pairs), kThreads, 0, s, S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris,
+               S.isect, 1e-3f);
+    else
+        launch(k_pairs<false>, grid_for(S.cap_pairs), kThreads, 0, s, S.pairs, S.dcnt, S.cap_pairs, S.pts, S.tris,
+               S.isect, 1e-3f);
     S.prof.end(s);
     return cudaGetLastError();
 }
@@ -1487,11 +1503,15 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, nxt, plane, elen4, quad, invalid_table,
                 edge_cost, vmin, tres, edge_s, is_stuck ? 1 : 0, nullptr, nullptr, nullptr,
                 quality ? (const double *)quad64 : nullptr, quality ? epos : nullptr};
-    launch(k_edge_cost, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
+    if (quality)
+        launch(k_edge_cost<true>, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
+    else
+        launch(k_edge_cost<false>, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
     CollapseArgs cl{edges, d_n_edges, edge_cost, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
                     collapse_t, nullptr, nullptr, nullptr, quality ? (const float4 *)epos : nullptr};
     prof.begin(PH_COLLAPSE, s);
-    launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
+    if (quality) launch(k_collapse<true>, grid_for(EMAX), kThreads, 0, s, cl);
+    else launch(k_collapse<false>, grid_for(EMAX), kThreads, 0, s, cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s, &dcnt->scan_fault));
     launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
     prof.begin(PH_CLEANUP, s);
@@ -1576,7 +1596,7 @@ cudaError_t query_and_test_pairs(const BvhNode *nodes, const int *vals, const in
 {
     launch(k_query, grid_for(m), kThreads, 0, s, nodes, vals, scene, pts, tris, active, m, pairs, cap_pairs, cnt,
            (const int *)nullptr, (const int *)nullptr, (const int *)nullptr, 2);
-    launch(k_pairs, grid_for(cap_pairs), kThreads, 0, s, pairs, cnt, cap_pairs, pts, tris, isect, 1e-3f, 0);
+    launch(k_pairs<false>, grid_for(cap_pairs), kThreads, 0, s, pairs, cnt, cap_pairs, pts, tris, isect, 1e-3f);
     return cudaGetLastError();
 }
 
@@ -1749,11 +1769,11 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
     prof.begin(PH_EDGE_COST, s);
     CostArgs ca{edges, d_n_edges, pts, tris, first_near, near_tris, nxt, plane, elen4, quad, nullptr,
                 nullptr, vmin, 0.f, 1.f, 0, slots, scnt, vslot, nullptr, nullptr};
-    launch(k_edge_cost, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
+    launch(k_edge_cost<false>, grid_for(m, kChunkFaces), kThreads, 0, s, ca, bvh.vals, bvh.scene, first_edge);
     CollapseArgs cl{edges, d_n_edges, nullptr, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
                     0u, slots, scnt, vslot, nullptr};
     prof.begin(PH_COLLAPSE, s);
-    launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
+    launch(k_collapse<false>, grid_for(EMAX), kThreads, 0, s, cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s, &dcnt->scan_fault));
     launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
     launch(k_b_main, grid_for(K), kThreads, 0, s, (const int *)uflag, (const RoundCounters *)dcnt, scnt, K);

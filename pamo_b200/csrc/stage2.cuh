@@ -93,6 +93,10 @@ enum Phase {
     PH_S3_CG,       // stage 3: Jacobi-PCG iterations
     PH_S3_CCD,      // stage 3: clamp + additive CCD
     PH_S3_LINE,     // stage 3: line-search energies
+    PH_S1_PREP,     // stage 1: centring mean, normalisation
+    PH_S1_DIST,     // stage 1: narrow-band unsigned distances
+    PH_S1_FLOOD,    // stage 1: flood fill of the outside, signed field
+    PH_S1_DMC,      // stage 1: dual marching cubes, quad split
     PH_COUNT
 };
 

@@ -18,12 +18,18 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 # FP32 solve vs FP64 solve of the same steps, set from the errors measured on a
-# B200: the largest vertex deviation as a fraction of the ground truth's
-# bounding-box diagonal (config 1: 4.4e-8; thin shells with ~30,000 blocks in
-# contact: 4.9e-5, of a 5.5e-4 move), the Newton energies (relative: 2.4e-7 and
-# 9.2e-4) and the CCD steps (0 and 8.0e-3)
-TOL = {"c1": {"diag": 1e-6, "energy": 1e-6, "ccd": 1e-4},
-       "contact": {"diag": 1e-4, "energy": 2e-3, "ccd": 2e-2}}
+# B200 over two runs (the assembled sums vary with scheduling): the largest
+# vertex deviation as a fraction of the ground truth's bounding-box diagonal,
+# the Newton energies (relative) and the CCD steps --
+#   config 1 (no contact):                 4.4e-8, 2.4e-7, 0
+#   thin shells, 7,840 faces, ~30,000 blocks within d_hat:
+#                                           4.9e-5 .. 5.6e-5 (of a 5.5e-4 move),
+#                                           9.2e-4 .. 1.5e-3, 8.0e-3 .. 1.2e-2
+#   config 3's shells, 500k faces, ~876,000 blocks: 5.6e-7, 3.1e-6, 0
+# For scale: the same steps in plain FP32 (the oracle run in float32) deviate
+# from FP64 by 3.0e-5, 3.2e-2 and 0.11 on the 7,840-face shells.
+TOL = {"c1": {"diag": 1e-6, "energy": 1e-6, "ccd": 1e-4, "moved": 10},
+       "contact": {"diag": 1.5e-4, "energy": 5e-3, "ccd": 5e-2, "moved": 3}}
 # a line-search trial taken differently is a tie: the energy it changes is
 # within float32 evaluation noise of the start's
 TIE = 1e-6
@@ -83,7 +89,7 @@ def _compare_case(torch_cuda, name, tol):
           f"{int(tr_w[:, 4].max())}, within d_hat {int(tr_g[:, 5].max())} vs {int(tr_w[:, 5].max())}; "
           f"{sysm.last_stats}")
     assert len(tr_g) == len(tr_w)
-    assert moved > 10 * err  # the projection does move the mesh
+    assert moved > tol["moved"] * err  # the projection does move the mesh
     assert err < tol["diag"]
     assert e_rel < tol["energy"]
     assert np.abs(tr_g[:, 2] - tr_w[:, 2]).max() < tol["ccd"]  # CCD step
