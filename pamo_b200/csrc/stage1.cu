@@ -230,13 +230,19 @@ __device__ double point_tri_d2(D3 p, D3 a, D3 b, D3 c)
     return ddot(d, d);
 }
 
-// one warp per triangle over the samples of its box grown by `band`
+// One warp per triangle over the samples of its box grown by `band`.  Before
+// the full closest-point computation a sample is skipped when a lower bound of
+// its distance to the triangle -- the distance to the triangle's bounding box,
+// and to its plane -- already reaches the sample's current value (the bounds
+// hold in exact arithmetic; the 1e-9 relative margin covers their rounding), so
+// the minimum, and therefore the field, is the same as without the test.
 __global__ void __launch_bounds__(256) k_s1_udist(const float *tris, int m, int R, double band,
                                                   unsigned long long *field)
 {
     const int lane = threadIdx.x & 31;
     const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const double band2 = band * band;
     for (long long t = warp0; t < m; t += nw) {
         const float *T = tris + 9 * t;
         const D3 a = {T[0], T[1], T[2]}, b = {T[3], T[4], T[5]}, c = {T[6], T[7], T[8]};
@@ -244,22 +250,36 @@ __global__ void __launch_bounds__(256) k_s1_udist(const float *tris, int m, int 
         const double mn[3] = {fmin(a.x, fmin(b.x, c.x)), fmin(a.y, fmin(b.y, c.y)), fmin(a.z, fmin(b.z, c.z))};
         const double mx[3] = {fmax(a.x, fmax(b.x, c.x)), fmax(a.y, fmax(b.y, c.y)), fmax(a.z, fmax(b.z, c.z))};
         for (int k = 0; k < 3; ++k) {
-            // samples (i + 0.5) / R within [mn - band, mx + band], one extra on each side
-            int l = (int)floor((mn[k] - band) * R - 0.5) - 1, h = (int)ceil((mx[k] + band) * R - 0.5) + 1;
+            // samples (i + 0.5) / R within [mn - band, mx + band]
+            int l = (int)floor((mn[k] - band) * R - 0.5), h = (int)ceil((mx[k] + band) * R - 0.5);
             l = max(l, 0);
             h = min(h, R - 1);
             lo[k] = l;
             n[k] = h >= l ? h - l + 1 : 0;
         }
-        const long long total = (long long)n[0] * n[1] * n[2];
-        for (long long s = lane; s < total; s += 32) {
-            const int ix = lo[0] + (int)(s % n[0]);
-            const int iy = lo[1] + (int)((s / n[0]) % n[1]);
-            const int iz = lo[2] + (int)(s / ((long long)n[0] * n[1]));
+        // the plane's normal (unnormalised) and 1 / |n|^2
+        const D3 ab = dsub(b, a), ac = dsub(c, a);
+        const D3 nrm = {ab.y * ac.z - ab.z * ac.y, ab.z * ac.x - ab.x * ac.z, ab.x * ac.y - ab.y * ac.x};
+        const double nn = ddot(nrm, nrm);
+        const double inv_nn = nn > 0.0 ? 1.0 / nn : 0.0;  // degenerate: no plane bound
+        const int nxy = n[0] * n[1];
+        const int total = nxy * n[2];
+        for (int s = lane; s < total; s += 32) {
+            const int iz = lo[2] + s / nxy, r = s % nxy;
+            const int iy = lo[1] + r / n[0], ix = lo[0] + r % n[0];
             const D3 p = {(ix + 0.5) / R, (iy + 0.5) / R, (iz + 0.5) / R};
+            const double bx = fmax(fmax(mn[0] - p.x, 0.0), p.x - mx[0]);
+            const double by = fmax(fmax(mn[1] - p.y, 0.0), p.y - mx[1]);
+            const double bz = fmax(fmax(mn[2] - p.z, 0.0), p.z - mx[2]);
+            const double box2 = bx * bx + by * by + bz * bz;
+            if (box2 >= band2 * (1.0 + 1e-9)) continue;  // the value stays band^2 or lower
+            unsigned long long *dst = field + gidx(ix, iy, iz, R);
+            const double cur = __longlong_as_double((long long)*dst);
+            if (box2 > cur * (1.0 + 1e-9)) continue;
+            const double hp = ddot(nrm, dsub(p, a));
+            if (hp * hp * inv_nn > cur * (1.0 + 1e-9)) continue;
             const double d2 = point_tri_d2(p, a, b, c);
             const unsigned long long bits = (unsigned long long)__double_as_longlong(d2);
-            unsigned long long *dst = field + gidx(ix, iy, iz, R);
             if (bits < *dst) atomicMin(dst, bits);
         }
     }
@@ -290,12 +310,17 @@ constexpr int kHalo = kTile + 2;
 
 // One block per 8^3 tile (one thread per sample): free samples next to an
 // outside sample become outside, repeated in shared memory until the tile
-// settles (at most 3 * 8^3 sweeps); a change is reported in dev[4].
-__global__ void __launch_bounds__(kTile * kTile * kTile) k_s1_flood(uint8_t *state, int R, int *dev)
+// settles (at most 3 * 8^3 sweeps); a change is reported in dev[4].  Only
+// tiles marked in `dirty_in` (changed, or next to a tile that changed, in the
+// previous launch; all tiles in the first) do the work; a tile that changes
+// marks itself and its six neighbours in `dirty_out`.
+__global__ void __launch_bounds__(kTile * kTile * kTile) k_s1_flood(uint8_t *state, int R, int *dev,
+                                                                   const uint8_t *dirty_in, uint8_t *dirty_out)
 {
     __shared__ uint8_t s[kHalo][kHalo][kHalo];
-    __shared__ int changed;
+    __shared__ int changed, any_change;
     const int tpr = (R + kTile - 1) / kTile;
+    if (!dirty_in[blockIdx.x]) return;
     const int bx = blockIdx.x % tpr, by = (blockIdx.x / tpr) % tpr, bz = blockIdx.x / (tpr * tpr);
     const int tx = threadIdx.x % kTile, ty = (threadIdx.x / kTile) % kTile, tz = threadIdx.x / (kTile * kTile);
     // the tile with its one-sample halo (outside the grid: near, never spreads)
@@ -306,6 +331,7 @@ __global__ void __launch_bounds__(kTile * kTile * kTile) k_s1_flood(uint8_t *sta
         if (gx >= 0 && gy >= 0 && gz >= 0 && gx < R && gy < R && gz < R) v = state[gidx(gx, gy, gz, R)];
         s[hz][hy][hx] = v;
     }
+    if (threadIdx.x == 0) any_change = 0;
     const int gx = bx * kTile + tx, gy = by * kTile + ty, gz = bz * kTile + tz;
     const bool in_grid = gx < R && gy < R && gz < R;
     const int x = tx + 1, y = ty + 1, z = tz + 1;
@@ -326,7 +352,18 @@ __global__ void __launch_bounds__(kTile * kTile * kTile) k_s1_flood(uint8_t *sta
     }
     if (any) {
         state[gidx(gx, gy, gz, R)] = 2;
+        any_change = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && any_change) {
         atomicExch(&dev[4], 1);
+        dirty_out[blockIdx.x] = 1;
+        if (bx > 0) dirty_out[blockIdx.x - 1] = 1;
+        if (bx + 1 < tpr) dirty_out[blockIdx.x + 1] = 1;
+        if (by > 0) dirty_out[blockIdx.x - tpr] = 1;
+        if (by + 1 < tpr) dirty_out[blockIdx.x + tpr] = 1;
+        if (bz > 0) dirty_out[blockIdx.x - tpr * tpr] = 1;
+        if (bz + 1 < tpr) dirty_out[blockIdx.x + tpr * tpr] = 1;
     }
 }
 
@@ -519,7 +556,7 @@ static_assert(kEdgeCorners[5][0] == 1 && kEdgeCorners[5][1] == 3 && kEdgeCorners
 void Stage1::release()
 {
     void *p[] = {tris, field, state, cell_cnt, edge_cnt, scan_cells, scan_edges, scan_quads, quads, q_first, verts,
-                 faces, dev, mean_dev};
+                 faces, dev, mean_dev, tile_dirty};
     for (void *x : p)
         if (x) cudaFree(x);
     if (h_dev) cudaFreeHost(h_dev);
@@ -533,13 +570,16 @@ void Stage1::release()
     faces = nullptr;
     dev = h_dev = nullptr;
     mean_dev = nullptr;
-    cap_tris = cap_grid = cap_cells = cap_edges = cap_verts = cap_quads = 0;
+    tile_dirty = nullptr;
+    cap_tris = cap_grid = cap_cells = cap_edges = cap_verts = cap_quads = cap_tiles = 0;
 }
 
 int Stage1::ensure(long long m, int R_)
 {
     const long long n3 = (long long)R_ * R_ * R_, c3 = (long long)(R_ - 1) * (R_ - 1) * (R_ - 1);
-    if (m <= cap_tris && n3 <= cap_grid && dev) return PAMO_OK;
+    const long long tpr = (R_ + kTile - 1) / kTile, nt = tpr * tpr * tpr;
+    if (m <= cap_tris && n3 <= cap_grid && nt <= cap_tiles && dev) return PAMO_OK;
+    const long long ctl = nt > cap_tiles ? nt : cap_tiles;
     const long long cm = m > cap_tris ? m : cap_tris, cg = n3 > cap_grid ? n3 : cap_grid;
     const long long cc = c3 > cap_cells ? c3 : cap_cells;
     void *keep_v = verts, *keep_f = faces, *keep_q = quads, *keep_qf = q_first, *keep_sq = scan_quads;
@@ -565,6 +605,7 @@ int Stage1::ensure(long long m, int R_)
     S1A(tris, 9 * 4 * (cm + 1));
     S1A(field, 8 * cg);
     S1A(state, cg);
+    S1A(tile_dirty, 2 * ctl);
     S1A(cell_cnt, 4 * (cc + 1));
     S1A(edge_cnt, 4 * (3 * cg + 1));
     S1A(scan_cells, 4 * scan_scratch_ints(cc + 1));
@@ -583,6 +624,7 @@ int Stage1::ensure(long long m, int R_)
     }
     cap_tris = cm;
     cap_grid = cg;
+    cap_tiles = ctl;
     cap_cells = cc;
     cap_edges = 3 * cg;
     return PAMO_OK;
@@ -660,10 +702,20 @@ int remesh(Stage1 &S, const float *d_points, const int *d_tris, int n_pts, int m
     if (S.prof) S.prof->begin(PH_S1_FLOOD, s);
     const int tpr = (R + kTile - 1) / kTile;
     const int tiles = tpr * tpr * tpr;
+    // two dirty-tile flag sets used in turn: every tile is dirty at first
+    uint8_t *dirty[2] = {S.tile_dirty, S.tile_dirty + tiles};
+    S1_TRY(cudaMemsetAsync(dirty[0], 1, (size_t)tiles, s));
+    S1_TRY(cudaMemsetAsync(dirty[1], 0, (size_t)tiles, s));
+    int cur = 0;
     bool settled = false;
     for (int round = 0; round < 4 * R + 64 && !settled; round += 8) {
         S1_TRY(cudaMemsetAsync(S.dev + 4, 0, 4, s));
-        for (int k = 0; k < 8; ++k) launch(k_s1_flood, tiles, kTile * kTile * kTile, 0, s, S.state, R, S.dev);
+        for (int k = 0; k < 8; ++k) {
+            launch(k_s1_flood, tiles, kTile * kTile * kTile, 0, s, S.state, R, S.dev, (const uint8_t *)dirty[cur],
+                   dirty[cur ^ 1]);
+            S1_TRY(cudaMemsetAsync(dirty[cur], 0, (size_t)tiles, s));
+            cur ^= 1;
+        }
         S1_TRY(cudaMemcpyAsync(S.h_dev, S.dev, 64, cudaMemcpyDeviceToHost, s));
         S1_TRY(cudaStreamSynchronize(s));
         if (S.prof) S.prof->collect();

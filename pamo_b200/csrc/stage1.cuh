@@ -12,10 +12,11 @@ namespace s1 {
 
 struct Stage1 {
     int R = 0;
-    long long cap_tris = 0, cap_grid = 0, cap_cells = 0, cap_edges = 0, cap_verts = 0, cap_quads = 0;
+    long long cap_tris = 0, cap_grid = 0, cap_cells = 0, cap_edges = 0, cap_verts = 0, cap_quads = 0, cap_tiles = 0;
     float *tris = nullptr;              // [m][9] normalised triangles (float32, the reference's arithmetic)
     unsigned long long *field = nullptr;  // [R^3]: squared distance bits, then the field as double
     uint8_t *state = nullptr;           // [R^3] flood fill: 0 near the surface, 1 free, 2 outside
+    uint8_t *tile_dirty = nullptr;      // [2 x tiles] flood-fill tiles to visit (two sets used in turn)
     int *cell_cnt = nullptr;            // [C^3 + 1] patches per cell, then their first vertex
     int *edge_cnt = nullptr;            // [3 R^3 + 1] quads per grid edge (0/1), then the quad index
     int *scan_cells = nullptr, *scan_edges = nullptr, *scan_quads = nullptr;  // scan scratch

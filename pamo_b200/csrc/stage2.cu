@@ -506,9 +506,12 @@ __device__ __forceinline__ bool faces_min_ok(const CollapseArgs &A, int lo, int 
     return true;
 }
 
-// One thread per edge: most edges fail the threshold or the key test at once,
-// and a winner's collapse is long, so no block-wide step waits on it.
-template <bool QUALITY>
+// The independent set: one thread per edge tests the threshold and the key
+// (most edges fail at once) and flags the winners; the collapse list is their
+// scan.  The winners' collapses then run one thread per winner
+// (k_collapse_apply), so no warp carries idle lanes through a collapse.
+// Winners have disjoint one-rings, and the tests read only the round input
+// (otris) and the key minima, so splitting the two changes nothing.
 __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
 {
     const int E = *A.n_edges;
@@ -526,56 +529,71 @@ __global__ void __launch_bounds__(kThreads) k_collapse(CollapseArgs A)
             collapse_t = A.slots[r].collapse_t;
         }
         if (c <= collapse_t) {
-            int2 ed = A.edges[e];
+            const int2 ed = A.edges[e];
             const int u = ed.x, v = ed.y;
-            unsigned long long key = ((unsigned long long)c << 32) | (unsigned)e;
-            const int ua = A.first_near[u], ub = A.first_near[u + 1];
-            const int va = A.first_near[v], vb = A.first_near[v + 1];
-            if (A.vmin[u] == key && A.vmin[v] == key && faces_min_ok(A, ua, ub, key) && faces_min_ok(A, va, vb, key)) {
-                win = 1;
-                V3 p0 = v3(A.opts[u]), p1 = v3(A.opts[v]);
-                V3 mid;
-                if constexpr (QUALITY) mid = v3(A.epos[e]);  // the position the edge cost chose
-                else mid = vmid(p0, p1);
-                A.pts[u] = make_float4(mid.x, mid.y, mid.z, 0.f);
-                A.pts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
-                A.occ[v] = 0;
-                for (int a = ua; a < ub; ++a) {
-                    int f = A.near_tris[a];
-                    int4 t = A.tris[f];
-                    if (face_has(t, v)) A.tris[f] = make_int4(-1, -1, -1, 0);
-                }
-                for (int a = va; a < vb; ++a) {
-                    int f = A.near_tris[a];
-                    int4 t = A.tris[f];
-                    if (face_has(t, u)) t = make_int4(-1, -1, -1, 0);
-                    else if (t.x == v) t.x = u;
-                    else if (t.y == v) t.y = u;
-                    else if (t.z == v) t.z = u;
-                    A.tris[f] = t;
-                }
-                bool sk = false;
-                for (int pass = 0; pass < 2 && !sk; ++pass) {
-                    int lo = pass ? va : ua, hi = pass ? vb : ub;
-                    for (int a = lo; a < hi; ++a) {
-                        int4 t = A.tris[A.near_tris[a]];
-                        if (t.x == -1) continue;
-                        if (is_skinny(v3(A.pts[t.x]), v3(A.pts[t.y]), v3(A.pts[t.z]))) {
-                            sk = true;
-                            break;
-                        }
-                    }
-                }
-                if (sk) {  // roll back; the edge stays in the collapsed list
-                    A.occ[v] = 1;
-                    A.pts[u] = A.opts[u];
-                    A.pts[v] = A.opts[v];
-                    for (int a = ua; a < ub; ++a) A.tris[A.near_tris[a]] = A.otris[A.near_tris[a]];
-                    for (int a = va; a < vb; ++a) A.tris[A.near_tris[a]] = A.otris[A.near_tris[a]];
+            const unsigned long long key = ((unsigned long long)c << 32) | (unsigned)e;
+            if (A.vmin[u] == key && A.vmin[v] == key)
+                win = faces_min_ok(A, A.first_near[u], A.first_near[u + 1], key) &&
+                      faces_min_ok(A, A.first_near[v], A.first_near[v + 1], key);
+        }
+        A.eflag[e] = win;
+    }
+}
+
+// Collapse of each winner (list[0, *n_list)): u moves to the midpoint (the
+// quality mode's chosen position), v goes, faces holding both die and v's faces
+// take u; if a surviving one-ring face is skinny the one-rings are restored from
+// the round input, and the edge stays in the collapsed list.
+template <bool QUALITY>
+__global__ void __launch_bounds__(kThreads) k_collapse_apply(CollapseArgs A, const int *list, const int *n_list)
+{
+    const int N = *n_list;
+    PAMO_GRID_STRIDE(k, N)
+    {
+        const int e = list[k];
+        const int2 ed = A.edges[e];
+        const int u = ed.x, v = ed.y;
+        const int ua = A.first_near[u], ub = A.first_near[u + 1];
+        const int va = A.first_near[v], vb = A.first_near[v + 1];
+        V3 mid;
+        if constexpr (QUALITY) mid = v3(A.epos[e]);  // the position the edge cost chose
+        else mid = vmid(v3(A.opts[u]), v3(A.opts[v]));
+        A.pts[u] = make_float4(mid.x, mid.y, mid.z, 0.f);
+        A.pts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+        A.occ[v] = 0;
+        for (int a = ua; a < ub; ++a) {
+            const int f = A.near_tris[a];
+            const int4 t = A.tris[f];
+            if (face_has(t, v)) A.tris[f] = make_int4(-1, -1, -1, 0);
+        }
+        for (int a = va; a < vb; ++a) {
+            const int f = A.near_tris[a];
+            int4 t = A.tris[f];
+            if (face_has(t, u)) t = make_int4(-1, -1, -1, 0);
+            else if (t.x == v) t.x = u;
+            else if (t.y == v) t.y = u;
+            else if (t.z == v) t.z = u;
+            A.tris[f] = t;
+        }
+        bool sk = false;
+        for (int pass = 0; pass < 2 && !sk; ++pass) {
+            const int lo = pass ? va : ua, hi = pass ? vb : ub;
+            for (int a = lo; a < hi; ++a) {
+                const int4 t = A.tris[A.near_tris[a]];
+                if (t.x == -1) continue;
+                if (is_skinny(v3(A.pts[t.x]), v3(A.pts[t.y]), v3(A.pts[t.z]))) {
+                    sk = true;
+                    break;
                 }
             }
         }
-        A.eflag[e] = win;
+        if (sk) {  // roll back; the edge stays in the collapsed list
+            A.occ[v] = 1;
+            A.pts[u] = A.opts[u];
+            A.pts[v] = A.opts[v];
+            for (int a = ua; a < ub; ++a) A.tris[A.near_tris[a]] = A.otris[A.near_tris[a]];
+            for (int a = va; a < vb; ++a) A.tris[A.near_tris[a]] = A.otris[A.near_tris[a]];
+        }
     }
 }
 
@@ -1510,10 +1528,15 @@ int Stage2::round(int n, int m, float scale, float threshold, bool is_stuck, con
     CollapseArgs cl{edges, d_n_edges, edge_cost, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
                     collapse_t, nullptr, nullptr, nullptr, quality ? (const float4 *)epos : nullptr};
     prof.begin(PH_COLLAPSE, s);
-    if (quality) launch(k_collapse<true>, grid_for(EMAX), kThreads, 0, s, cl);
-    else launch(k_collapse<false>, grid_for(EMAX), kThreads, 0, s, cl);
+    launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s, &dcnt->scan_fault));
     launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
+    if (quality)
+        launch(k_collapse_apply<true>, grid_for(EMAX), kThreads, 0, s, cl, (const int *)collapsed,
+               (const int *)&dcnt->n_main);
+    else
+        launch(k_collapse_apply<false>, grid_for(EMAX), kThreads, 0, s, cl, (const int *)collapsed,
+               (const int *)&dcnt->n_main);
     prof.begin(PH_CLEANUP, s);
     launch(k_remove_invalid_faces, grid_for(m), kThreads, 0, s, tris, m);
     launch(k_line_flags, grid_for(EMAX), kThreads, 0, s, edges, d_n_edges, pts, eflag, &dcnt->n_line);
@@ -1773,9 +1796,11 @@ int Stage2::round_batch(int n, int m, int K, int *nvu_out, cudaStream_t s)
     CollapseArgs cl{edges, d_n_edges, nullptr, vmin, first_near, near_tris, opts, otris, pts, tris, occ, eflag,
                     0u, slots, scnt, vslot, nullptr};
     prof.begin(PH_COLLAPSE, s);
-    launch(k_collapse<false>, grid_for(EMAX), kThreads, 0, s, cl);
+    launch(k_collapse, grid_for(EMAX), kThreads, 0, s, cl);
     S2_TRY(exclusive_scan(eflag, uflag, EMAX, d_n_edges, scan_scratch, &dcnt->n_main, s, &dcnt->scan_fault));
     launch(k_scatter_flagged, grid_for(EMAX), kThreads, 0, s, eflag, uflag, d_n_edges, collapsed, 0);
+    launch(k_collapse_apply<false>, grid_for(EMAX), kThreads, 0, s, cl, (const int *)collapsed,
+           (const int *)&dcnt->n_main);
     launch(k_b_main, grid_for(K), kThreads, 0, s, (const int *)uflag, (const RoundCounters *)dcnt, scnt, K);
     prof.begin(PH_CLEANUP, s);
     launch(k_remove_invalid_faces, grid_for(m), kThreads, 0, s, tris, m);
