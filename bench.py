@@ -144,9 +144,10 @@ def stage3_stand_in(name):
 def cpu_sample(args, V, F, ratio):
     """The CPU restatement (oracle/) timed on the host cores, on bounded samples:
     stage 2 = its first `sample_rounds` rounds (C, OpenMP on all host threads),
-    extrapolated by the face-rounds of the whole run; stage 3 = one Newton
-    iteration of the FP64 numpy restatement on a stand-in of the stage-2 output,
-    extrapolated to PaMO.run's 5 steps x 10 Newton iterations (plus its setup).
+    extrapolated by the face-rounds of the whole run; stage 3 = all of PaMO.run's
+    5 steps x 10 Newton iterations in the C++ float32 restatement
+    (oracle/s3_cpu.cpp, OpenMP on all host threads) on a stand-in of the
+    stage-2 output, measured whole.
     Returns (measured seconds of the sample, estimated seconds for the whole
     workload, sample description, threads)."""
     from oracle import oracle as O
@@ -169,27 +170,18 @@ def cpu_sample(args, V, F, ratio):
         total = t2
         desc = f"stage 2: the whole loop ({t2:.1f} s)"
     if "3" in args.stages:
-        from oracle import s3_oracle as S3  # numpy FP64 restatement
+        from oracle import s3_cpu  # C++ FP32 restatement, OpenMP
 
         v, f = stage3_stand_in(args.workload)
-        scale, t = S3.normalization(np.asarray(V, np.float64))
-        gV = np.asarray(V, np.float64) * scale + t
-        sV = np.asarray(v, np.float64) * scale + t
-        s3 = S3.Stage3Oracle()
+        st = {}
         t0 = time.perf_counter()
-        s3.register(gV, F, sV, f)
-        t_reg = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        s3.update_target()
-        t_tgt = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        s3.newton()
-        t_newton = time.perf_counter() - t0
-        measured += t_reg + t_tgt + t_newton
-        n_newton = 5 * s3.c.n_newton_iters
-        total += t_reg + 5 * t_tgt + n_newton * t_newton
-        desc += (f"; stage 3: one Newton iteration on a {len(f):,}-face stand-in of the stage-2 output "
-                 f"({t_newton:.1f} s, {len(s3.blocks):,} contact blocks) x {n_newton} + setup")
+        s3_cpu.process(V, F, v, f, 5, stats=st)
+        t3 = time.perf_counter() - t0
+        measured += t3
+        total += t3
+        desc += (f"; stage 3: the whole of it (5 steps x 10 Newton iterations, C++ float32 restatement on "
+                 f"{s3_cpu.num_threads()} threads) on a {len(f):,}-face stand-in of the stage-2 output "
+                 f"({t3:.1f} s, {st['blocks']:,} contact blocks at the end)")
     if "1" in args.stages:
         desc += ("; stage 1 is not in the sample (the reference runs it through GPU libraries only; its "
                  "restatement under oracle/ is a numpy test oracle)")
@@ -234,8 +226,8 @@ def reference_arm(args):
 
     `ms_per_step` is the measured time of one sample.  `value` is the input
     Mfaces/s of the whole workload estimated from the sample (stage 2 by the
-    face-rounds the sample covers, stage 3 by Newton iterations); the line
-    says so under `extrapolated`.  The reference's own stage-2 GPU build is
+    face-rounds the sample covers; stage 3 is measured whole); the line says
+    so under `extrapolated`.  The reference's own stage-2 GPU build is
     timed beside it on the full workload (`reference_gpu_stage2`)."""
     ws, rank, _ = dist_init(args)
     if rank != 0:
@@ -826,6 +818,30 @@ def serving_arm(args):
     return 0
 
 
+def kernel_case(which):
+    """A small case of the stage-1 or checker kernels for `ncu --set full`
+    captures: stage 1 once on a 512x512 noisy torus (524,288 faces) at R=256
+    (a 256^3 field, 134 MB of distance bits: larger than L2), then the exact
+    checker and the Hausdorff sampler on its output."""
+    import torch
+
+    import pamo_b200
+    from pamo_b200 import meshgen as mg
+
+    V, F = mg.noisy_torus(512, 512, 0)
+    ctx = pamo_b200.Context(0)
+    v, f, _ = pamo_b200.remesh(ctx, torch.from_numpy(V).cuda(), torch.from_numpy(F).cuda(), 256)
+    out = {"case": which, "faces_in": len(F), "faces_out": int(len(f))}
+    if which == "checker":
+        r = pamo_b200.metrics.check_mesh(v, f)
+        h = pamo_b200.metrics.hausdorff(V, F, v, f, 1, 2)
+        out.update(intersecting_pairs=r["intersecting_pairs"], watertight=r["watertight_manifold"],
+                   hausdorff=h["hausdorff"])
+    torch.cuda.synchronize()
+    print(out, flush=True)
+    return 0
+
+
 def main():
     import gc
 
@@ -853,7 +869,11 @@ def main():
     ap.add_argument("--dump-rounds", action="store_true")
     ap.add_argument("--iters", type=int, default=1000000,
                     help="PaMO.run's iter: the most collapse rounds per simplification")
+    ap.add_argument("--kernel-case", choices=["stage1", "checker"],
+                    help="one small untimed invocation for profiler captures (no JSON line)")
     args = ap.parse_args()
+    if args.kernel_case:
+        return kernel_case(args.kernel_case)
     if args.impl == "reference":
         return reference_arm(args)
     if args.workload == "c4":
