@@ -292,7 +292,7 @@ def roofline_edge_cost(phases, round_faces, peaks):
     (int4) 16 B/face, points (float4) 16 B/vertex, quadrics 48 B/vertex,
     invalid flags 1 B/vertex, per-vertex key minimum read+write 16 B/vertex:
     12 E + 85 V + 28 F = 88.5 B/face.  Traffic: DRAM bytes per face of the
-    round-0 launch on config 2 (ncu, profiles/stage2_kernels_c2_round0.txt),
+    round-0 launch on config 2 (ncu, profiles/stage2_kernels_c2_first_collapse_round.txt),
     times the average faces per launch."""
     ph = phases.get("edge_cost")
     if not ph or not ph["ms"] or not round_faces:
@@ -313,7 +313,7 @@ def roofline_edge_cost(phases, round_faces, peaks):
 # DRAM read + write of k_edge_cost and k_query per input face of the launch,
 # from an ncu capture of round 0 of config 2 (2,097,152 faces): edge cost
 # 904.0 MB read + 57.0 MB written, query 254.9 MB read + 22.5 MB written;
-# profiles/stage2_kernels_c2_round0.txt.
+# profiles/stage2_kernels_c2_first_collapse_round.txt.
 EDGE_COST_DRAM_BYTES_PER_FACE = 458.2
 QUERY_DRAM_BYTES_PER_FACE = 132.3
 

@@ -27,8 +27,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I", os.path.join(ROOT, "include")]
 # translation units whose arithmetic must round exactly like the reference
-# (checker.cu: its exact predicates' error-free sums need one rounding per operation)
-NO_FMA = {"stage2.cu", "lbvh.cu", "scan.cu", "abi.cu", "shuffle.cu", "noalloc.cu", "checker.cu"}
+# (checker.cu: its exact predicates' error-free sums need one rounding per operation;
+# stage1.cu: its FP64 distances follow the CPU restatement's operation order)
+NO_FMA = {"stage2.cu", "lbvh.cu", "scan.cu", "abi.cu", "shuffle.cu", "noalloc.cu", "checker.cu", "stage1.cu"}
 
 
 def sources():

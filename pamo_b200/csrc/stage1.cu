@@ -236,7 +236,14 @@ __device__ double point_tri_d2(D3 p, D3 a, D3 b, D3 c)
 // and to its plane -- already reaches the sample's current value (the bounds
 // hold in exact arithmetic; the 1e-9 relative margin covers their rounding), so
 // the minimum, and therefore the field, is the same as without the test.
-__global__ void __launch_bounds__(256) k_s1_udist(const float *tris, int m, int R, double band,
+// (i + 0.5) / R, the coordinate of sample i; for R a power of two (inv_r > 0)
+// the product with 1 / R is that same number and spares the FP64 division
+__device__ __forceinline__ double s1_coord(int i, int R, double inv_r)
+{
+    return inv_r > 0.0 ? (i + 0.5) * inv_r : (i + 0.5) / R;
+}
+
+__global__ void __launch_bounds__(256, 3) k_s1_udist(const float *tris, int m, int R, double inv_r, double band,
                                                   unsigned long long *field)
 {
     const int lane = threadIdx.x & 31;
@@ -264,10 +271,27 @@ __global__ void __launch_bounds__(256) k_s1_udist(const float *tris, int m, int 
         const double inv_nn = nn > 0.0 ? 1.0 / nn : 0.0;  // degenerate: no plane bound
         const int nxy = n[0] * n[1];
         const int total = nxy * n[2];
+        // the lane's sample (ox, oy, oz) in the box, stepped by 32 without divisions
+        int ox = 0, oy = 0, oz = 0;
+        if (total > 0) {
+            ox = lane % n[0];
+            oy = (lane / n[0]) % n[1];
+            oz = lane / nxy;
+        }
+        const int qx = total > 0 ? 32 / n[0] : 0, rx = total > 0 ? 32 % n[0] : 0;
         for (int s = lane; s < total; s += 32) {
-            const int iz = lo[2] + s / nxy, r = s % nxy;
-            const int iy = lo[1] + r / n[0], ix = lo[0] + r % n[0];
-            const D3 p = {(ix + 0.5) / R, (iy + 0.5) / R, (iz + 0.5) / R};
+            const int ix = lo[0] + ox, iy = lo[1] + oy, iz = lo[2] + oz;
+            ox += rx;
+            oy += qx;
+            if (ox >= n[0]) {
+                ox -= n[0];
+                ++oy;
+            }
+            while (oy >= n[1]) {
+                oy -= n[1];
+                ++oz;
+            }
+            const D3 p = {s1_coord(ix, R, inv_r), s1_coord(iy, R, inv_r), s1_coord(iz, R, inv_r)};
             const double bx = fmax(fmax(mn[0] - p.x, 0.0), p.x - mx[0]);
             const double by = fmax(fmax(mn[1] - p.y, 0.0), p.y - mx[1]);
             const double bz = fmax(fmax(mn[2] - p.z, 0.0), p.z - mx[2]);
@@ -696,7 +720,8 @@ int remesh(Stage1 &S, const float *d_points, const int *d_tris, int n_pts, int m
         // fill by a kernel: cudaMemset only sets bytes
         launch(k_s1_fill, grid_for(n3), kThreads, 0, s, S.field, n3, bits);
     }
-    launch(k_s1_udist, grid_for(32LL * m), 256, 0, s, (const float *)S.tris, m, R, band, S.field);
+    const double inv_r = (R & (R - 1)) == 0 ? 1.0 / R : 0.0;
+    launch(k_s1_udist, grid_for(32LL * m), 256, 0, s, (const float *)S.tris, m, R, inv_r, band, S.field);
     launch(k_s1_state, grid_for(n3), kThreads, 0, s, S.field, n3, R, band, S.state);
     // 3. flood fill from the boundary, until nothing changes
     if (S.prof) S.prof->begin(PH_S1_FLOOD, s);
