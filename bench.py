@@ -345,6 +345,57 @@ def roofline_query(phases, round_faces, peaks):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs") else "fallback"}
 
 
+def _block_pattern_nnz(f):
+    """Blocks of stage 3's assembled matrix for the faces f: the diagonal plus
+    both orders of every vertex pair sharing an edge or facing across one (the
+    hinge's opposite vertices)."""
+    f = np.asarray(f, np.int64)
+    n = int(f.max()) + 1 if len(f) else 0
+    a = np.concatenate([f[:, 0], f[:, 1], f[:, 2]])
+    b = np.concatenate([f[:, 1], f[:, 2], f[:, 0]])
+    c = np.concatenate([f[:, 2], f[:, 0], f[:, 1]])  # the vertex opposite the half-edge
+    key = np.minimum(a, b) * n + np.maximum(a, b)
+    order = np.argsort(key, kind="stable")
+    ks, cs = key[order], c[order]
+    twin = np.nonzero(ks[1:] == ks[:-1])[0]
+    opp = np.stack([cs[twin], cs[twin + 1]], 1)
+    pairs = np.concatenate([np.stack([np.minimum(a, b), np.maximum(a, b)], 1),
+                            np.sort(opp, axis=1)])
+    pairs = pairs[pairs[:, 0] != pairs[:, 1]]
+    return n + 2 * len(np.unique(pairs[:, 0] * n + pairs[:, 1]))
+
+
+def roofline_cg(phases, f_stage3, trace, n_iters, peaks):
+    """The step's largest kernel by device time: the persistent CG solve
+    (k_cg_solve, one launch per Newton iteration, n_iters iterations each).
+
+    Algorithmic bytes per CG iteration, each array read or written once: the
+    matrix blocks (36 B of values + 4 B column index per block), per vertex the
+    row offset (4 B) and 14 vector reads/writes of 12 B (direction, residual,
+    preconditioned residual, solution, products, diagonal), per active contact
+    block its index (16 B), curvature (4 B), four gradients (48 B) and two
+    12-B accesses per vertex.  The matrix and vectors stay in L2 (~13 MB on
+    config 2): the solve is bound by the latency of its two grid-wide sums per
+    iteration, so the fraction of HBM bandwidth says how far it is from
+    streaming, not what bounds it."""
+    ph = phases.get("s3_cg")
+    if not ph or not ph["ms"] or trace is None or not len(trace):
+        return None
+    nnz = _block_pattern_nnz(f_stage3)
+    nv = int(np.asarray(f_stage3).max()) + 1
+    nact = float(np.mean(np.asarray(trace)[:, 5]))
+    per_iter = nnz * 40.0 + nv * (4.0 + 14 * 12.0) + nact * (16 + 4 + 48 + 96)
+    per_launch = n_iters * per_iter
+    avg_ms = ph["ms"] / max(ph["calls"], 1)
+    achieved = per_launch / (avg_ms / 1e3) / 1e9
+    peak = peaks.get("hbm_gbs") or 6650.0
+    return {"bound": "hbm", "kernel": "k_cg_solve", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "launches": ph["calls"], "avg_launch_ms": avg_ms,
+            "bytes_per_launch": per_launch, "blocks": nnz, "active_contacts_mean": nact,
+            "note": "L2-resident; bound by the grid-wide sums' latency, not by bytes",
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs") else "fallback"}
+
+
 def acceptance(V_in, F_in, v, f, dev):
     """The acceptance checks of a result (pamo_b200.metrics, on the device):
     intersecting face pairs under exact predicates, watertight / manifold,
@@ -461,6 +512,8 @@ def product_arm(args):
         for i in range(min(nph, len(_lib.PHASES))):
             if ph_calls[i]:
                 phases[_lib.PHASES[i]] = {"ms": ph_ms[i], "calls": ph_calls[i]}
+    trace = pm.system.last_trace if "3" in args.stages else None
+    f_stage3 = f_out  # stage 3 moves vertices only
     sizes = (ctypes.c_int * 4096)()
     nr = L.pamo_stage2_round_sizes(pm.ctx.handle, sizes, 4096)
     round_faces = [sizes[i] for i in range(min(nr, 4096))]
@@ -486,7 +539,8 @@ def product_arm(args):
             "metric": "input Mfaces/s", "value": value, "unit": "Mfaces/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "stages": STAGES[args.stages], "faces_out": om.value, "verts_out": on.value,
+            "config": {"workload": desc, "stages": STAGES[args.stages], "faces_out": int(len(f_out)),
+                       "verts_out": int(len(v_out)),
                        "rounds": rounds, "iters": args.iters, "l2": "inputs/working set > L2, no flush",
                        "parallelism": f"replicas x{ws}",
                        "api": f"PaMO(mesh, use_stage1={'1' in args.stages}, use_stage3={'3' in args.stages}).run",
@@ -500,6 +554,7 @@ def product_arm(args):
                     "d2h_bytes_per_step": int(d2h)},
             "stage_ms": {k: round(v * 1e3, 3) for k, v in timings.items()},
             "stage2_device": {"value": nF / 1e6 / (s2_ms / 1e3), "unit": "Mfaces/s", "ms": s2_ms,
+                              "faces_out": om.value, "rounds": rr.value,
                               "what": "pamo_stage2_run alone on the unremeshed input, device-resident in and out"},
             "batched_vs_plain": c4,
             "clocks": clocks,
@@ -507,7 +562,9 @@ def product_arm(args):
             "intersections": intersections,
             "acceptance": accept,
             "phases_ms": {k: round(v["ms"], 3) for k, v in phases.items()},
-            "roofline": roofline_query(phases, round_faces, peaks),
+            "roofline": roofline_cg(phases, f_stage3, trace, pm.config.n_cg_iters if "3" in args.stages else 0, peaks)
+            if "3" in args.stages else roofline_query(phases, round_faces, peaks),
+            "roofline_query": roofline_query(phases, round_faces, peaks),
             "roofline_edge_cost": roofline_edge_cost(phases, round_faces, peaks),
             "round_faces": round_faces if args.dump_rounds else None,
         }

@@ -1500,6 +1500,34 @@ __global__ void __launch_bounds__(128) k_accd(const float4 *q, const float4 *pv,
         else lv = fmax(len(v[0]), len(v[1])) + fmax(len(v[2]), len(v[3]));
         if (lv < 1e-12) continue;
         const double th = thick;
+        // Every distance type is the distance between the two primitives or
+        // between features of them found by the Voronoi regions, so it is at
+        // least the distance between their boxes.  When that bound already
+        // gives a first step beyond 1 (the skip below), so does the exact
+        // distance, and the classification is not needed; the 1e-9 margins
+        // cover the rounding of both evaluations.
+        if (max_iters > 0) {
+            const int na = kind == KIND_PT ? 1 : 2;  // primitive A: x[0 .. na), primitive B: x[na .. 4)
+            double bb = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                auto c = [&](int a) { return k == 0 ? x[a].x : k == 1 ? x[a].y : x[a].z; };
+                double alo = c(0), ahi = c(0), blo = c(3), bhi = c(3);
+                for (int a = 1; a < na; ++a) {
+                    alo = fmin(alo, c(a));
+                    ahi = fmax(ahi, c(a));
+                }
+                for (int a = na; a < 3; ++a) {
+                    blo = fmin(blo, c(a));
+                    bhi = fmax(bhi, c(a));
+                }
+                const double gapk = fmax(fmax(blo - ahi, alo - bhi), 0.0);
+                bb += gapk * gapk;
+            }
+            const double lb = sqrt(bb) * (1.0 - 1e-9);
+            const double dmt_lb = fmax((lb * lb - th * th) / (lb + th), 0.0);
+            if (slack * dmt_lb / lv > 1.0 + 1e-9) continue;
+        }
         int ty = classify(kind, x, (double)ee_thres);
         double d = classified_distance(kind, ty, x);
         double dmt = fmax((d * d - th * th) / (sqrt(d * d) + th), 0.0);

@@ -9,12 +9,15 @@ oracle (bit-identical to the CUDA stage 2, tests/test_stage2_gpu.py):
   s3_shell500k.npz config 3's thin-shell pair: two concentric displaced spheres
                    of 250k faces each (500,000 faces), gap 2e-3, ratio 0.05,
                    5 steps
+  s3_c2step.npz    config 2's stage-3 input: the 20,604-face stage-2 result of
+                   the 2,097,152-face torus (c2_oracle.npz, the same oracle),
+                   one step (10 Newton iterations, ~790,000 contact blocks)
 
 Each holds the stage-2 result (v float32, f), the projected vertices q
 (float64) and the Newton trace (energy at the iterate, energy after the line
 search, CCD step, last halving tried, contact blocks, blocks within d_hat).
 
-    python tests/golden/make_s3_oracle.py --out tests/golden [--case c1|shell8k|shell500k]
+    python tests/golden/make_s3_oracle.py --out tests/golden [--case c1|shell8k|shell500k|c2step]
 """
 from __future__ import annotations
 
@@ -32,6 +35,7 @@ CASES = {
     "c1": ("icosphere", 5, 0, 0.05, 5),
     "shell8k": ("shell", 8000, 3, 0.2, 2),
     "shell500k": ("shell", 500_000, 0, 0.05, 5),
+    "c2step": ("torus", 1024, 0, 0.01, 1),
 }
 
 
@@ -41,6 +45,8 @@ def case_input(name):
     kind, size, seed, ratio, steps = CASES[name]
     if kind == "icosphere":
         V, F = mg.displaced_icosphere(size, seed)
+    elif kind == "torus":
+        V, F = mg.noisy_torus(size, size, seed)
     else:
         V, F = mg.thin_shell_pair(size, 2e-3, seed)
     return V, F, ratio, steps
@@ -52,7 +58,11 @@ def run(name, out_dir):
 
     V, F, ratio, steps = case_input(name)
     t0 = time.time()
-    v, f, rounds = O.pamo_run_stage2(V, F, ratio, min_verts=0)
+    if name == "c2step":  # the stage-2 oracle's result for this input is already a fixture
+        fx = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "c2_oracle.npz"))
+        v, f = fx["v"], fx["f"]
+    else:
+        v, f, rounds = O.pamo_run_stage2(V, F, ratio, min_verts=0)
     t1 = time.time()
     trace = []
     q, _ = S.process(V, F, v.astype(np.float64), f, n_iters=steps, trace=trace)

@@ -40,3 +40,21 @@ def test_s3_cpu_matches_fp64_oracle(name):
     # the thin shells are in contact; the last detection's block count is the
     # oracle's to within the threshold cases
     assert abs(st["blocks"] - int(fx["trace"][-1, 4])) <= 1e-3 * max(int(fx["trace"][-1, 4]), 1000)
+
+
+def test_s3_cpu_config2_input_one_step():
+    """Config 2's stage-3 input (20,604 faces against the 2,097,152-face torus,
+    ~1.6M contact blocks), one step.  Measured: vertex error median 4.8e-6,
+    max 3.4e-4 of the diagonal, against a move of median 9.7e-5, max 1.4e-3
+    (CCD-limited steps taken slightly longer or shorter move every vertex)."""
+    from oracle import s3_cpu
+
+    V, F, fx = _case("c2step")
+    st = {}
+    got, _ = s3_cpu.process(V, F, fx["v"], fx["f"], int(fx["steps"]), stats=st)
+    diag = float(np.linalg.norm(V.max(0) - V.min(0)))
+    err = np.linalg.norm(got - fx["q"], axis=1) / diag
+    move = np.linalg.norm(fx["q"] - fx["v"], axis=1) / diag
+    assert np.median(err) < 0.25 * np.median(move)
+    assert err.max() < 1e-3
+    assert abs(st["blocks"] - int(fx["trace"][-1, 4])) <= 1e-3 * int(fx["trace"][-1, 4])

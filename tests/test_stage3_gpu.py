@@ -18,18 +18,20 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 # FP32 solve vs FP64 solve of the same steps, set from the errors measured on a
-# B200 over two runs (the assembled sums vary with scheduling): the largest
-# vertex deviation as a fraction of the ground truth's bounding-box diagonal,
-# the Newton energies (relative) and the CCD steps --
+# B200 (the assembled sums vary with scheduling, so each run differs): the
+# largest vertex deviation as a fraction of the ground truth's bounding-box
+# diagonal, the Newton energies (relative) and the CCD steps --
 #   config 1 (no contact):                 4.4e-8, 2.4e-7, 0
-#   thin shells, 7,840 faces, ~30,000 blocks within d_hat:
-#                                           4.9e-5 .. 5.6e-5 (of a 5.5e-4 move),
+#   thin shells, 7,840 faces, ~30,000 blocks within d_hat, 24 runs:
+#                                           4.3e-5 .. 1.48e-4 (of a 5.5e-4 move;
+#                                           two groups, near 5e-5 and near 1.47e-4),
 #                                           9.2e-4 .. 1.5e-3, 8.0e-3 .. 1.2e-2
 #   config 3's shells, 500k faces, ~876,000 blocks: 5.6e-7, 3.1e-6, 0
 # For scale: the same steps in plain FP32 (the oracle run in float32) deviate
-# from FP64 by 3.0e-5, 3.2e-2 and 0.11 on the 7,840-face shells.
+# from FP64 by 3.0e-5, 3.2e-2 and 0.11 on the 7,840-face shells, and the C++
+# float32 restatement (oracle/s3_cpu.cpp) by 7.2e-5 in the vertices.
 TOL = {"c1": {"diag": 1e-6, "energy": 1e-6, "ccd": 1e-4, "moved": 10},
-       "contact": {"diag": 1.5e-4, "energy": 5e-3, "ccd": 5e-2, "moved": 3}}
+       "contact": {"diag": 3e-4, "energy": 5e-3, "ccd": 5e-2, "moved": 1.5}}
 # a line-search trial taken differently is a tie: the energy it changes is
 # within float32 evaluation noise of the start's
 TIE = 1e-6
@@ -122,6 +124,45 @@ def test_stage3_config3_thin_shell_pair_at_size(torch_cuda):
     if not os.path.exists(os.path.join(GOLDEN, "s3_shell500k.npz")):
         pytest.skip("fixture not generated")
     _compare_case(torch_cuda, "shell500k", TOL["contact"])
+
+
+def test_stage3_config2_input_one_step(torch_cuda):
+    """Config 2's own stage-3 input: the 20,604-face stage-2 result of the
+    2,097,152-face torus against that torus, one step (10 Newton iterations,
+    ~1.6M contact blocks, ~46,000 within d_hat, three CCD-limited steps).
+    Measured on a B200: vertex error median 3.0e-6, p99 3.1e-5, max 2.5e-4 of
+    the diagonal (the move: median 9.7e-5, max 1.4e-3); Newton energies within
+    1.8e-2 (1.4e-3 at the last); the C++ float32 restatement lands at max
+    3.4e-4, median 4.8e-6 -- a CCD-limited step taken 1% shorter or longer
+    moves every vertex by that fraction of its move."""
+    import pamo_b200
+    from pamo_b200 import safe_project as SP
+
+    if not os.path.exists(os.path.join(GOLDEN, "s3_c2step.npz")):
+        pytest.skip("fixture not generated")
+    V, F, ratio, steps, fx = _golden_case("c2step")
+    ctx = pamo_b200.Context(0)
+    v2, f2, _ = pamo_b200.stage2_run(ctx, torch_cuda.from_numpy(V).cuda(), torch_cuda.from_numpy(F).cuda(),
+                                     int(ratio * len(F)))
+    assert np.array_equal(f2.cpu().numpy(), fx["f"])
+    assert np.array_equal(v2.cpu().numpy().view(np.uint32), fx["v"].view(np.uint32))
+    sysm = SP.Stage3System()
+    got, _ = SP.process(V, F, fx["v"], fx["f"], int(fx["steps"]), system=sysm)
+    want, tr_w, tr_g = fx["q"], fx["trace"], sysm.last_trace
+    diag = _diag(V)
+    err = np.linalg.norm(got - want, axis=1) / diag
+    move = np.linalg.norm(want - fx["v"], axis=1) / diag
+    e_rel = np.abs(tr_g[:, :2] - tr_w[:, :2]) / np.abs(tr_w[:, :2])
+    print(f"stage3 c2step: vertex error vs FP64 median {np.median(err):.3e} p99 {np.quantile(err, 0.99):.3e} "
+          f"max {err.max():.3e} of diag (move median {np.median(move):.3e}, max {move.max():.3e}); energies rel "
+          f"max {e_rel.max():.3e}, last {e_rel[-1].max():.3e}; CCD steps {np.round(tr_g[:, 2], 4).tolist()} vs "
+          f"{np.round(tr_w[:, 2], 4).tolist()}; blocks {int(tr_g[-1, 4])} vs {int(tr_w[-1, 4])}, within d_hat "
+          f"{int(tr_g[-1, 5])} vs {int(tr_w[-1, 5])}")
+    assert len(tr_g) == len(tr_w)
+    assert np.all(np.abs(tr_g[:, 4] - tr_w[:, 4]) <= 1e-3 * tr_w[:, 4])
+    assert np.median(err) < 0.25 * np.median(move)
+    assert err.max() < 1e-3
+    assert e_rel.max() < 5e-2
 
 
 def test_cg_known_answer(torch_cuda):
