@@ -131,13 +131,18 @@ def dist_init(args):
     return ws, rank, local
 
 
-def stage3_stand_in(name):
+def stage3_stand_in(name, stages="123"):
     """A mesh of the family and size of the stage-2 output (the input of stage 3)
-    for the CPU sample: 20,604 faces for config 2, ~1k for config 1."""
+    for the CPU sample: 20,604 faces for config 2, ~1k for config 1.  After
+    stage 1 the surface stage 2 simplifies is the smooth remeshed one, so the
+    config-2 stand-in is then a smooth torus; without stage 1 it carries the
+    input's kind of noise (many more blocks within d_hat)."""
     from pamo_b200 import meshgen as mg
 
     if name == "c1":
         return mg.displaced_geodesic(980, 1)
+    if "1" in stages:
+        return mg.noisy_torus(101, 102, 1, amplitude=0.0)
     return mg.noisy_torus(101, 102, 1)
 
 
@@ -172,7 +177,7 @@ def cpu_sample(args, V, F, ratio):
     if "3" in args.stages:
         from oracle import s3_cpu  # C++ FP32 restatement, OpenMP
 
-        v, f = stage3_stand_in(args.workload)
+        v, f = stage3_stand_in(args.workload, args.stages)
         st = {}
         t0 = time.perf_counter()
         s3_cpu.process(V, F, v, f, 5, stats=st)
