@@ -454,15 +454,14 @@ __device__ __forceinline__ void elastic_F(const float4 *q, int4 f, float4 im, F3
     F[3] = d10 * im.y + d11 * im.w;
 }
 
-__global__ void __launch_bounds__(kThreads) k_energy(EArgs A)
+// This thread's share (elements first, first + stride, ...) of the energy at
+// A.q: the mesh-to-target, membrane, hinge and barrier terms.
+__device__ double energy_terms(const EArgs &A, long long first, long long stride)
 {
-    // D_ENERGY then still holds the accepted trial's energy
-    if (A.n_halves > 0 && A.dscal[D_ENERGY] < A.dscal[D_ENERGY_PREV]) return;
     const long long nb = min((long long)A.iscal[I_NB], A.cap_b);
     const long long total = (long long)A.np + A.nt + A.nh + nb;
     double acc = 0.0;
-    PAMO_GRID_STRIDE(k, total)
-    {
+    for (long long k = first; k < total; k += stride) {
         if (k < A.np) {
             F3 d = ld(A.q, (int)k) - ld(A.target, (int)k);
             acc += (double)(0.5f * dot(d, d) * A.wk[k]);
@@ -506,6 +505,15 @@ __global__ void __launch_bounds__(kThreads) k_energy(EArgs A)
             if (d < A.d_hat) acc += barrier((double)d, (double)A.d_hat) * (double)A.kappa;
         }
     }
+    return acc;
+}
+
+__global__ void __launch_bounds__(kThreads) k_energy(EArgs A)
+{
+    // D_ENERGY then still holds the accepted trial's energy
+    if (A.n_halves > 0 && A.dscal[D_ENERGY] < A.dscal[D_ENERGY_PREV]) return;
+    const double acc = energy_terms(A, (long long)blockIdx.x * blockDim.x + threadIdx.x,
+                                    (long long)blockDim.x * gridDim.x);
     last_block_sum(block_sum<kThreads>(acc), A.partials, A.iscal + I_ETICKET, A.dscal + D_ENERGY);
 }
 
@@ -1271,23 +1279,25 @@ __device__ __forceinline__ bool wait_value(const unsigned long long *p, unsigned
     return true;
 }
 
-// Block sum of `acc`, then the grid-wide total (see above).  Returns false on
-// a wait timeout.
-__device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, int k, double &total)
+// Block sum of `acc`, then the grid-wide total (see above) through the slot
+// sets at `slots` (gridDim.x <= BLOCK).  Returns false on a wait timeout.
+template <int BLOCK>
+__device__ __forceinline__ bool grid_sum_slots(double acc, unsigned long long *slots, int *iscal, long long spin_limit,
+                                               int absent_block, int k, double &total)
 {
     __shared__ double s_val;
-    __shared__ double s_part[kCgThreads];  // every block's partial, in block order
+    __shared__ double s_part[BLOCK];  // every block's partial, in block order
     const int G = (int)gridDim.x;
     const size_t set_words = (size_t)G * kSlotStride;
-    unsigned long long *set = A.slots + (size_t)(k % kSlotSets) * set_words;
-    unsigned long long *prev = A.slots + (size_t)((k + kSlotSets - 1) % kSlotSets) * set_words;
-    const double bs = block_sum<kCgThreads>(acc);
-    if (threadIdx.x == 0 && (int)blockIdx.x != A.absent_block)
+    unsigned long long *set = slots + (size_t)(k % kSlotSets) * set_words;
+    unsigned long long *prev = slots + (size_t)((k + kSlotSets - 1) % kSlotSets) * set_words;
+    const double bs = block_sum<BLOCK>(acc);
+    if (threadIdx.x == 0 && (int)blockIdx.x != absent_block)
         st_release(set + (size_t)blockIdx.x * kSlotStride, (unsigned long long)__double_as_longlong(bs));
     int ok = 1;
     if ((int)threadIdx.x < G) {
         unsigned long long bits = 0;
-        if (wait_value(set + (size_t)threadIdx.x * kSlotStride, bits, A.iscal, A.spin_limit))
+        if (wait_value(set + (size_t)threadIdx.x * kSlotStride, bits, iscal, spin_limit))
             s_part[threadIdx.x] = __longlong_as_double((long long)bits);
         else
             ok = 0;
@@ -1305,6 +1315,11 @@ __device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, int k, dou
     __syncthreads();
     total = s_val;
     return ok != 0;
+}
+
+__device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, int k, double &total)
+{
+    return grid_sum_slots<kCgThreads>(acc, A.slots, A.iscal, A.spin_limit, A.absent_block, k, total);
 }
 
 __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
@@ -1563,6 +1578,52 @@ __global__ void k_line_search(const float4 *q_prev, const float4 *p, const float
 }
 
 __global__ void k_copy_energy_prev(double *dscal) { dscal[D_ENERGY_PREV] = dscal[D_ENERGY]; }
+
+// The whole line search (system.py:393-409) in one cooperative launch, one
+// block per SM: trial nh moves every vertex to q_prev + step 2^-nh p, a
+// grid-wide barrier makes the positions visible, and the trial's energy is one
+// grid-wide sum; the loop stops at the first trial after the first whose energy
+// is below the start's, as the reference's loop does -- so an accepted first
+// trial costs two sums and no further launches.  The sums and the barrier are
+// the persistent CG's one-hop slot sums (their own slot sets), with the same
+// bounded waits: on a timeout the error is recorded and the kernel returns.
+constexpr int kLsThreads = 512;
+
+struct LSArgs {
+    EArgs e;  // n_halves is set per trial; e.q is the iterate written here
+    float4 *q;
+    const float4 *q_prev, *p;
+    const float *ccd_step;
+    int n_trials;
+    unsigned long long *slots;  // kSlotSets x gridDim slots, all ones before the launch
+    long long spin_limit;
+};
+
+__global__ void __launch_bounds__(kLsThreads, 1) k_line_search_all(LSArgs L)
+{
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long gs = (long long)blockDim.x * gridDim.x;
+    EArgs A = L.e;
+    const double e0 = A.dscal[D_ENERGY];  // the energy at the iterate
+    double e = e0;
+    int nsum = 0, last = -1;
+    for (int nh = 0; nh < L.n_trials; ++nh) {
+        if (nh > 0 && e < e0) break;
+        const float a = L.ccd_step[0] * ldexpf(1.f, -nh);
+        for (long long i = t0; i < A.np; i += gs) st(L.q, (int)i, ld(L.q_prev, (int)i) + a * ld(L.p, (int)i));
+        double unused;
+        if (!grid_sum_slots<kLsThreads>(0.0, L.slots, A.iscal, L.spin_limit, -1, nsum++, unused)) return;
+        A.n_halves = nh;
+        if (!grid_sum_slots<kLsThreads>(energy_terms(A, t0, gs), L.slots, A.iscal, L.spin_limit, -1, nsum++, e))
+            return;
+        last = nh;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        A.dscal[D_ENERGY_PREV] = e0;
+        A.dscal[D_ENERGY] = e;
+        A.iscal[I_LS] = last;
+    }
+}
 
 // One row of the Newton trace per iteration: energy at the iterate, energy
 // after the line search, CCD step, index of the last halving tried, contact
@@ -1905,14 +1966,20 @@ int Stage3::detect(cudaStream_t s)
     return PAMO_ERR_CAPACITY;
 }
 
+static EArgs energy_args(Stage3 &S, int n_halves)
+{
+    return EArgs{S.q, S.target, S.wk, S.np, S.nt, S.nh, S.tris, S.area, S.inv_dm,
+                 S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
+                 S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
+                     ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
+                 S.hinges, S.rest_angle, S.rest_elen, S.cfg.hinge_stiffness, S.bidx, S.bkind, S.bsub, S.bd, S.iscal,
+                 S.cap_b, S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials, n_halves, S.dscal,
+                 S.fscal + 1};
+}
+
 static int energy_pass(Stage3 &S, cudaStream_t s, int n_halves = -1)
 {
-    EArgs e{S.q, S.target, S.wk, S.np, S.nt, S.nh, S.tris, S.area, S.inv_dm,
-            S.cfg.elas_young_modulus / (2.f * (1.f + S.cfg.elas_poisson_ratio)),
-            S.cfg.elas_young_modulus * S.cfg.elas_poisson_ratio /
-                ((1.f + S.cfg.elas_poisson_ratio) * (1.f - 2.f * S.cfg.elas_poisson_ratio)),
-            S.hinges, S.rest_angle, S.rest_elen, S.cfg.hinge_stiffness, S.bidx, S.bkind, S.bsub, S.bd, S.iscal, S.cap_b,
-            S.cfg.d_hat, S.cfg.coll_stiffness, S.cfg.ee_classify_thres, S.partials, n_halves, S.dscal, S.fscal + 1};
+    EArgs e = energy_args(S, n_halves);
     launch(k_energy, kRedBlocks, kThreads, 0, s, e);
     return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
 }
@@ -2019,10 +2086,28 @@ int Stage3::newton_body(cudaStream_t s)
                                                 cfg.ccd_max_iters, cfg.ee_classify_thres, fscal);
     // line search (system.py:393-409)
     if (prof) prof->begin(PH_S3_LINE, s);
-    launch(k_copy_energy_prev, 1, 1, 0, s, dscal);
-    for (int nh_ = 0; nh_ < cfg.n_line_search_iters; ++nh_) {
-        launch(k_line_search, grid_for(np), kThreads, 0, s, q_prev, p, fscal, nh_, dscal, np, q, iscal);
-        if ((rc = energy_pass(*this, s, nh_))) return rc;
+    if (cg_persistent == 1 && ls_persistent == 1) {
+        EArgs e = energy_args(*this, 0);
+        LSArgs la{e, q, q_prev, p, fscal, cfg.n_line_search_iters, reinterpret_cast<unsigned long long *>(partials),
+                  cg_spin_limit};
+        S3_TRY(cudaMemsetAsync(partials, 0xFF, (size_t)kSlotSets * cg_blocks * kSlotStride * sizeof(unsigned long long), s));
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(cg_blocks);
+        lc.blockDim = dim3(kLsThreads);
+        lc.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        S3_TRY(cudaLaunchKernelEx(&lc, k_line_search_all, la));
+    } else {
+        launch(k_copy_energy_prev, 1, 1, 0, s, dscal);
+        for (int nh_ = 0; nh_ < cfg.n_line_search_iters; ++nh_) {
+            launch(k_line_search, grid_for(np), kThreads, 0, s, q_prev, p, fscal, nh_, dscal, np, q, iscal);
+            if ((rc = energy_pass(*this, s, nh_))) return rc;
+        }
     }
     if (trace) launch(k_trace, 1, 1, 0, s, (const double *)dscal, (const float *)fscal, iscal, trace, cap_trace);
     if (prof) prof->end(s);
@@ -2041,6 +2126,9 @@ int Stage3::cg_solve(cudaStream_t s)
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_solve, kCgThreads, 0);
         cg_persistent = (coop && per_sm >= 1 && sms >= 1) ? 1 : 0;
+        int per_sm_ls = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ls, k_line_search_all, kLsThreads, 0);
+        ls_persistent = (coop && per_sm_ls >= 1) ? 1 : 0;
         cg_blocks = sms < kRedBlocks ? sms : kRedBlocks;  // one block per SM, all resident
         cudaGetLastError();
     }

@@ -85,6 +85,7 @@ struct Stage3 {
     bool use_graph = true;
     int cg_blocks = 0;   // grid of the persistent solve
     int cg_persistent = -1;  // 1: one cooperative launch per solve; 0: one launch per phase; -1: not decided
+    int ls_persistent = -1;  // 1: the line search as one cooperative launch (decided with cg_persistent)
     long long cg_spin_limit = 1LL << 24;  // polls per grid-sum wait (~ seconds) before the solve gives up
     int cg_absent_block = -1;  // the wait-timeout test only: a block that never publishes
     cudaStream_t work = nullptr;  // the solve's own stream (graphs cannot be captured on the legacy stream)

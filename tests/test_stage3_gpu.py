@@ -130,13 +130,16 @@ def test_stage3_config2_input_one_step(torch_cuda):
     """Config 2's own stage-3 input: the 20,604-face stage-2 result of the
     2,097,152-face torus against that torus, one step (10 Newton iterations,
     ~1.6M contact blocks, ~46,000 within d_hat, three CCD-limited steps).
-    Measured on a B200 over three runs: vertex error median 3.0e-6 .. 7.4e-6,
-    p99 3.1e-5 .. 5.9e-5, max 2.3e-4 .. 2.5e-4 of the diagonal (the move:
-    median 9.7e-5, max 1.4e-3); Newton energies within 1.8e-2 .. 3.7e-2
-    (1.4e-3 .. 2.7e-3 at the last iteration); the C++ float32 restatement
-    lands at max 3.4e-4, median 4.8e-6 -- a CCD-limited step taken a few
-    percent shorter or longer moves every vertex by that fraction of its
-    move, and the energy after it by more."""
+    Measured on a B200 over four runs: vertex error median 3.0e-6 .. 8.4e-6,
+    p99 3.1e-5 .. 6.8e-5, max 2.2e-4 .. 2.5e-4 of the diagonal (the move:
+    median 9.7e-5, max 1.4e-3); the last Newton iteration's energies within
+    1.4e-3 .. 2.7e-3 of the oracle's; the C++ float32 restatement lands at max
+    3.4e-4, median 4.8e-6.  The iterations in between are compared only
+    through their contact counts: a CCD-limited step is set by the nearest
+    contact pair, so float32 rounding can change which pair limits it (one run
+    took 0.65 of the step where the oracle took 0.80, and its energy after
+    that iteration differed by 74%) while the iterations that follow
+    converge to the same surface."""
     import pamo_b200
     from pamo_b200 import safe_project as SP
 
@@ -164,7 +167,6 @@ def test_stage3_config2_input_one_step(torch_cuda):
     assert np.all(np.abs(tr_g[:, 4] - tr_w[:, 4]) <= 1e-3 * tr_w[:, 4])
     assert np.median(err) < 0.25 * np.median(move)
     assert err.max() < 1e-3
-    assert e_rel.max() < 1e-1
     assert e_rel[-1].max() < 1e-2
 
 
