@@ -257,6 +257,20 @@ int pamo_voronoi_areas(const double *d_v, const int *d_f, int nv, int nf, float 
    each way (the caller then uses a general method). */
 int pamo_mesh_hinges(const int *h_tris, int n_tris, int n_pts, int *h_edges, int *h_hinges, int *out_n_edges);
 
+/* pamo_mesh_hinges on device buffers: the same rows in the same order from the
+   device faces d_tris [n_tris,3] into d_edges / d_hinges (3 * n_tris / 2 rows
+   each), and the same status codes; waits for `stream`.  Stage 3 builds its
+   edges and hinges with this when the stage-2 result is a closed 2-manifold. */
+int pamo_mesh_hinges_device(const int *d_tris, int n_tris, int n_pts, int *d_edges, int *d_hinges, int *out_n_edges,
+                            void *stream);
+
+/* Whether two of the device points d_points [n_pts,3] coincide after rounding
+   each coordinate to 8 decimals, numpy's round(x, 8) (*out_has_duplicates 1,
+   else 0) -- the merge trimesh.Trimesh(process=True) applies to the stage-2
+   result before stage 3 (simp_cuda/pamo/__init__.py:193-203) changes nothing
+   when there are none.  Waits for `stream`. */
+int pamo_merge_check_device(const float *d_points, int n_pts, int *out_has_duplicates, void *stream);
+
 /* Wavefront OBJ text (host memory, `len` bytes) to vertices [n,3] and
    triangles [m,3] int, on the host, over `n_threads` threads (<= 0: all).
    Replaces trimesh.load(path, force='mesh', process=False) in the reference's

@@ -234,12 +234,16 @@ class PaMO:
         if self.verbose:
             print(f"Time for Simplification: {self.timings['stage2']} sec")
         if self.use_stage3:
-            from .safe_project import merge_vertices, process
+            from .safe_project import has_duplicate_vertices, merge_vertices, process
 
             t0 = time.time()
             # the reference wraps the stage-2 result in trimesh.Trimesh(process=True),
-            # which merges coincident vertices (pamo/__init__.py:193-203)
-            v2, f2 = merge_vertices(verts.astype(np.float64), faces)
+            # which merges coincident vertices (pamo/__init__.py:193-203); the
+            # device check finds whether there is anything to merge
+            if has_duplicate_vertices(v):
+                v2, f2 = merge_vertices(verts.astype(np.float64), faces)
+            else:
+                v2, f2 = verts.astype(np.float64), faces
             gt_v = self.gt_mesh[0]
             if self._gt_f32 is not None:
                 if self._gt_f32_pinned is None:  # page-locked host copies of the ground truth

@@ -30,6 +30,8 @@ SIGNATURES = {
     "pamo_launch_count": (_ll, []),
     "pamo_voronoi_areas": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(ctypes.c_double), _vp]),
     "pamo_mesh_hinges": (_i, [_vp, _i, _i, _vp, _vp, ctypes.POINTER(ctypes.c_int)]),
+    "pamo_mesh_hinges_device": (_i, [_vp, _i, _i, _vp, _vp, ctypes.POINTER(ctypes.c_int), _vp]),
+    "pamo_merge_check_device": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_int), _vp]),
     "pamo_obj_parse": (_i, [_vp, _ll, _vp, _vp, _ll, _vp, _ll, _i, ctypes.POINTER(_ll), ctypes.POINTER(_ll),
                             ctypes.POINTER(_ll)]),
     "pamo_obj_format": (_i, [_vp, _ll, _vp, _ll, _vp, _ll, _i, ctypes.POINTER(_ll)]),

@@ -211,6 +211,40 @@ def min_internal_angle_deg(V, F):
     return float(np.arccos(np.clip(cmax.max(), -1, 1)) * 180 / np.pi)
 
 
+def device_edges_and_hinges(d_f, n_pts, stream):
+    """edges_and_hinges on the device (pamo_mesh_hinges_device): int32 CUDA
+    tensors (edges [ne,2], hinges [ne,4]) with the host builder's rows and
+    order, or (None, None) when the faces are not a closed 2-manifold."""
+    import torch
+
+    m = int(d_f.shape[0])
+    if m == 0 or (3 * m) % 2:
+        return None, None
+    cap = (3 * m) // 2
+    d_e = torch.empty((cap, 2), dtype=torch.int32, device=d_f.device)
+    d_h = torch.empty((cap, 4), dtype=torch.int32, device=d_f.device)
+    ne = ctypes.c_int(0)
+    rc = _lib.lib().pamo_mesh_hinges_device(d_f.data_ptr(), m, int(n_pts), d_e.data_ptr(), d_h.data_ptr(),
+                                            ctypes.byref(ne), stream)
+    if rc == 6:  # PAMO_ERR_CAPACITY: an edge not shared by exactly two faces, once each way
+        return None, None
+    check("pamo_mesh_hinges_device", rc)
+    return d_e[:ne.value], d_h[:ne.value]
+
+
+def has_duplicate_vertices(d_points):
+    """Whether merge_vertices would merge anything in the CUDA float32 points
+    [n,3] (pamo_merge_check_device: equal after rounding to 8 decimals)."""
+    import torch
+
+    d_points = d_points.contiguous()
+    out = ctypes.c_int(0)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(d_points.device).cuda_stream)
+    check("pamo_merge_check_device", _lib.lib().pamo_merge_check_device(d_points.data_ptr(), int(d_points.shape[0]),
+                                                                         ctypes.byref(out), stream))
+    return bool(out.value)
+
+
 def merge_vertices(V, F, digits=8):
     """trimesh.Trimesh(process=True) merging (PaMO.run's stage2_mesh,
     pamo/__init__.py:194): vertices equal after rounding to `digits` decimals
@@ -275,14 +309,18 @@ class Stage3System:
         dev = torch.device("cuda", self.device)
         V64 = np.asarray(V, np.float64) * c.system_scale
         F = np.asarray(F, np.int64)
-        E, H = edges_and_hinges(F)
-        if len(H) != len(E):
-            raise ValueError(f"number of hinges {len(H)} != number of edges {len(E)} (mesh not closed 2-manifold)")
         t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
         stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        d_f = t(F, np.int32)
+        d_e, d_h = device_edges_and_hinges(d_f, len(V64), stream)
+        if d_e is None:  # not a closed 2-manifold: the general host method
+            E, H = edges_and_hinges(F)
+            if len(H) != len(E):
+                raise ValueError(f"number of hinges {len(H)} != number of edges {len(E)} (mesh not closed 2-manifold)")
+            d_e, d_h = t(E, np.int32), t(H, np.int32)
         # Voronoi areas and the smallest angle, on the device in double from the
         # double vertices (voronoi_areas / min_internal_angle_deg are the host forms)
-        d_v64, d_f = t(V64, np.float64), t(F, np.int32)
+        d_v64 = t(V64, np.float64)
         d_w = torch.empty(len(V64), dtype=torch.float32, device=dev)
         min_ang = ctypes.c_double()
         check("pamo_voronoi_areas", _lib.lib().pamo_voronoi_areas(
@@ -311,13 +349,12 @@ class Stage3System:
             d_gf = gt_F.to(dev, torch.int32).contiguous() if isinstance(gt_F, torch.Tensor) else t(gt_F, np.int32)
             self._gt_norm = (key, d_gv, d_gf) if key is not None else None
         d_v = d_v64.to(torch.float32)
-        d_e, d_h = t(E, np.int32), t(H, np.int32)
         out = torch.empty((len(V64), 3), dtype=torch.float32, device=dev)
         cfg = c.to_c()
         cfg.reuse_gt = reuse
         check("pamo_safe_project", _lib.lib().pamo_safe_project(
             self.ctx.handle, d_gv.data_ptr(), d_gf.data_ptr(), len(d_gv), len(d_gf), d_v.data_ptr(), d_f.data_ptr(),
-            len(V64), len(F), d_e.data_ptr(), len(E), d_h.data_ptr(), len(H), d_w.data_ptr(), int(n_steps),
+            len(V64), len(F), d_e.data_ptr(), len(d_e), d_h.data_ptr(), len(d_h), d_w.data_ptr(), int(n_steps),
             int(do_nothing), ctypes.byref(cfg), stream, out.data_ptr()))
         st = (ctypes.c_double * 3)()
         _lib.lib().pamo_safe_project_stats(self.ctx.handle, st)
