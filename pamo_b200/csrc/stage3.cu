@@ -2000,9 +2000,11 @@ void Stage3::drop_graph()
 int Stage3::newton(cudaStream_t s)
 {
     S3_TRY(cudaMemcpyAsync(q_prev, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
-    if (prof) prof->begin(PH_S3_DETECT, s);
-    int rc = detect(s);
+    int rc = newton_elements(s);
     if (rc) return rc;
+    if (prof) prof->begin(PH_S3_DETECT, s);
+    if ((rc = detect(s))) return rc;
+    if ((rc = newton_contacts(s))) return rc;
     const bool timed = prof && prof->on;
     if (timed || !use_graph) return newton_body(s);
     if (!graph || graph_cap_b != cap_b) {
@@ -2040,40 +2042,62 @@ int Stage3::newton(cudaStream_t s)
     return PAMO_OK;
 }
 
-int Stage3::newton_body(cudaStream_t s)
+static DArgs diff_args(Stage3 &S)
 {
-    int rc;
+    const pamo_s3_config &c = S.cfg;
+    return DArgs{S.q, S.nt, S.nh, S.tris, S.area, S.inv_dm, c.elas_young_modulus / (2.f * (1.f + c.elas_poisson_ratio)),
+                 c.elas_young_modulus * c.elas_poisson_ratio /
+                     ((1.f + c.elas_poisson_ratio) * (1.f - 2.f * c.elas_poisson_ratio)),
+                 S.hinges, S.rest_angle, S.rest_elen, c.hinge_stiffness, c.spd_max_iters, S.kval, S.tri_slot,
+                 S.hinge_slot, S.hblk, S.bidx, S.bkind, S.bsub, S.bd, S.bg, S.bb2, S.iscal, S.cap_b, c.d_hat,
+                 c.coll_stiffness, S.grad, S.diag, S.bact};
+}
+
+// The element terms that do not depend on the contacts -- the vertex term, the
+// membranes, and the hinges with their SPD projection -- all adding into grad,
+// diag and the Hessian's values by atomics.  They are issued before detection,
+// which leaves q, grad, diag and the Hessian alone: the hinge branch runs on
+// side[1] while the host waits for detection's counts.
+int Stage3::newton_elements(cudaStream_t s)
+{
     if (prof) prof->begin(PH_S3_DIFF, s);
     S3_TRY(cudaMemcpyAsync(q_det, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
     // gradient (coefficient -1) and diagonal
     launch(k_diff_vertex, grid_for(np), kThreads, 0, s, q, target, wk, np, grad, diag);
-    DArgs d{q, nt, nh, tris, area, inv_dm, cfg.elas_young_modulus / (2.f * (1.f + cfg.elas_poisson_ratio)),
-            cfg.elas_young_modulus * cfg.elas_poisson_ratio /
-                ((1.f + cfg.elas_poisson_ratio) * (1.f - 2.f * cfg.elas_poisson_ratio)),
-            hinges, rest_angle, rest_elen, cfg.hinge_stiffness, cfg.spd_max_iters, kval, tri_slot, hinge_slot, hblk, bidx,
-            bkind, bsub, bd, bg, bb2, iscal, cap_b, cfg.d_hat, cfg.coll_stiffness, grad, diag, bact};
+    const DArgs d = diff_args(*this);
     // the Hessian's values: zero and the vertex term, then the elements
     S3_TRY(cudaMemsetAsync(kval, 0, (size_t)nnz * 48, s));
     launch(k_diag_term, grid_for(np), kThreads, 0, s, (const float *)wk, (const int *)diag_slot, np, kval);
-    S3_TRY(cudaMemsetAsync(iscal + I_NACT, 0, sizeof(int), s));
-    // Three independent branches, all adding into grad, diag and the Hessian's
-    // values by atomics: [energy at the iterate (the blocks' distances and
-    // classes) -> contact terms] and [hinge terms -> their SPD projection] on
-    // the side streams, the membranes here; they meet before the solve.
     S3_TRY(cudaEventRecord(ev_fork, s));
-    for (int b = 0; b < 2; ++b) S3_TRY(cudaStreamWaitEvent(side[b], ev_fork, 0));
-    if ((rc = energy_pass(*this, side[0]))) return rc;
-    launch(k_diff_part<2>, grid_for(cap_b, 128), 128, 0, side[0], d);
+    S3_TRY(cudaStreamWaitEvent(side[1], ev_fork, 0));
     if (nh > 0) {
         launch(k_diff_part<1>, grid_for(nh, 128), 128, 0, side[1], d);
         launch(k_hinge_spd, (int)((nh + 63) / 64), 64, 0, side[1], (const float *)hblk, nh, cfg.spd_max_iters,
                (const int *)hinge_slot, kval);
     }
     launch(k_diff_part<0>, grid_for(nt, 128), 128, 0, s, d);
-    for (int b = 0; b < 2; ++b) {
-        S3_TRY(cudaEventRecord(ev_join[b], side[b]));
-        S3_TRY(cudaStreamWaitEvent(s, ev_join[b], 0));
-    }
+    S3_TRY(cudaEventRecord(ev_join[1], side[1]));
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+// After detection: the energy at the iterate (which fixes the contact blocks'
+// distances and classes), the contact terms, and the join with the hinge
+// branch.
+int Stage3::newton_contacts(cudaStream_t s)
+{
+    int rc;
+    if (prof) prof->begin(PH_S3_DIFF, s);
+    S3_TRY(cudaMemsetAsync(iscal + I_NACT, 0, sizeof(int), s));
+    if ((rc = energy_pass(*this, s))) return rc;
+    launch(k_diff_part<2>, grid_for(cap_b, 128), 128, 0, s, diff_args(*this));
+    S3_TRY(cudaStreamWaitEvent(s, ev_join[1], 0));
+    return cudaGetLastError() == cudaSuccess ? PAMO_OK : PAMO_ERR_DEVICE;
+}
+
+// The solve, the CCD and the line search: one CUDA graph per registration.
+int Stage3::newton_body(cudaStream_t s)
+{
+    int rc;
     // Jacobi-preconditioned CG (cg_solver.py:96-158)
     if (prof) prof->begin(PH_S3_CG, s);
     if ((rc = cg_solve(s))) return rc;

@@ -106,6 +106,8 @@ struct Stage3 {
                       const float *d_vor, cudaStream_t s);
     int step(cudaStream_t s);
     int newton(cudaStream_t s);
+    int newton_elements(cudaStream_t s);
+    int newton_contacts(cudaStream_t s);
     int newton_body(cudaStream_t s);
     int detect(cudaStream_t s);
     int cg_solve(cudaStream_t s);
