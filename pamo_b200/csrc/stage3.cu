@@ -531,12 +531,6 @@ __global__ void k_diff_vertex(const float4 *q, const float4 *target, const float
     }
 }
 
-__device__ __forceinline__ void mat3_zero(float *m)
-{
-#pragma unroll
-    for (int k = 0; k < 9; ++k) m[k] = 0.f;
-}
-
 // Hinge gradient and Hessian blocks (Tamstorf & Grinspun 2013, in the form of
 // hinge_energy.py:91-254): writes the 16 row-major 3x3 blocks into B.
 __device__ void hinge_blocks(F3 x0, F3 x1, F3 x2, F3 x3, float rest_angle, float rest_elen, float k, F3 g[4],
@@ -1203,48 +1197,49 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const f
 }
 
 // The whole Jacobi-PCG solve of a Newton iteration (the 40 iterations of
-// cg_solver.py:96-158) in one cooperative launch, one block per SM and two
-// grid-wide sums per iteration:
-//   (B) the new direction v = z + beta v is formed where it is read -- every
-//       row and contact block computes it for its own vertices from z and the
-//       last direction (both final since the previous sum), and each row's
-//       owner stores it into the other direction buffer -- while the rows of
-//       K v go to Av, the contact terms are added into Avc (zeroed by the owner
-//       in the previous pass), and v . A v is gathered;
-//   (D) p += alpha v, r -= alpha (Av + Avc), z = r / diag, Avc = 0, and z . r.
-// The time of an iteration is the length of its chains of dependent memory
+// cg_solver.py:96-158) in one cooperative launch, one block per SM and one
+// grid-wide sum per iteration.  The reference's iteration
+//     Av = A v; alpha = (z.r) / (v.Av); p += alpha v; r -= alpha Av;
+//     z = r / diag; v = z + ((z.r)_new / (z.r)) v
+// needs v.Av before the update and z.r after it: two sums.  Here (the
+// single-reduction form of Chronopoulos and Gear, 1989) A v is carried by the
+// recurrence A v_i = A z_i + beta A v_{i-1}, and v.Av by the identity
+//     v_i.Av_i = z_i.(A z_i) + 2 beta z_i.(A v_{i-1}) + beta^2 v_{i-1}.(A v_{i-1}),
+// which holds for any symmetric A whatever the preconditioner, so the first
+// iteration's diag + 1e-6 is kept as the reference has it; the guard
+// v.Av > 1e-16 and the update order are the reference's.  An iteration is one
+// pass: every vertex keeps a record of three float4 per iteration parity --
+// z_i (= r_i / diag), the rows of A z_i / diag and A v_{i-1} / diag -- so a
+// row gathers one record per column, forms z_{i+1} there
+//     z_{i+1} = z_i - alpha (A z_i / diag + beta A v_{i-1} / diag),
+// and computes its row of A z_{i+1}; the contact blocks add their rank-one
+// terms (scaled by 1 / diag) into a separate buffer (three copies: read,
+// accumulated, zeroed for the one after); the three dot products of the next
+// iteration, z.r = sum diag z^2, z.(A z) and z.(A v_i), go into one sum.  The
+// time of an iteration is the length of its chains of dependent memory
 // accesses, so what stays fixed during the solve is read once: each lane keeps
-// the columns of its first row slots in registers, and the contact count is
-// read at the start.
+// the columns of its first row slots in registers.
 //
-// A sum: every block writes its partial with a release store into its own slot
-// of the sum's set (three sets, used in turn; slots hold an all-ones pattern
+// A sum: every block writes its partials into its own slot of the sum's set
+// (three sets, used in turn; a slot's first word holds an all-ones pattern
 // until written: a negative NaN that no sum produces, since sums and products
-// give the positive canonical NaN), then waits for all slots of the set with
-// acquire loads, one thread per slot, and adds them in block order -- the same
-// order in every block, so every block gets the same total, independent of
-// scheduling, with one hop between the blocks.  A block's writes before its
-// partial are visible to every block after the sum.  Once a block has seen all
-// partials of sum k, every block has finished reading sum k - 1, so it resets
-// its own slot of that set, which sum k + 2 reuses (the reset precedes its
-// release of sum k + 1, which every reader of sum k + 2 has acquired).  Slots
-// sit one 128-byte line apart.  Waits spin with a limit; on timeout the error
-// is recorded and the kernel returns.
+// give the positive canonical NaN; the other words are written before the
+// first, which is stored with release semantics), then waits for all slots of
+// the set with acquire loads, one thread per slot, and adds them in block
+// order -- the same order in every block, so every block gets the same totals,
+// independent of scheduling, with one hop between the blocks.  A block's
+// writes before its partials are visible to every block after the sum.  Once
+// a block has seen all partials of sum k, every block has finished reading sum
+// k - 1, so it resets its own slot of that set, which sum k + 2 reuses (the
+// reset precedes its release of sum k + 1, which every reader of sum k + 2 has
+// acquired).  Slots sit one 128-byte line apart.  Waits spin with a limit; on
+// timeout the error is recorded and the kernel returns.  The line search uses
+// the same sums for its barrier and energy.
 constexpr int kCgThreads = 512;
 constexpr unsigned long long kSumPending = ~0ull;
 constexpr int kSlotStride = 16;  // u64 words per slot
 constexpr int kSlotSets = 3;
 
-struct CGArgs {
-    OpArgs op;
-    const float4 *grad, *diag;
-    float4 *p, *r, *z, *v0, *v1, *Av, *Avc;
-    unsigned long long *slots;  // kSlotSets x gridDim slots, kSlotStride apart (all ones before the solve)
-    int *iscal;
-    int np, n_iters;
-    long long spin_limit;  // polls per wait before it gives up
-    int absent_block;      // >= 0: that block never publishes its partials (the wait-timeout test); else -1
-};
 
 __device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v)
 {
@@ -1317,9 +1312,102 @@ __device__ __forceinline__ bool grid_sum_slots(double acc, unsigned long long *s
     return ok != 0;
 }
 
-__device__ __forceinline__ bool grid_sum(double acc, const CGArgs &A, int k, double &total)
+struct CGArgs {
+    OpArgs op;
+    const float4 *grad, *diag;
+    float4 *x, *v;
+    float4 *rec0, *rec1;      // the records of even and odd iterations, 3 float4 per vertex
+    float4 *wc0, *wc1, *wc2;  // contact part of A z / diag, three copies, zero before the solve
+    unsigned long long *slots;  // kSlotSets x gridDim slots, kSlotStride apart (all ones before the solve)
+    int *iscal;
+    int np, n_iters;
+    long long spin_limit;  // polls per wait before it gives up
+    int absent_block;      // >= 0: that block never publishes its partials (the wait-timeout test); else -1
+};
+
+struct D3s {
+    double a, b, c;
+};
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
 {
-    return grid_sum_slots<kCgThreads>(acc, A.slots, A.iscal, A.spin_limit, A.absent_block, k, total);
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// three block sums, then the grid-wide totals: a slot's words 1 and 2 are
+// written first, word 0 last with a release store; readers acquire word 0
+__device__ __forceinline__ bool grid_sum3(D3s acc, const CGArgs &A, int k, D3s &total)
+{
+    __shared__ double ws[3][kCgThreads / 32];
+    __shared__ double s_part[3][kCgThreads];
+    __shared__ D3s s_val;
+    const int G = (int)gridDim.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        acc.a += __shfl_down_sync(0xffffffffu, acc.a, o);
+        acc.b += __shfl_down_sync(0xffffffffu, acc.b, o);
+        acc.c += __shfl_down_sync(0xffffffffu, acc.c, o);
+    }
+    if (lane == 0) {
+        ws[0][wid] = acc.a;
+        ws[1][wid] = acc.b;
+        ws[2][wid] = acc.c;
+    }
+    __syncthreads();
+    const size_t set_words = (size_t)G * kSlotStride;
+    unsigned long long *set = A.slots + (size_t)(k % kSlotSets) * set_words;
+    unsigned long long *prev = A.slots + (size_t)((k + kSlotSets - 1) % kSlotSets) * set_words;
+    if (wid == 0) {
+        double ra = lane < kCgThreads / 32 ? ws[0][lane] : 0.0;
+        double rb = lane < kCgThreads / 32 ? ws[1][lane] : 0.0;
+        double rc = lane < kCgThreads / 32 ? ws[2][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            ra += __shfl_down_sync(0xffffffffu, ra, o);
+            rb += __shfl_down_sync(0xffffffffu, rb, o);
+            rc += __shfl_down_sync(0xffffffffu, rc, o);
+        }
+        if (lane == 0 && (int)blockIdx.x != A.absent_block) {
+            unsigned long long *slot = set + (size_t)blockIdx.x * kSlotStride;
+            st_relaxed(slot + 1, (unsigned long long)__double_as_longlong(rb));
+            st_relaxed(slot + 2, (unsigned long long)__double_as_longlong(rc));
+            st_release(slot, (unsigned long long)__double_as_longlong(ra));
+        }
+    }
+    int ok = 1;
+    if ((int)threadIdx.x < G) {
+        const unsigned long long *slot = set + (size_t)threadIdx.x * kSlotStride;
+        unsigned long long bits = 0;
+        if (wait_value(slot, bits, A.iscal, A.spin_limit)) {
+            s_part[0][threadIdx.x] = __longlong_as_double((long long)bits);
+            s_part[1][threadIdx.x] = __longlong_as_double((long long)ld_relaxed_u64(slot + 1));
+            s_part[2][threadIdx.x] = __longlong_as_double((long long)ld_relaxed_u64(slot + 2));
+        } else {
+            ok = 0;
+        }
+    }
+    ok = __syncthreads_and(ok);
+    if (threadIdx.x < 32) {
+        double va = 0.0, vb = 0.0, vc = 0.0;
+        for (int i = threadIdx.x; i < G; i += 32) {
+            va += s_part[0][i];
+            vb += s_part[1][i];
+            vc += s_part[2][i];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            va += __shfl_down_sync(0xffffffffu, va, o);
+            vb += __shfl_down_sync(0xffffffffu, vb, o);
+            vc += __shfl_down_sync(0xffffffffu, vc, o);
+        }
+        if (threadIdx.x == 0) {
+            s_val = D3s{va, vb, vc};
+            if (ok) st_relaxed(prev + (size_t)blockIdx.x * kSlotStride, kSumPending);
+        }
+    }
+    __syncthreads();
+    total = s_val;
+    return ok != 0;
 }
 
 __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
@@ -1330,8 +1418,6 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
     const long long warp0 = t0 >> 5, nwarps = gs >> 5;
     const OpArgs &O = A.op;
     const long long nb = min((long long)A.iscal[I_NACT], O.cap_b);
-    // this lane's first row (eight rows per warp, four lanes per row) and the
-    // columns of its first four slots, kept for the whole solve
     constexpr int kRowBatch = 4;
     const long long i0 = warp0 * 8 + (lane >> 2);
     int s0 = 0, e0 = 0, c0[kRowBatch];
@@ -1341,47 +1427,19 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
     }
 #pragma unroll
     for (int k = 0; k < kRowBatch; ++k) c0[k] = s0 + 4 * k < e0 ? O.col[s0 + 4 * k] : -1;
-    // contact blocks are taken from the top of the grid down, by threads that
-    // hold no rows when there are few of them; a thread's first block (index,
-    // curvature, vertices) is kept for the whole solve
     const long long tc = gs - 1 - t0;
-    int cb0 = -1;
-    float cc0 = 0.f;
-    int4 ci0 = make_int4(0, 0, 0, 0);
-    if (tc < nb) {
-        cb0 = O.bact[tc];
-        cc0 = O.bb2[cb0];
-        ci0 = O.bidx[cb0];
-    }
-    // r = g, z = g / (diag + 1e-6), p = 0, Avc = 0
-    double acc = 0.0;
-    for (long long i = t0; i < A.np; i += gs) {
-        F3 g = ld(A.grad, (int)i), d = ld(A.diag, (int)i);
-        F3 zz = mk(g.x / (d.x + 1e-6f), g.y / (d.y + 1e-6f), g.z / (d.z + 1e-6f));
-        A.p[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        A.Avc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        st(A.r, (int)i, g);
-        st(A.z, (int)i, zz);
-        acc += (double)dot(zz, g);
-    }
-    double zr, zr_last, vav;
-    int nsum = 0;
-    if (!grid_sum(acc, A, nsum++, zr)) return;
-    zr_last = zr;
-    for (int it = 0; it < A.n_iters; ++it) {
-        const float beta = it == 0 ? 0.f : (float)(zr / zr_last);
-        const float4 *vo = (it & 1) ? A.v1 : A.v0;  // last direction
-        float4 *vn = (it & 1) ? A.v0 : A.v1;        // this one
-        const float4 *z = A.z;
-        auto dir = [&](int j) -> F3 {
-            if (it == 0) return ld(z, j);
-            return ld(z, j) + beta * ld(vo, j);
-        };
-        acc = 0.0;
-        // rows of K v: every load of a lane's row slots, and the row owner's own
-        // direction, issued before any use
+    const float4 *diag = A.diag;
+
+    // rows of K z (z(k) at column k) into the owner's record, scaled by 1 / diag;
+    // contact terms (scaled by 1 / diag at each vertex) into wcout; returns this
+    // thread's share of z . (K z + contacts)
+    auto pass = [&](auto zn, auto own, float4 *recout, float4 *wcout, bool spmv) -> double {
+        double zw = 0.0;
         for (long long base = warp0 * 8, g = 0; base < A.np; base += nwarps * 8, ++g) {
             const long long i = base + (lane >> 2);
+            F3 zi = mk(0.f, 0.f, 0.f);
+            if (i < A.np && sub == 0) zi = own((int)i);
+            if (!spmv) continue;
             int s = s0, e = e0, cidx[kRowBatch];
             if (g == 0) {
 #pragma unroll
@@ -1396,22 +1454,23 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
 #pragma unroll
                 for (int k = 0; k < kRowBatch; ++k) cidx[k] = s + 4 * k < e ? O.col[s + 4 * k] : -1;
             }
-            F3 x[kRowBatch];
+            F3 xz[kRowBatch];
 #pragma unroll
-            for (int k = 0; k < kRowBatch; ++k) x[k] = cidx[k] >= 0 ? dir(cidx[k]) : mk(0.f, 0.f, 0.f);
-            const F3 own = (i < A.np && sub == 0) ? dir((int)i) : mk(0.f, 0.f, 0.f);
+            for (int k = 0; k < kRowBatch; ++k) xz[k] = cidx[k] >= 0 ? zn(cidx[k]) : mk(0.f, 0.f, 0.f);
             F3 kv = mk(0.f, 0.f, 0.f);
 #pragma unroll
             for (int k = 0; k < kRowBatch; ++k) {
                 if (cidx[k] < 0) continue;
                 const size_t b = 3 * (size_t)(s + 4 * k);
                 const float4 k0 = O.kval[b], k1 = O.kval[b + 1], k2 = O.kval[b + 2];
-                kv = kv + mk(k0.x * x[k].x + k0.y * x[k].y + k0.z * x[k].z, k1.x * x[k].x + k1.y * x[k].y + k1.z * x[k].z,
-                             k2.x * x[k].x + k2.y * x[k].y + k2.z * x[k].z);
+                kv = kv + mk(k0.x * xz[k].x + k0.y * xz[k].y + k0.z * xz[k].z,
+                             k1.x * xz[k].x + k1.y * xz[k].y + k1.z * xz[k].z,
+                             k2.x * xz[k].x + k2.y * xz[k].y + k2.z * xz[k].z);
             }
-            for (int ss = s + 4 * kRowBatch; ss < e; ss += 4) {  // rows longer than 4 x kRowBatch
-                const F3 xx = dir(O.col[ss]);
-                const float4 k0 = O.kval[3 * (size_t)ss], k1 = O.kval[3 * (size_t)ss + 1], k2 = O.kval[3 * (size_t)ss + 2];
+            for (int ss = s + 4 * kRowBatch; ss < e; ss += 4) {
+                const F3 xx = zn(O.col[ss]);
+                const float4 k0 = O.kval[3 * (size_t)ss], k1 = O.kval[3 * (size_t)ss + 1],
+                             k2 = O.kval[3 * (size_t)ss + 2];
                 kv = kv + mk(k0.x * xx.x + k0.y * xx.y + k0.z * xx.z, k1.x * xx.x + k1.y * xx.y + k1.z * xx.z,
                              k2.x * xx.x + k2.y * xx.y + k2.z * xx.z);
             }
@@ -1422,52 +1481,123 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
                 kv.z += __shfl_xor_sync(0xffffffffu, kv.z, o);
             }
             if (i < A.np && sub == 0) {
-                st(vn, (int)i, own);
-                st(A.Av, (int)i, kv);
-                acc += (double)dot(own, kv);
+                const F3 d = ld(diag, (int)i);
+                st(recout + 3 * (size_t)i + 1, 0, mk(kv.x / d.x, kv.y / d.y, kv.z / d.z));
+                zw += (double)dot(zi, kv);
             }
         }
+        if (!spmv) return zw;
         for (long long k = tc; k < nb; k += gs) {
-            int b = cb0;
-            float c = cc0;
-            int4 i4 = ci0;
-            if (k != tc) {
-                b = O.bact[k];
-                c = O.bb2[b];
-                i4 = O.bidx[b];
-            }
+            const int b = O.bact[k];
+            const float c = O.bb2[b];
             if (c == 0.f) continue;
+            const int4 i4 = O.bidx[b];
             const int idx[4] = {i4.x, i4.y, i4.z, i4.w};
             F3 g[4];
             float sdx = 0.f;
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
                 g[a] = f3(O.bg[4 * (size_t)b + a]);
-                sdx += dot(g[a], dir(idx[a]));
+                sdx += dot(g[a], zn(idx[a]));
             }
 #pragma unroll
-            for (int a = 0; a < 4; ++a) atomic_add3(A.Avc, idx[a], (c * sdx) * g[a]);
-            acc += (double)(c * sdx) * (double)sdx;
-        }
-        if (!grid_sum(acc, A, nsum++, vav)) return;
-        zr_last = zr;
-        const bool upd = vav > 1e-16;
-        const float alpha = upd ? (float)(zr_last / vav) : 0.f;
-        acc = 0.0;
-        for (long long i = t0; i < A.np; i += gs) {
-            F3 rr = ld(A.r, (int)i);
-            if (upd) {
-                st(A.p, (int)i, ld(A.p, (int)i) + alpha * ld(vn, (int)i));
-                rr = rr - alpha * (ld(A.Av, (int)i) + ld(A.Avc, (int)i));
-                st(A.r, (int)i, rr);
+            for (int a = 0; a < 4; ++a) {
+                const F3 d = ld(diag, idx[a]);
+                const F3 t = (c * sdx) * g[a];
+                atomic_add3(wcout, idx[a], mk(t.x / d.x, t.y / d.y, t.z / d.z));
             }
-            A.Avc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            F3 d = ld(A.diag, (int)i);
-            F3 zz = mk(rr.x / d.x, rr.y / d.y, rr.z / d.z);
-            st(A.z, (int)i, zz);
-            acc += (double)dot(zz, rr);
+            zw += (double)(c * sdx) * (double)sdx;
         }
-        if (!grid_sum(acc, A, nsum++, zr)) return;
+        return zw;
+    };
+
+    // pass 0: x = 0; record 0 = (g / diag, rows of K z_0 / diag, 0) with
+    // z_0 = g / (diag + 1e-6)
+    D3s acc{0.0, 0.0, 0.0};
+    {
+        auto z0 = [&](int k) -> F3 {
+            const F3 g = ld(A.grad, k), d = ld(diag, k);
+            return mk(g.x / (d.x + 1e-6f), g.y / (d.y + 1e-6f), g.z / (d.z + 1e-6f));
+        };
+        auto own0 = [&](int j) -> F3 {
+            const F3 g = ld(A.grad, j), d = ld(diag, j);
+            A.x[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            st(A.rec0 + 3 * (size_t)j, 0, mk(g.x / d.x, g.y / d.y, g.z / d.z));
+            st(A.rec0 + 3 * (size_t)j + 2, 0, mk(0.f, 0.f, 0.f));
+            const F3 z = z0(j);
+            acc.a += (double)dot(z, g);
+            return z;
+        };
+        acc.b = pass(z0, own0, A.rec0, A.wc0, true);
+    }
+    D3s sums;
+    int nsum = 0;
+    if (!grid_sum3(acc, A, nsum++, sums)) return;
+    double gam = sums.a, del = sums.b, eps = 0.0, gam_prev = 0.0, vav = 0.0;
+    for (int it = 0; it < A.n_iters; ++it) {
+        float beta = 0.f;
+        if (it == 0) {
+            vav = del;
+        } else {
+            beta = (float)(gam / gam_prev);
+            const double bd = (double)beta;
+            vav = del + 2.0 * bd * eps + bd * bd * vav;
+        }
+        const bool upd = vav > 1e-16;
+        const float alpha = upd ? (float)(gam / vav) : 0.f;
+        const bool odd = it & 1;
+        const float4 *rc = odd ? A.rec1 : A.rec0;
+        float4 *rn = odd ? A.rec0 : A.rec1;
+        const int m3 = it % 3;
+        const float4 *wcc = m3 == 0 ? A.wc0 : m3 == 1 ? A.wc1 : A.wc2;
+        float4 *wcn = m3 == 0 ? A.wc1 : m3 == 1 ? A.wc2 : A.wc0;
+        float4 *wcz = m3 == 0 ? A.wc2 : m3 == 1 ? A.wc0 : A.wc1;
+        const bool last = it == A.n_iters - 1;
+        const bool contacts = nb > 0;
+        // A v_i / diag and z_{i+1} at vertex k from its record
+        auto avs = [&](const float4 *R, int k) -> F3 {
+            F3 w = f3(R[1]);
+            if (contacts) w = w + ld(wcc, k);
+            return it == 0 ? w : w + beta * f3(R[2]);
+        };
+        auto zn = [&](int k) -> F3 {
+            const float4 *R = rc + 3 * (size_t)k;
+            const F3 r = f3(R[0]);
+            return upd ? r - alpha * avs(R, k) : r;
+        };
+        acc = D3s{0.0, 0.0, 0.0};
+        auto own = [&](int j) -> F3 {
+            const float4 *R = rc + 3 * (size_t)j;
+            const F3 d = ld(diag, j);
+            F3 zc;
+            if (it == 0) {
+                const F3 g = ld(A.grad, j);
+                zc = mk(g.x / (d.x + 1e-6f), g.y / (d.y + 1e-6f), g.z / (d.z + 1e-6f));
+            } else {
+                zc = f3(R[0]);
+            }
+            const F3 vj = it == 0 ? zc : zc + beta * ld(A.v, j);
+            const F3 av = avs(R, j);
+            const F3 r0 = f3(R[0]);
+            const F3 z = upd ? r0 - alpha * av : r0;
+            if (upd) st(A.x, j, ld(A.x, j) + alpha * vj);
+            if (!last) {
+                st(A.v, j, vj);
+                st(rn + 3 * (size_t)j, 0, z);
+                st(rn + 3 * (size_t)j + 2, 0, av);
+                if (contacts) wcz[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                acc.a += (double)(d.x * z.x * z.x + d.y * z.y * z.y + d.z * z.z * z.z);
+                acc.c += (double)(z.x * av.x * d.x + z.y * av.y * d.y + z.z * av.z * d.z);
+            }
+            return z;
+        };
+        acc.b = pass(zn, own, rn, wcn, !last);
+        if (last) break;
+        if (!grid_sum3(acc, A, nsum++, sums)) return;
+        gam_prev = gam;
+        gam = sums.a;
+        del = sums.b;
+        eps = sums.c;
     }
 }
 
@@ -1692,7 +1822,7 @@ __global__ void k_f4_to_aos(const float4 *in, float *out, int n)
 void Stage3::release()
 {
     gt_ready = false;
-    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, v2, Av, Avc, q_gather, wk, tris, area, inv_dm,
+    void *ptrs[] = {q, q_prev, q_det, p, grad, diag, target, r, z, v, v2, Av, Avc, cg_rec, q_gather, wk, tris, area, inv_dm,
                     edges4, hinges, rest_angle, rest_elen, row_ptr, col, kval, tri_slot, hinge_slot, diag_slot, hblk, pat_cnt,
                     pat_cur, pat_off, pat_cand, pat_scan, bidx, bkind, bsub, bd, bb2, bg, bact, gt_pts, gt_tris, dscal, fscal,
                     iscal, partials, trace};
@@ -1718,7 +1848,7 @@ void Stage3::release()
         if (x) cudaFree(x);
     if (h_iscal) cudaFreeHost(h_iscal);
     if (h_dscal) cudaFreeHost(h_dscal);
-    q = q_prev = q_det = p = grad = diag = target = r = z = v = v2 = Av = Avc = q_gather = nullptr;
+    q = q_prev = q_det = p = grad = diag = target = r = z = v = v2 = Av = Avc = cg_rec = q_gather = nullptr;
     row_ptr = col = tri_slot = hinge_slot = diag_slot = nullptr;
     hblk = nullptr;
     pat_cnt = pat_cur = pat_off = pat_cand = pat_scan = nullptr;
@@ -1756,6 +1886,7 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
     } while (0)
     A3(q, cp * 16); A3(q_prev, cp * 16); A3(q_det, cp * 16); A3(p, cp * 16); A3(grad, cp * 16);
     A3(diag, cp * 16); A3(target, cp * 16); A3(r, cp * 16); A3(z, cp * 16); A3(v, cp * 16); A3(v2, cp * 16); A3(Av, cp * 16); A3(Avc, cp * 16);
+    A3(cg_rec, cp * 16 * 6);
     A3(q_gather, cp * 16);
     A3(wk, cp * 4);
     A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16); A3(tri_slot, ct * 36);
@@ -2160,8 +2291,12 @@ int Stage3::cg_solve(cudaStream_t s)
     if (cg_persistent == 1) {
         // partials hold the solve's kSlotSets x cg_blocks slots, all set to kSumPending
         unsigned long long *slots = reinterpret_cast<unsigned long long *>(partials);
-        CGArgs ca{op, grad, diag, p, r, z, v, v2, Av, Avc, slots, iscal, np, cfg.n_cg_iters, cg_spin_limit,
-                  cg_absent_block};
+        // the records: cg_rec (two copies of 3 float4 per vertex); the contact parts: Avc, r, z
+        CGArgs ca{op, grad, diag, p, v, cg_rec, cg_rec + 3 * cap_p, Avc, r, z, slots, iscal, np, cfg.n_cg_iters,
+                  cg_spin_limit, cg_absent_block};
+        S3_TRY(cudaMemsetAsync(Avc, 0, (size_t)np * sizeof(float4), s));
+        S3_TRY(cudaMemsetAsync(r, 0, (size_t)np * sizeof(float4), s));
+        S3_TRY(cudaMemsetAsync(z, 0, (size_t)np * sizeof(float4), s));
         S3_TRY(cudaMemsetAsync(slots, 0xFF, (size_t)kSlotSets * cg_blocks * kSlotStride * sizeof(unsigned long long), s));
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(cg_blocks);

@@ -50,7 +50,8 @@ struct Stage3 {
     float *hblk = nullptr;      // [81 nh]: the unprojected hinge blocks of vertices 0-2 (current Newton iteration)
     int *pat_cnt = nullptr, *pat_cur = nullptr, *pat_off = nullptr, *pat_cand = nullptr, *pat_scan = nullptr;
     long long nnz = 0, cap_nnz = 0, cap_cand = 0;
-    float4 *Avc = nullptr;      // contact terms of A v (the persistent solve)
+    float4 *Avc = nullptr;      // contact terms of A v (the four-launch solve) / A z (the persistent solve)
+    float4 *cg_rec = nullptr;   // the persistent solve's vertex records: 2 x 3 float4 per vertex
     // contact blocks
     int4 *bidx = nullptr;
     int *bkind = nullptr, *bsub = nullptr;
