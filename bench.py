@@ -880,15 +880,70 @@ def serving_arm(args):
     return 0
 
 
+def _cg_case():
+    """The stage-3 CG on a block system of config 2's stage-3 size: the block
+    pattern of the 20,604-face stand-in (diagonal plus both orders of every
+    vertex pair sharing an edge or facing across one), blocks w I with a
+    symmetric weight per pair and the row sums plus 0.01 on the diagonal (SPD),
+    a seeded right-hand side; pamo_bsr_pcg, 40 iterations, twice."""
+    import torch
+
+    import pamo_b200
+    from pamo_b200 import _lib
+
+    v, f = stage3_stand_in("c2", "23")
+    n = len(v)
+    f = np.asarray(f, np.int64)
+    a = np.concatenate([f[:, 0], f[:, 1], f[:, 2]])
+    b = np.concatenate([f[:, 1], f[:, 2], f[:, 0]])
+    c = np.concatenate([f[:, 2], f[:, 0], f[:, 1]])
+    key = np.minimum(a, b) * n + np.maximum(a, b)
+    o = np.argsort(key, kind="stable")
+    ks, cs = key[o], c[o]
+    tw = np.nonzero(ks[1:] == ks[:-1])[0]
+    und = np.unique(np.sort(np.concatenate([np.stack([a, b], 1), np.stack([cs[tw], cs[tw + 1]], 1)]), axis=1), axis=0)
+    und = und[und[:, 0] != und[:, 1]]
+    rng = np.random.default_rng(0)
+    w = rng.uniform(0.1, 1.0, len(und))
+    rows = np.concatenate([np.arange(n), und[:, 0], und[:, 1]])
+    cols = np.concatenate([np.arange(n), und[:, 1], und[:, 0]])
+    wt = np.concatenate([np.zeros(n), -w, -w])
+    deg = np.bincount(und[:, 0], w, n) + np.bincount(und[:, 1], w, n) + 0.01
+    wt[:n] = deg
+    o = np.lexsort((cols, rows))
+    rows, cols, wt = rows[o], cols[o], wt[o]
+    blks = (wt[:, None, None] * np.eye(3)[None]).astype(np.float32)
+    row_ptr = np.searchsorted(rows, np.arange(n + 1)).astype(np.int32)
+    dg = np.repeat(deg, 3).astype(np.float32)
+    g = rng.standard_normal(3 * n).astype(np.float32)
+    ctx = pamo_b200.Context(0)
+    t = lambda arr, dt: torch.from_numpy(np.ascontiguousarray(arr, dt)).cuda()
+    keep = [t(row_ptr, np.int32), t(cols, np.int32), t(blks.reshape(-1), np.float32), t(dg, np.float32),
+            t(g, np.float32)]
+    out = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):
+        _lib.check("pamo_bsr_pcg", _lib.lib().pamo_bsr_pcg(ctx.handle, n, keep[0].data_ptr(), keep[1].data_ptr(),
+                                                            keep[2].data_ptr(), len(cols), keep[3].data_ptr(),
+                                                            keep[4].data_ptr(), 40, out.data_ptr(), stream))
+    torch.cuda.synchronize()
+    return {"case": "cg", "vertices": n, "blocks": int(len(cols)), "solution_norm": float(out.norm())}
+
+
 def kernel_case(which):
-    """A small case of the stage-1 or checker kernels for `ncu --set full`
-    captures: stage 1 once on a 512x512 noisy torus (524,288 faces) at R=256
-    (a 256^3 field, 134 MB of distance bits: larger than L2), then the exact
-    checker and the Hausdorff sampler on its output."""
+    """A small case of one group of kernels for `ncu --set full` captures.
+    stage1 / checker: stage 1 once on a 512x512 noisy torus (524,288 faces) at
+    R=256 (a 256^3 field, 134 MB of distance bits: larger than L2), then the
+    exact checker and the Hausdorff sampler on its output.  cg: the stage-3 CG
+    on a config-2-sized block system (_cg_case)."""
     import torch
 
     import pamo_b200
     from pamo_b200 import meshgen as mg
+
+    if which == "cg":
+        print(_cg_case(), flush=True)
+        return 0
 
     V, F = mg.noisy_torus(512, 512, 0)
     ctx = pamo_b200.Context(0)
@@ -931,7 +986,7 @@ def main():
     ap.add_argument("--dump-rounds", action="store_true")
     ap.add_argument("--iters", type=int, default=1000000,
                     help="PaMO.run's iter: the most collapse rounds per simplification")
-    ap.add_argument("--kernel-case", choices=["stage1", "checker"],
+    ap.add_argument("--kernel-case", choices=["stage1", "checker", "cg"],
                     help="one small untimed invocation for profiler captures (no JSON line)")
     args = ap.parse_args()
     if args.kernel_case:

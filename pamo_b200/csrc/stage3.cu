@@ -1236,6 +1236,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(const float4 *v, const f
 // timeout the error is recorded and the kernel returns.  The line search uses
 // the same sums for its barrier and energy.
 constexpr int kCgThreads = 512;
+constexpr int kRec = 3;  // float4 per vertex record of the solve
 constexpr unsigned long long kSumPending = ~0ull;
 constexpr int kSlotStride = 16;  // u64 words per slot
 constexpr int kSlotSets = 3;
@@ -1482,7 +1483,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
             }
             if (i < A.np && sub == 0) {
                 const F3 d = ld(diag, (int)i);
-                st(recout + 3 * (size_t)i + 1, 0, mk(kv.x / d.x, kv.y / d.y, kv.z / d.z));
+                st(recout + kRec * (size_t)i + 1, 0, mk(kv.x / d.x, kv.y / d.y, kv.z / d.z));
                 zw += (double)dot(zi, kv);
             }
         }
@@ -1522,8 +1523,8 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
         auto own0 = [&](int j) -> F3 {
             const F3 g = ld(A.grad, j), d = ld(diag, j);
             A.x[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            st(A.rec0 + 3 * (size_t)j, 0, mk(g.x / d.x, g.y / d.y, g.z / d.z));
-            st(A.rec0 + 3 * (size_t)j + 2, 0, mk(0.f, 0.f, 0.f));
+            st(A.rec0 + kRec * (size_t)j, 0, mk(g.x / d.x, g.y / d.y, g.z / d.z));
+            st(A.rec0 + kRec * (size_t)j + 2, 0, mk(0.f, 0.f, 0.f));
             const F3 z = z0(j);
             acc.a += (double)dot(z, g);
             return z;
@@ -1561,13 +1562,13 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
             return it == 0 ? w : w + beta * f3(R[2]);
         };
         auto zn = [&](int k) -> F3 {
-            const float4 *R = rc + 3 * (size_t)k;
+            const float4 *R = rc + kRec * (size_t)k;
             const F3 r = f3(R[0]);
             return upd ? r - alpha * avs(R, k) : r;
         };
         acc = D3s{0.0, 0.0, 0.0};
         auto own = [&](int j) -> F3 {
-            const float4 *R = rc + 3 * (size_t)j;
+            const float4 *R = rc + kRec * (size_t)j;
             const F3 d = ld(diag, j);
             F3 zc;
             if (it == 0) {
@@ -1583,8 +1584,8 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg_solve(CGArgs A)
             if (upd) st(A.x, j, ld(A.x, j) + alpha * vj);
             if (!last) {
                 st(A.v, j, vj);
-                st(rn + 3 * (size_t)j, 0, z);
-                st(rn + 3 * (size_t)j + 2, 0, av);
+                st(rn + kRec * (size_t)j, 0, z);
+                st(rn + kRec * (size_t)j + 2, 0, av);
                 if (contacts) wcz[j] = make_float4(0.f, 0.f, 0.f, 0.f);
                 acc.a += (double)(d.x * z.x * z.x + d.y * z.y * z.y + d.z * z.z * z.z);
                 acc.c += (double)(z.x * av.x * d.x + z.y * av.y * d.y + z.z * av.z * d.z);
@@ -1886,7 +1887,7 @@ int Stage3::ensure(long long np_, long long nt_, long long ne_, long long nh_, l
     } while (0)
     A3(q, cp * 16); A3(q_prev, cp * 16); A3(q_det, cp * 16); A3(p, cp * 16); A3(grad, cp * 16);
     A3(diag, cp * 16); A3(target, cp * 16); A3(r, cp * 16); A3(z, cp * 16); A3(v, cp * 16); A3(v2, cp * 16); A3(Av, cp * 16); A3(Avc, cp * 16);
-    A3(cg_rec, cp * 16 * 6);
+    A3(cg_rec, cp * 16 * 2 * kRec);
     A3(q_gather, cp * 16);
     A3(wk, cp * 4);
     A3(tris, ct * 16); A3(area, ct * 4); A3(inv_dm, ct * 16); A3(tri_slot, ct * 36);
@@ -2291,8 +2292,8 @@ int Stage3::cg_solve(cudaStream_t s)
     if (cg_persistent == 1) {
         // partials hold the solve's kSlotSets x cg_blocks slots, all set to kSumPending
         unsigned long long *slots = reinterpret_cast<unsigned long long *>(partials);
-        // the records: cg_rec (two copies of 3 float4 per vertex); the contact parts: Avc, r, z
-        CGArgs ca{op, grad, diag, p, v, cg_rec, cg_rec + 3 * cap_p, Avc, r, z, slots, iscal, np, cfg.n_cg_iters,
+        // the records: cg_rec (two copies of kRec float4 per vertex); the contact parts: Avc, r, z
+        CGArgs ca{op, grad, diag, p, v, cg_rec, cg_rec + kRec * cap_p, Avc, r, z, slots, iscal, np, cfg.n_cg_iters,
                   cg_spin_limit, cg_absent_block};
         S3_TRY(cudaMemsetAsync(Avc, 0, (size_t)np * sizeof(float4), s));
         S3_TRY(cudaMemsetAsync(r, 0, (size_t)np * sizeof(float4), s));
