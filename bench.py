@@ -374,22 +374,24 @@ def roofline_cg(phases, f_stage3, trace, n_iters, peaks):
     """The step's largest kernel by device time: the persistent CG solve
     (k_cg_solve, one launch per Newton iteration, n_iters iterations each).
 
-    Algorithmic bytes per CG iteration, each array read or written once: the
-    matrix blocks (36 B of values + 4 B column index per block), per vertex the
-    row offset (4 B) and 14 vector reads/writes of 12 B (direction, residual,
-    preconditioned residual, solution, products, diagonal), per active contact
-    block its index (16 B), curvature (4 B), four gradients (48 B) and two
-    12-B accesses per vertex.  The matrix and vectors stay in L2 (~13 MB on
-    config 2): the solve is bound by the latency of its two grid-wide sums per
-    iteration, so the fraction of HBM bandwidth says how far it is from
-    streaming, not what bounds it."""
+    Algorithmic bytes per CG iteration (the single-reduction form), each array
+    read or written once: the matrix blocks (36 B of values + 4 B column index
+    per block), per vertex the row offset (4 B), its record read and the next
+    one written (3 x 12 B each), the direction and the solution read and
+    written (4 x 12 B) and the diagonal (12 B); per active contact block its
+    index (16 B), curvature (4 B), four gradients (48 B) and, per vertex, the
+    record (36 B), the diagonal (12 B) and the contact term's read and atomic
+    update (24 B).  The matrix and records stay in L2 (~11 MB on config 2): the
+    solve is bound by the latency of its grid-wide sum and of the gathers, so
+    the fraction of HBM bandwidth says how far it is from streaming, not what
+    bounds it."""
     ph = phases.get("s3_cg")
     if not ph or not ph["ms"] or trace is None or not len(trace):
         return None
     nnz = _block_pattern_nnz(f_stage3)
     nv = int(np.asarray(f_stage3).max()) + 1
     nact = float(np.mean(np.asarray(trace)[:, 5]))
-    per_iter = nnz * 40.0 + nv * (4.0 + 14 * 12.0) + nact * (16 + 4 + 48 + 96)
+    per_iter = nnz * 40.0 + nv * (4.0 + 6 * 12.0 + 4 * 12.0 + 12.0) + nact * (16 + 4 + 48 + 4 * (36 + 12 + 24))
     per_launch = n_iters * per_iter
     avg_ms = ph["ms"] / max(ph["calls"], 1)
     achieved = per_launch / (avg_ms / 1e3) / 1e9
@@ -397,7 +399,7 @@ def roofline_cg(phases, f_stage3, trace, n_iters, peaks):
     return {"bound": "hbm", "kernel": "k_cg_solve", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": None, "launches": ph["calls"], "avg_launch_ms": avg_ms,
             "bytes_per_launch": per_launch, "blocks": nnz, "active_contacts_mean": nact,
-            "note": "L2-resident; bound by the grid-wide sums' latency, not by bytes",
+            "note": "L2-resident; bound by the latency of its grid-wide sum and gathers, not by bytes",
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs") else "fallback"}
 
 
