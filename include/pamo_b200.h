@@ -376,10 +376,9 @@ int pamo_bsr_pcg(pamo_ctx *ctx, int n, const int *d_row_ptr, const int *d_col, c
  * candidate pairs (box-overlapping face pairs) in total; larger inputs return
  * PAMO_ERR_CAPACITY.  An empty mesh (n_tris == 0) returns at once with
  * *out_n_pairs = 0.  Each call looks up the array's device address on the
- * current device; the first call on a device also loads the library's device
- * code there, so make that first call before any stream capture.  Each call
- * waits for its stream twice (index validation, then the counters are read
- * back to the host).  Every call shares the array: calls that overlap on the
+ * current device, and waits for its stream twice (index validation, then the
+ * counters are read back to the host), so no call can be captured into a CUDA
+ * graph.  Every call shares the array: calls that overlap on the
  * GPU, on any stream or host thread, race and must be serialised by the
  * caller.
  */
