@@ -146,38 +146,88 @@ def stage3_stand_in(name, stages="123"):
     return mg.noisy_torus(101, 102, 1)
 
 
+_STAGE1_OUT = {}
+
+
+def _stage1_output(V, F, ratio):
+    """Stage 1's result for (V, F) from the device (pamo_b200.remesh), in the
+    frame centred on the input's tris_mean, and that offset: the input of the
+    CPU sample's stage 2 when the workload includes stage 1 (the remesh itself
+    is not restated at this size on the host; preparing the input is not
+    timed).  Computed once per process."""
+    key = (id(V), id(F))
+    if key not in _STAGE1_OUT:
+        import torch
+
+        import pamo_b200
+
+        ctx = pamo_b200.Context(0)
+        R = pamo_b200.stage1_resolution(int(ratio * len(F)))
+        v, f, off = pamo_b200.remesh(ctx, torch.from_numpy(np.ascontiguousarray(V)).cuda(),
+                                     torch.from_numpy(np.ascontiguousarray(F)).cuda(), R)
+        _STAGE1_OUT[key] = (v.cpu().numpy(), f.cpu().numpy(), np.asarray(off, np.float32))
+        del ctx
+    return _STAGE1_OUT[key]
+
+
 def cpu_sample(args, V, F, ratio):
-    """The CPU restatement (oracle/) timed on the host cores, on bounded samples:
-    stage 2 = its first `sample_rounds` rounds (C, OpenMP on all host threads),
-    extrapolated by the face-rounds of the whole run; stage 3 = all of PaMO.run's
-    5 steps x 10 Newton iterations in the C++ float32 restatement
-    (oracle/s3_cpu.cpp, OpenMP on all host threads) on a stand-in of the
-    stage-2 output, measured whole.
+    """The CPU restatement (oracle/) timed on the host cores, all host threads
+    (OpenMP).  With stage 1 in the workload: stage 2 = its whole loop (C) on
+    stage 1's output, and stage 3 = all of PaMO.run's 5 steps x 10 Newton
+    iterations (C++ float32) on that loop's result -- both measured whole;
+    stage 1 itself is not in the sample (its input for stage 2 comes from the
+    device, untimed).  Without stage 1: stage 2 = its first `sample_rounds`
+    rounds on the raw input, extrapolated by the face-rounds of the whole run,
+    and stage 3 on a stand-in of the stage-2 output.
     Returns (measured seconds of the sample, estimated seconds for the whole
-    workload, sample description, threads)."""
+    workload, sample description, threads, extrapolated)."""
     from oracle import oracle as O
 
     target = int(ratio * len(F))
-    tm = O.tris_mean(V, F)
-    Vc = (V - tm).astype(np.float32)
-    Fs = O.shuffle_faces(F)
-    o = O.Stage2Oracle()
-    frac = _sample_fraction(args, args.sample_rounds)
-    t0 = time.perf_counter()
-    o.run(Vc, Fs, target, 4, 1e-3, args.sample_rounds if frac else 1000000)
-    t2 = time.perf_counter() - t0
-    measured = t2
-    if frac:
-        total = t2 / frac
-        desc = (f"stage 2: first {args.sample_rounds} rounds ({frac * 100:.1f}% of the run's face-rounds, "
-                f"{t2:.1f} s) extrapolated by face-rounds")
-    else:  # no recorded round sizes for this workload: the whole loop
-        total = t2
-        desc = f"stage 2: the whole loop ({t2:.1f} s)"
+    extrapolated = False
+    stage1_in = None
+    if "1" in args.stages:
+        try:
+            stage1_in = _stage1_output(V, F, ratio)
+        except Exception:  # no device here: stage 2 on the raw input instead, labelled below
+            stage1_in = None
+    if stage1_in is not None:
+        v1, f1, off = stage1_in
+        Fs = O.shuffle_faces(f1)
+        o = O.Stage2Oracle()
+        t0 = time.perf_counter()
+        v2, f2, rounds = o.run(v1, Fs, target, 4, 1e-3, 1000000)
+        t2 = time.perf_counter() - t0
+        measured = total = t2
+        desc = (f"stage 2: its whole loop on stage 1's output ({len(f1):,} faces, computed on the device beforehand "
+                f"and not timed) -> {len(f2):,} faces in {rounds} rounds ({t2:.1f} s)")
+        s3_in = ((v2 + off).astype(np.float32), f2, "that loop's result")
+    else:
+        tm = O.tris_mean(V, F)
+        Vc = (V - tm).astype(np.float32)
+        Fs = O.shuffle_faces(F)
+        o = O.Stage2Oracle()
+        frac = _sample_fraction(args, args.sample_rounds)
+        t0 = time.perf_counter()
+        o.run(Vc, Fs, target, 4, 1e-3, args.sample_rounds if frac else 1000000)
+        t2 = time.perf_counter() - t0
+        measured = t2
+        if frac:
+            total = t2 / frac
+            extrapolated = True
+            desc = (f"stage 2: first {args.sample_rounds} rounds ({frac * 100:.1f}% of the run's face-rounds, "
+                    f"{t2:.1f} s) extrapolated by face-rounds")
+        else:  # no recorded round sizes for this workload: the whole loop
+            total = t2
+            desc = f"stage 2: the whole loop ({t2:.1f} s)"
+        if "1" in args.stages:
+            desc += " on the raw input (no device here to compute stage 1's output)"
+        v, f = stage3_stand_in(args.workload, args.stages)
+        s3_in = (v, f, f"a {len(f):,}-face stand-in of the stage-2 output")
     if "3" in args.stages:
         from oracle import s3_cpu  # C++ FP32 restatement, OpenMP
 
-        v, f = stage3_stand_in(args.workload, args.stages)
+        v, f, what = s3_in
         st = {}
         t0 = time.perf_counter()
         s3_cpu.process(V, F, v, f, 5, stats=st)
@@ -185,12 +235,12 @@ def cpu_sample(args, V, F, ratio):
         measured += t3
         total += t3
         desc += (f"; stage 3: the whole of it (5 steps x 10 Newton iterations, C++ float32 restatement on "
-                 f"{s3_cpu.num_threads()} threads) on a {len(f):,}-face stand-in of the stage-2 output "
-                 f"({t3:.1f} s, {st['blocks']:,} contact blocks at the end)")
+                 f"{s3_cpu.num_threads()} threads) on {what} ({t3:.1f} s, {st['blocks']:,} contact blocks at "
+                 f"the end)")
     if "1" in args.stages:
         desc += ("; stage 1 is not in the sample (the reference runs it through GPU libraries only; its "
                  "restatement under oracle/ is a numpy test oracle)")
-    return measured, total, desc, O.lib().s2o_num_threads()
+    return measured, total, desc, O.lib().s2o_num_threads(), extrapolated
 
 
 def reference_gpu_stage2(V, F, ratio, reps=3):
@@ -229,19 +279,21 @@ def reference_arm(args):
     oracle/ (the reference has no CPU path for stage 2, and its stage-3 CPU
     device, Warp, is absent), one bounded sample of the workload per step.
 
-    `ms_per_step` is the measured time of one sample.  `value` is the input
-    Mfaces/s of the whole workload estimated from the sample (stage 2 by the
-    face-rounds the sample covers; stage 3 is measured whole); the line says
-    so under `extrapolated`.  The reference's own stage-2 GPU build is
-    timed beside it on the full workload (`reference_gpu_stage2`)."""
+    `ms_per_step` is the measured time of one sample.  With stage 1 in the
+    workload the sample is stages 2 and 3 whole (stage 1 excluded, see
+    cpu_sample) and `value` is input faces over that time; without it, stage 2
+    is extrapolated from its first rounds by face-rounds, and the line says so
+    under `extrapolated`.  The reference's own stage-2 GPU build is timed beside
+    it on the full workload (`reference_gpu_stage2`)."""
     ws, rank, _ = dist_init(args)
     if rank != 0:
         return 0
     V, F, ratio, desc = workload(args.workload)
     measured, totals = [], []
     sample = cores = None
+    extrapolated = False
     for _ in range(args.warmup + args.steps):
-        t_meas, total, sample, cores = cpu_sample(args, V, F, ratio)
+        t_meas, total, sample, cores, extrapolated = cpu_sample(args, V, F, ratio)
         measured.append(t_meas)
         totals.append(total)
     t_step = float(np.median(measured[args.warmup:]))
@@ -257,10 +309,13 @@ def reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "stages": STAGES[args.stages], "sample": sample},
-            "extrapolated": {"measured_s_per_step": t_step, "estimated_s_whole_workload": total_s,
-                             "basis": "each step times a bounded sample (ms_per_step); value = input faces / the "
-                                      "whole workload's time estimated from that sample"},
-            "cpu_baseline": {"value": value, "unit": "Mfaces/s", "cores": cores, "kind": "port", "sample": sample},
+            "extrapolated": ({"measured_s_per_step": t_step, "estimated_s_whole_workload": total_s,
+                              "basis": "each step times a bounded sample (ms_per_step); value = input faces / the "
+                                       "whole workload's time estimated from that sample"} if extrapolated else
+                             {"measured_s_per_step": t_step, "estimated_s_whole_workload": total_s,
+                              "basis": "measured whole: stages 2 and 3 of the workload (stage 1 excluded)"}),
+            "cpu_baseline": {"value": value, "unit": "Mfaces/s", "cores": cores, "kind": "port", "sample": sample,
+                             "extrapolated": extrapolated},
             "e2e": {"value": value, "unit": "Mfaces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "reference_gpu_stage2": gpu}
     print(json.dumps(line), flush=True)
@@ -535,9 +590,9 @@ def product_arm(args):
         c4 = c4_compare(local)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        _, total, sample, cores = cpu_sample(args, V, F, ratio)
+        _, total, sample, cores, extrapolated = cpu_sample(args, V, F, ratio)
         cpu = {"value": nF / 1e6 / total, "unit": "Mfaces/s", "cores": cores, "kind": "port", "sample": sample,
-               "extrapolated": True}
+               "extrapolated": extrapolated}
     if rank == 0:
         value = ws * nF / 1e6 / (ms_max / 1e3)
         e2e = ws * nF / 1e6 / (e2e_ms / 1e3)
@@ -973,8 +1028,9 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4", "c5"],
                     help="c1/c2: one mesh (plain loop); c4: 256-mesh batch; c5: Poisson serving")
     ap.add_argument("--no-c4", action="store_true", help="c2 at one GPU: skip the config-4 batched-vs-plain keys")
-    ap.add_argument("--stages", default="123", choices=["123", "23", "2"],
-                    help="c1/c2: PaMO.run with all three stages (default), stages 2 + 3, or stage 2 alone")
+    ap.add_argument("--stages", default=None, choices=["123", "23", "2"],
+                    help="c1/c2: PaMO.run with all three stages (c2's default), stages 2 + 3 (c1's default: "
+                         "config 1 has stage 1 off), or stage 2 alone")
     ap.add_argument("--n-meshes", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--pool", type=int, default=24, help="c5: distinct request meshes")
@@ -991,6 +1047,8 @@ def main():
     ap.add_argument("--kernel-case", choices=["stage1", "checker", "cg"],
                     help="one small untimed invocation for profiler captures (no JSON line)")
     args = ap.parse_args()
+    if args.stages is None:
+        args.stages = "23" if args.workload == "c1" else "123"
     if args.kernel_case:
         return kernel_case(args.kernel_case)
     if args.impl == "reference":
