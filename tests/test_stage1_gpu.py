@@ -41,6 +41,45 @@ def test_remesh_matches_oracle(torch_cuda):
         assert np.array_equal(v.view(np.uint32), ov.view(np.uint32)), (name, np.abs(v - ov).max())
 
 
+def test_remesh_matches_oracle_at_benchmark_resolution(torch_cuda):
+    """R = 256, config 2's resolution, on config 1's 20,480-face mesh (583,556
+    faces out): the same bits as the CPU restatement (about 20 s of numpy)."""
+    import pamo_b200
+    from oracle import s1_oracle as S1
+    from pamo_b200 import meshgen as mg
+
+    V, F = mg.displaced_icosphere(5, 0)
+    ctx = pamo_b200.Context(0)
+    v, f, off = pamo_b200.remesh(ctx, torch_cuda.from_numpy(V).cuda(), torch_cuda.from_numpy(F).cuda(), 256)
+    ov, of, om = S1.remesh(V, F, 256)
+    v, f = v.cpu().numpy(), f.cpu().numpy()
+    assert np.array_equal(off.view(np.uint32), om.view(np.uint32))
+    assert len(f) == len(of) == 583556
+    assert np.array_equal(f, of)
+    assert np.array_equal(v.view(np.uint32), ov.view(np.uint32))
+
+
+def test_config2_stage2_after_remesh_matches_oracle(torch_cuda):
+    """Config 2 as benchmarked: stage 1 on the 2,097,152-face torus on the
+    device, then the stage-2 loop on its output as PaMO.run runs it with stage 1
+    on (no second centring, the offset added back at the end), on the device
+    and in the C restatement: the same rounds, faces and vertex bits."""
+    import pamo_b200
+    from oracle import oracle as O
+    from pamo_b200 import meshgen as mg
+
+    V, F = mg.noisy_torus(1024, 1024, 0)
+    ctx = pamo_b200.Context(0)
+    v1, f1, off = pamo_b200.remesh(ctx, torch_cuda.from_numpy(V).cuda(), torch_cuda.from_numpy(F).cuda(), 256)
+    target = int(0.01 * len(F))
+    v2, f2, rounds = pamo_b200.stage2_run(pamo_b200.Context(0), v1, f1, target, offset=off)
+    ov, of, orounds = O.Stage2Oracle().run(v1.cpu().numpy(), O.shuffle_faces(f1.cpu().numpy()), target, 4, 1e-3,
+                                           1000000)
+    assert rounds == orounds
+    assert np.array_equal(f2.cpu().numpy(), of)
+    assert np.array_equal(v2.cpu().numpy().view(np.uint32), (ov + off).astype(np.float32).view(np.uint32))
+
+
 def test_remesh_output_is_closed_and_clean(torch_cuda):
     import pamo_b200
     from pamo_b200 import meshgen as mg
