@@ -147,6 +147,16 @@ int pamo_stage2_fetch(pamo_ctx *ctx, float *out_points, int *out_tris, int to_ho
 int pamo_stage2_offset(pamo_ctx *ctx, float *h_out3);
 
 /*
+ * The centring offset PaMO.run subtracts (simp_cuda/pamo/__init__.py, the
+ * tris_mean of the input): each face's corner mean ((a + b) + c) / 3, then
+ * numpy's float32 mean(axis=0) of those rows, whose adds run one after another
+ * -- computed on the device, bit for bit.  d_points [n_pts,3] float32, d_tris
+ * [n_tris,3] int32 (device); h_out3: host float[3].  Indices outside [0, n_pts)
+ * return PAMO_ERR_INVALID_ARG.  Synchronises the stream.
+ */
+int pamo_tris_mean(const float *d_points, const int *d_tris, int n_pts, int n_tris, float *h_out3, void *stream);
+
+/*
  * Per-round statistics of the last pamo_stage2_run / pamo_free_forward:
  * h_out[0..7] = {n_edges, n_collapsed, n_collapsed_with_coincident,
  *               n_undo_passes, n_undo_vertices, candidate_pairs_pass0,

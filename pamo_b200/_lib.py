@@ -62,6 +62,7 @@ SIGNATURES = {
     "pamo_remesh": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _ip, _ip]),
     "pamo_remesh_fetch": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "pamo_stage2_offset": (_i, [_vp, _vp]),
+    "pamo_tris_mean": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
     "pamo_stage2_last_round_stats": (_i, [_vp, _vp]),
     "pamo_self_intersect": (_i, [_vp, _vp, _vp, _i, _i, _vp, ctypes.POINTER(_ll), _vp]),
     "pamo_profile_enable": (_i, [_vp, _i]),
