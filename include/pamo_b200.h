@@ -147,7 +147,7 @@ int pamo_stage2_fetch(pamo_ctx *ctx, float *out_points, int *out_tris, int to_ho
 int pamo_stage2_offset(pamo_ctx *ctx, float *h_out3);
 
 /*
- * The centring offset PaMO.run subtracts (simp_cuda/pamo/__init__.py, the
+ * The centring offset PaMO.run subtracts (simp_cuda/pamo/__init__.py:64, the
  * tris_mean of the input): each face's corner mean ((a + b) + c) / 3, then
  * numpy's float32 mean(axis=0) of those rows, whose adds run one after another
  * -- computed on the device, bit for bit.  d_points [n_pts,3] float32, d_tris

@@ -29,7 +29,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 # translation units whose arithmetic must round exactly like the reference
 # (checker.cu: its exact predicates' error-free sums need one rounding per operation;
 # stage1.cu: its FP64 distances follow the CPU restatement's operation order)
-NO_FMA = {"stage2.cu", "lbvh.cu", "scan.cu", "abi.cu", "shuffle.cu", "noalloc.cu", "checker.cu", "stage1.cu", "seqsum.cu"}
+NO_FMA = {"stage2.cu", "lbvh.cu", "scan.cu", "abi.cu", "shuffle.cu", "noalloc.cu", "checker.cu", "stage1.cu"}
 
 
 def sources():

@@ -7,7 +7,6 @@
 #include <vector>
 
 #include "scan.cuh"
-#include "seqsum.cuh"
 #include "stage1.cuh"
 #include "stage2.cuh"
 #include "stage3.cuh"
@@ -84,6 +83,80 @@ __global__ void k_face_means(const float *pts, const int *tris, int m, float *mx
     }
 }
 
+// numpy's .mean(axis=0) of a C-contiguous (F,3) float32 array adds the rows one
+// after another into a float32 accumulator (no pairwise split on this axis), then
+// divides by F.  Each coordinate's chain is inherently sequential, so the bound
+// is the latency of F dependent adds.  One block: lane 0 of warps 0, 1, 2 runs
+// the x, y, z chains (reading four values per shared-memory load) while warps
+// 3..31 stream the next chunk into the other shared buffer.
+constexpr int kMeanChunk = 8192;
+constexpr int kMeanLoadFirst = 3 * 32;
+
+__global__ void __launch_bounds__(1024) k_sequential_mean(const float *mx, const float *my, const float *mz, int m,
+                                                          float *out)
+{
+    extern __shared__ float4 sm4[];  // 2 buffers x 3 coordinates x kMeanChunk floats
+    float *sm = reinterpret_cast<float *>(sm4);
+    if (m <= 0) return;
+    const int n_chunks = (m + kMeanChunk - 1) / kMeanChunk;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto load = [&](int c, int buf) {
+        float *dst = sm + buf * 3 * kMeanChunk;
+        int base = c * kMeanChunk;
+        int cnt = min(kMeanChunk, m - base);
+        for (int i = threadIdx.x - kMeanLoadFirst; i < cnt; i += blockDim.x - kMeanLoadFirst) {
+            dst[i] = mx[base + i];
+            dst[kMeanChunk + i] = my[base + i];
+            dst[2 * kMeanChunk + i] = mz[base + i];
+        }
+    };
+    if (threadIdx.x >= kMeanLoadFirst) load(0, 0);
+    __syncthreads();
+    float acc = 0.f;
+    for (int c = 0; c < n_chunks; ++c) {
+        const int buf = c & 1;
+        if (threadIdx.x >= kMeanLoadFirst) {
+            if (c + 1 < n_chunks) load(c + 1, buf ^ 1);
+        } else if (lane == 0) {
+            const float *bs = sm + (buf * 3 + warp) * kMeanChunk;
+            const float4 *b4 = reinterpret_cast<const float4 *>(bs);
+            const int cnt = min(kMeanChunk, m - c * kMeanChunk);
+            int i = 0;
+            if (c == 0) {  // the accumulator starts from the first row
+                acc = bs[0];
+                i = 1;
+            }
+            for (; i < cnt && (i & 3); ++i) acc += bs[i];
+            const int n4 = cnt >> 2;
+            int q = i >> 2;
+            // sixteen values per step, the next sixteen loaded while these are
+            // added (the clamped loads stay inside the buffer and are unused at
+            // the end), so the chain waits on the adds alone
+            if (q + 4 <= n4) {
+                float4 c0 = b4[q], c1 = b4[q + 1], c2 = b4[q + 2], c3 = b4[q + 3];
+                for (; q + 4 <= n4; q += 4) {
+                    const int nq = min(q + 4, n4 - 4);
+                    const float4 d0 = b4[nq], d1 = b4[nq + 1], d2 = b4[nq + 2], d3 = b4[nq + 3];
+                    acc += c0.x; acc += c0.y; acc += c0.z; acc += c0.w;
+                    acc += c1.x; acc += c1.y; acc += c1.z; acc += c1.w;
+                    acc += c2.x; acc += c2.y; acc += c2.z; acc += c2.w;
+                    acc += c3.x; acc += c3.y; acc += c3.z; acc += c3.w;
+                    c0 = d0; c1 = d1; c2 = d2; c3 = d3;
+                }
+            }
+            for (; q < n4; ++q) {
+                const float4 v = b4[q];
+                acc += v.x;
+                acc += v.y;
+                acc += v.z;
+                acc += v.w;
+            }
+            for (i = max(i, n4 * 4); i < cnt; ++i) acc += bs[i];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < kMeanLoadFirst && lane == 0) out[warp] = acc / (float)m;
+}
 
 __global__ void k_centre(const float *pts, int n, const float *mean, float4 *out, int *bounds)
 {
@@ -339,23 +412,16 @@ using namespace pamo;
         if (_e != cudaSuccess) return map_cuda_error(_e); \
     } while (0)
 
-// tris_mean of PaMO.run: each face's corner mean, then numpy's mean(axis=0) of
-// those rows, which adds them one after another into a float32 accumulator (no
-// pairwise split on this axis) and divides by m (seq_mean3 evaluates that chain
-// exactly).  scratch: scratch_bytes of device memory, 16-byte aligned.
-static size_t centring_scratch_bytes(int m)
+// tris_mean of PaMO.run: each face's corner mean, then the rows added one by
+// one in float32 (numpy's order); scratch holds 3 m floats
+static int centring_mean(const float *d_points, const int *d_tris, int m, float *scratch, float *mean_dev,
+                         cudaStream_t s)
 {
-    return (((size_t)3 * m * sizeof(float) + 15) & ~(size_t)15) + seq_mean_scratch_bytes(m);
-}
-
-static int centring_mean(const float *d_points, const int *d_tris, int m, void *scratch, size_t scratch_bytes,
-                         float *mean_dev, cudaStream_t s)
-{
-    if (centring_scratch_bytes(m) > scratch_bytes) return PAMO_ERR_CAPACITY;
-    float *f = static_cast<float *>(scratch);
-    launch(k_face_means, grid_for(m), kThreads, 0, s, d_points, d_tris, m, f, f + m, f + 2LL * m);
-    void *rest = static_cast<char *>(scratch) + (((size_t)3 * m * sizeof(float) + 15) & ~(size_t)15);
-    CU_RET(seq_mean3(f, f + m, f + 2LL * m, m, rest, mean_dev, s));
+    launch(k_face_means, grid_for(m), kThreads, 0, s, d_points, d_tris, m, scratch, scratch + m, scratch + 2LL * m);
+    const int smem = 2 * 3 * kMeanChunk * (int)sizeof(float);
+    CU_RET(cudaFuncSetAttribute(k_sequential_mean, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    launch(k_sequential_mean, 1, 1024, smem, s, scratch, scratch + m, scratch + 2LL * m, m, mean_dev);
+    CU_RET(cudaGetLastError());
     return PAMO_OK;
 }
 
@@ -470,14 +536,14 @@ static int stage2_loop(pamo_ctx *ctx, const float *d_points, const int *d_tris, 
     RET_IF(ensure_undo_prev(ctx, S.cap_undo));
     RET_IF(S.validate(d_tris, n_pts, n_tris, nullptr, 0, 0, s));
     // centring (tris_mean in numpy's float32 order) and scale, as PaMO.run does
+    float *mxyz = reinterpret_cast<float *>(S.plane);  // 3*m floats of scratch (plane has 4*m)
     float *mean_dev = reinterpret_cast<float *>(S.dev_misc);
     int *bounds = S.dev_misc + 8;
     float *bounds_f = reinterpret_cast<float *>(S.dev_misc + 16);
     if (offset3) {
         CU_RET(cudaMemsetAsync(mean_dev, 0, 3 * sizeof(float), s));  // already centred
     } else {
-        // scratch: the face planes, 16 bytes per face (written later in the round)
-        RET_IF(centring_mean(d_points, d_tris, n_tris, S.plane, (size_t)(S.cap_tris + 1) * 16, mean_dev, s));
+        RET_IF(centring_mean(d_points, d_tris, n_tris, mxyz, mean_dev, s));
     }
     launch(k_bounds_init, 1, 32, 0, s, bounds);
     launch(k_centre, grid_for(n_pts), kThreads, 0, s, d_points, n_pts, mean_dev, S.opts, bounds);
@@ -534,14 +600,15 @@ int pamo_tris_mean(const float *d_points, const int *d_tris, int n_pts, int n_tr
     if (cudaGetDevice(&dev) != cudaSuccess) return PAMO_ERR_NO_DEVICE;
     cudaStream_t s = (cudaStream_t)stream;
     CU_RET(retain_pool_memory());
-    const size_t cb = centring_scratch_bytes(n_tris);
+    // 3 n_tris floats of face means, then the bad-index flag and the result
+    const size_t cb = ((size_t)3 * n_tris * sizeof(float) + 15) & ~(size_t)15;
     char *scratch = nullptr;
     if (cudaMallocAsync((void **)&scratch, cb + 32, s) != cudaSuccess) return PAMO_ERR_OOM;
     int *d_bad = reinterpret_cast<int *>(scratch + cb);
     float *d_mean = reinterpret_cast<float *>(scratch + cb + 16);
     int h_bad = 0;
     int rc = s3_validate(d_tris, 3LL * n_tris, n_pts, d_bad, &h_bad, s);
-    if (rc == PAMO_OK) rc = centring_mean(d_points, d_tris, n_tris, scratch, cb, d_mean, s);
+    if (rc == PAMO_OK) rc = centring_mean(d_points, d_tris, n_tris, reinterpret_cast<float *>(scratch), d_mean, s);
     if (rc == PAMO_OK && cudaMemcpyAsync(h_out3, d_mean, 3 * sizeof(float), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         rc = PAMO_ERR_DEVICE;
     cudaFreeAsync(scratch, s);
@@ -586,7 +653,7 @@ int pamo_remesh(pamo_ctx *ctx, const float *d_points, const int *d_tris, int n_p
     int h_bad = 0;
     RET_IF(s3_validate(d_tris, 3LL * n_tris, n_pts, S.dev + 15, &h_bad, s));
     // tris_mean of the input (the scratch: the normalised-triangle buffer, 9 m floats)
-    RET_IF(centring_mean(d_points, d_tris, n_tris, S.tris, (size_t)S.cap_tris * 9 * sizeof(float), S.mean_dev, s));
+    RET_IF(centring_mean(d_points, d_tris, n_tris, S.tris, S.mean_dev, s));
     CU_RET(cudaMemcpyAsync(S.offset, S.mean_dev, 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
     RET_IF(pamo::s1::remesh(S, d_points, d_tris, n_pts, n_tris, S.mean_dev, resolution, s));
     CU_RET(cudaStreamSynchronize(s));
@@ -1240,9 +1307,13 @@ int batch_admit(pamo_batch *b, BatchJob *j)
     t.tres = j->threshold;
     // centring and scale as the single-mesh loop does, written at the packed tail
     const int voff = b->n_packed, foff = b->m_packed, n = j->n0, m = j->m0;
-    // scratch: the face planes, 16 bytes per face of the arena (written later in the round)
-    RET_IF(centring_mean((const float *)j->raw_p, (const int *)j->raw_t, m, S.plane, (size_t)(S.cap_tris + 1) * 16,
-                         j->hdr->mean, s));
+    float *mxyz = reinterpret_cast<float *>(S.plane);  // 3*m floats of scratch
+    launch(k_face_means, grid_for(m), kThreads, 0, s, (const float *)j->raw_p, (const int *)j->raw_t, m, mxyz,
+           mxyz + m, mxyz + 2LL * m);
+    const int smem = 2 * 3 * kMeanChunk * (int)sizeof(float);
+    CU_RET(cudaFuncSetAttribute(k_sequential_mean, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    launch(k_sequential_mean, 1, 1024, smem, s, (const float *)mxyz, (const float *)(mxyz + m),
+           (const float *)(mxyz + 2LL * m), m, j->hdr->mean);
     launch(k_bounds_init, 1, 32, 0, s, j->hdr->bounds);
     launch(k_centre, grid_for(n), kThreads, 0, s, (const float *)j->raw_p, n, (const float *)j->hdr->mean,
            S.opts + voff, j->hdr->bounds);

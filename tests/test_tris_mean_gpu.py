@@ -1,11 +1,8 @@
 """The centring offset (PaMO.run's tris_mean) on the device, pamo_tris_mean,
 against the oracle's sequential float32 chain (itself pinned to numpy in
-test_oracle.py), bit for bit.  Above a few thousand faces the device evaluates
-the chain in blocks of 32 steps (an integer sum inside one binade, with ties
-taken by parity) and falls back to float32 adds where a block leaves its
-binade; the inputs here make both happen often: sums that hover around zero,
-values on coarse dyadic grids (ties), mixed magnitudes, subnormals, and
-non-finite coordinates."""
+test_oracle.py), bit for bit, on inputs that stress a float32 chain: sums that
+hover around zero, values on coarse dyadic grids (round-half-even ties), mixed
+magnitudes, subnormals, signed zeros and non-finite coordinates."""
 import ctypes
 
 import numpy as np
