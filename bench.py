@@ -992,7 +992,8 @@ def kernel_case(which):
     stage1 / checker: stage 1 once on a 512x512 noisy torus (524,288 faces) at
     R=256 (a 256^3 field, 134 MB of distance bits: larger than L2), then the
     exact checker and the Hausdorff sampler on its output.  cg: the stage-3 CG
-    on a config-2-sized block system (_cg_case)."""
+    on a config-2-sized block system (_cg_case).  stage23: stages 2 and 3 once
+    on a 256x256 noisy torus (131,072 faces, ratio 0.15)."""
     import torch
 
     import pamo_b200
@@ -1000,6 +1001,15 @@ def kernel_case(which):
 
     if which == "cg":
         print(_cg_case(), flush=True)
+        return 0
+    if which == "stage23":
+        # stages 2 + 3 once: stage 2 from 131,072 faces, stage 3 on its ~20k-face
+        # result (the size of config 2's stage-3 input)
+        V, F = mg.noisy_torus(256, 256, 0)
+        pm = pamo_b200.PaMO((V, F), use_stage1=False, use_stage3=True, device=0)
+        v, f = pm.run(torch.from_numpy(V).cuda(), torch.from_numpy(F).cuda(), 0.15, min_verts=0)
+        torch.cuda.synchronize()
+        print({"case": which, "faces_in": len(F), "faces_out": int(len(f))}, flush=True)
         return 0
 
     V, F = mg.noisy_torus(512, 512, 0)
@@ -1044,7 +1054,7 @@ def main():
     ap.add_argument("--dump-rounds", action="store_true")
     ap.add_argument("--iters", type=int, default=1000000,
                     help="PaMO.run's iter: the most collapse rounds per simplification")
-    ap.add_argument("--kernel-case", choices=["stage1", "checker", "cg"],
+    ap.add_argument("--kernel-case", choices=["stage1", "checker", "cg", "stage23"],
                     help="one small untimed invocation for profiler captures (no JSON line)")
     args = ap.parse_args()
     if args.stages is None:
