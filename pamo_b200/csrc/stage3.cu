@@ -1955,7 +1955,7 @@ int Stage3::register_mesh(const float *d_gt_v, const int *d_gt_f, int n_gt_v, in
     if (rc) return rc;
     const bool keep_gt = cfg.reuse_gt && gt_ready && d_gt_v == gt_src_v && d_gt_f == gt_src_f && n_gt_v == prev_gp &&
                          n_gt_f == prev_gt;
-    drop_graph();  // sizes and configuration are baked into the captured iteration
+    graph_stale = true;  // sizes and configuration are baked into the captured iteration
     gathered = false;  // new geometry: contact candidates are gathered again
     np = n_v; nt = n_f; ne = n_e; nh = n_h; ngp = n_gt_v; ngt = n_gt_f;
     radius = cfg.contact_detection_radius;
@@ -2122,13 +2122,18 @@ void Stage3::drop_graph()
     graph = nullptr;
     graph_cap_b = -1;
     graph_kernels = 0;
+    graph_stale = false;
 }
 
 // One Newton iteration (system.py:354-409).  Contact detection ends with a host
 // synchronisation (block count, buffer growth); everything after it has fixed
 // sizes and pointers and no host decision, so it is captured once as a CUDA
-// graph and replayed (recaptured when the contact buffer grows).  With the phase
-// timer on, the iteration runs eagerly so its events can be recorded.
+// graph and replayed (recaptured when the contact buffer grows or a new mesh is
+// registered).  A recapture updates the executable graph in place when its
+// shape is unchanged -- the usual case, as only sizes and pointers move -- which
+// costs the host far less than instantiating it again (the device idles
+// meanwhile); otherwise the graph is instantiated anew.  With the phase timer
+// on, the iteration runs eagerly so its events can be recorded.
 int Stage3::newton(cudaStream_t s)
 {
     S3_TRY(cudaMemcpyAsync(q_prev, q, (size_t)np * 16, cudaMemcpyDeviceToDevice, s));
@@ -2139,8 +2144,7 @@ int Stage3::newton(cudaStream_t s)
     if ((rc = newton_contacts(s))) return rc;
     const bool timed = prof && prof->on;
     if (timed || !use_graph) return newton_body(s);
-    if (!graph || graph_cap_b != cap_b) {
-        drop_graph();
+    if (!graph || graph_stale || graph_cap_b != cap_b) {
         const long long before = g_launches.load();
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
@@ -2150,24 +2154,39 @@ int Stage3::newton(cudaStream_t s)
         }
         rc = newton_body(s);
         cudaError_t ce = cudaStreamEndCapture(s, &g);
-        graph_kernels = g_launches.load() - before;
-        g_launches.fetch_sub(graph_kernels);  // captured, not launched
+        const long long kernels = g_launches.load() - before;
+        g_launches.fetch_sub(kernels);  // captured, not launched
         if (rc || ce != cudaSuccess || !g) {
             if (g) cudaGraphDestroy(g);
             cudaGetLastError();
+            drop_graph();
             if (rc) return rc;
             use_graph = false;  // this stream cannot be captured: run the iteration directly
             return newton_body(s);
         }
-        ce = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess) {
-            graph = nullptr;
-            cudaGetLastError();
-            use_graph = false;
-            return newton_body(s);
+        if (graph) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(graph, g, &info) != cudaSuccess) {  // another shape: instantiate anew
+                cudaGetLastError();
+                cudaGraphExecDestroy(graph);
+                graph = nullptr;
+            }
         }
+        if (!graph) {
+            ce = cudaGraphInstantiate(&graph, g, 0);
+            if (ce != cudaSuccess) {
+                cudaGraphDestroy(g);
+                graph = nullptr;
+                drop_graph();
+                cudaGetLastError();
+                use_graph = false;
+                return newton_body(s);
+            }
+        }
+        cudaGraphDestroy(g);
+        graph_kernels = kernels;
         graph_cap_b = cap_b;
+        graph_stale = false;
     }
     S3_TRY(cudaGraphLaunch(graph, s));
     g_launches.fetch_add(graph_kernels);

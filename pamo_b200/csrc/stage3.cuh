@@ -83,6 +83,9 @@ struct Stage3 {
     Profiler *prof = nullptr;  // the context's phase timer (optional)
     cudaGraphExec_t graph = nullptr;  // one Newton iteration after detection
     long long graph_cap_b = -1, graph_kernels = 0;
+    // a new registration changed the iteration's sizes and pointers: the next
+    // iteration is captured again and the executable graph updated in place
+    bool graph_stale = false;
     bool use_graph = true;
     int cg_blocks = 0;   // grid of the persistent solve
     int cg_persistent = -1;  // 1: one cooperative launch per solve; 0: one launch per phase; -1: not decided
